@@ -1,0 +1,174 @@
+/*
+ * sph_abi.h — C-ABI of the B200 SPH step engine (libsph.so).
+ *
+ * This is the drop-in boundary that replaces the reference's process
+ * boundary: the Python driver used to spawn `./execute` and exchange state
+ * through `output/dump_full.h5` (playground/runner/fortdriver/core.py:152-169,
+ * 321-326, 465-470).  Here the driver keeps the same two arrays in memory and
+ * hands them to the engine through plain pointers:
+ *
+ *   state[49]  : FP64 state vector, slot k-1 holds statevars(k)
+ *                (playground/src/state.f90:36, enum in const.f90:14-66)
+ *   store[N*32]: FP64 particle table, row-major, one row of 32 fields per
+ *                particle (the Fortran store(32,N) seen from C / h5py as
+ *                (N,32); field map const.f90:69-103).  Rows are the real
+ *                particles followed by the fixed ones (dumper.f90:33-34).
+ *
+ * Conventions
+ *  - every entry point returns an int status: 0 = ok, >0 = one of SPH_ERR_*,
+ *    each mirroring an abort site of the reference (`error stop` / `stop`);
+ *  - buffers are caller-owned; a handle owns its device memory and one CUDA
+ *    stream; a handle is not thread-safe; no C++ exception crosses the ABI;
+ *  - there is no CPU fallback: if no CUDA device is usable, sph_create
+ *    returns SPH_ERR_CUDA.
+ */
+#ifndef SPH_ABI_H
+#define SPH_ABI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- sizes of the interchange arrays (const.f90:66, :102) ---------------- */
+#define SPH_EC_TOTAL 49
+#define SPH_ES_TOTAL 32
+
+/* ---- kernel choice: the reference picks it at compile time with
+ *      `make kernel=<k>` (playground/Makefile:14,84-86); here it is a
+ *      run-time argument of sph_create. ------------------------------------ */
+#define SPH_KERNEL_M4    0   /* kernel/base_m4.f90    */
+#define SPH_KERNEL_M6    1   /* kernel/base_m6.f90    */
+#define SPH_KERNEL_GAUSS 2   /* kernel/base_gauss.f90 */
+
+/* ---- precision of the pair arithmetic ------------------------------------ */
+#define SPH_PREC_FP64      0 /* plain FP64 everywhere (parity mode)          */
+#define SPH_PREC_FP32_COMP 1 /* FP32 pair sums, two-sum compensated; FP64
+                                Newton h/Omega update, integrator, dt         */
+
+/* ---- parameters beyond the 49 state slots (sph_set_param index) ---------
+ * Indices 1..49 address statevars(k) exactly as setStateVal does
+ * (state.f90:47-52).  The following extra slots hold values that the
+ * reference hard-codes; their defaults reproduce it. */
+#define SPH_P_AV_ALPHA        50 /* circuit2.f90:565, default 1              */
+#define SPH_P_AV_BETA         51 /* circuit2.f90:566, default 2              */
+#define SPH_P_NEWTON_TOL      52 /* circuit1.f90:104, default 1e-8           */
+#define SPH_P_NEWTON_MAXITER  53 /* circuit1.f90:114, default 100            */
+#define SPH_P_FULL_TENSOR     54 /* 0: diagonal K (circuit2.f90:203-205,371-373),
+                                    1: full k_par * b b^T (new)              */
+#define SPH_P_NEIB_CAP_CHECK  55 /* 1: abort like neighboursearch.f90:127-131
+                                    when n_i+1 > maxneibnum; default 0       */
+#define SPH_P_CELL_FACTOR     56 /* cell edge / (krad*h_min), default 1.0    */
+#define SPH_P_REORDER_EVERY   57 /* physical re-sort interval in steps (8)   */
+#define SPH_P_TIMING          58 /* 1: record per-kernel CUDA-event times    */
+#define SPH_P_NEIB_CAP        59 /* neighbour slots per centre (0 = auto)    */
+#define SPH_P_LAST            59
+
+/* ---- status codes --------------------------------------------------------- */
+#define SPH_OK                     0
+#define SPH_ERR_ARG                1  /* bad argument / null pointer          */
+#define SPH_ERR_CUDA               2  /* CUDA runtime error / no device       */
+#define SPH_ERR_Q_NAN              3  /* base_m6.f90:49-50 'q is nan'         */
+#define SPH_ERR_Q_NEG              4  /* base_m6.f90:51-52 'q is negative'    */
+#define SPH_ERR_H_NEG              5  /* circuit1.f90:202-204                 */
+#define SPH_ERR_NEIB_OVERFLOW      6  /* neighboursearch.f90:127-131          */
+#define SPH_ERR_IC_DENSITY         7  /* preruncheck.f90:39-42                */
+#define SPH_ERR_IC_CSOUND          8  /* preruncheck.f90:43-46                */
+#define SPH_ERR_IC_H               9  /* preruncheck.f90:47-50                */
+#define SPH_ERR_IC_PRESSURE       10  /* preruncheck.f90:51-54                */
+#define SPH_ERR_IC_ENERGY         11  /* preruncheck.f90:55-57                */
+#define SPH_ERR_IC_MUZERO         12  /* preruncheck.f90:28-31                */
+#define SPH_ERR_IC_DIFFCOND       13  /* preruncheck.f90:32-35                */
+#define SPH_ERR_UNSUPPORTED       14  /* option outside this engine's scope   */
+#define SPH_ERR_FLD_ANISO         15  /* circuit2.f90:189, :367               */
+#define SPH_ERR_DDW               16  /* circuit2.f90:422-423                 */
+#define SPH_ERR_PROCESS           17  /* iterator.f90:173-177                 */
+#define SPH_ERR_GRID              18  /* cell grid would not fit              */
+#define SPH_ERR_OOM               19  /* device allocation failed             */
+#define SPH_ERR_TIMEOUT           20  /* a bounded device wait gave up        */
+#define SPH_ERR_STATE             21  /* call not valid in this handle state  */
+
+/* ---- work counters (sph_get_counters, cumulative since create/reset) ----- */
+#define SPH_CNT_ITERATES        0 /* calls of iterate (iterator.f90:44)       */
+#define SPH_CNT_STEPS           1 /* completed time steps                     */
+#define SPH_CNT_NEIB_PAIRS      2 /* in-support pairs found (sum over iterates)*/
+#define SPH_CNT_C1_PAIRS        3 /* pair evaluations in circuit1 (all sweeps)*/
+#define SPH_CNT_C1_SWEEPS       4 /* Newton sweeps (max over particles)       */
+#define SPH_CNT_C2_PAIRS        5 /* pair evaluations in circuit2             */
+#define SPH_CNT_GHOSTS          6 /* periodic images built (last iterate)     */
+#define SPH_CNT_CANDIDATES      7 /* cell-list candidates tested              */
+#define SPH_CNT_CENTRES         8 /* real centres processed (sum)             */
+#define SPH_CNT_C1_CENTRE_SWEEPS 9 /* sum over particles of their sweeps      */
+#define SPH_CNT_TOTAL          10
+
+/* ---- per-kernel timers (sph_get_timers, milliseconds, cumulative) ------- */
+#define SPH_T_PREDICT    0
+#define SPH_T_GHOSTS     1
+#define SPH_T_SORT       2
+#define SPH_T_NEIGHBOURS 3
+#define SPH_T_CIRCUIT1   4
+#define SPH_T_CIRCUIT2   5
+#define SPH_T_CORRECT    6
+#define SPH_T_TIMESTEP   7
+#define SPH_T_STS        8
+#define SPH_T_TOTAL      9
+
+typedef struct sph_handle sph_handle;
+
+/* Create an engine from the dump pair.  Replaces `./execute` start-up with
+ * restore() (main.f90:112-116, dumper.f90:44-66) and initkernel
+ * (kernel.f90:91-152).  n_rows = realpn + fixedpn rows of store.  The state
+ * vector is validated like preruncheck.f90:13-60 when the run starts. */
+int sph_create(const double* state49, const double* store, int64_t n_rows,
+               int kernel_id, int precision_mode, sph_handle** out);
+
+/* statevars(k) = value (state.f90:47-52) for k in 1..49, or an SPH_P_* slot. */
+int sph_set_param(sph_handle* h, int index, double value);
+int sph_get_param(sph_handle* h, int index, double* value);
+
+/* Replace the particle table (same layout as sph_create). */
+int sph_set_store(sph_handle* h, const double* store, int64_t n_rows);
+
+/* One iterate(): periodic ghosts, neighbour search, circuit1, EOS, circuit2
+ * (iterator.f90:44-179). */
+int sph_iterate(sph_handle* h);
+
+/* The density half of iterate(): ghosts, neighbour search, circuit1, EOS. */
+int sph_density(sph_handle* h);
+
+/* Advance the time loop of main.f90:241-373 by nsteps steps (the first call
+ * also runs the initial iterate of main.f90:216-225). */
+int sph_step(sph_handle* h, int nsteps);
+
+/* Run the time loop until statevars(ec_time) reaches tfinish. */
+int sph_run_to(sph_handle* h, double tfinish);
+
+/* Read back the particle table (real + fixed rows, original row order) and
+ * the state vector, in the dump layout (dumper.f90:26-34). */
+int sph_get_store(sph_handle* h, double* out, int64_t cap_rows);
+int sph_get_state(sph_handle* h, double* out49);
+
+/* Neighbour sets of the last neighbour search, one row per real centre in
+ * original order.  offsets has n_real+1 entries.  Each entry of `pairs` is
+ * (rj << 5) | image where rj is the 0-based row of the real/fixed particle
+ * the neighbour is (or is an image of, BC.f90:36-44) and image =
+ * (sx+1) + 3(sy+1) + 9(sz+1) encodes the periodic shift (13 = no shift).
+ * Entries are sorted ascending.  If cap is too small, offsets are filled and
+ * SPH_ERR_ARG is returned. */
+int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs,
+                       int64_t cap);
+
+int sph_get_counters(sph_handle* h, int64_t* out, int n);
+int sph_reset_counters(sph_handle* h);
+int sph_get_timers(sph_handle* h, double* out_ms, int n);
+
+/* Last error message (static storage, valid until the next call). */
+const char* sph_last_error(void);
+
+void sph_destroy(sph_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_ABI_H */

@@ -1,0 +1,218 @@
+// sph_device.cuh — device-side building blocks of the SPH step engine:
+// kernel shapes (M4/M6/Gauss), two-sum accumulators, packed pair-data
+// layouts and the launch-parameter block shared by all kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sph_abi.h"
+
+namespace sph {
+
+// ---- enums mirrored from playground/src/const.f90 --------------------------
+enum : int { esd_fab = 400, esd_n2w = 401, esd_fw = 402, esd_2nw_ds = 403,
+             esd_2nw_sd = 404 };
+enum : int { ept_empty = 0, ept_real = 1, ept_fixed = 2, ept_fixedreal = 21,
+             ept_fixedmirror = 22, ept_periodic = 3 };
+// 0-based store columns (const.f90:69-103 minus one)
+enum : int {
+  es_rx = 0, es_ry, es_rz, es_vx, es_vy, es_vz, es_ax, es_ay, es_az, es_m,
+  es_den, es_h, es_dh, es_p, es_u, es_du, es_t, es_kappa, es_dtdx, es_dtdy,
+  es_dtdz, es_ddt, es_bx, es_by, es_bz, es_dbx, es_dby, es_dbz, es_c, es_om,
+  es_type, es_vfld
+};
+constexpr int NCOL = SPH_ES_TOTAL;
+constexpr double kLightspeed = 2.997924e10;  // const.f90:6
+
+// ---- kernel shapes ------------------------------------------------------------
+// The reference evaluates f(q), f'(q), f''(q) piecewise (kernel/base_m6.f90:36-97,
+// base_m4.f90:35-90, base_gauss.f90:39-82).  On the device the pieces are
+// written branch-free with clamped terms t_k = max(k - q, 0): for q beyond a
+// break point the clamped term is exactly zero, so the sum equals the
+// reference's piece without divergent branches inside a warp.
+enum KernelId : int { KM4 = SPH_KERNEL_M4, KM6 = SPH_KERNEL_M6, KGAUSS = SPH_KERNEL_GAUSS };
+
+template <int K> struct KRad;
+template <> struct KRad<KM4> { static constexpr double v = 2.0; };
+template <> struct KRad<KM6> { static constexpr double v = 3.0; };
+template <> struct KRad<KGAUSS> { static constexpr double v = 10.0; };
+
+template <class R> __device__ __forceinline__ R rmax0(R x) { return x > R(0) ? x : R(0); }
+
+template <int K, class R>
+__device__ __forceinline__ void kshape_f_df(R q, R& f, R& df) {
+  if constexpr (K == KM6) {
+    R t3 = rmax0(R(3) - q), t2 = rmax0(R(2) - q), t1 = rmax0(R(1) - q);
+    R s3 = t3 * t3, s2 = t2 * t2, s1 = t1 * t1;
+    R q3 = s3 * s3, q2 = s2 * s2, q1 = s1 * s1;
+    f = q3 * t3 - R(6) * (q2 * t2) + R(15) * (q1 * t1);
+    df = R(-5) * q3 + R(30) * q2 - R(75) * q1;
+  } else if constexpr (K == KM4) {
+    R t2 = rmax0(R(2) - q), t1 = rmax0(R(1) - q);
+    R s2 = t2 * t2, s1 = t1 * t1;
+    f = R(0.25) * (s2 * t2) - s1 * t1;
+    df = R(-0.75) * s2 + R(3) * s1;
+  } else {
+    R e = exp(-q * q);
+    f = e;
+    df = R(-2) * e * q;
+  }
+}
+
+template <int K, class R>
+__device__ __forceinline__ R kshape_df(R q) {
+  if constexpr (K == KM6) {
+    R t3 = rmax0(R(3) - q), t2 = rmax0(R(2) - q), t1 = rmax0(R(1) - q);
+    R s3 = t3 * t3, s2 = t2 * t2, s1 = t1 * t1;
+    return R(-5) * (s3 * s3) + R(30) * (s2 * s2) - R(75) * (s1 * s1);
+  } else if constexpr (K == KM4) {
+    R t2 = rmax0(R(2) - q), t1 = rmax0(R(1) - q);
+    return R(-0.75) * (t2 * t2) + R(3) * (t1 * t1);
+  } else {
+    return R(-2) * exp(-q * q) * q;
+  }
+}
+
+template <int K, class R>
+__device__ __forceinline__ void kshape_all(R q, R& f, R& df, R& ddf) {
+  if constexpr (K == KM6) {
+    R t3 = rmax0(R(3) - q), t2 = rmax0(R(2) - q), t1 = rmax0(R(1) - q);
+    R s3 = t3 * t3, s2 = t2 * t2, s1 = t1 * t1;
+    R c3 = s3 * t3, c2 = s2 * t2, c1 = s1 * t1;
+    R q3 = s3 * s3, q2 = s2 * s2, q1 = s1 * s1;
+    f = q3 * t3 - R(6) * (q2 * t2) + R(15) * (q1 * t1);
+    df = R(-5) * q3 + R(30) * q2 - R(75) * q1;
+    ddf = R(20) * c3 - R(120) * c2 + R(300) * c1;
+  } else if constexpr (K == KM4) {
+    R t2 = rmax0(R(2) - q), t1 = rmax0(R(1) - q);
+    R s2 = t2 * t2, s1 = t1 * t1;
+    f = R(0.25) * (s2 * t2) - s1 * t1;
+    df = R(-0.75) * s2 + R(3) * s1;
+    ddf = R(1.5) * t2 - R(6) * t1;
+  } else {
+    R e = exp(-q * q);
+    f = e;
+    df = R(-2) * e * q;
+    ddf = R(-2) * e + R(4) * e * q * q;
+  }
+}
+
+template <int K, class R>
+__device__ __forceinline__ R kshape_f(R q) {
+  R f, df;
+  kshape_f_df<K, R>(q, f, df);
+  return f;
+}
+
+// h^n for small non-negative n (the reference's h**dim, h**(dim+2)).
+template <int N, class R>
+__device__ __forceinline__ R ipow(R x) {
+  if constexpr (N == 0) return R(1);
+  else if constexpr (N == 1) return x;
+  else if constexpr (N == 2) return x * x;
+  else if constexpr (N == 3) return x * (x * x);
+  else if constexpr (N == 4) { R s = x * x; return s * s; }
+  else { R s = x * x; return (s * s) * x; }
+}
+
+// ---- compensated accumulation ---------------------------------------------------
+// Two-sum (Knuth): s + e == a + b exactly.  The FP32 path keeps every
+// per-particle sum as (s, c) so that summing ~200 pair terms loses no more
+// than one rounding of the final value.
+template <class R> struct Acc {
+  R s, c;
+  __device__ __forceinline__ void init() { s = R(0); c = R(0); }
+  __device__ __forceinline__ void add(R x) {
+    R t = s + x;
+    R bp = t - s;
+    R e = (s - (t - bp)) + (x - bp);
+    s = t;
+    c += e;
+  }
+  __device__ __forceinline__ R val() const { return s + c; }
+  __device__ __forceinline__ double dval() const { return double(s) + double(c); }
+};
+// Plain FP64 accumulator with the same interface.
+template <> struct Acc<double> {
+  double s;
+  __device__ __forceinline__ void init() { s = 0.0; }
+  __device__ __forceinline__ void add(double x) { s += x; }
+  __device__ __forceinline__ double val() const { return s; }
+  __device__ __forceinline__ double dval() const { return s; }
+};
+
+// ---- packed pair data (sorted order) ----------------------------------------------
+// FP64: eleven double2 streams.  FP32: six float4 streams; positions are a
+// hi/lo float pair of (x - origin + 2^E), all in one binade, so hi_i - hi_j
+// is exact and dx = (hi_i - hi_j) + (lo_i - lo_j) carries one FP32 rounding.
+struct PackF64 {
+  const double2* p0;  // x, y
+  const double2* p1;  // z, m
+  const double2* p2;  // h, rho
+  const double2* p3;  // om, P
+  const double2* p4;  // c, u
+  const double2* p5;  // vx, vy
+  const double2* p6;  // vz, T
+  const double2* p7;  // kappa, dtdx
+  const double2* p8;  // dtdy, dtdz
+  const double2* p9;  // bx, by
+  const double2* p10; // bz, 0
+};
+struct PackF32 {
+  const float4* q0;  // xhi, yhi, zhi, m
+  const float4* q1;  // xlo, ylo, zlo, h
+  const float4* q2;  // rho, om, P, c
+  const float4* q3;  // u, vx, vy, vz
+  const float4* q4;  // T, kappa, dtdx, dtdy
+  const float4* q5;  // dtdz, bx, by, bz
+};
+
+template <class R> struct PairPos;  // position handle for dx computation
+template <> struct PairPos<double> {
+  double x, y, z;
+};
+template <> struct PairPos<float> {
+  float xh, yh, zh, xl, yl, zl;
+};
+
+__device__ __forceinline__ void pos_delta(const PairPos<double>& a, const PairPos<double>& b,
+                                          double& dx, double& dy, double& dz) {
+  dx = a.x - b.x; dy = a.y - b.y; dz = a.z - b.z;
+}
+__device__ __forceinline__ void pos_delta(const PairPos<float>& a, const PairPos<float>& b,
+                                          float& dx, float& dy, float& dz) {
+  dx = (a.xh - b.xh) + (a.xl - b.xl);
+  dy = (a.yh - b.yh) + (a.yl - b.yl);
+  dz = (a.zh - b.zh) + (a.zl - b.zl);
+}
+
+// ---- launch parameters -------------------------------------------------------------
+struct Params {
+  int dim;
+  int kernel;
+  double krad;
+  double wCv;      // knorm(dim)
+  double fwc;      // fwcl(dim)
+  double hfac;
+  double alpha, beta, au;
+  double gamma;
+  double muzero;
+  double difcond;
+  int difiso;
+  int ddw;
+  int full_tensor;
+  int eq_hydro, eq_magneto, eq_diff, eq_fld;
+  int adden, artts;
+  double tol;
+  int maxiter;
+  int eos_kind;  // 0 none, 1 adiabatic, 2 isothermal
+  double c_iso;  // c of row 1 for eos_isothermal
+};
+
+// status word helper: first error wins
+__device__ __forceinline__ void raise_status(int* status, int code) {
+  atomicCAS(status, 0, code);
+}
+
+}  // namespace sph

@@ -1,0 +1,1118 @@
+// sph_engine.cu — the C-ABI of include/sph_abi.h and the host-side
+// orchestration of one SPH step on the device:
+//   iterate  (iterator.f90:44-179): reflect -> periodic images -> cell keys ->
+//            radix sort -> cell ranges -> neighbour lists -> circuit1 (+EOS)
+//            -> circuit2
+//   step     (main.f90:241-373): timestep -> predictor -> iterate ->
+//            corrector -> STS stages
+// Everything runs on one CUDA stream per handle.  The host reads back a few
+// scalars per iterate (image count and bounding box, the largest neighbour
+// count, the Newton "still active" flag on the Jacobi path, the timestep
+// reductions) and nothing else.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "sph_internal.h"
+
+using namespace sph;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(SPH_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define RC(call)             \
+  do {                       \
+    int rc_ = (call);        \
+    if (rc_) return rc_;     \
+  } while (0)
+
+// state slots (const.f90:14-66)
+enum : int {
+  ec_dim = 1, ec_eqs = 2, ec_ddw = 3, ec_ics = 4, ec_adden = 5, ec_artts = 6,
+  ec_coordsys = 7, ec_disotropic = 8, ec_dcondconst = 9, ec_muzero = 10,
+  ec_tfinish = 11, ec_hfac = 13, ec_xmin = 17, ec_xmax = 18, ec_ymin = 19,
+  ec_ymax = 20, ec_zmin = 21, ec_zmax = 22, ec_bordsize = 23, ec_padding = 24,
+  ec_realpn = 25, ec_fixedpn = 26, ec_gamma = 27, ec_dtprint = 30,
+  ec_process = 31, ec_au = 32, ec_eqonhydro = 34, ec_eqondiff = 35,
+  ec_eqonfluxlim = 36, ec_eqonradexch = 37, ec_eqonsts = 38, ec_time = 46,
+  ec_ststype = 48, ec_stsfixeds = 49
+};
+enum : int { eeq_hydro = 300, eeq_diffusion = 301, eeq_magnetohydro = 302,
+             eeq_magnetohydrodiffusion = 303, eeq_hydrodiffusion = 304,
+             eeq_kd2 = 305, eeq_hyrad = 306, eeq_manual = 307 };
+enum : int { epc_backcompatibility = 600, epc_fullyperiodic = 601, epc_borderless = 602 };
+enum : int { ett_mti = 101, ett_shock12 = 102, ett_pulse = 103, ett_ring = 104,
+             ett_soundwave = 105, ett_hydroshock = 106, ett_OTvortex = 108,
+             ett_mtilowres = 110, ett_fld_gauss = 111 };
+
+const double kPi = 4.0 * std::atan(1.0);
+
+// kernel bases (kernel/base_m4.f90:12-32, base_m6.f90:13-33, base_gauss.f90:15-36)
+struct KBase {
+  double knorm[3], fwcl[3];
+  int maxneib[3];
+  double krad, cn_hydro, cn_2nw, cn_fab, cn_n2w;
+};
+KBase kbase(int id) {
+  KBase k;
+  if (id == SPH_KERNEL_M6) {
+    k = {{1. / 120., 7. / (478. * kPi), 1. / (120. * kPi)}, {4., 9.31505 / 2.25, 9.6429 / 2.25},
+         {50, 10000, 150}, 3., 0.3, 1.1, 0.2, 0.4};
+  } else if (id == SPH_KERNEL_M4) {
+    k = {{2. / 3., 10. / (7. * kPi), 1. / kPi}, {6., 6.3226, 6.66400}, {35, 250, 150},
+         2., 0.1, 0.96, 0.15, 0.2};
+  } else {
+    k = {{1. / std::sqrt(kPi), 1. / kPi, 1. / std::pow(kPi, 1.5)}, {4., 4., 4.},
+         {100, 5000, 50000}, 10., 0.55, 1.25, 0.24, 0.50};
+  }
+  return k;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  int ensure(size_t b) {
+    if (b <= bytes && p) return SPH_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t nb = std::max<size_t>(b, 256);
+    cudaError_t e = cudaMalloc(&p, nb);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(SPH_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    bytes = nb;
+    return SPH_OK;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct Mode {
+  bool ghosts = false;
+  int periodic[3] = {0, 0, 0};
+  int reflect[3] = {0, 0, 0};
+  int eos_kind = 1;
+  int mti = 0;  // 1 mti, 2 mtilowres
+};
+
+}  // namespace
+
+struct sph_handle {
+  int kernel_id = SPH_KERNEL_M6;
+  int prec = SPH_PREC_FP64;
+  KBase kb;
+  std::vector<double> st;  // 1-based
+  int64_t nrows = 0, nreal = 0, nfixed = 0, n_int = 0;
+  cudaStream_t s = nullptr;
+
+  // canonical store, SoA columns of length nrows
+  DevBuf cols, cols_alt, orig, orig_alt, staging;
+  // predictor saves, STS stages, circuit1 iterates
+  DevBuf save, stsY, hkp1, dkp1, okp1, epsb;
+  // images
+  DevBuf gcount, goff, gx, gy, gz, gsrc, gcode, scan_tmp;
+  int64_t nghost = 0;
+  // sort + cells
+  DevBuf keys, keys_alt, vals, vals_alt, sort_tmp, cstart, cend;
+  // sorted arrays
+  DevBuf sx, sy, sz, ssrc, cflag, cpos, centre_k, centre_p;
+  DevBuf hk_s, dk_s, ok_s;
+  DevBuf pk[11], qk[6];
+  // neighbours
+  DevBuf nl, ncnt;
+  int cap = 0;
+  // scalars
+  DevBuf status, red, dcnt, maxcnt, ctrl, ciso;
+  unsigned long long* h_red = nullptr;  // pinned
+  double* h_ctrl = nullptr;             // pinned
+  int32_t* h_i32 = nullptr;             // pinned scratch
+
+  Grid grid{};
+  PackGeom pgeom{};
+  double mref = 1.0;
+  bool have_order = false;
+  int steps_since_reorder = 0;
+
+  // time loop state (main.f90)
+  bool started = false, stopped = false;
+  double ltout = 0., dtout = 0.;
+
+  int64_t cnt_host[SPH_CNT_TOTAL] = {0};
+  int64_t host_max_sweeps = 0;  // Newton sweeps of the Jacobi path
+  double timers[SPH_T_TOTAL] = {0};
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending_ev;
+  std::vector<cudaEvent_t> ev_pool;
+
+  // equation set (state.f90:117-149)
+  bool eq_hydro = false, eq_magneto = false, eq_diff = false, eq_fld = false,
+       eq_radexch = false, eq_sts = false;
+
+  int ival(int k) const { return int(st[k]); }
+
+  double* col(int f) const { return cols.as<double>() + int64_t(f) * nrows; }
+
+  // ---- timing -------------------------------------------------------------------
+  cudaEvent_t get_event() {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  struct Phase {
+    sph_handle* h;
+    int slot;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Phase(sph_handle* hh, int sl) : h(hh), slot(sl) {
+      if (h->st[SPH_P_TIMING] != 0) {
+        a = h->get_event();
+        b = h->get_event();
+        cudaEventRecord(a, h->s);
+      }
+    }
+    ~Phase() {
+      if (a) {
+        cudaEventRecord(b, h->s);
+        h->pending_ev.push_back({slot, {a, b}});
+      }
+    }
+  };
+  void collect_timers() {
+    for (auto& pe : pending_ev) {
+      float ms = 0.f;
+      cudaEventSynchronize(pe.second.second);
+      if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess)
+        timers[pe.first] += ms;
+      ev_pool.push_back(pe.second.first);
+      ev_pool.push_back(pe.second.second);
+    }
+    pending_ev.clear();
+  }
+
+  // ---- configuration ------------------------------------------------------------------
+  void eqset() {
+    eq_hydro = eq_magneto = eq_diff = eq_fld = eq_radexch = eq_sts = false;
+    switch (ival(ec_eqs)) {
+      case eeq_hydro: eq_hydro = true; break;
+      case eeq_magnetohydro: eq_hydro = eq_magneto = true; break;
+      case eeq_diffusion: eq_diff = true; break;
+      case eeq_hyrad: eq_fld = eq_hydro = eq_radexch = true; break;
+      case eeq_magnetohydrodiffusion: eq_hydro = eq_magneto = eq_diff = true; break;
+      case eeq_hydrodiffusion: eq_hydro = eq_diff = true; break;
+      case eeq_manual:
+        eq_diff = ival(ec_eqondiff) == 1;
+        eq_hydro = ival(ec_eqonhydro) == 1;
+        eq_fld = ival(ec_eqonfluxlim) == 1;
+        eq_radexch = ival(ec_eqonradexch) == 1;
+        eq_sts = ival(ec_eqonsts) == 1;
+        break;
+      default: break;
+    }
+  }
+  int dim() const { return ival(ec_dim); }
+
+  int params(Params& P) {
+    eqset();
+    int d = dim();
+    if (d < 1 || d > 3) return fail(SPH_ERR_ARG, "Dimmention is wrong");
+    if (ival(ec_coordsys) == 2)
+      return fail(SPH_ERR_UNSUPPORTED, "cylindric coordinates: Fab_cylindric does not exist (kernel.f90:137)");
+    P.dim = d;
+    P.kernel = kernel_id;
+    P.krad = kb.krad;
+    P.wCv = kb.knorm[d - 1];
+    P.fwc = kb.fwcl[d - 1];
+    P.hfac = st[ec_hfac];
+    P.alpha = st[SPH_P_AV_ALPHA];
+    P.beta = st[SPH_P_AV_BETA];
+    P.au = st[ec_au];
+    P.gamma = st[ec_gamma];
+    P.muzero = st[ec_muzero];
+    P.difcond = st[ec_dcondconst];
+    P.difiso = ival(ec_disotropic);
+    P.ddw = ival(ec_ddw);
+    P.full_tensor = st[SPH_P_FULL_TENSOR] != 0;
+    P.eq_hydro = eq_hydro; P.eq_magneto = eq_magneto; P.eq_diff = eq_diff; P.eq_fld = eq_fld;
+    P.adden = ival(ec_adden);
+    P.artts = ival(ec_artts);
+    P.tol = st[SPH_P_NEWTON_TOL];
+    P.maxiter = std::max(0, int(st[SPH_P_NEWTON_MAXITER]));
+    P.eos_kind = 1;
+    P.c_iso = 0.;
+    if (eq_diff && eq_fld && P.difiso != 1)
+      return fail(SPH_ERR_FLD_ANISO, "There is no anisotropic for FLD");
+    if (eq_diff && !(P.ddw == esd_fw || P.ddw == esd_fab || P.ddw == esd_n2w ||
+                     P.ddw == esd_2nw_ds || P.ddw == esd_2nw_sd))
+      return fail(SPH_ERR_DDW, "second deriv id not found");
+    return SPH_OK;
+  }
+  // cnd2 (kernel.f90:108-134)
+  double cnd2() const {
+    int ddw = ival(ec_ddw);
+    if (ddw == esd_n2w) return kb.cn_n2w;
+    if (ddw == esd_2nw_ds || ddw == esd_2nw_sd) return kb.cn_2nw;
+    return kb.cn_fab;
+  }
+
+  int mode(Mode& m) {
+    int ipc = ival(ec_process), ivt = ival(ec_ics), d = dim();
+    auto all = [&](int* a) { for (int k = 0; k < d; ++k) a[k] = 1; };
+    if (ipc == epc_fullyperiodic) {
+      m.ghosts = true; all(m.periodic); all(m.reflect);
+    } else if (ipc == epc_borderless) {
+    } else if (ipc == epc_backcompatibility) {
+      switch (ivt) {
+        case ett_shock12: m.ghosts = true; if (d > 1) m.periodic[1] = 1; break;
+        case ett_pulse: case ett_ring: case ett_fld_gauss: m.eos_kind = 0; break;
+        case ett_soundwave: m.ghosts = true; all(m.periodic); all(m.reflect); m.eos_kind = 2; break;
+        case ett_OTvortex: m.ghosts = true; all(m.periodic); all(m.reflect); break;
+        case ett_hydroshock:
+          m.ghosts = true;
+          if (d > 1) { m.periodic[1] = m.reflect[1] = 1; }
+          if (d > 2) { m.periodic[2] = m.reflect[2] = 1; }
+          break;
+        case ett_mti: case ett_mtilowres:
+          m.ghosts = true; m.periodic[0] = m.reflect[0] = 1; m.mti = ivt == ett_mti ? 1 : 2; break;
+        default: return fail(SPH_ERR_PROCESS, "Task type was not set");
+      }
+    } else {
+      return fail(SPH_ERR_PROCESS, "Process type was not set");
+    }
+    return SPH_OK;
+  }
+
+  BoxGeom box(const Mode& m) const {
+    BoxGeom g;
+    double bs = st[ec_bordsize], pad = st[ec_padding];
+    g.emin[0] = st[ec_xmin]; g.emax[0] = st[ec_xmax];
+    g.emin[1] = st[ec_ymin]; g.emax[1] = st[ec_ymax];
+    g.emin[2] = st[ec_zmin]; g.emax[2] = st[ec_zmax];
+    for (int k = 0; k < 3; ++k) {
+      g.boxmin[k] = g.emin[k] + bs;  // BC.f90:63-64
+      g.boxmax[k] = g.emax[k] - bs;
+      g.pmin[k] = g.emin[k];         // BC.f90:210-223 (padding/10 only when padding == 0)
+      g.pmax[k] = g.emax[k];
+      if (pad == 0) { g.pmin[k] = g.emin[k] + pad / 10; g.pmax[k] = g.emax[k] - pad / 10; }
+      g.periodic[k] = m.periodic[k];
+      g.reflect[k] = m.reflect[k];
+    }
+    return g;
+  }
+
+  // ---- allocation -----------------------------------------------------------------------
+  int alloc_base() {
+    RC(cols.ensure(sizeof(double) * NCOL * nrows));
+    RC(cols_alt.ensure(sizeof(double) * NCOL * nrows));
+    RC(orig.ensure(sizeof(int32_t) * nrows));
+    RC(orig_alt.ensure(sizeof(int32_t) * nrows));
+    RC(staging.ensure(sizeof(double) * NCOL * nrows));
+    RC(save.ensure(sizeof(double) * 9 * nrows));
+    RC(hkp1.ensure(sizeof(double) * nrows));
+    RC(dkp1.ensure(sizeof(double) * nrows));
+    RC(okp1.ensure(sizeof(double) * nrows));
+    RC(epsb.ensure(sizeof(double) * nrows));
+    RC(gcount.ensure(sizeof(int32_t) * (nrows + 1)));
+    RC(goff.ensure(sizeof(int32_t) * (nrows + 1)));
+    RC(status.ensure(sizeof(int)));
+    RC(red.ensure(sizeof(unsigned long long) * RED_TOTAL));
+    RC(dcnt.ensure(sizeof(unsigned long long) * DC_TOTAL));
+    RC(maxcnt.ensure(sizeof(int32_t)));
+    RC(ctrl.ensure(sizeof(double) * 8));
+    RC(ciso.ensure(sizeof(double)));
+    CK(cudaMemsetAsync(status.p, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(dcnt.p, 0, sizeof(unsigned long long) * DC_TOTAL, s));
+    CK(cudaMemsetAsync(ctrl.p, 0, sizeof(double) * 8, s));
+    CK(cudaMemsetAsync(save.p, 0, sizeof(double) * 9 * nrows, s));
+    size_t sb = scan_temp_bytes(nrows + 1);
+    RC(scan_tmp.ensure(sb));
+    return SPH_OK;
+  }
+  int alloc_all(int64_t nall) {
+    RC(keys.ensure(sizeof(uint32_t) * nall));
+    RC(keys_alt.ensure(sizeof(uint32_t) * nall));
+    RC(vals.ensure(sizeof(int32_t) * nall));
+    RC(vals_alt.ensure(sizeof(int32_t) * nall));
+    RC(sort_tmp.ensure(sort_temp_bytes(nall)));
+    RC(sx.ensure(sizeof(double) * nall));
+    RC(sy.ensure(sizeof(double) * nall));
+    RC(sz.ensure(sizeof(double) * nall));
+    RC(ssrc.ensure(sizeof(int32_t) * nall));
+    RC(cflag.ensure(sizeof(int32_t) * (nall + 1)));
+    RC(cpos.ensure(sizeof(int32_t) * (nall + 1)));
+    RC(centre_k.ensure(sizeof(int32_t) * std::max<int64_t>(nreal, 1)));
+    RC(centre_p.ensure(sizeof(int32_t) * std::max<int64_t>(nreal, 1)));
+    RC(hk_s.ensure(sizeof(double) * nall));
+    RC(dk_s.ensure(sizeof(double) * nall));
+    RC(ok_s.ensure(sizeof(double) * nall));
+    size_t sb = scan_temp_bytes(nall + 1);
+    if (sb > scan_tmp.bytes) RC(scan_tmp.ensure(sb));
+    if (prec == SPH_PREC_FP64) {
+      for (int i = 0; i < 11; ++i) RC(pk[i].ensure(sizeof(double2) * nall));
+    } else {
+      for (int i = 0; i < 6; ++i) RC(qk[i].ensure(sizeof(float4) * nall));
+    }
+    return SPH_OK;
+  }
+  PackBufs packs() const {
+    PackBufs pb;
+    for (int i = 0; i < 11; ++i) pb.p[i] = pk[i].as<double2>();
+    for (int i = 0; i < 6; ++i) pb.q[i] = qk[i].as<float4>();
+    return pb;
+  }
+
+  int check_status() {
+    int code = 0;
+    CK(cudaMemcpyAsync(h_i32, status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    code = h_i32[0];
+    if (code) {
+      CK(cudaMemsetAsync(status.p, 0, sizeof(int), s));
+      const char* msg = "device error";
+      switch (code) {
+        case SPH_ERR_Q_NAN: msg = "q is nan"; break;
+        case SPH_ERR_Q_NEG: msg = "q is negative"; break;
+        case SPH_ERR_H_NEG: msg = "Negative smoothing length in c1 advanced"; break;
+        default: break;
+      }
+      return fail(code, msg);
+    }
+    return SPH_OK;
+  }
+
+  // ---- physical re-ordering of the rows (locality of the pair loops) ---------------------
+  int reorder_rows() {
+    if (!have_order) return SPH_OK;
+    // perm = real rows in cell order, then the fixed rows as they are
+    int32_t* perm = cpos.as<int32_t>();
+    CK(cudaMemcpyAsync(perm, centre_p.p, sizeof(int32_t) * nreal, cudaMemcpyDeviceToDevice, s));
+    if (nfixed > 0) {
+      std::vector<int32_t> tail(nfixed);
+      for (int64_t i = 0; i < nfixed; ++i) tail[i] = int32_t(nreal + i);
+      CK(cudaMemcpyAsync(perm + nreal, tail.data(), sizeof(int32_t) * nfixed,
+                         cudaMemcpyHostToDevice, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    launch_reorder(cols.as<double>(), cols_alt.as<double>(), orig.as<int32_t>(),
+                   orig_alt.as<int32_t>(), perm, nrows, nrows, nrows, s);
+    std::swap(cols.p, cols_alt.p);
+    std::swap(cols.bytes, cols_alt.bytes);
+    std::swap(orig.p, orig_alt.p);
+    std::swap(orig.bytes, orig_alt.bytes);
+    have_order = false;
+    steps_since_reorder = 0;
+    CK(cudaGetLastError());
+    return SPH_OK;
+  }
+
+  // ---- neighbour phase: images, grid, sort, lists --------------------------------------------
+  int neighbour_phase(const Mode& m, const Params& P) {
+    const int d = P.dim;
+    BoxGeom g = box(m);
+    {
+      Phase ph(this, SPH_T_GHOSTS);
+      if (m.ghosts) launch_reflect(cols.as<double>(), nrows, nreal, g, s);
+      // reduction slots: lo (min), hi (max), hmin
+      launch_fill_u64(red.as<unsigned long long>() + RED_LO_X, 3, dkey(1e308), s);
+      launch_fill_u64(red.as<unsigned long long>() + RED_HI_X, 3, dkey(-1e308), s);
+      launch_fill_u64(red.as<unsigned long long>() + RED_HMIN, 1, dkey(1e308), s);
+      BoxGeom gg = g;
+      if (!m.ghosts) for (int k = 0; k < 3; ++k) gg.periodic[k] = 0;
+      launch_ghost_count(cols.as<double>(), nrows, nreal, gg, d, gcount.as<int32_t>(),
+                         red.as<unsigned long long>(), s);
+      CK(cudaMemsetAsync(gcount.as<int32_t>() + nrows, 0, sizeof(int32_t), s));
+      exclusive_scan(scan_tmp.p, scan_tmp.bytes, gcount.as<int32_t>(), goff.as<int32_t>(),
+                     nrows + 1, s);
+      CK(cudaMemcpyAsync(h_i32, goff.as<int32_t>() + nrows, sizeof(int32_t),
+                         cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(h_red, red.p, sizeof(unsigned long long) * (RED_HMIN + 1),
+                         cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      nghost = h_i32[0];
+      RC(gx.ensure(sizeof(double) * std::max<int64_t>(nghost, 1)));
+      RC(gy.ensure(sizeof(double) * std::max<int64_t>(nghost, 1)));
+      RC(gz.ensure(sizeof(double) * std::max<int64_t>(nghost, 1)));
+      RC(gsrc.ensure(sizeof(int32_t) * std::max<int64_t>(nghost, 1)));
+      RC(gcode.ensure(sizeof(int8_t) * std::max<int64_t>(nghost, 1)));
+      if (nghost > 0)
+        launch_ghost_write(cols.as<double>(), nrows, gg, d, goff.as<int32_t>(), gx.as<double>(),
+                           gy.as<double>(), gz.as<double>(), gsrc.as<int32_t>(),
+                           gcode.as<int8_t>(), nullptr, s);
+    }
+    const int64_t nall = nrows + nghost;
+    RC(alloc_all(nall));
+    // grid: cell edge krad * h_min * factor, at most 1024 cells per axis
+    double lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = dkey_inv(h_red[RED_LO_X + k]);
+      hi[k] = dkey_inv(h_red[RED_HI_X + k]);
+    }
+    double hmin = dkey_inv(h_red[RED_HMIN]);
+    if (!(hmin > 0) || !std::isfinite(hmin)) return fail(SPH_ERR_IC_H, "smoothing length <= 0");
+    for (int k = 0; k < 3; ++k)
+      if (!std::isfinite(lo[k]) || !std::isfinite(hi[k])) return fail(SPH_ERR_Q_NAN, "q is nan");
+    double cf = st[SPH_P_CELL_FACTOR] > 0 ? st[SPH_P_CELL_FACTOR] : 1.0;
+    double L = P.krad * hmin * cf;
+    int64_t ncell = 0;
+    int n3[3];
+    for (int guard = 0;; ++guard) {
+      bool ok = true;
+      ncell = 1;
+      for (int k = 0; k < 3; ++k) {
+        double e = (hi[k] - lo[k]) / L;
+        if (!(e < 1023.0)) { ok = false; break; }
+        n3[k] = int(std::floor(e)) + 1;
+        ncell *= n3[k];
+      }
+      if (ok && ncell <= std::max<int64_t>(8 * nall, 1 << 20)) break;
+      L *= 1.25;
+      if (guard > 400) return fail(SPH_ERR_GRID, "cell grid would not fit");
+    }
+    grid.ox = lo[0]; grid.oy = lo[1]; grid.oz = lo[2];
+    grid.L = L; grid.invL = 1.0 / L;
+    grid.nx = n3[0]; grid.ny = n3[1]; grid.nz = n3[2];
+    int maxn = std::max(n3[0], std::max(n3[1], n3[2]));
+    int bits = 0;
+    while ((1 << bits) < maxn) ++bits;
+    int end_bit = std::max(1, 3 * bits);
+    // FP32 position packing: one binade [2^E, 2^(E+1)) over the whole extent
+    double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    double sh = 1.0;
+    if (ext > 0) {
+      while (sh < ext * 1.0001) sh *= 2.0;
+      while (sh * 0.5 >= ext * 1.0001) sh *= 0.5;
+    }
+    pgeom.ox = lo[0]; pgeom.oy = lo[1]; pgeom.oz = lo[2];
+    pgeom.shift = sh;
+    pgeom.mref = mref;
+    {
+      Phase ph(this, SPH_T_SORT);
+      launch_keys(cols.as<double>(), nrows, gx.as<double>(), gy.as<double>(), gz.as<double>(),
+                  nghost, grid, keys.as<uint32_t>(), vals.as<int32_t>(), s);
+      sort_pairs(sort_tmp.p, sort_tmp.bytes, keys.as<uint32_t>(), keys_alt.as<uint32_t>(),
+                 vals.as<int32_t>(), vals_alt.as<int32_t>(), nall, end_bit, s);
+      RC(cstart.ensure(sizeof(int32_t) * ncell));
+      RC(cend.ensure(sizeof(int32_t) * ncell));
+      CK(cudaMemsetAsync(cstart.p, 0, sizeof(int32_t) * ncell, s));
+      CK(cudaMemsetAsync(cend.p, 0, sizeof(int32_t) * ncell, s));
+      launch_cell_ranges(keys_alt.as<uint32_t>(), nall, grid, cstart.as<int32_t>(),
+                         cend.as<int32_t>(), s);
+      launch_sorted_gather(vals_alt.as<int32_t>(), nall, nrows, nreal, cols.as<double>(),
+                           gx.as<double>(), gy.as<double>(), gz.as<double>(), gsrc.as<int32_t>(),
+                           sx.as<double>(), sy.as<double>(), sz.as<double>(), ssrc.as<int32_t>(),
+                           cflag.as<int32_t>(), nullptr, nullptr, s);
+      CK(cudaMemsetAsync(cflag.as<int32_t>() + nall, 0, sizeof(int32_t), s));
+      exclusive_scan(scan_tmp.p, scan_tmp.bytes, cflag.as<int32_t>(), cpos.as<int32_t>(),
+                     nall + 1, s);
+      launch_centres(vals_alt.as<int32_t>(), cflag.as<int32_t>(), cpos.as<int32_t>(), nall,
+                     centre_k.as<int32_t>(), centre_p.as<int32_t>(), s);
+    }
+    // neighbour lists, grown until every list fits
+    if (cap <= 0) {
+      double sp = 1.0, kh = P.krad * P.hfac;
+      double est = d == 3 ? 4.0 / 3.0 * kPi * kh * kh * kh : (d == 2 ? kPi * kh * kh : 2 * kh);
+      (void)sp;
+      cap = int(est * 1.5) + 32;
+      if (st[SPH_P_NEIB_CAP] > 0) cap = int(st[SPH_P_NEIB_CAP]);
+    }
+    for (int attempt = 0; attempt < 4; ++attempt) {
+      Phase ph(this, SPH_T_NEIGHBOURS);
+      RC(nl.ensure(sizeof(int32_t) * size_t(cap) * std::max<int64_t>(nreal, 1)));
+      RC(ncnt.ensure(sizeof(int32_t) * std::max<int64_t>(nreal, 1)));
+      CK(cudaMemsetAsync(maxcnt.p, 0, sizeof(int32_t), s));
+      launch_neighbours(d, nreal, centre_k.as<int32_t>(), centre_p.as<int32_t>(), sx.as<double>(),
+                        sy.as<double>(), sz.as<double>(), col(es_h), P.krad, grid,
+                        cstart.as<int32_t>(), cend.as<int32_t>(), cap, nl.as<int32_t>(),
+                        ncnt.as<int32_t>(), maxcnt.as<int32_t>(), dcnt.as<unsigned long long>(),
+                        s);
+      CK(cudaMemcpyAsync(h_i32, maxcnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      CK(cudaGetLastError());
+      int mc = h_i32[0];
+      if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc + 1 > kb.maxneib[d - 1])
+        return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
+      if (mc <= cap) break;
+      cap = int(mc * 1.15) + 8;
+      if (attempt == 3) return fail(SPH_ERR_NEIB_OVERFLOW, "neighbour list capacity");
+    }
+    have_order = true;
+    cnt_host[SPH_CNT_GHOSTS] = nghost;
+    return SPH_OK;
+  }
+
+  // ---- circuit1 + EOS ----------------------------------------------------------------------
+  int circuit1(const Mode& m, Params& P) {
+    Phase ph(this, SPH_T_CIRCUIT1);
+    const int64_t nall = nrows + nghost;
+    PackBufs pb = packs();
+    P.eos_kind = m.eos_kind;
+    if (m.eos_kind == 2) {
+      // c of row 1 (eos.f90:43): find the physical row whose original index is 0
+      std::vector<int32_t> og(nrows);
+      CK(cudaMemcpyAsync(og.data(), orig.p, sizeof(int32_t) * nrows, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      int64_t p0 = std::find(og.begin(), og.end(), 0) - og.begin();
+      CK(cudaMemcpyAsync(h_ctrl + 7, col(es_c) + p0, sizeof(double), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      P.c_iso = h_ctrl[7];
+    }
+    launch_pack(prec, PACK_POS, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+                sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+    C1Args a{};
+    a.nc = nreal;
+    a.centre_k = centre_k.as<int32_t>();
+    a.centre_p = centre_p.as<int32_t>();
+    a.nl = nl.as<int32_t>();
+    a.ncnt = ncnt.as<int32_t>();
+    a.cols = cols.as<double>();
+    a.ld = nrows;
+    a.hk_s = hk_s.as<double>();
+    a.dk_s = dk_s.as<double>();
+    a.ok_s = ok_s.as<double>();
+    a.hkp1 = hkp1.as<double>();
+    a.dkp1 = dkp1.as<double>();
+    a.okp1 = okp1.as<double>();
+    a.eps = epsb.as<double>();
+    a.mref = mref;
+    a.status = status.as<int>();
+    a.dcnt = dcnt.as<unsigned long long>();
+    a.red = red.as<unsigned long long>();
+    const bool advanced = ival(ec_adden) == 1;
+    if (advanced && P.maxiter == 0) {  // zero sweeps: h, rho, Omega stay (circuit1.f90:114)
+      launch_eos(cols.as<double>(), nrows, nreal, P, s);
+      CK(cudaGetLastError());
+      return SPH_OK;
+    }
+    if (advanced && !eq_diff && !eq_fld) {
+      launch_c1_newton(prec, kernel_id, P.dim, a, pb, P, s);
+      CK(cudaGetLastError());
+      return SPH_OK;
+    }
+    // Jacobi sweeps (circuit1.f90:105-211) / direct summation (:237-301)
+    a.simple = advanced ? 0 : 1;
+    CK(cudaMemcpyAsync(hkp1.p, col(es_h), sizeof(double) * nrows, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(dkp1.p, col(es_den), sizeof(double) * nrows, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(okp1.p, col(es_om), sizeof(double) * nrows, cudaMemcpyDeviceToDevice, s));
+    launch_set_col(epsb.as<double>(), nrows, 1.0, s);
+    int iter = 0;
+    for (;;) {
+      ++iter;
+      launch_c1_snapshot(nall, ssrc.as<int32_t>(), hkp1.as<double>(), dkp1.as<double>(),
+                         okp1.as<double>(), hk_s.as<double>(), dk_s.as<double>(),
+                         ok_s.as<double>(), s);
+      launch_fill_u64(red.as<unsigned long long>() + RED_C1_ACTIVE, 1, 0ull, s);
+      launch_c1_sweep(prec, kernel_id, P.dim, a, pb, P, s);
+      if (a.simple) break;
+      CK(cudaMemcpyAsync(h_red + RED_C1_ACTIVE, red.as<unsigned long long>() + RED_C1_ACTIVE,
+                         sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      CK(cudaGetLastError());
+      if (!h_red[RED_C1_ACTIVE] || iter >= P.maxiter) break;
+    }
+    launch_c1_finalize(nrows, nreal, cols.as<double>(), nrows, hkp1.as<double>(),
+                       dkp1.as<double>(), okp1.as<double>(), a.simple, P, s);
+    host_max_sweeps = std::max<int64_t>(host_max_sweeps, iter);
+    CK(cudaGetLastError());
+    return SPH_OK;
+  }
+
+  int circuit2(const Mode& m, const Params& P) {
+    Phase ph(this, SPH_T_CIRCUIT2);
+    const int64_t nall = nrows + nghost;
+    PackBufs pb = packs();
+    int groups = PACK_POS | PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
+    launch_pack(prec, groups, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+                sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+    C2Args a{};
+    a.nc = nreal;
+    a.centre_k = centre_k.as<int32_t>();
+    a.centre_p = centre_p.as<int32_t>();
+    a.nl = nl.as<int32_t>();
+    a.ncnt = ncnt.as<int32_t>();
+    a.cols = cols.as<double>();
+    a.ld = nrows;
+    a.mref = mref;
+    a.status = status.as<int>();
+    a.dcnt = dcnt.as<unsigned long long>();
+    launch_c2(prec, kernel_id, P.dim, a, pb, P, s);
+    if (m.mti) launch_apply_mti(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, nreal,
+                                m.mti == 2, s);
+    CK(cudaGetLastError());
+    return SPH_OK;
+  }
+
+  // iterate() (iterator.f90:44-179); full = false stops after circuit1 + EOS
+  int iterate(bool full) {
+    Params P{};
+    RC(params(P));
+    Mode m;
+    RC(mode(m));
+    RC(neighbour_phase(m, P));
+    RC(circuit1(m, P));
+    if (full) RC(circuit2(m, P));
+    RC(check_status());
+    cnt_host[SPH_CNT_ITERATES] += full ? 1 : 0;
+    cnt_host[SPH_CNT_CENTRES] += nreal;
+    collect_timers();
+    return SPH_OK;
+  }
+
+  // ---- pre-run check (preruncheck.f90:13-60) -------------------------------------------------
+  int check_vars_ready() {
+    int s_tt = ival(ec_eqs);
+    if (st[ec_muzero] <= 0. && (s_tt == eeq_magnetohydro || s_tt == eeq_magnetohydrodiffusion))
+      return fail(SPH_ERR_IC_MUZERO, "mhd_magneticconstant <= 0");
+    if (ival(ec_disotropic) > 0 && st[ec_dcondconst] <= 0)
+      return fail(SPH_ERR_IC_DIFFCOND, "diff_conductivity <= 0");
+    std::vector<double> h(NCOL * nrows);
+    CK(cudaMemcpyAsync(h.data(), cols.p, sizeof(double) * NCOL * nrows, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    auto C = [&](int f, int64_t i) { return h[size_t(f) * nrows + i]; };
+    for (int64_t i = 0; i < nrows; ++i) {
+      if (int(C(es_type, i)) == ept_empty) continue;
+      if (C(es_den, i) <= 0.) return fail(SPH_ERR_IC_DENSITY, "density <= 0");
+      if (C(es_c, i) <= 0.) return fail(SPH_ERR_IC_CSOUND, "csound <= 0");
+      if (C(es_h, i) <= 0.) return fail(SPH_ERR_IC_H, "smoothing length <= 0");
+      if (C(es_p, i) <= 0.) return fail(SPH_ERR_IC_PRESSURE, "pressure <= 0");
+      if (C(es_u, i) <= 0.) return fail(SPH_ERR_IC_ENERGY, "internal energy <= 0");
+    }
+    return SPH_OK;
+  }
+
+  // ---- time loop (main.f90:216-373) ------------------------------------------------------------
+  int start_run() {
+    eqset();
+    double t = st[ec_time];
+    dtout = st[ec_dtprint];
+    double tfinish = st[ec_tfinish];
+    stopped = false;
+    if (tfinish > 0.) {
+      RC(check_vars_ready());
+      if (ival(ec_eqs) != eeq_kd2) RC(iterate(true));
+      else stopped = true;
+    } else {
+      stopped = true;
+    }
+    ltout = 0.;
+    if (dtout > 0) while (ltout < t) ltout = ltout + dtout;
+    started = true;
+    return SPH_OK;
+  }
+
+  int timestep(double& dthydro, double& dtdiff, double& dtfld, double& dt) {
+    Phase ph(this, SPH_T_TIMESTEP);
+    Params P{};
+    RC(params(P));
+    unsigned long long* r = red.as<unsigned long long>();
+    launch_fill_u64(r + RED_TS_HMIN, 1, dkey(1e308), s);
+    launch_fill_u64(r + RED_TS_CMAX, 1, dkey(-1e308), s);
+    launch_fill_u64(r + RED_TS_DENMIN, 1, dkey(1e308), s);
+    launch_fill_u64(r + RED_TS_CMIN, 1, dkey(1e308), s);
+    launch_fill_u64(r + RED_TS_KAPMAX, 1, dkey(-1e308), s);
+    launch_fill_u64(r + RED_TS_BMAX, 1, dkey(-1e308), s);
+    launch_fill_u64(r + RED_TS_KAPMIN, 1, dkey(1e308), s);
+    launch_fill_u64(r + RED_TS_LAMMAX, 1, dkey(-1e308), s);
+    launch_timestep_reduce(cols.as<double>(), nrows, orig.as<int32_t>(), nrows,
+                           int64_t(st[ec_realpn]), P, r, s);
+    CK(cudaMemcpyAsync(h_red + RED_TS_HMIN, r + RED_TS_HMIN,
+                       sizeof(unsigned long long) * (RED_TS_LAMMAX - RED_TS_HMIN + 1),
+                       cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaGetLastError());
+    double hmin = dkey_inv(h_red[RED_TS_HMIN]), cmax = dkey_inv(h_red[RED_TS_CMAX]);
+    double denmin = dkey_inv(h_red[RED_TS_DENMIN]), cmin = dkey_inv(h_red[RED_TS_CMIN]);
+    double kapmax = dkey_inv(h_red[RED_TS_KAPMAX]), bmax = dkey_inv(h_red[RED_TS_BMAX]);
+    double kapmin = dkey_inv(h_red[RED_TS_KAPMIN]), lammax = dkey_inv(h_red[RED_TS_LAMMAX]);
+    dt = std::numeric_limits<double>::max();
+    dthydro = 0.;
+    dtdiff = std::numeric_limits<double>::infinity();
+    dtfld = std::numeric_limits<double>::infinity();
+    if (eq_hydro) {
+      dthydro = kb.cn_hydro * hmin / cmax;
+      dt = std::min(dt, dthydro);
+    }
+    if (eq_magneto) dt = std::min(dt, .1 * hmin / cmax / bmax);
+    if (eq_diff) {
+      dtdiff = cnd2() * denmin * cmin * (hmin * hmin) / kapmax;
+      dt = std::min(dt, dtdiff);
+    }
+    if (eq_fld) {
+      dtfld = cnd2() * hmin * hmin * denmin * kapmin / kLightspeed / lammax;
+      dt = std::min(dt, dtfld);
+    }
+    return SPH_OK;
+  }
+
+  int sts_integrate(int sts_s, double dt) {
+    // sts_integrator.f90:87-124; coefficients :10-51
+    auto b = [](int j) { return j <= 2 ? 1. / 3. : (double(j * j + j) - 2.) / (2. * j * (j + 1.)); };
+    auto a_ = [&](int j) { return 1 - b(j); };
+    auto mu = [&](int j) { return (2. * j - 1.) / j * b(j) / b(j - 1); };
+    auto nu = [&](int j) { return -((j - 1.) / j * b(j) / b(j - 2)); };
+    auto w = [](int s_) { return 4. / (double(s_ * s_ + s_) - 2.); };
+    auto mu_hat = [&](int j, int s_) { return j == 1 ? b(1) * w(s_) : mu(j) * w(s_); };
+    auto gm_hat = [&](int j, int s_) { return -a_(j - 1) * mu_hat(j, s_); };
+    RC(stsY.ensure(sizeof(double) * 6 * nrows));
+    double* Y = stsY.as<double>();
+    {
+      Phase ph(this, SPH_T_STS);
+      launch_sts_stage(0, cols.as<double>(), nrows, nrows, Y, 0, 0, 0, 0, 0, ctrl.as<double>(), s);
+    }
+    RC(iterate(true));
+    {
+      Phase ph(this, SPH_T_STS);
+      launch_sts_stage(1, cols.as<double>(), nrows, nrows, Y, mu_hat(1, sts_s), 0, 0, 0, 0,
+                       ctrl.as<double>(), s);
+    }
+    for (int j = 2; j <= sts_s; ++j) {
+      RC(iterate(true));
+      Phase ph(this, SPH_T_STS);
+      launch_sts_stage(2, cols.as<double>(), nrows, nrows, Y, mu(j), nu(j), mu_hat(j, sts_s),
+                       gm_hat(j, sts_s), 0, ctrl.as<double>(), s);
+    }
+    {
+      Phase ph(this, SPH_T_STS);
+      launch_sts_stage(3, cols.as<double>(), nrows, nrows, Y, 0, 0, 0, 0, 0, ctrl.as<double>(), s);
+    }
+    CK(cudaGetLastError());
+    return SPH_OK;
+  }
+
+  int one_step(double tfinish, bool& done) {
+    double t = st[ec_time];
+    if (!((t < tfinish + std::numeric_limits<double>::epsilon()) && !stopped)) {
+      done = true;
+      return SPH_OK;
+    }
+    done = false;
+    int reorder_every = int(st[SPH_P_REORDER_EVERY]);
+    if (reorder_every > 0 && steps_since_reorder >= reorder_every) RC(reorder_rows());
+    double dthydro, dtdiff, dtfld, dt;
+    RC(timestep(dthydro, dtdiff, dtfld, dt));
+    bool do_sts = false;
+    int sts_s = 0;
+    if (eq_sts) {
+      double sts_dt_min = std::min(dtdiff, dtfld);
+      int sts_type = ival(ec_ststype);
+      if (sts_type == 1) {
+        sts_s = ival(ec_stsfixeds);
+        dthydro = (sts_s * sts_s + sts_s - 2.) * 0.25 * sts_dt_min;
+        dt = dthydro;
+        do_sts = true;
+      } else if (sts_type == 0) {
+        if (dthydro > 0.) {
+          double sts_classic = dthydro / sts_dt_min;
+          sts_s = int(0.5 * std::sqrt(9. + 16. * sts_classic)) + 1;
+          if (sts_classic > 1. && 2 * sts_s <= sts_classic) { dt = dthydro; do_sts = true; }
+        }
+      }
+    }
+    if (t + dt > tfinish) { dt = tfinish - t; stopped = true; }
+    if (dtout > 0) {
+      if (t >= ltout) { while (ltout <= t) ltout = ltout + dtout; }
+      if (t + dt > ltout) {
+        if (dtout < dt) ltout = ltout - dtout + dt;
+        else dt = ltout - t;
+      }
+    }
+    h_ctrl[0] = dt;
+    CK(cudaMemcpyAsync(ctrl.p, h_ctrl, sizeof(double), cudaMemcpyHostToDevice, s));
+    {
+      Phase ph(this, SPH_T_PREDICT);
+      launch_predict(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
+                     ctrl.as<double>(), do_sts, s);
+    }
+    RC(iterate(true));
+    {
+      Phase ph(this, SPH_T_CORRECT);
+      launch_correct(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
+                     ctrl.as<double>(), do_sts, s);
+    }
+    if (do_sts) RC(sts_integrate(sts_s, dt));
+    if (eq_radexch)
+      return fail(SPH_ERR_UNSUPPORTED, "radiation exchange (rad_exchange.f90) is not part of this engine");
+    st[ec_time] = t + dt;
+    cnt_host[SPH_CNT_STEPS]++;
+    steps_since_reorder++;
+    CK(cudaGetLastError());
+    collect_timers();
+    return SPH_OK;
+  }
+
+  void destroy() {
+    if (s) cudaStreamSynchronize(s);
+    for (auto& pe : pending_ev) {
+      cudaEventDestroy(pe.second.first);
+      cudaEventDestroy(pe.second.second);
+    }
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    if (h_red) cudaFreeHost(h_red);
+    if (h_ctrl) cudaFreeHost(h_ctrl);
+    if (h_i32) cudaFreeHost(h_i32);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+extern "C" {
+
+const char* sph_last_error(void) { return g_err.c_str(); }
+
+int sph_create(const double* state49, const double* store, int64_t n_rows, int kernel_id,
+               int precision_mode, sph_handle** out) {
+  if (!state49 || !store || !out || n_rows <= 0) return fail(SPH_ERR_ARG, "null argument");
+  if (kernel_id < 0 || kernel_id > 2) return fail(SPH_ERR_ARG, "bad kernel id");
+  if (precision_mode != SPH_PREC_FP64 && precision_mode != SPH_PREC_FP32_COMP)
+    return fail(SPH_ERR_ARG, "bad precision mode");
+  if (n_rows > int64_t(INT32_MAX) / 8) return fail(SPH_ERR_ARG, "too many rows");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(SPH_ERR_CUDA, "no CUDA device");
+  }
+  auto* h = new sph_handle();
+  h->kernel_id = kernel_id;
+  h->prec = precision_mode;
+  h->kb = kbase(kernel_id);
+  h->st.assign(SPH_P_LAST + 1, 0.);
+  for (int k = 1; k <= SPH_EC_TOTAL; ++k) h->st[k] = state49[k - 1];
+  h->st[SPH_P_AV_ALPHA] = 1.;
+  h->st[SPH_P_AV_BETA] = 2.;
+  h->st[SPH_P_NEWTON_TOL] = 1e-8;
+  h->st[SPH_P_NEWTON_MAXITER] = 100;
+  h->st[SPH_P_CELL_FACTOR] = 1.;
+  h->st[SPH_P_REORDER_EVERY] = 8;
+  h->nreal = int64_t(h->st[ec_realpn]);
+  h->nfixed = std::max<int64_t>(0, int64_t(h->st[ec_fixedpn]));
+  if (h->nreal <= 0 || h->nreal + h->nfixed != n_rows) {
+    delete h;
+    return fail(SPH_ERR_ARG, "n_rows must equal realpn + fixedpn");
+  }
+  h->nrows = n_rows;
+  // integrated rows: reals + fixedreal rows after them (main.f90:181-184)
+  h->n_int = h->nreal;
+  for (int64_t i = std::max<int64_t>(h->nreal - 1, 0); i < n_rows; ++i)
+    if (int(store[i * NCOL + es_type]) == ept_fixedreal) h->n_int++;
+  // mass scale for the packed streams
+  double msum = 0.;
+  for (int64_t i = 0; i < n_rows; ++i) msum += std::fabs(store[i * NCOL + es_m]);
+  h->mref = msum > 0 ? store[0 * NCOL + es_m] : 1.0;
+  if (!(h->mref > 0)) h->mref = msum / n_rows > 0 ? msum / n_rows : 1.0;
+  int rc = SPH_OK;
+  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return fail(SPH_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  if (cudaMallocHost(&h->h_red, sizeof(unsigned long long) * RED_TOTAL) != cudaSuccess ||
+      cudaMallocHost(&h->h_ctrl, sizeof(double) * 8) != cudaSuccess ||
+      cudaMallocHost(&h->h_i32, sizeof(int32_t) * 8) != cudaSuccess) {
+    cudaGetLastError();
+    h->destroy();
+    delete h;
+    return fail(SPH_ERR_OOM, "cudaMallocHost failed");
+  }
+  rc = h->alloc_base();
+  if (!rc) {
+    if (cudaMemcpyAsync(h->staging.p, store, sizeof(double) * NCOL * n_rows,
+                        cudaMemcpyHostToDevice, h->s) != cudaSuccess)
+      rc = fail(SPH_ERR_CUDA, "upload failed");
+  }
+  if (!rc) {
+    launch_upload_store(h->staging.as<double>(), h->cols.as<double>(), h->orig.as<int32_t>(),
+                        n_rows, h->s);
+    if (cudaStreamSynchronize(h->s) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+      rc = fail(SPH_ERR_CUDA, "upload kernel failed");
+  }
+  if (rc) {
+    h->destroy();
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return SPH_OK;
+}
+
+int sph_set_param(sph_handle* h, int index, double value) {
+  if (!h || index < 1 || index > SPH_P_LAST) return fail(SPH_ERR_ARG, "bad param index");
+  if ((index == ec_realpn || index == ec_fixedpn) && value != h->st[index])
+    return fail(SPH_ERR_ARG, "particle counts are fixed by the store");
+  h->st[index] = value;
+  if (index == SPH_P_NEIB_CAP && value > 0) h->cap = int(value);
+  return SPH_OK;
+}
+
+int sph_get_param(sph_handle* h, int index, double* value) {
+  if (!h || !value || index < 1 || index > SPH_P_LAST) return fail(SPH_ERR_ARG, "bad param index");
+  *value = h->st[index];
+  return SPH_OK;
+}
+
+int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
+  if (!h || !store || n_rows != h->nrows) return fail(SPH_ERR_ARG, "row count mismatch");
+  CK(cudaMemcpyAsync(h->staging.p, store, sizeof(double) * NCOL * n_rows, cudaMemcpyHostToDevice, h->s));
+  launch_upload_store(h->staging.as<double>(), h->cols.as<double>(), h->orig.as<int32_t>(), n_rows, h->s);
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
+  h->have_order = false;
+  return SPH_OK;
+}
+
+int sph_iterate(sph_handle* h) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  RC(h->reorder_rows());
+  return h->iterate(true);
+}
+
+int sph_density(sph_handle* h) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  RC(h->reorder_rows());
+  return h->iterate(false);
+}
+
+int sph_step(sph_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return fail(SPH_ERR_ARG, "bad argument");
+  if (!h->started) RC(h->start_run());
+  if (h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
+  for (int i = 0; i < nsteps; ++i) {
+    bool done = false;
+    RC(h->one_step(h->st[ec_tfinish], done));
+    if (done) break;
+  }
+  return SPH_OK;
+}
+
+int sph_run_to(sph_handle* h, double tfinish) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  h->st[ec_tfinish] = tfinish;
+  if (!h->started) RC(h->start_run());
+  if (h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
+  for (;;) {
+    bool done = false;
+    RC(h->one_step(tfinish, done));
+    if (done) break;
+  }
+  return SPH_OK;
+}
+
+int sph_get_store(sph_handle* h, double* out, int64_t cap_rows) {
+  if (!h || !out || cap_rows < h->nrows) return fail(SPH_ERR_ARG, "buffer too small");
+  launch_download_store(h->cols.as<double>(), h->orig.as<int32_t>(), h->staging.as<double>(),
+                        h->nrows, h->s);
+  CK(cudaMemcpyAsync(out, h->staging.p, sizeof(double) * NCOL * h->nrows, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
+  return SPH_OK;
+}
+
+int sph_get_state(sph_handle* h, double* out49) {
+  if (!h || !out49) return fail(SPH_ERR_ARG, "null argument");
+  for (int k = 1; k <= SPH_EC_TOTAL; ++k) out49[k - 1] = h->st[k];
+  return SPH_OK;
+}
+
+int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs, int64_t cap) {
+  if (!h || !offsets) return fail(SPH_ERR_ARG, "null argument");
+  if (!h->have_order) return fail(SPH_ERR_STATE, "no neighbour search since the last re-ordering");
+  const int64_t nc = h->nreal, nall = h->nrows + h->nghost;
+  std::vector<int32_t> cnt(nc), cp(nc), og(h->nrows), sidx(nall), ssrc(nall);
+  std::vector<int8_t> gcode(std::max<int64_t>(h->nghost, 1));
+  std::vector<int32_t> nl(size_t(h->cap) * nc);
+  cudaStream_t s = h->s;
+  CK(cudaMemcpyAsync(cnt.data(), h->ncnt.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cp.data(), h->centre_p.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(og.data(), h->orig.p, sizeof(int32_t) * h->nrows, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(sidx.data(), h->vals_alt.p, sizeof(int32_t) * nall, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ssrc.data(), h->ssrc.p, sizeof(int32_t) * nall, cudaMemcpyDeviceToHost, s));
+  if (h->nghost > 0)
+    CK(cudaMemcpyAsync(gcode.data(), h->gcode.p, sizeof(int8_t) * h->nghost, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nl.data(), h->nl.p, sizeof(int32_t) * nl.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::vector<int64_t> cnt_by_orig(nc, 0), centre_of_orig(nc, -1);
+  for (int64_t c = 0; c < nc; ++c) {
+    int64_t o = og[cp[c]];
+    if (o < 0 || o >= nc) return fail(SPH_ERR_STATE, "centre row out of range");
+    cnt_by_orig[o] = cnt[c];
+    centre_of_orig[o] = c;
+  }
+  offsets[0] = 0;
+  for (int64_t o = 0; o < nc; ++o) offsets[o + 1] = offsets[o] + cnt_by_orig[o];
+  if (!pairs || cap < offsets[nc]) return fail(SPH_ERR_ARG, "pairs buffer too small");
+  for (int64_t o = 0; o < nc; ++o) {
+    int64_t c = centre_of_orig[o];
+    int64_t base = offsets[o];
+    for (int l = 0; l < cnt[c]; ++l) {
+      int64_t q = nl[size_t(l) * nc + c];
+      int64_t u = sidx[q];
+      int64_t rj = og[ssrc[q]];
+      int64_t code = u < h->nrows ? 13 : gcode[u - h->nrows];
+      pairs[base + l] = (rj << 5) | code;
+    }
+    std::sort(pairs + base, pairs + base + cnt[c]);
+  }
+  return SPH_OK;
+}
+
+int sph_get_counters(sph_handle* h, int64_t* out, int n) {
+  if (!h || !out) return fail(SPH_ERR_ARG, "null argument");
+  unsigned long long d[DC_TOTAL];
+  CK(cudaMemcpyAsync(d, h->dcnt.p, sizeof(d), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  int64_t all[SPH_CNT_TOTAL];
+  for (int k = 0; k < SPH_CNT_TOTAL; ++k) all[k] = h->cnt_host[k];
+  all[SPH_CNT_NEIB_PAIRS] = int64_t(d[DC_NEIB_PAIRS]);
+  all[SPH_CNT_C1_PAIRS] = int64_t(d[DC_C1_PAIRS]);
+  all[SPH_CNT_C1_SWEEPS] = std::max<int64_t>(int64_t(d[DC_C1_MAXSWEEPS]), h->host_max_sweeps);
+  all[SPH_CNT_C2_PAIRS] = int64_t(d[DC_C2_PAIRS]);
+  all[SPH_CNT_CANDIDATES] = int64_t(d[DC_CANDIDATES]);
+  all[SPH_CNT_C1_CENTRE_SWEEPS] = int64_t(d[DC_C1_CENTRE_SWEEPS]);
+  for (int k = 0; k < n && k < SPH_CNT_TOTAL; ++k) out[k] = all[k];
+  return SPH_OK;
+}
+
+int sph_reset_counters(sph_handle* h) {
+  if (!h) return fail(SPH_ERR_ARG, "null argument");
+  CK(cudaMemsetAsync(h->dcnt.p, 0, sizeof(unsigned long long) * DC_TOTAL, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  for (auto& c : h->cnt_host) c = 0;
+  for (auto& t : h->timers) t = 0.;
+  h->host_max_sweeps = 0;
+  return SPH_OK;
+}
+
+int sph_get_timers(sph_handle* h, double* out_ms, int n) {
+  if (!h || !out_ms) return fail(SPH_ERR_ARG, "null argument");
+  h->collect_timers();
+  for (int k = 0; k < n && k < SPH_T_TOTAL; ++k) out_ms[k] = h->timers[k];
+  return SPH_OK;
+}
+
+void sph_destroy(sph_handle* h) {
+  if (!h) return;
+  h->destroy();
+  delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,733 @@
+// sph_grid.cu — the non-pair kernels of one SPH step on the device:
+// store upload/download and re-ordering, periodic wrap and periodic images
+// (BC.f90:102-475), Morton cell keys + radix sort + cell ranges (replacing the
+// kd-tree of neighboursearch.f90:74-180), the FP64 fixed-ball neighbour
+// predicate (kdtree2.f90:1673-1678), packing of pair data, the leapfrog
+// predictor/corrector (main.f90:323-362), timestep reductions
+// (timestep.f90:40-166), EOS (eos.f90:21-45) and the STS stage update
+// (sts_integrator.f90:87-124).
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "sph_internal.h"
+
+namespace sph {
+
+namespace {
+
+constexpr int TPB = 256;
+
+inline int nblocks(int64_t n, int tpb = TPB) {
+  int64_t b = (n + tpb - 1) / tpb;
+  return int(b < 1 ? 1 : b);
+}
+
+__device__ __forceinline__ void red_min(unsigned long long* slot, double v) {
+  atomicMin(slot, dkey(v));
+}
+__device__ __forceinline__ void red_max(unsigned long long* slot, double v) {
+  atomicMax(slot, dkey(v));
+}
+
+// warp-level min/max of doubles, then one atomic per warp
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ---- store transposes -----------------------------------------------------------
+__global__ void k_upload(const double* __restrict__ rm, double* __restrict__ cols,
+                         int32_t* __restrict__ orig, int64_t n) {
+  int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (t >= n * NCOL) return;
+  int64_t i = t / NCOL;
+  int f = int(t - i * NCOL);
+  cols[f * n + i] = rm[t];
+  if (f == 0) orig[i] = int32_t(i);
+}
+
+__global__ void k_download(const double* __restrict__ cols, const int32_t* __restrict__ orig,
+                           double* __restrict__ rm, int64_t n) {
+  int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (t >= n * NCOL) return;
+  int64_t i = t / NCOL;
+  int f = int(t - i * NCOL);
+  rm[int64_t(orig[i]) * NCOL + f] = cols[f * n + i];
+}
+
+__global__ void k_reorder(const double* __restrict__ cin, double* __restrict__ cout,
+                          const int32_t* __restrict__ oin, int32_t* __restrict__ oout,
+                          const int32_t* __restrict__ perm, int64_t n, int64_t ldi,
+                          int64_t ldo) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  int64_t src = perm[i];
+  for (int f = 0; f < NCOL; ++f) cout[f * ldo + i] = cin[f * ldi + src];
+  oout[i] = oin[src];
+}
+
+// ---- periodic wrap of real particles (BC.f90:102-194) ----------------------------
+__global__ void k_reflect(double* __restrict__ cols, int64_t ld, int64_t nreal, BoxGeom g) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nreal) return;
+  double r[3], dxmin[3], dxmax[3];
+  for (int k = 0; k < 3; ++k) {
+    r[k] = cols[(es_rx + k) * ld + i];
+    dxmin[k] = __dadd_rn(g.emin[k], -r[k]);
+    dxmax[k] = __dadd_rn(r[k], -g.emax[k]);
+  }
+  for (int k = 0; k < 3; ++k) {
+    if (!g.reflect[k]) continue;
+    double v = r[k];
+    if (dxmax[k] > 0) v = __dadd_rn(g.emin[k], dxmax[k]);
+    if (dxmin[k] > 0) v = __dadd_rn(g.emax[k], -dxmin[k]);
+    cols[(es_rx + k) * ld + i] = v;
+  }
+}
+
+// ---- periodic images --------------------------------------------------------------
+// Image rule equivalent to createPeriodicBorder's list walk (BC.f90:311-475):
+// an image shifts a subset S of the periodic axes; the first axis of S (in x,
+// y, z order) is tested on the real particle with the padding bound of
+// findInsideBorderParticles (BC.f90:277-303), every later axis of S is tested
+// on the intermediate image without it (BC.f90:342-354, 402-407).  On each
+// axis at most one of the two sides can hold, so S fixes the image.
+struct AxisSigns {
+  int pad[3];   // +1 low strip, -1 high strip, 0 none (padded test)
+  int npad[3];  // same without the padding bound
+};
+
+__device__ __forceinline__ int type_of(double t) { return int(t); }
+
+__device__ __forceinline__ bool ghost_source(double t) {
+  int ty = type_of(t);
+  return ty == ept_real || ty == ept_fixed || ty == ept_fixedreal;
+}
+
+__device__ __forceinline__ AxisSigns axis_signs(const double* r, const BoxGeom& g, int dim) {
+  AxisSigns s;
+  for (int k = 0; k < 3; ++k) {
+    s.pad[k] = 0;
+    s.npad[k] = 0;
+    if (k >= dim || !g.periodic[k]) continue;
+    double ra = r[k];
+    if (ra < g.boxmin[k]) {
+      if (ra > g.pmin[k]) s.pad[k] = +1;
+      s.npad[k] = +1;
+    } else if (ra > g.boxmax[k]) {
+      if (ra < g.pmax[k]) s.pad[k] = -1;
+      s.npad[k] = -1;
+    }
+  }
+  return s;
+}
+
+// Image `mask` (bits of S) -> shift signs; returns false if the image does not exist.
+__device__ __forceinline__ bool image_of(const AxisSigns& s, int mask, int sg[3]) {
+  bool first = true;
+  for (int k = 0; k < 3; ++k) {
+    sg[k] = 0;
+    if (!(mask & (1 << k))) continue;
+    int v = first ? s.pad[k] : s.npad[k];
+    if (v == 0) return false;
+    sg[k] = v;
+    first = false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ double image_coord(double x, int sign, double emin, double emax) {
+  if (sign > 0) return __dadd_rn(emax, __dadd_rn(x, -emin));  // xmax + (x - xmin)
+  if (sign < 0) return __dadd_rn(emin, __dadd_rn(x, -emax));  // xmin + (x - xmax)
+  return x;
+}
+
+__global__ void k_ghost_count(const double* __restrict__ cols, int64_t ld, int64_t nrows,
+                              int64_t nreal, BoxGeom g, int dim, int32_t* __restrict__ count,
+                              unsigned long long* __restrict__ red) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  double hmin = 1e300;
+  int c = 0;
+  if (i < nrows) {
+    double r[3] = {cols[es_rx * ld + i], cols[es_ry * ld + i], cols[es_rz * ld + i]};
+    for (int k = 0; k < 3; ++k) { lo[k] = r[k]; hi[k] = r[k]; }
+    if (i < nreal) hmin = cols[es_h * ld + i];
+    if (ghost_source(cols[es_type * ld + i])) {
+      AxisSigns s = axis_signs(r, g, dim);
+      for (int mask = 1; mask < 8; ++mask) {
+        int sg[3];
+        if (!image_of(s, mask, sg)) continue;
+        ++c;
+        for (int k = 0; k < 3; ++k) {
+          double v = image_coord(r[k], sg[k], g.emin[k], g.emax[k]);
+          lo[k] = fmin(lo[k], v);
+          hi[k] = fmax(hi[k], v);
+        }
+      }
+    }
+    count[i] = c;
+  }
+  for (int k = 0; k < 3; ++k) { lo[k] = warp_min(lo[k]); hi[k] = warp_max(hi[k]); }
+  hmin = warp_min(hmin);
+  if ((threadIdx.x & 31) == 0) {
+    for (int k = 0; k < 3; ++k) {
+      if (lo[k] < 1e300) red_min(&red[RED_LO_X + k], lo[k]);
+      if (hi[k] > -1e300) red_max(&red[RED_HI_X + k], hi[k]);
+    }
+    if (hmin < 1e300) red_min(&red[RED_HMIN], hmin);
+  }
+}
+
+__global__ void k_ghost_write(const double* __restrict__ cols, int64_t ld, int64_t nrows,
+                              BoxGeom g, int dim, const int32_t* __restrict__ offset,
+                              double* __restrict__ gx, double* __restrict__ gy,
+                              double* __restrict__ gz, int32_t* __restrict__ gsrc,
+                              int8_t* __restrict__ gcode) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nrows) return;
+  if (!ghost_source(cols[es_type * ld + i])) return;
+  double r[3] = {cols[es_rx * ld + i], cols[es_ry * ld + i], cols[es_rz * ld + i]};
+  AxisSigns s = axis_signs(r, g, dim);
+  int64_t o = offset[i];
+  for (int mask = 1; mask < 8; ++mask) {
+    int sg[3];
+    if (!image_of(s, mask, sg)) continue;
+    gx[o] = image_coord(r[0], sg[0], g.emin[0], g.emax[0]);
+    gy[o] = image_coord(r[1], sg[1], g.emin[1], g.emax[1]);
+    gz[o] = image_coord(r[2], sg[2], g.emin[2], g.emax[2]);
+    gsrc[o] = int32_t(i);
+    gcode[o] = int8_t((sg[0] + 1) + 3 * (sg[1] + 1) + 9 * (sg[2] + 1));
+    ++o;
+  }
+}
+
+// ---- cell keys ----------------------------------------------------------------------
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000FFu;
+  x = (x | (x << 8)) & 0x0300F00Fu;
+  x = (x | (x << 4)) & 0x030C30C3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+__device__ __forceinline__ uint32_t compact3(uint32_t x) {
+  x &= 0x09249249u;
+  x = (x | (x >> 2)) & 0x030C30C3u;
+  x = (x | (x >> 4)) & 0x0300F00Fu;
+  x = (x | (x >> 8)) & 0x030000FFu;
+  x = (x | (x >> 16)) & 0x000003FFu;
+  return x;
+}
+__device__ __forceinline__ int cell_coord(double x, double o, double invL, int n) {
+  double f = floor((x - o) * invL);
+  int c = f < 0.0 ? 0 : (f > double(n - 1) ? n - 1 : int(f));
+  return c;
+}
+
+__global__ void k_keys(const double* __restrict__ cols, int64_t ld, int64_t nrows,
+                       const double* __restrict__ gx, const double* __restrict__ gy,
+                       const double* __restrict__ gz, int64_t nghost, Grid g,
+                       uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+  int64_t u = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (u >= nrows + nghost) return;
+  double x, y, z;
+  if (u < nrows) {
+    x = cols[es_rx * ld + u]; y = cols[es_ry * ld + u]; z = cols[es_rz * ld + u];
+  } else {
+    int64_t q = u - nrows;
+    x = gx[q]; y = gy[q]; z = gz[q];
+  }
+  uint32_t cx = cell_coord(x, g.ox, g.invL, g.nx);
+  uint32_t cy = cell_coord(y, g.oy, g.invL, g.ny);
+  uint32_t cz = cell_coord(z, g.oz, g.invL, g.nz);
+  keys[u] = spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
+  vals[u] = int32_t(u);
+}
+
+__global__ void k_cell_ranges(const uint32_t* __restrict__ keys, int64_t n, Grid g,
+                              int32_t* __restrict__ cstart, int32_t* __restrict__ cend) {
+  int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (k >= n) return;
+  uint32_t key = keys[k];
+  bool first = (k == 0) || keys[k - 1] != key;
+  bool last = (k == n - 1) || keys[k + 1] != key;
+  if (!first && !last) return;
+  int cx = compact3(key), cy = compact3(key >> 1), cz = compact3(key >> 2);
+  int64_t d = cx + int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+  if (first) cstart[d] = int32_t(k);
+  if (last) cend[d] = int32_t(k + 1);
+}
+
+// Sorted-order gather of positions and source rows; compaction of centres
+// (the real rows, which the reference iterates as alllistlv1 = 1..realpn).
+__global__ void k_sorted_gather(const int32_t* __restrict__ sidx, int64_t n, int64_t nrows,
+                                int64_t nreal, const double* __restrict__ cols, int64_t ld,
+                                const double* __restrict__ gx, const double* __restrict__ gy,
+                                const double* __restrict__ gz, const int32_t* __restrict__ gsrc,
+                                double* __restrict__ sx, double* __restrict__ sy,
+                                double* __restrict__ sz, int32_t* __restrict__ ssrc,
+                                int32_t* __restrict__ centre_slot) {
+  int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (k >= n) return;
+  int64_t u = sidx[k];
+  if (u < nrows) {
+    sx[k] = cols[es_rx * ld + u]; sy[k] = cols[es_ry * ld + u]; sz[k] = cols[es_rz * ld + u];
+    ssrc[k] = int32_t(u);
+    centre_slot[k] = (u < nreal) ? 1 : 0;
+  } else {
+    int64_t q = u - nrows;
+    sx[k] = gx[q]; sy[k] = gy[q]; sz[k] = gz[q];
+    ssrc[k] = gsrc[q];
+    centre_slot[k] = 0;
+  }
+}
+
+__global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __restrict__ flag,
+                          const int32_t* __restrict__ pos, int64_t n,
+                          int32_t* __restrict__ centre_k, int32_t* __restrict__ centre_p) {
+  int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (k >= n) return;
+  if (!flag[k]) return;
+  int64_t c = pos[k];
+  centre_k[c] = int32_t(k);
+  centre_p[c] = sidx[k];
+}
+
+// ---- neighbour search -------------------------------------------------------------------
+// One thread per centre.  Candidates come from the cells that overlap the
+// box [x - R, x + R]; cells whose nearest point lies beyond R are skipped.
+// Inclusion is the kd-tree's FP64 test, summed x, y, z in order without
+// fused multiply-adds: ((dx*dx + dy*dy) + dz*dz) <= (krad*h)^2
+// (kdtree2.f90:1673-1678, neighboursearch.f90:126), self excluded
+// (neighboursearch.f90:190).
+template <int DIM>
+__global__ void __launch_bounds__(128)
+k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
+             const int32_t* __restrict__ centre_p, const double* __restrict__ sx,
+             const double* __restrict__ sy, const double* __restrict__ sz,
+             const double* __restrict__ hcol, double krad, Grid g,
+             const int32_t* __restrict__ cstart, const int32_t* __restrict__ cend, int cap,
+             int32_t* __restrict__ nl, int32_t* __restrict__ ncnt, int32_t* __restrict__ maxcnt,
+             unsigned long long* __restrict__ dcnt) {
+  int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  unsigned int ncand = 0, nfound = 0;
+  if (c < nc) {
+    const int32_t k = centre_k[c];
+    const int32_t p = centre_p[c];
+    const double xi = sx[k], yi = sy[k], zi = sz[k];
+    const double kh = __dmul_rn(krad, hcol[p]);
+    const double R2 = __dmul_rn(kh, kh);
+    const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
+    const double tolc = 1e-9 * g.L;
+    int c0[3], c1[3];
+    const double xs[3] = {xi, yi, zi};
+    const double os[3] = {g.ox, g.oy, g.oz};
+    const int ns[3] = {g.nx, g.ny, g.nz};
+    for (int a = 0; a < 3; ++a) {
+      double sl = fabs(xs[a]) * 1e-15;
+      c0[a] = cell_coord(xs[a] - R - sl, os[a], g.invL, ns[a]);
+      c1[a] = cell_coord(xs[a] + R + sl, os[a], g.invL, ns[a]);
+    }
+    int cnt = 0;
+    for (int cz = c0[2]; cz <= c1[2]; ++cz) {
+      double dzc = 0.0;
+      if (DIM == 3) {
+        double lo = g.oz + cz * g.L - tolc, hi = g.oz + (cz + 1) * g.L + tolc;
+        dzc = zi < lo ? lo - zi : (zi > hi ? zi - hi : 0.0);
+      }
+      for (int cy = c0[1]; cy <= c1[1]; ++cy) {
+        double dyc = 0.0;
+        if (DIM >= 2) {
+          double lo = g.oy + cy * g.L - tolc, hi = g.oy + (cy + 1) * g.L + tolc;
+          dyc = yi < lo ? lo - yi : (yi > hi ? yi - hi : 0.0);
+        }
+        for (int cx = c0[0]; cx <= c1[0]; ++cx) {
+          double lo = g.ox + cx * g.L - tolc, hi = g.ox + (cx + 1) * g.L + tolc;
+          double dxc = xi < lo ? lo - xi : (xi > hi ? xi - hi : 0.0);
+          if (dxc * dxc + dyc * dyc + dzc * dzc > R * R) continue;
+          int64_t d = cx + int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+          int32_t s = cstart[d], e = cend[d];
+          for (int32_t q = s; q < e; ++q) {
+            ++ncand;
+            double d0 = __dadd_rn(sx[q], -xi);
+            double d1 = __dadd_rn(sy[q], -yi);
+            double d2 = __dadd_rn(sz[q], -zi);
+            double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                  __dmul_rn(d2, d2));
+            if (sd > R2 || q == k) continue;
+            if (cnt < cap) nl[int64_t(cnt) * nc + c] = q;
+            ++cnt;
+          }
+        }
+      }
+    }
+    ncnt[c] = cnt;
+    nfound = unsigned(cnt);
+    atomicMax(maxcnt, cnt);
+  }
+  unsigned int wc = __reduce_add_sync(0xffffffffu, ncand);
+  unsigned int wf = __reduce_add_sync(0xffffffffu, nfound);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&dcnt[DC_CANDIDATES], (unsigned long long)wc);
+    atomicAdd(&dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
+  }
+}
+
+// ---- pair-data packing (sorted order) --------------------------------------------------------
+__global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restrict__ ssrc,
+                       const double* __restrict__ sx, const double* __restrict__ sy,
+                       const double* __restrict__ sz, const double* __restrict__ cols, int64_t ld,
+                       PackGeom pg, PackBufs pb) {
+  int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (k >= n) return;
+  const int64_t p = ssrc[k];
+  auto C = [&](int f) { return cols[f * ld + p]; };
+  const double m = C(es_m) / pg.mref;
+  if (prec == SPH_PREC_FP64) {
+    if (groups & PACK_POS) {
+      pb.p[0][k] = make_double2(sx[k], sy[k]);
+      pb.p[1][k] = make_double2(sz[k], m);
+      pb.p[6][k] = make_double2(C(es_vz), C(es_t));
+    }
+    if (groups & PACK_HYDRO) {
+      double h = C(es_h), rho = C(es_den), om = C(es_om), P = C(es_p);
+      pb.p[2][k] = make_double2(1.0 / h, rho);
+      pb.p[3][k] = make_double2(1.0 / (rho * rho * om), P);
+      pb.p[4][k] = make_double2(C(es_c), C(es_u));
+      pb.p[5][k] = make_double2(C(es_vx), C(es_vy));
+      pb.p[6][k] = make_double2(C(es_vz), C(es_t));
+    }
+    if (groups & PACK_EXTRA) {
+      pb.p[7][k] = make_double2(C(es_kappa), C(es_dtdx));
+      pb.p[8][k] = make_double2(C(es_dtdy), C(es_dtdz));
+      pb.p[9][k] = make_double2(C(es_bx), C(es_by));
+      pb.p[10][k] = make_double2(C(es_bz), 0.0);
+    }
+  } else {
+    if (groups & PACK_POS) {
+      double xs = (sx[k] - pg.ox) + pg.shift;
+      double ys = (sy[k] - pg.oy) + pg.shift;
+      double zs = (sz[k] - pg.oz) + pg.shift;
+      float xh = __double2float_rn(xs), yh = __double2float_rn(ys), zh = __double2float_rn(zs);
+      float xl = __double2float_rn(xs - double(xh));
+      float yl = __double2float_rn(ys - double(yh));
+      float zl = __double2float_rn(zs - double(zh));
+      pb.q[0][k] = make_float4(xh, yh, zh, float(m));
+      pb.q[1][k] = make_float4(xl, yl, zl, float(1.0 / C(es_h)));
+      pb.q[4][k] = make_float4(float(C(es_t)), float(C(es_kappa)), float(C(es_dtdx)),
+                               float(C(es_dtdy)));
+    }
+    if (groups & PACK_HYDRO) {
+      double h = C(es_h), rho = C(es_den), om = C(es_om), P = C(es_p);
+      float4 q1 = pb.q[1][k];
+      q1.w = float(1.0 / h);
+      pb.q[1][k] = q1;
+      pb.q[2][k] = make_float4(float(rho), float(1.0 / (rho * rho * om)), float(P), float(C(es_c)));
+      pb.q[3][k] = make_float4(float(C(es_u)), float(C(es_vx)), float(C(es_vy)), float(C(es_vz)));
+    }
+    if (groups & PACK_EXTRA) {
+      pb.q[4][k] = make_float4(float(C(es_t)), float(C(es_kappa)), float(C(es_dtdx)),
+                               float(C(es_dtdy)));
+      pb.q[5][k] = make_float4(float(C(es_dtdz)), float(C(es_bx)), float(C(es_by)),
+                               float(C(es_bz)));
+    }
+  }
+}
+
+// ---- leapfrog (main.f90:323-362) ----------------------------------------------------------
+// Integrated rows: the reals and the fixedreal rows that follow them
+// (main.f90:181-184), selected by original row index.  Arithmetic in the
+// reference's evaluation order without contraction, so the update is bitwise
+// reproducible by the CPU oracle.
+enum SaveSlot : int { SV_AX = 0, SV_AY, SV_AZ, SV_DU, SV_DH, SV_DDT, SV_DBX, SV_DBY, SV_DBZ, SV_N };
+
+__global__ void k_predict(double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
+                          int64_t nrows, int64_t n_int, double* __restrict__ save,
+                          const double* __restrict__ ctrl, int do_sts) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nrows || orig[i] >= n_int) return;
+  const double dt = ctrl[0];
+  const double hdt2 = __dmul_rn(__dmul_rn(0.5, dt), dt);
+  auto C = [&](int f) -> double& { return cols[f * ld + i]; };
+  double ta[3], tv[3];
+  for (int k = 0; k < 3; ++k) {
+    ta[k] = C(es_ax + k);
+    tv[k] = C(es_vx + k);
+    save[(SV_AX + k) * ld + i] = ta[k];
+    save[(SV_DBX + k) * ld + i] = C(es_dbx + k);
+  }
+  double tdu = C(es_du), tdh = C(es_dh), tddt = C(es_ddt);
+  save[SV_DU * ld + i] = tdu;
+  save[SV_DH * ld + i] = tdh;
+  if (!do_sts) save[SV_DDT * ld + i] = tddt;
+  for (int k = 0; k < 3; ++k) {
+    C(es_rx + k) = __dadd_rn(__dadd_rn(C(es_rx + k), __dmul_rn(dt, tv[k])), __dmul_rn(hdt2, ta[k]));
+    C(es_vx + k) = __dadd_rn(tv[k], __dmul_rn(dt, ta[k]));
+  }
+  C(es_u) = __dadd_rn(C(es_u), __dmul_rn(dt, tdu));
+  C(es_h) = __dadd_rn(C(es_h), __dmul_rn(dt, tdh));
+  if (!do_sts) C(es_t) = __dadd_rn(C(es_t), __dmul_rn(dt, tddt));
+  for (int k = 0; k < 3; ++k)
+    C(es_bx + k) = __dadd_rn(C(es_bx + k), __dmul_rn(dt, save[(SV_DBX + k) * ld + i]));
+}
+
+__global__ void k_correct(double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
+                          int64_t nrows, int64_t n_int, const double* __restrict__ save,
+                          const double* __restrict__ ctrl, int do_sts) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nrows || orig[i] >= n_int) return;
+  const double hdt = __dmul_rn(0.5, ctrl[0]);
+  auto C = [&](int f) -> double& { return cols[f * ld + i]; };
+  for (int k = 0; k < 3; ++k)
+    C(es_vx + k) = __dadd_rn(C(es_vx + k), __dmul_rn(hdt, __dadd_rn(C(es_ax + k), -save[(SV_AX + k) * ld + i])));
+  C(es_u) = __dadd_rn(C(es_u), __dmul_rn(hdt, __dadd_rn(C(es_du), -save[SV_DU * ld + i])));
+  C(es_h) = __dadd_rn(C(es_h), __dmul_rn(hdt, __dadd_rn(C(es_dh), -save[SV_DH * ld + i])));
+  for (int k = 0; k < 3; ++k)
+    C(es_bx + k) = __dadd_rn(C(es_bx + k), __dmul_rn(hdt, __dadd_rn(C(es_dbx + k), -save[(SV_DBX + k) * ld + i])));
+  if (!do_sts) C(es_t) = __dadd_rn(C(es_t), __dmul_rn(hdt, __dadd_rn(C(es_ddt), -save[SV_DDT * ld + i])));
+}
+
+// ---- timestep reductions (timestep.f90:40-166) -----------------------------------------------
+// Over the first realpn rows in original order.
+__global__ void k_timestep_reduce(const double* __restrict__ cols, int64_t ld,
+                                  const int32_t* __restrict__ orig, int64_t nrows, int64_t n_ts,
+                                  Params P, unsigned long long* __restrict__ red) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  double hmin = 1e308, cmax = -1e308, dmin = 1e308, cmin = 1e308, kmax = -1e308,
+         bmax = -1e308, kmin = 1e308, lmax = -1e308;
+  if (i < nrows && orig[i] < n_ts) {
+    double h = cols[es_h * ld + i], c = cols[es_c * ld + i], d = cols[es_den * ld + i];
+    double ka = cols[es_kappa * ld + i];
+    hmin = h; cmax = c; dmin = d; cmin = c; kmax = ka; kmin = ka;
+    bmax = fmax(fmax(cols[es_bx * ld + i], cols[es_by * ld + i]), cols[es_bz * ld + i]);
+    if (P.eq_fld) {
+      double n0 = cols[es_dtdx * ld + i], n1 = cols[es_dtdy * ld + i], n2 = cols[es_dtdz * ld + i];
+      double ta = cols[es_t * ld + i];
+      double g = sqrt(((0.0 + n0 * n0) + n1 * n1) + n2 * n2);
+      double fr = g / (ka * d * d * ta);
+      lmax = (2. + fr) / (6. + 3 * fr + fr * fr);
+    }
+  }
+  hmin = warp_min(hmin); cmax = warp_max(cmax); dmin = warp_min(dmin); cmin = warp_min(cmin);
+  kmax = warp_max(kmax); bmax = warp_max(bmax); kmin = warp_min(kmin); lmax = warp_max(lmax);
+  if ((threadIdx.x & 31) == 0) {
+    red_min(&red[RED_TS_HMIN], hmin);
+    red_max(&red[RED_TS_CMAX], cmax);
+    red_min(&red[RED_TS_DENMIN], dmin);
+    red_min(&red[RED_TS_CMIN], cmin);
+    red_max(&red[RED_TS_KAPMAX], kmax);
+    red_max(&red[RED_TS_BMAX], bmax);
+    red_min(&red[RED_TS_KAPMIN], kmin);
+    red_max(&red[RED_TS_LAMMAX], lmax);
+  }
+}
+
+__global__ void k_fill_u64(unsigned long long* p, int n, unsigned long long v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// ---- STS stage updates (sts_integrator.f90:100-123) ------------------------------------------
+// Y holds six columns of length ld: Y0, Yjm1, Yjm2, Yj, DY0, DYjm1.
+enum { Y0 = 0, YJM1, YJM2, YJ, DY0, DYJM1 };
+__global__ void k_sts(int kind, double* __restrict__ cols, int64_t ld, int64_t n,
+                      double* __restrict__ Y, double a0, double a1, double a2, double a3,
+                      double a4, const double* __restrict__ ctrl) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  auto y = [&](int s) -> double& { return Y[s * ld + i]; };
+  double* T = cols + es_t * ld;
+  const double* ddt = cols + es_ddt * ld;
+  const double dt = ctrl[0];
+  switch (kind) {
+    case 0:  // Y0 = T
+      y(Y0) = T[i];
+      break;
+    case 1:  // after the first iterate: DY0, Yjm2 = Y0, Yjm1 = Y0 + muhat1*dt*DY0
+      y(DY0) = ddt[i];
+      y(YJM2) = y(Y0);
+      y(YJM1) = __dadd_rn(y(Y0), __dmul_rn(__dmul_rn(a0, dt), y(DY0)));
+      y(YJ) = y(YJM1);
+      T[i] = y(YJM1);
+      break;
+    case 2: {  // stage j: a0 = mu, a1 = nu, a2 = muhat, a3 = gmhat
+      y(DYJM1) = ddt[i];
+      double v = __dadd_rn(__dmul_rn(a0, y(YJM1)), __dmul_rn(a1, y(YJM2)));
+      v = __dadd_rn(v, __dmul_rn(__dadd_rn(__dadd_rn(1.0, -a0), -a1), y(Y0)));
+      v = __dadd_rn(v, __dmul_rn(__dmul_rn(a2, dt), y(DYJM1)));
+      v = __dadd_rn(v, __dmul_rn(__dmul_rn(a3, dt), y(DY0)));
+      y(YJ) = v;
+      y(YJM2) = y(YJM1);
+      y(YJM1) = v;
+      T[i] = v;
+      break;
+    }
+    case 3:  // final: T = Yj
+      T[i] = y(YJ);
+      break;
+    default:
+      break;
+  }
+}
+
+// ---- EOS (eos.f90:21-45), only for a separate call; circuit1 fuses it ------------------------
+__global__ void k_eos(double* __restrict__ cols, int64_t ld, int64_t nreal, Params P) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nreal) return;
+  double rho = cols[es_den * ld + i];
+  if (P.eos_kind == 1) {
+    double p = (P.gamma - 1.) * rho * cols[es_u * ld + i];
+    cols[es_p * ld + i] = p;
+    cols[es_c * ld + i] = sqrt(P.gamma * p / rho);
+  } else if (P.eos_kind == 2) {
+    cols[es_p * ld + i] = rho * P.c_iso * P.c_iso;
+  }
+}
+
+// iterator.f90:143, :153-163 — the MTI set-ups add a gravity term after c2
+__global__ void k_mti(double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
+                      int64_t nrows, int64_t nreal, int lowres) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nrows || orig[i] >= nreal) return;
+  double ay = cols[es_ay * ld + i];
+  if (lowres) ay = ay - erf(cols[es_ry * ld + i] * 8.);
+  else ay = ay - 1.;
+  cols[es_ay * ld + i] = ay;
+}
+
+__global__ void k_set(double* col, int64_t n, double v) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) col[i] = v;
+}
+
+}  // namespace
+
+// ---- launchers ------------------------------------------------------------------------------
+void launch_upload_store(const double* rm, double* cols, int32_t* orig, int64_t n, cudaStream_t s) {
+  k_upload<<<nblocks(n * NCOL), TPB, 0, s>>>(rm, cols, orig, n);
+}
+void launch_download_store(const double* cols, const int32_t* orig, double* rm, int64_t n,
+                           cudaStream_t s) {
+  k_download<<<nblocks(n * NCOL), TPB, 0, s>>>(cols, orig, rm, n);
+}
+void launch_reorder(const double* cin, double* cout, const int32_t* oin, int32_t* oout,
+                    const int32_t* perm, int64_t n, int64_t ldi, int64_t ldo, cudaStream_t s) {
+  k_reorder<<<nblocks(n), TPB, 0, s>>>(cin, cout, oin, oout, perm, n, ldi, ldo);
+}
+void launch_reflect(double* cols, int64_t ld, int64_t nreal, BoxGeom g, cudaStream_t s) {
+  if (nreal > 0) k_reflect<<<nblocks(nreal), TPB, 0, s>>>(cols, ld, nreal, g);
+}
+void launch_ghost_count(const double* cols, int64_t nrows, int64_t nreal, BoxGeom g, int dim,
+                        int32_t* count, unsigned long long* red, cudaStream_t s) {
+  k_ghost_count<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, nreal, g, dim, count, red);
+}
+void launch_ghost_write(const double* cols, int64_t nrows, BoxGeom g, int dim,
+                        const int32_t* offset, double* gx, double* gy, double* gz,
+                        int32_t* gsrc, int8_t* gcode, unsigned long long*, cudaStream_t s) {
+  k_ghost_write<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, g, dim, offset, gx, gy, gz,
+                                               gsrc, gcode);
+}
+void launch_keys(const double* cols, int64_t nrows, const double* gx, const double* gy,
+                 const double* gz, int64_t nghost, Grid g, uint32_t* keys, int32_t* vals,
+                 cudaStream_t s) {
+  k_keys<<<nblocks(nrows + nghost), TPB, 0, s>>>(cols, nrows, nrows, gx, gy, gz, nghost, g,
+                                                 keys, vals);
+}
+void launch_cell_ranges(const uint32_t* keys, int64_t n, Grid g, int32_t* cstart, int32_t* cend,
+                        cudaStream_t s) {
+  k_cell_ranges<<<nblocks(n), TPB, 0, s>>>(keys, n, g, cstart, cend);
+}
+void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
+                          const double* cols, const double* gx, const double* gy,
+                          const double* gz, const int32_t* gsrc, double* sx, double* sy,
+                          double* sz, int32_t* ssrc, int32_t* centre_slot, int32_t* centre_k,
+                          int32_t* centre_p, cudaStream_t s) {
+  // centre_slot receives flags first; the exclusive scan of the flags is
+  // written into centre_k's tail scratch by the caller, see sph_engine.cu.
+  k_sorted_gather<<<nblocks(n), TPB, 0, s>>>(sidx, n, nrows, nreal, cols, nrows, gx, gy, gz,
+                                             gsrc, sx, sy, sz, ssrc, centre_slot);
+  (void)centre_k;
+  (void)centre_p;
+}
+void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
+                    int32_t* centre_k, int32_t* centre_p, cudaStream_t s) {
+  k_centres<<<nblocks(n), TPB, 0, s>>>(sidx, flag, pos, n, centre_k, centre_p);
+}
+void launch_neighbours(int dim, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
+                       const double* sx, const double* sy, const double* sz, const double* hcol,
+                       double krad, Grid g, const int32_t* cstart, const int32_t* cend, int cap,
+                       int32_t* nl, int32_t* ncnt, int32_t* maxcnt, unsigned long long* dcnt,
+                       cudaStream_t s) {
+  const int tpb = 128;
+  if (dim == 3)
+    k_neighbours<3><<<nblocks(nc, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, hcol, krad,
+                                                     g, cstart, cend, cap, nl, ncnt, maxcnt, dcnt);
+  else if (dim == 2)
+    k_neighbours<2><<<nblocks(nc, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, hcol, krad,
+                                                     g, cstart, cend, cap, nl, ncnt, maxcnt, dcnt);
+  else
+    k_neighbours<1><<<nblocks(nc, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, hcol, krad,
+                                                     g, cstart, cend, cap, nl, ncnt, maxcnt, dcnt);
+}
+void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
+                 const double* sy, const double* sz, const double* cols, int64_t ld, PackGeom pg,
+                 PackBufs pb, cudaStream_t s) {
+  k_pack<<<nblocks(n), TPB, 0, s>>>(prec, groups, n, ssrc, sx, sy, sz, cols, ld, pg, pb);
+}
+void launch_predict(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
+                    double* save, const double* ctrl, int do_sts, cudaStream_t s) {
+  k_predict<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, do_sts);
+}
+void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
+                    const double* save, const double* ctrl, int do_sts, cudaStream_t s) {
+  k_correct<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, do_sts);
+}
+void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                            int64_t n_ts, Params P, unsigned long long* red, cudaStream_t s) {
+  k_timestep_reduce<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_ts, P, red);
+}
+void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s) {
+  k_fill_u64<<<nblocks(n), TPB, 0, s>>>(p, n, v);
+}
+void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, double a0,
+                      double a1, double a2, double a3, double a4, const double* ctrl,
+                      cudaStream_t s) {
+  k_sts<<<nblocks(n), TPB, 0, s>>>(kind, cols, ld, n, Y, a0, a1, a2, a3, a4, ctrl);
+}
+void launch_eos(double* cols, int64_t ld, int64_t nreal, Params P, cudaStream_t s) {
+  k_eos<<<nblocks(nreal), TPB, 0, s>>>(cols, ld, nreal, P);
+}
+void launch_apply_mti(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t nreal,
+                      int lowres, cudaStream_t s) {
+  k_mti<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, nreal, lowres);
+}
+void launch_set_col(double* col, int64_t n, double v, cudaStream_t s) {
+  k_set<<<nblocks(n), TPB, 0, s>>>(col, n, v);
+}
+
+size_t sort_temp_bytes(int64_t n) {
+  size_t b = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (const int32_t*)nullptr, (int32_t*)nullptr, int(n), 0, 30);
+  return b;
+}
+void sort_pairs(void* tmp, size_t tmp_bytes, const uint32_t* kin, uint32_t* kout, const int32_t* vin,
+                int32_t* vout, int64_t n, int end_bit, cudaStream_t s) {
+  cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kin, kout, vin, vout, int(n), 0, end_bit, s);
+}
+size_t scan_temp_bytes(int64_t n) {
+  size_t b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (const int32_t*)nullptr, (int32_t*)nullptr, int(n));
+  return b;
+}
+void exclusive_scan(void* tmp, size_t tmp_bytes, const int32_t* in, int32_t* out, int64_t n,
+                    cudaStream_t s) {
+  cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, int(n), s);
+}
+
+}  // namespace sph

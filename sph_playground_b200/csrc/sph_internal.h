@@ -1,0 +1,185 @@
+// sph_internal.h — host-side declarations shared by the engine's translation
+// units: device buffers of one handle, the cell grid and the kernel launchers.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sph_device.cuh"
+
+namespace sph {
+
+// Uniform cell grid over all particles (reals, fixed, periodic images).
+struct Grid {
+  double ox, oy, oz;  // origin (lower corner)
+  double L, invL;     // cell edge
+  int nx, ny, nz;     // cells per axis
+};
+
+// Order-preserving uint64 image of a double, for atomicMin/atomicMax.
+__host__ __device__ inline unsigned long long dkey(double v) {
+  long long b;
+#ifdef __CUDA_ARCH__
+  b = __double_as_longlong(v);
+#else
+  static_assert(sizeof(double) == sizeof(long long), "");
+  __builtin_memcpy(&b, &v, sizeof(b));
+#endif
+  unsigned long long u = (unsigned long long)b;
+  return (b >= 0) ? (u | 0x8000000000000000ull) : ~u;
+}
+__host__ __device__ inline double dkey_inv(unsigned long long u) {
+  unsigned long long b = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+  double v;
+#ifdef __CUDA_ARCH__
+  v = __longlong_as_double((long long)b);
+#else
+  __builtin_memcpy(&v, &b, sizeof(v));
+#endif
+  return v;
+}
+
+// Reduction slots (unsigned long long, dkey-encoded min/max).
+enum RedSlot : int {
+  RED_LO_X = 0, RED_LO_Y, RED_LO_Z, RED_HI_X, RED_HI_Y, RED_HI_Z, RED_HMIN,
+  RED_TS_HMIN, RED_TS_CMAX, RED_TS_DENMIN, RED_TS_CMIN, RED_TS_KAPMAX,
+  RED_TS_BMAX, RED_TS_KAPMIN, RED_TS_LAMMAX, RED_C1_ACTIVE, RED_TOTAL
+};
+
+// Device counters (unsigned long long, cumulative).
+enum DevCnt : int {
+  DC_NEIB_PAIRS = 0, DC_C1_PAIRS, DC_C2_PAIRS, DC_CANDIDATES,
+  DC_C1_CENTRE_SWEEPS, DC_C1_MAXSWEEPS, DC_TOTAL
+};
+
+// Periodic geometry for the image builder (BC.f90:46-68, 196-475).
+struct BoxGeom {
+  double emin[3], emax[3];
+  double boxmin[3], boxmax[3];
+  double pmin[3], pmax[3];
+  int periodic[3];  // axes that get periodic images
+  int reflect[3];   // axes whose real particles are wrapped
+};
+
+// ---- launchers (sph_grid.cu) -----------------------------------------------------
+void launch_upload_store(const double* rowmajor, double* cols, int32_t* orig, int64_t n,
+                         cudaStream_t s);
+void launch_download_store(const double* cols, const int32_t* orig, double* rowmajor,
+                           int64_t n, cudaStream_t s);
+void launch_reorder(const double* cols_in, double* cols_out, const int32_t* orig_in,
+                    int32_t* orig_out, const int32_t* perm, int64_t n, int64_t ld_in,
+                    int64_t ld_out, cudaStream_t s);
+void launch_reflect(double* cols, int64_t ld, int64_t nreal, BoxGeom g, cudaStream_t s);
+void launch_ghost_count(const double* cols, int64_t nrows, int64_t nreal, BoxGeom g,
+                        int dim, int32_t* count, unsigned long long* red, cudaStream_t s);
+void launch_ghost_write(const double* cols, int64_t nrows, BoxGeom g, int dim,
+                        const int32_t* offset, double* gx, double* gy, double* gz,
+                        int32_t* gsrc, int8_t* gcode, unsigned long long* red, cudaStream_t s);
+void launch_keys(const double* cols, int64_t nrows, const double* gx, const double* gy,
+                 const double* gz, int64_t nghost, Grid g, uint32_t* keys, int32_t* vals,
+                 cudaStream_t s);
+void launch_cell_ranges(const uint32_t* keys, int64_t n, Grid g, int32_t* cstart,
+                        int32_t* cend, cudaStream_t s);
+void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
+                          const double* cols, const double* gx, const double* gy,
+                          const double* gz, const int32_t* gsrc, double* sx, double* sy,
+                          double* sz, int32_t* ssrc, int32_t* centre_slot,
+                          int32_t* centre_k, int32_t* centre_p, cudaStream_t s);
+void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
+                    int32_t* centre_k, int32_t* centre_p, cudaStream_t s);
+void launch_neighbours(int dim, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
+                       const double* sx, const double* sy, const double* sz,
+                       const double* hcol, double krad, Grid g, const int32_t* cstart,
+                       const int32_t* cend, int cap, int32_t* nl, int32_t* ncnt,
+                       int32_t* maxcnt, unsigned long long* dcnt, cudaStream_t s);
+// pack groups
+enum PackGroup : int { PACK_POS = 1, PACK_HYDRO = 2, PACK_EXTRA = 4 };
+struct PackBufs {
+  double2* p[11];
+  float4* q[6];
+};
+struct PackGeom {
+  double ox, oy, oz;  // origin subtracted before the binade shift
+  double shift;       // 2^E
+  double mref;        // mass scale (packed m = m / mref)
+};
+void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
+                 const double* sy, const double* sz, const double* cols, int64_t ld,
+                 PackGeom pg, PackBufs pb, cudaStream_t s);
+void launch_predict(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                    int64_t n_int, double* save, const double* ctrl, int do_sts,
+                    cudaStream_t s);
+void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                    int64_t n_int, const double* save, const double* ctrl, int do_sts,
+                    cudaStream_t s);
+void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig,
+                            int64_t nrows, int64_t n_ts, Params P,
+                            unsigned long long* red, cudaStream_t s);
+void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s);
+void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, double a0,
+                      double a1, double a2, double a3, double a4, const double* ctrl,
+                      cudaStream_t s);
+void launch_eos(double* cols, int64_t ld, int64_t nreal, Params P, cudaStream_t s);
+void launch_apply_mti(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                      int64_t nreal, int lowres, cudaStream_t s);
+void launch_set_col(double* col, int64_t n, double v, cudaStream_t s);
+
+// CUB wrappers (sph_grid.cu)
+size_t sort_temp_bytes(int64_t n);
+void sort_pairs(void* tmp, size_t tmp_bytes, const uint32_t* kin, uint32_t* kout,
+                const int32_t* vin, int32_t* vout, int64_t n, int end_bit, cudaStream_t s);
+size_t scan_temp_bytes(int64_t n);
+void exclusive_scan(void* tmp, size_t tmp_bytes, const int32_t* in, int32_t* out, int64_t n,
+                    cudaStream_t s);
+
+// ---- circuit1 (sph_circuit1.cu) ---------------------------------------------------
+struct C1Args {
+  int64_t nc;
+  const int32_t* centre_k;
+  const int32_t* centre_p;
+  const int32_t* nl;
+  const int32_t* ncnt;
+  double* cols;
+  int64_t ld;
+  // Jacobi-sweep path
+  const double* hk_s;  // snapshots in sorted order
+  const double* dk_s;
+  const double* ok_s;
+  double* hkp1;
+  double* dkp1;
+  double* okp1;
+  double* eps;
+  int simple;  // c1simple
+  double mref;
+  int* status;
+  unsigned long long* dcnt;
+  unsigned long long* red;
+};
+void launch_c1_newton(int prec, int kernel, int dim, const C1Args& a, PackBufs pb, Params P,
+                      cudaStream_t s);
+void launch_c1_sweep(int prec, int kernel, int dim, const C1Args& a, PackBufs pb, Params P,
+                     cudaStream_t s);
+void launch_c1_finalize(int64_t nrows, int64_t nreal, double* cols, int64_t ld, const double* hkp1,
+                        const double* dkp1, const double* okp1, int simple, Params P,
+                        cudaStream_t s);
+void launch_c1_snapshot(int64_t n, const int32_t* ssrc, const double* hkp1,
+                        const double* dkp1, const double* okp1, double* hk_s, double* dk_s,
+                        double* ok_s, cudaStream_t s);
+
+// ---- circuit2 (sph_circuit2.cu) ---------------------------------------------------
+struct C2Args {
+  int64_t nc;
+  const int32_t* centre_k;
+  const int32_t* centre_p;
+  const int32_t* nl;
+  const int32_t* ncnt;
+  double* cols;
+  int64_t ld;
+  double mref;
+  int* status;
+  unsigned long long* dcnt;
+};
+void launch_c2(int prec, int kernel, int dim, const C2Args& a, PackBufs pb, Params P,
+               cudaStream_t s);
+
+}  // namespace sph

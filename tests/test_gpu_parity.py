@@ -1,0 +1,211 @@
+"""Parity of the CUDA engine against the CPU oracle on the same seeded inputs.
+
+Tolerances (stated per field):
+  FP64 path      : rho, h, Omega, P, c per particle <= 1e-12 relative;
+                   a, du/dt, dh/dt, dT/dt, grad T, dB/dt <= 1e-12 of the
+                   field's largest magnitude; neighbour sets bit-exact.
+  FP32-comp path : rho, h per particle <= 1e-6; a, du/dt, dh/dt, dT/dt,
+                   dB/dt <= 1e-5 of the field's largest magnitude;
+                   neighbour sets bit-exact (the predicate stays FP64).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from sph_playground_b200 import abi, consts, ic
+from tests.parity import COL, neighbour_sets_equal, rel_field, rel_particle, run_pass
+
+pytestmark = pytest.mark.gpu
+
+FP64, FP32 = abi.PREC_FP64, abi.PREC_FP32_COMP
+TOL = {FP64: dict(part=1e-12, field=1e-12), FP32: dict(part=1e-6, field=1e-5)}
+
+
+def compare(ref, got, prec, part_fields=(), field_fields=()):
+    bad = {}
+    for f in part_fields:
+        e = rel_particle(got[:, COL[f]], ref[:, COL[f]])
+        if not e <= TOL[prec]["part"]:
+            bad[f] = e
+    for f in field_fields:
+        e = rel_field(got[:, COL[f]], ref[:, COL[f]])
+        if not e <= TOL[prec]["field"]:
+            bad[f] = e
+    return bad
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+@pytest.mark.parametrize("kernel", ["m6", "m4"])
+def test_density3d(oracle_lib, engine_lib, cuda_ok, prec, kernel):
+    st, store = ic.density3d(n=16, seed=2, kernel=kernel)
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, kernel, FP64, "density")
+    got, nb_got, cnt, _ = run_pass(engine_lib, st, store, kernel, prec, "density")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    assert cnt["neib_pairs"] == nb_ref[0][-1]
+    bad = compare(ref, got, prec, part_fields=("den", "h", "om", "p", "c"))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_sedov_iterate(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = ic.sedov3d(n=14)
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    bad = compare(ref, got, prec, part_fields=("den", "h", "om", "c"),
+                  field_fields=("ax", "ay", "az", "du", "dh"))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_sod_shock12_iterate(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = ic.sod2d()
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    bad = compare(ref, got, prec, part_fields=("den", "h", "om"),
+                  field_fields=("ax", "ay", "du", "dh"))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("ddw", ["fab", "n2w", "fw", "2nw_ds", "2nw_sd"])
+@pytest.mark.parametrize("full", [False, True])
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_diffusion_iterate(oracle_lib, engine_lib, cuda_ok, ddw, full, prec):
+    st, store = ic.diffusion2d(24, ddw=ddw, full_tensor=full)
+    params = {abi.P_FULL_TENSOR: 1.0 if full else 0.0}
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate", params)
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate", params)
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    bad = compare(ref, got, prec, part_fields=("den", "h", "om"),
+                  field_fields=("ddt", "dtdx", "dtdy"))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("ddw", ["fab", "2nw_ds", "2nw_sd"])
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_simple_density_2nw(oracle_lib, engine_lib, cuda_ok, ddw, prec):
+    st, store = ic.diffusion2d(20, ddw=ddw)
+    ic.set_state(st, "adden", 0.0)
+    ref, _, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, _, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate")
+    bad = compare(ref, got, prec, part_fields=("den", "h"),
+                  field_fields=("ddt", "dtdx", "dtdy"))
+    assert not bad, bad
+
+
+def _mhd_case(seed=7, n=20):
+    st, store = ic.shear2d(n=n, amp=0.1)
+    ic.set_state(st, "eqs", consts.eeq["magnetohydrodiffusion"])
+    ic.set_state(st, "muzero", 1.0)
+    ic.set_state(st, "dcondconst", 0.5)
+    ic.set_state(st, "disotropic", 0.0)
+    ic.set_state(st, "ddw", consts.esd["2nw_ds"])
+    ic.set_state(st, "au", 1.0)
+    rng = np.random.default_rng(seed)
+    N = store.shape[0]
+    store[:, COL["bx"]] = 0.3 + 0.05 * rng.standard_normal(N)
+    store[:, COL["by"]] = 0.1 * rng.standard_normal(N)
+    store[:, COL["bz"]] = 0.2 + 0.05 * rng.standard_normal(N)
+    store[:, COL["vy"]] = 0.01 * rng.standard_normal(N)
+    store[:, COL["vz"]] = 0.01 * rng.standard_normal(N)
+    store[:, COL["t"]] = 1.0 + 0.1 * np.sin(2 * np.pi * store[:, 0])
+    store[:, COL["kappa"]] = 1.0
+    return st, store
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_mhd_iterate(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = _mhd_case()
+    ref, _, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, _, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate")
+    bad = compare(ref, got, prec, part_fields=("den", "h"),
+                  field_fields=("ax", "ay", "az", "du", "dh", "ddt", "dbx", "dby", "dbz"))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_fld_iterate(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = ic.diffusion2d(20, ddw="fab")
+    ic.set_state(st, "eqonfluxlim", 1.0)
+    ic.set_state(st, "disotropic", 1.0)
+    ic.set_state(st, "eqonsts", 0.0)
+    store[:, COL["t"]] = 1.0 + 0.2 * np.sin(2 * np.pi * store[:, 0]) * np.cos(2 * np.pi * store[:, 1])
+    store[:, COL["kappa"]] = 1e9
+    ref, _, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, _, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate")
+    bad = compare(ref, got, prec, part_fields=("den", "h"),
+                  field_fields=("ddt", "dtdx", "dtdy", "vfld"))
+    assert not bad, bad
+
+
+def test_fld_anisotropic_is_rejected(engine_lib, cuda_ok):
+    st, store = ic.diffusion2d(12, ddw="fab")
+    ic.set_state(st, "eqonfluxlim", 1.0)
+    ic.set_state(st, "disotropic", 0.0)
+    e = abi.Engine(st, store, "m6", lib=engine_lib)
+    with pytest.raises(abi.SphError) as ex:
+        e.iterate()
+    assert ex.value.code == 15
+    e.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_sedov_steps(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = ic.sedov3d(n=12, tfinish=1.0)
+    ref, _, cref, sref = run_pass(oracle_lib, st, store, "m6", FP64, "steps", steps=3)
+    got, _, cgot, sgot = run_pass(engine_lib, st, store, "m6", prec, "steps", steps=3)
+    assert cgot["steps"] == cref["steps"] == 3
+    t_rel = abs(sgot[consts.ec["time"] - 1] - sref[consts.ec["time"] - 1]) / sref[consts.ec["time"] - 1]
+    tol = 1e-11 if prec == FP64 else 1e-5
+    assert t_rel <= tol
+    for f in ("rx", "ry", "rz"):
+        assert np.max(np.abs(got[:, COL[f]] - ref[:, COL[f]])) <= tol * 1e-2
+    bad = {}
+    for f in ("vx", "vy", "vz", "u", "h", "den"):
+        e = rel_field(got[:, COL[f]], ref[:, COL[f]])
+        if not e <= (1e-10 if prec == FP64 else 1e-5):
+            bad[f] = e
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_sts_steps(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = ic.diffusion2d(16, ddw="2nw_ds", sts_stages=4, tfinish=1.0)
+    ref, _, cref, sref = run_pass(oracle_lib, st, store, "m6", FP64, "steps", steps=2)
+    got, _, cgot, sgot = run_pass(engine_lib, st, store, "m6", prec, "steps", steps=2)
+    assert cgot["iterates"] == cref["iterates"]
+    assert abs(sgot[consts.ec["time"] - 1] - sref[consts.ec["time"] - 1]) <= 1e-12 * sref[consts.ec["time"] - 1] * (1 if prec == FP64 else 1e6)
+    e = rel_field(got[:, COL["t"]], ref[:, COL["t"]])
+    assert e <= (1e-11 if prec == FP64 else 1e-5), e
+
+
+def test_borderless_and_fixed(oracle_lib, engine_lib, cuda_ok):
+    st, store = ic.sedov3d(n=10)
+    ic.set_state(st, "process", consts.epc["borderless"])
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", FP64, "iterate")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    bad = compare(ref, got, FP64, part_fields=("den", "h"), field_fields=("ax", "du"))
+    assert not bad, bad
+
+
+def test_bad_ic_reports_status(engine_lib, cuda_ok):
+    st, store = ic.sedov3d(n=8)
+    store[5, COL["h"]] = 0.0
+    e = abi.Engine(st, store, "m6", lib=engine_lib)
+    with pytest.raises(abi.SphError) as ex:
+        e.step(1)
+    assert ex.value.code == 9
+    e.close()
+
+
+def test_nan_position_reports_status(engine_lib, cuda_ok):
+    st, store = ic.sedov3d(n=8)
+    store[3, COL["rx"]] = float("nan")
+    e = abi.Engine(st, store, "m6", lib=engine_lib)
+    with pytest.raises(abi.SphError) as ex:
+        e.iterate()
+    assert ex.value.code in (3, 4)
+    e.close()
