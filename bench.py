@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""SPH step throughput on B200: particle-steps/s of the two-loop SPH step.
+
+Workload: Sedov blast, 128^3 = 2,097,152 lattice particles in the unit
+periodic box, M6 kernel, hfac 1.2, alpha = 1, beta = 2, gamma = 5/3.  One
+step is the full leapfrog step of the reference's time loop: timestep
+reductions, predictor, periodic images, neighbour lists, circuit1 (Newton
+h-iteration + EOS), circuit2 (hydro + AV + conductivity + dh/dt) and
+corrector.  The headline runs the FP32-compensated pair path; the plain FP64
+path is timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (launched under torchrun) every rank runs an independent replica
+of the workload on its own GPU (the reference has no domain decomposition):
+`value` is the sum over ranks, timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s, 2.1M 3D: FP32-comp vs FP64 on B200 at rho err<=1e-6"
+UNIT = "particle-steps/s"
+# per-pair algorithmic FLOP weights (circuit1 per pair per Newton sweep,
+# circuit2 per pair for hydro + AV + conductivity + dh/dt), counted from the
+# reference formulas with sqrt/div each as one FLOP
+F1_C1 = 50.0
+F2_C2 = 150.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="lattice particles per axis")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-n", type=int, default=64, help="lattice per axis of the CPU sample")
+    return ap.parse_args()
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                   "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(rows), "reasons": reasons}
+
+
+def measure_peak():
+    import ctypes
+    path = os.path.join(ROOT, "sph_playground_b200", "_lib", "libsph_peak.so")
+    lib = ctypes.CDLL(path)
+    lib.sph_peak_flops.restype = ctypes.c_double
+    lib.sph_peak_flops.argtypes = [ctypes.c_int, ctypes.c_int]
+    fp32 = max(lib.sph_peak_flops(0, 20) for _ in range(3))
+    fp64 = max(lib.sph_peak_flops(1, 10) for _ in range(2))
+    return fp32, fp64
+
+
+def cpu_baseline(n):
+    """The oracle (CPU FP64 OpenMP restatement) on a bounded sample: one
+    leapfrog step of the same Sedov set-up at n^3 after its start-up iterate."""
+    from sph_playground_b200 import abi, ic
+    lib = abi.load(os.path.join(ROOT, "oracle", "liboracle.so"))
+    st, store = ic.sedov3d(n=n)
+    e = abi.Engine(st, store, "m6", lib=lib)
+    e.step(0)
+    t0 = time.perf_counter()
+    e.step(1)
+    dt = time.perf_counter() - t0
+    e.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": store.shape[0] / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"sedov3d {n}^3 ({store.shape[0]} particles), 1 leapfrog step after the "
+                      f"start-up iterate, CPU oracle (FP64, OpenMP {cores} threads)"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from sph_playground_b200 import abi, ic
+    lib = abi.load(os.path.join(ROOT, "oracle", "liboracle.so"))
+    n = args.cpu_n
+    st, store = ic.sedov3d(n=n)
+    e = abi.Engine(st, store, "m6", lib=lib)
+    e.step(0)
+    for _ in range(args.warmup):
+        e.step(1)
+    t0 = time.perf_counter()
+    e.step(args.steps)
+    dt = time.perf_counter() - t0
+    e.close()
+    N = store.shape[0]
+    value = N * args.steps / dt
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"sedov3d {n}^3 ({N} particles) sample of the 128^3 Sedov step, "
+                               "M6 hfac 1.2, full leapfrog step",
+                   "particles": N, "note": "reference Fortran not compiled (no gfortran/HDF5 "
+                   "in the image); the CPU oracle restatement of its path is timed instead"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"sedov3d {n}^3, {args.steps} steps after {args.warmup} warm-up"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def timed_steps(e, K):
+    """Run K steps; returns (device ms from the engine's stream events,
+    counters delta, per-phase ms delta)."""
+    e.reset_counters()
+    e.set_param(58, 1)  # SPH_P_TIMING
+    e.step(K)
+    return e.timers()["step"], e.counters(), e.timers()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from sph_playground_b200 import abi, ic
+
+    lib = abi.load()
+    st, store = ic.sedov3d(n=args.n)
+    N = store.shape[0]
+    peak32, peak64 = measure_peak()
+
+    # FP32 vs FP64 density error on the bench input (the metric's rho bound)
+    e32 = abi.Engine(st, store, "m6", precision=abi.PREC_FP32_COMP, lib=lib)
+    e64 = abi.Engine(st, store, "m6", precision=abi.PREC_FP64, lib=lib)
+    e32.density()
+    e64.density()
+    r32, r64 = e32.get_store(), e64.get_store()
+    col = abi.consts.es["den"] - 1
+    rel = np.abs(r32[:, col] - r64[:, col]) / np.abs(r64[:, col])
+    rho_err = {"max": float(rel.max()), "p99.9": float(np.quantile(rel, 0.999))}
+    hcol = abi.consts.es["h"] - 1
+    relh = np.abs(r32[:, hcol] - r64[:, hcol]) / np.abs(r64[:, hcol])
+    e32.close()
+    e64.close()
+
+    def run(prec):
+        e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+        e.set_param(abi.consts.ec["tfinish"], 1.0)
+        for _ in range(args.warmup):
+            e.step(1)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        uuid = None
+        try:
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+        except Exception:
+            uuid = None
+        with Clocks(uuid) as ck:
+            ms, cnt, tm = timed_steps(e, args.steps)
+            torch.cuda.synchronize()
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return e, ms, cnt, tm, ck.summary()
+
+    e, ms, cnt, tm, clocks = run(abi.PREC_FP32_COMP)
+    value = ws * N * args.steps / (ms * 1e-3)
+
+    # roofline of the dominant pair kernel: algorithmic FLOPs / its event time
+    c1_flops = cnt["c1_pairs"] * F1_C1
+    c2_flops = cnt["c2_pairs"] * F2_C2
+    kern = {"circuit1": (c1_flops, tm["circuit1"]), "circuit2": (c2_flops, tm["circuit2"])}
+    dom = max(kern, key=lambda k: kern[k][1])
+    ach = kern[dom][0] / (kern[dom][1] * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": peak32 / 1e12,
+                "unit": "TFLOP/s", "frac": ach / (peak32 / 1e12), "traffic": None,
+                "peak_source": "live FFMA-chain probe (libsph_peak.so) on this GPU; "
+                               "MEASURED_PEAKS.json holds no non-tensor FP32 figure"}
+
+    # end to end through the C-ABI with pinned host buffers, per step:
+    # H2D of the particle table, one step, D2H of the particle table
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.empty((N, 32), dtype=torch.float64).pin_memory().numpy()
+        host_out = torch.empty((N, 32), dtype=torch.float64).pin_memory().numpy()
+        e.get_store(host_in)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e.set_store(host_in)
+            e.step(1)
+            e.get_store(host_out)
+            host_in, host_out = host_out, host_in
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if ws > 1:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": ws * N * args.e2e_steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": N * 32 * 8, "d2h_bytes_per_step": N * 32 * 8,
+               "steps": args.e2e_steps,
+               "timing": "host clock around synchronous C-ABI calls (set_store, step, get_store)"}
+    e.close()
+
+    fp64 = None
+    if not args.no_fp64:
+        e6, ms6, cnt6, tm6, _ = run(abi.PREC_FP64)
+        e6.close()
+        fp64 = {"value": ws * N * args.steps / (ms6 * 1e-3), "ms_per_step": ms6 / args.steps,
+                "phases_ms_per_step": {k: v / args.steps for k, v in tm6.items()},
+                "peak_fp64_tflops": peak64 / 1e12}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_n)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"sedov3d {args.n}^3 ({N} particles), M6 hfac 1.2, "
+                                   "FP32-comp pair sums, full leapfrog step",
+                       "particles": N, "kernel": "m6", "precision": "fp32_comp",
+                       "l2": "inputs larger than L2 (particle table "
+                             f"{N * 32 * 8 / 1e6:.0f} MB + pair streams)",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": cnt["launches"],
+            "clocks": clocks,
+            "rho_rel_err_fp32_vs_fp64": rho_err,
+            "h_rel_err_fp32_vs_fp64": {"max": float(relh.max())},
+            "phases_ms_per_step": {k: v / args.steps for k, v in tm.items()},
+            "work_per_step": {"neib_pairs": cnt["neib_pairs"] / args.steps,
+                              "c1_pairs": cnt["c1_pairs"] / args.steps,
+                              "c2_pairs": cnt["c2_pairs"] / args.steps,
+                              "c1_max_sweeps": cnt["c1_sweeps"],
+                              "candidates": cnt["candidates"] / args.steps},
+            "fp64": fp64,
+            "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
+            "peak_fp32_tflops": peak32 / 1e12,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

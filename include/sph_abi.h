@@ -100,7 +100,8 @@ extern "C" {
 #define SPH_CNT_CANDIDATES      7 /* cell-list candidates tested              */
 #define SPH_CNT_CENTRES         8 /* real centres processed (sum)             */
 #define SPH_CNT_C1_CENTRE_SWEEPS 9 /* sum over particles of their sweeps      */
-#define SPH_CNT_TOTAL          10
+#define SPH_CNT_LAUNCHES      10 /* kernels of this library launched         */
+#define SPH_CNT_TOTAL          11
 
 /* ---- per-kernel timers (sph_get_timers, milliseconds, cumulative) ------- */
 #define SPH_T_PREDICT    0
@@ -112,7 +113,8 @@ extern "C" {
 #define SPH_T_CORRECT    6
 #define SPH_T_TIMESTEP   7
 #define SPH_T_STS        8
-#define SPH_T_TOTAL      9
+#define SPH_T_STEP       9 /* whole sph_step / sph_run_to calls */
+#define SPH_T_TOTAL      10
 
 typedef struct sph_handle sph_handle;
 

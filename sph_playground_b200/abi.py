@@ -42,9 +42,9 @@ P_NEIB_CAP = 59
 
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",
-            "c1_centre_sweeps"]
+            "c1_centre_sweeps", "launches"]
 TIMERS = ["predict", "ghosts", "sort", "neighbours", "circuit1", "circuit2",
-          "correct", "timestep", "sts"]
+          "correct", "timestep", "sts", "step"]
 
 # every symbol include/sph_abi.h declares
 ABI_SYMBOLS = [

@@ -316,10 +316,12 @@ __global__ void k_c1_finalize(int64_t nrows, int64_t nreal, double* __restrict__
 template <int K, int DIM, class R>
 void dispatch_newton(const C1Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
   k_c1_newton<K, DIM, R><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
+  note_launch();
 }
 template <int K, int DIM, class R>
 void dispatch_sweep(const C1Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
   k_c1_sweep<K, DIM, R><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
+  note_launch();
 }
 
 #define SPH_DISPATCH(FN)                                                             \
@@ -361,11 +363,13 @@ void launch_c1_finalize(int64_t nrows, int64_t nreal, double* cols, int64_t ld, 
                         cudaStream_t s) {
   k_c1_finalize<<<nblocks(nrows, 256), 256, 0, s>>>(nrows, nreal, cols, ld, hkp1, dkp1, okp1,
                                                     simple, P);
+  note_launch();
 }
 void launch_c1_snapshot(int64_t n, const int32_t* ssrc, const double* hkp1, const double* dkp1,
                         const double* okp1, double* hk_s, double* dk_s, double* ok_s,
                         cudaStream_t s) {
   k_c1_snapshot<<<nblocks(n, 256), 256, 0, s>>>(n, ssrc, hkp1, dkp1, okp1, hk_s, dk_s, ok_s);
+  note_launch();
 }
 
 }  // namespace sph

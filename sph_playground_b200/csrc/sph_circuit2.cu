@@ -297,6 +297,7 @@ void run(const C2Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
   const bool general = P.eq_diff || P.eq_magneto;
   if (general) k_c2<K, DIM, R, true><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
   else k_c2<K, DIM, R, false><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
+  note_launch();
 }
 template <int K, int DIM>
 void run_prec(int prec, const C2Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {

@@ -24,6 +24,7 @@ using namespace sph;
 namespace {
 
 thread_local std::string g_err;
+long long g_launches = 0;
 
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -118,6 +119,11 @@ struct Mode {
 
 }  // namespace
 
+namespace sph {
+void note_launch(int n) { g_launches += n; }
+long long launches_so_far() { return g_launches; }
+}  // namespace sph
+
 struct sph_handle {
   int kernel_id = SPH_KERNEL_M6;
   int prec = SPH_PREC_FP64;
@@ -160,6 +166,7 @@ struct sph_handle {
 
   int64_t cnt_host[SPH_CNT_TOTAL] = {0};
   int64_t host_max_sweeps = 0;  // Newton sweeps of the Jacobi path
+  long long launch_base = 0;    // g_launches at create / reset
   double timers[SPH_T_TOTAL] = {0};
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending_ev;
   std::vector<cudaEvent_t> ev_pool;
@@ -676,7 +683,6 @@ struct sph_handle {
     RC(check_status());
     cnt_host[SPH_CNT_ITERATES] += full ? 1 : 0;
     cnt_host[SPH_CNT_CENTRES] += nreal;
-    collect_timers();
     return SPH_OK;
   }
 
@@ -742,6 +748,7 @@ struct sph_handle {
                        cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     CK(cudaGetLastError());
+    collect_timers();  // every earlier phase has completed at this point
     double hmin = dkey_inv(h_red[RED_TS_HMIN]), cmax = dkey_inv(h_red[RED_TS_CMAX]);
     double denmin = dkey_inv(h_red[RED_TS_DENMIN]), cmin = dkey_inv(h_red[RED_TS_CMIN]);
     double kapmax = dkey_inv(h_red[RED_TS_KAPMAX]), bmax = dkey_inv(h_red[RED_TS_BMAX]);
@@ -858,7 +865,6 @@ struct sph_handle {
     cnt_host[SPH_CNT_STEPS]++;
     steps_since_reorder++;
     CK(cudaGetLastError());
-    collect_timers();
     return SPH_OK;
   }
 
@@ -951,6 +957,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
     delete h;
     return rc;
   }
+  h->launch_base = launches_so_far();
   *out = h;
   return SPH_OK;
 }
@@ -983,38 +990,52 @@ int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
 int sph_iterate(sph_handle* h) {
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   RC(h->reorder_rows());
-  return h->iterate(true);
+  int rc = h->iterate(true);
+  h->collect_timers();
+  return rc;
 }
 
 int sph_density(sph_handle* h) {
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   RC(h->reorder_rows());
-  return h->iterate(false);
+  int rc = h->iterate(false);
+  h->collect_timers();
+  return rc;
 }
 
 int sph_step(sph_handle* h, int nsteps) {
   if (!h || nsteps < 0) return fail(SPH_ERR_ARG, "bad argument");
-  if (!h->started) RC(h->start_run());
-  if (h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
-  for (int i = 0; i < nsteps; ++i) {
-    bool done = false;
-    RC(h->one_step(h->st[ec_tfinish], done));
-    if (done) break;
+  int rc = SPH_OK;
+  {
+    sph_handle::Phase ph(h, SPH_T_STEP);
+    if (!h->started) rc = h->start_run();
+    if (!rc && h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
+    for (int i = 0; !rc && i < nsteps; ++i) {
+      bool done = false;
+      rc = h->one_step(h->st[ec_tfinish], done);
+      if (done) break;
+    }
   }
-  return SPH_OK;
+  h->collect_timers();
+  return rc;
 }
 
 int sph_run_to(sph_handle* h, double tfinish) {
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   h->st[ec_tfinish] = tfinish;
-  if (!h->started) RC(h->start_run());
-  if (h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
-  for (;;) {
-    bool done = false;
-    RC(h->one_step(tfinish, done));
-    if (done) break;
+  int rc = SPH_OK;
+  {
+    sph_handle::Phase ph(h, SPH_T_STEP);
+    if (!h->started) rc = h->start_run();
+    if (!rc && h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
+    while (!rc) {
+      bool done = false;
+      rc = h->one_step(tfinish, done);
+      if (done) break;
+    }
   }
-  return SPH_OK;
+  h->collect_timers();
+  return rc;
 }
 
 int sph_get_store(sph_handle* h, double* out, int64_t cap_rows) {
@@ -1088,6 +1109,7 @@ int sph_get_counters(sph_handle* h, int64_t* out, int n) {
   all[SPH_CNT_C2_PAIRS] = int64_t(d[DC_C2_PAIRS]);
   all[SPH_CNT_CANDIDATES] = int64_t(d[DC_CANDIDATES]);
   all[SPH_CNT_C1_CENTRE_SWEEPS] = int64_t(d[DC_C1_CENTRE_SWEEPS]);
+  all[SPH_CNT_LAUNCHES] = int64_t(launches_so_far() - h->launch_base);
   for (int k = 0; k < n && k < SPH_CNT_TOTAL; ++k) out[k] = all[k];
   return SPH_OK;
 }
@@ -1099,6 +1121,7 @@ int sph_reset_counters(sph_handle* h) {
   for (auto& c : h->cnt_host) c = 0;
   for (auto& t : h->timers) t = 0.;
   h->host_max_sweeps = 0;
+  h->launch_base = launches_so_far();
   return SPH_OK;
 }
 

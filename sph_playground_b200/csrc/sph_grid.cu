@@ -223,10 +223,13 @@ __device__ __forceinline__ uint32_t compact3(uint32_t x) {
   x = (x | (x >> 16)) & 0x000003FFu;
   return x;
 }
+// Cell index along one axis, clamped to [0, n-1].  NaN and -inf map to 0
+// and +inf to n-1 before any float-to-int conversion happens.
 __device__ __forceinline__ int cell_coord(double x, double o, double invL, int n) {
   double f = floor((x - o) * invL);
-  int c = f < 0.0 ? 0 : (f > double(n - 1) ? n - 1 : int(f));
-  return c;
+  if (!(f >= 0.0)) return 0;
+  if (f >= double(n - 1)) return n - 1;
+  return int(f);
 }
 
 __global__ void k_keys(const double* __restrict__ cols, int64_t ld, int64_t nrows,
@@ -610,37 +613,47 @@ __global__ void k_set(double* col, int64_t n, double v) {
 // ---- launchers ------------------------------------------------------------------------------
 void launch_upload_store(const double* rm, double* cols, int32_t* orig, int64_t n, cudaStream_t s) {
   k_upload<<<nblocks(n * NCOL), TPB, 0, s>>>(rm, cols, orig, n);
+  note_launch();
 }
 void launch_download_store(const double* cols, const int32_t* orig, double* rm, int64_t n,
                            cudaStream_t s) {
   k_download<<<nblocks(n * NCOL), TPB, 0, s>>>(cols, orig, rm, n);
+  note_launch();
 }
 void launch_reorder(const double* cin, double* cout, const int32_t* oin, int32_t* oout,
                     const int32_t* perm, int64_t n, int64_t ldi, int64_t ldo, cudaStream_t s) {
   k_reorder<<<nblocks(n), TPB, 0, s>>>(cin, cout, oin, oout, perm, n, ldi, ldo);
+  note_launch();
 }
 void launch_reflect(double* cols, int64_t ld, int64_t nreal, BoxGeom g, cudaStream_t s) {
-  if (nreal > 0) k_reflect<<<nblocks(nreal), TPB, 0, s>>>(cols, ld, nreal, g);
+  if (nreal > 0) {
+    k_reflect<<<nblocks(nreal), TPB, 0, s>>>(cols, ld, nreal, g);
+    note_launch();
+  }
 }
 void launch_ghost_count(const double* cols, int64_t nrows, int64_t nreal, BoxGeom g, int dim,
                         int32_t* count, unsigned long long* red, cudaStream_t s) {
   k_ghost_count<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, nreal, g, dim, count, red);
+  note_launch();
 }
 void launch_ghost_write(const double* cols, int64_t nrows, BoxGeom g, int dim,
                         const int32_t* offset, double* gx, double* gy, double* gz,
                         int32_t* gsrc, int8_t* gcode, unsigned long long*, cudaStream_t s) {
   k_ghost_write<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, g, dim, offset, gx, gy, gz,
                                                gsrc, gcode);
+  note_launch();
 }
 void launch_keys(const double* cols, int64_t nrows, const double* gx, const double* gy,
                  const double* gz, int64_t nghost, Grid g, uint32_t* keys, int32_t* vals,
                  cudaStream_t s) {
   k_keys<<<nblocks(nrows + nghost), TPB, 0, s>>>(cols, nrows, nrows, gx, gy, gz, nghost, g,
                                                  keys, vals);
+  note_launch();
 }
 void launch_cell_ranges(const uint32_t* keys, int64_t n, Grid g, int32_t* cstart, int32_t* cend,
                         cudaStream_t s) {
   k_cell_ranges<<<nblocks(n), TPB, 0, s>>>(keys, n, g, cstart, cend);
+  note_launch();
 }
 void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
                           const double* cols, const double* gx, const double* gy,
@@ -651,12 +664,14 @@ void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t
   // written into centre_k's tail scratch by the caller, see sph_engine.cu.
   k_sorted_gather<<<nblocks(n), TPB, 0, s>>>(sidx, n, nrows, nreal, cols, nrows, gx, gy, gz,
                                              gsrc, sx, sy, sz, ssrc, centre_slot);
+  note_launch();
   (void)centre_k;
   (void)centre_p;
 }
 void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
                     int32_t* centre_k, int32_t* centre_p, cudaStream_t s) {
   k_centres<<<nblocks(n), TPB, 0, s>>>(sidx, flag, pos, n, centre_k, centre_p);
+  note_launch();
 }
 void launch_neighbours(int dim, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
                        const double* sx, const double* sy, const double* sz, const double* hcol,
@@ -673,41 +688,51 @@ void launch_neighbours(int dim, int64_t nc, const int32_t* centre_k, const int32
   else
     k_neighbours<1><<<nblocks(nc, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, hcol, krad,
                                                      g, cstart, cend, cap, nl, ncnt, maxcnt, dcnt);
+  note_launch();
 }
 void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
                  const double* sy, const double* sz, const double* cols, int64_t ld, PackGeom pg,
                  PackBufs pb, cudaStream_t s) {
   k_pack<<<nblocks(n), TPB, 0, s>>>(prec, groups, n, ssrc, sx, sy, sz, cols, ld, pg, pb);
+  note_launch();
 }
 void launch_predict(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
                     double* save, const double* ctrl, int do_sts, cudaStream_t s) {
   k_predict<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, do_sts);
+  note_launch();
 }
 void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
                     const double* save, const double* ctrl, int do_sts, cudaStream_t s) {
   k_correct<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, do_sts);
+  note_launch();
 }
 void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
                             int64_t n_ts, Params P, unsigned long long* red, cudaStream_t s) {
   k_timestep_reduce<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_ts, P, red);
+  note_launch();
 }
 void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s) {
   k_fill_u64<<<nblocks(n), TPB, 0, s>>>(p, n, v);
+  note_launch();
 }
 void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, double a0,
                       double a1, double a2, double a3, double a4, const double* ctrl,
                       cudaStream_t s) {
   k_sts<<<nblocks(n), TPB, 0, s>>>(kind, cols, ld, n, Y, a0, a1, a2, a3, a4, ctrl);
+  note_launch();
 }
 void launch_eos(double* cols, int64_t ld, int64_t nreal, Params P, cudaStream_t s) {
   k_eos<<<nblocks(nreal), TPB, 0, s>>>(cols, ld, nreal, P);
+  note_launch();
 }
 void launch_apply_mti(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t nreal,
                       int lowres, cudaStream_t s) {
   k_mti<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, nreal, lowres);
+  note_launch();
 }
 void launch_set_col(double* col, int64_t n, double v, cudaStream_t s) {
   k_set<<<nblocks(n), TPB, 0, s>>>(col, n, v);
+  note_launch();
 }
 
 size_t sort_temp_bytes(int64_t n) {

@@ -61,6 +61,10 @@ struct BoxGeom {
   int reflect[3];   // axes whose real particles are wrapped
 };
 
+// Count of this library's kernel launches (process-wide).
+void note_launch(int n = 1);
+long long launches_so_far();
+
 // ---- launchers (sph_grid.cu) -----------------------------------------------------
 void launch_upload_store(const double* rowmajor, double* cols, int32_t* orig, int64_t n,
                          cudaStream_t s);
