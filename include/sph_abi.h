@@ -59,11 +59,14 @@ extern "C" {
                                     1: full k_par * b b^T (new)              */
 #define SPH_P_NEIB_CAP_CHECK  55 /* 1: abort like neighboursearch.f90:127-131
                                     when n_i+1 > maxneibnum; default 0       */
-#define SPH_P_CELL_FACTOR     56 /* cell edge / (krad*h_min), default 1.0    */
+#define SPH_P_CELL_FACTOR     56 /* cell edge / (krad*h_min), default 0.5    */
 #define SPH_P_REORDER_EVERY   57 /* physical re-sort interval in steps (8)   */
 #define SPH_P_TIMING          58 /* 1: record per-kernel CUDA-event times    */
 #define SPH_P_NEIB_CAP        59 /* neighbour slots per centre (0 = auto)    */
-#define SPH_P_LAST            59
+#define SPH_P_LANES_SEARCH    60 /* lanes per centre in the neighbour search
+                                    (4, 8, 16, 32; 0 = auto)                  */
+#define SPH_P_LANES_PAIR      61 /* lanes per centre in circuit1/circuit2     */
+#define SPH_P_LAST            61
 
 /* ---- status codes --------------------------------------------------------- */
 #define SPH_OK                     0

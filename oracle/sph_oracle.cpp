@@ -1240,7 +1240,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows,
   o.st[SPH_P_AV_BETA] = 2.;
   o.st[SPH_P_NEWTON_TOL] = 1e-8;
   o.st[SPH_P_NEWTON_MAXITER] = 100;
-  o.st[SPH_P_CELL_FACTOR] = 1.;
+  o.st[SPH_P_CELL_FACTOR] = 0.5;
   o.st[SPH_P_REORDER_EVERY] = 8;
   o.realpn = int64_t(o.st[ec_realpn]);
   o.fixedpn = int64_t(o.st[ec_fixedpn]);

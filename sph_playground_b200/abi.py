@@ -39,6 +39,8 @@ P_CELL_FACTOR = 56
 P_REORDER_EVERY = 57
 P_TIMING = 58
 P_NEIB_CAP = 59
+P_LANES_SEARCH = 60
+P_LANES_PAIR = 61
 
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",

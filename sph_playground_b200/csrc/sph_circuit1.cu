@@ -83,11 +83,30 @@ __device__ __forceinline__ void eos_epilogue(double* cols, int64_t ld, int64_t p
   }
 }
 
+// Sum a per-lane double over the G lanes of a group (all lanes get the sum).
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned gmask) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+  return v;
+}
+
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+  const int wl = threadIdx.x & 31;
+  return (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (wl & ~(G - 1)));
+}
+
 // ---- fused Newton loop (no temperature gradient) ------------------------------------------
-template <int K, int DIM, class R>
+// G lanes per centre: each lane sums every G-th neighbour of the centre's
+// row of the neighbour list (coalesced), the group adds its lanes' two-sum
+// partials in FP64, and every lane takes the same FP64 Newton step.
+template <int K, int DIM, class R, int G>
 __global__ void __launch_bounds__(TPB)
 k_c1_newton(C1Args a, PackBufs pb, Params P) {
-  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gmask = group_mask<G>();
   unsigned long long pairs = 0, sweeps = 0;
   int maxit = 0;
   if (c < a.nc) {
@@ -100,6 +119,7 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
     const double ma = cols[es_m * ld + p];
     const double ha0 = cols[es_h * ld + p];
     const int n = a.ncnt[c];
+    const int32_t* __restrict__ row = a.nl + c * int64_t(a.cap);
     const double wcv = P.wCv;
     // kernel shape at q = 0 for the self term (circuit1.f90:191-194)
     R f0, df0;
@@ -109,12 +129,14 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
     bool bad = false;
     for (;;) {
       ++it;
-      const R ih = R(1.0 / ha);
+      const double ihd_full = 1.0 / ha;
+      const R ih = R(ihd_full);
+      const R ih_lo = R(ihd_full - double(ih));
       Acc<R> sw, so;
       sw.init();
       so.init();
-      for (int l = 0; l < n; ++l) {
-        const int64_t j = a.nl[int64_t(l) * a.nc + c];
+      for (int l = lane; l < n; l += G) {
+        const int64_t j = row[l];
         R mj;
         const PairPos<R> pj = PosAccess<R>::load(pb, j, mj);
         R dx, dy, dz;
@@ -122,36 +144,51 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
         R r2 = dx * dx;
         if (DIM >= 2) r2 += dy * dy;
         if (DIM == 3) r2 += dz * dz;
-        const R q = rsq<R>(r2) * ih;
+        const R r = rsq<R>(r2);
+        const R q = r * ih;
         bad |= !(q >= R(0));
         R f, df;
-        kshape_f_df<K, R>(q, f, df);
+        if constexpr (sizeof(R) == 4) {
+          // q carries the FP32 rounding of r/h; its residual (exact via FMA)
+          // and the residuals of the kernel pieces enter f to first order, so
+          // the density sum varies smoothly with h below FP32 resolution and
+          // the Newton iterates converge instead of cycling between
+          // neighbouring FP32 values (kshape_f_df_res).
+          const R q_lo = fmaf(r, ih, -q) + r * ih_lo;
+          kshape_f_df_res<K>(q, q_lo, f, df);
+        } else {
+          kshape_f_df<K, R>(q, f, df);
+        }
         sw.add(mj * f);
         so.add(mj * (R(DIM) * f + q * df));
       }
-      pairs += n;
+      const double swt = group_sum<G>(sw.dval(), gmask);
+      const double sot = group_sum<G>(so.dval(), gmask);
       // W = wCv f / h^d; dW/dh = -wCv / h^(d+1) (d f + q f')  (kernel.f90:178-187, 239-249)
       const double ihd = 1.0 / ipow<DIM>(ha);
-      const double wsum = wcv * ihd * (a.mref * sw.dval() + ma * double(f0));
-      const double osum = -wcv * ihd / ha * (a.mref * so.dval() + ma * (DIM * double(f0)));
+      const double wsum = wcv * ihd * (a.mref * swt + ma * double(f0));
+      const double osum = -wcv * ihd / ha * (a.mref * sot + ma * (DIM * double(f0)));
       const double eps = newton_update<DIM>(ha, ha0, ma, P.hfac, wsum, osum, rho, om, hn);
       if (hn <= 0.) {
-        raise_status(a.status, SPH_ERR_H_NEG);
+        if (lane == 0) raise_status(a.status, SPH_ERR_H_NEG);
         break;
       }
       if (!(eps > P.tol) || it >= P.maxiter) break;
       ha = hn;
     }
     if (bad) raise_status(a.status, (ha > 0.0) ? SPH_ERR_Q_NAN : SPH_ERR_Q_NEG);
-    sweeps = it;
-    maxit = it;
-    cols[es_h * ld + p] = hn;
-    cols[es_den * ld + p] = rho;
-    cols[es_om * ld + p] = om;
-    cols[es_dtdx * ld + p] = 0.;
-    cols[es_dtdy * ld + p] = 0.;
-    cols[es_dtdz * ld + p] = 0.;
-    eos_epilogue(cols, ld, p, rho, P);
+    if (lane == 0) {
+      pairs = (unsigned long long)n * it;
+      sweeps = it;
+      maxit = it;
+      cols[es_h * ld + p] = hn;
+      cols[es_den * ld + p] = rho;
+      cols[es_om * ld + p] = om;
+      cols[es_dtdx * ld + p] = 0.;
+      cols[es_dtdy * ld + p] = 0.;
+      cols[es_dtdz * ld + p] = 0.;
+      eos_epilogue(cols, ld, p, rho, P);
+    }
   }
   unsigned long long wp = pairs, ws = sweeps;
   for (int o = 16; o > 0; o >>= 1) {
@@ -160,17 +197,19 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
     maxit = max(maxit, __shfl_xor_sync(0xffffffffu, maxit, o));
   }
   if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&a.dcnt[DC_C1_PAIRS], wp);
-    atomicAdd(&a.dcnt[DC_C1_CENTRE_SWEEPS], ws);
-    atomicMax(&a.dcnt[DC_C1_MAXSWEEPS], (unsigned long long)maxit);
+    if (wp) atomicAdd(&a.dcnt[DC_C1_PAIRS], wp);
+    if (ws) atomicAdd(&a.dcnt[DC_C1_CENTRE_SWEEPS], ws);
+    if (maxit) atomicMax(&a.dcnt[DC_C1_MAXSWEEPS], (unsigned long long)maxit);
   }
 }
 
 // ---- one Jacobi sweep (diffusion / FLD, and the direct summation) ------------------------
-template <int K, int DIM, class R>
+template <int K, int DIM, class R, int G>
 __global__ void __launch_bounds__(TPB)
 k_c1_sweep(C1Args a, PackBufs pb, Params P) {
-  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gmask = group_mask<G>();
   unsigned long long pairs = 0, sweeps = 0;
   int active_left = 0;
   if (c < a.nc) {
@@ -186,9 +225,11 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
       const double ha = a.hk_s[k], rhoa = a.dk_s[k], oma = a.ok_s[k];
       const double ta = cols[es_t * ld + p];
       const int n = a.ncnt[c];
+      const int32_t* __restrict__ row = a.nl + c * int64_t(a.cap);
       const bool dT = a.simple ? (P.eq_diff && (P.ddw == esd_2nw_ds || P.ddw == esd_2nw_sd))
                                : (P.eq_diff || P.eq_fld);
       const R ih = R(1.0 / ha);
+      const R ih_lo = R(1.0 / ha - double(ih));
       const double Ka = P.wCv / ipow<DIM + 1>(ha);  // wCv / h^(d+1)
       Acc<R> sw, so;
       sw.init();
@@ -197,8 +238,8 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
       g[0].init(); g[1].init(); g[2].init();
       bool bad = false;
       const R rta = R(ta), rrhoa = R(rhoa), roma = R(oma);
-      for (int l = 0; l < n; ++l) {
-        const int64_t j = a.nl[int64_t(l) * a.nc + c];
+      for (int l = lane; l < n; l += G) {
+        const int64_t j = row[l];
         R mj;
         const PairPos<R> pj = PosAccess<R>::load(pb, j, mj);
         R dx, dy, dz;
@@ -210,7 +251,8 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
         const R q = r * ih;
         bad |= !(q >= R(0));
         R f, df;
-        kshape_f_df<K, R>(q, f, df);
+        if constexpr (sizeof(R) == 4) kshape_f_df_res<K>(q, fmaf(r, ih, -q) + r * ih_lo, f, df);
+        else kshape_f_df<K, R>(q, f, df);
         sw.add(mj * f);
         if (!a.simple) so.add(mj * (R(DIM) * f + q * df));
         if (dT) {
@@ -243,32 +285,39 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
           if (DIM == 3) g[2].add(coef * dz);
         }
       }
-      pairs += n;
-      sweeps = 1;
+      pairs = (lane == 0) ? n : 0;
+      sweeps = (lane == 0) ? 1 : 0;
       if (bad) raise_status(a.status, (ha > 0.0) ? SPH_ERR_Q_NAN : SPH_ERR_Q_NEG);
+      const double swt = group_sum<G>(sw.dval(), gmask);
+      const double sot = group_sum<G>(so.dval(), gmask);
+      const double g0 = group_sum<G>(g[0].dval(), gmask);
+      const double g1 = group_sum<G>(g[1].dval(), gmask);
+      const double g2 = group_sum<G>(g[2].dval(), gmask);
       R f0, df0;
       kshape_f_df<K, R>(R(0), f0, df0);
       const double ihd = 1.0 / ipow<DIM>(ha);
-      const double wsum = P.wCv * ihd * (a.mref * sw.dval() + ma * double(f0));
-      cols[es_dtdx * ld + p] = a.mref * g[0].dval();
-      cols[es_dtdy * ld + p] = a.mref * g[1].dval();
-      cols[es_dtdz * ld + p] = a.mref * g[2].dval();
-      if (a.simple) {
-        // circuit1.f90:293-301
-        const double hnew = P.hfac * pow(ma / wsum, 1. / DIM);
-        a.dkp1[p] = wsum;
-        a.hkp1[p] = hnew;
-        a.okp1[p] = 1.;
-      } else {
-        const double osum = -P.wCv * ihd / ha * (a.mref * so.dval() + ma * (DIM * double(f0)));
-        double rho, om, hn;
-        const double eps = newton_update<DIM>(ha, ha0, ma, P.hfac, wsum, osum, rho, om, hn);
-        if (hn <= 0.) raise_status(a.status, SPH_ERR_H_NEG);
-        a.eps[p] = eps;
-        a.dkp1[p] = rho;
-        a.okp1[p] = om;
-        a.hkp1[p] = hn;
-        active_left = eps > P.tol ? 1 : 0;
+      const double wsum = P.wCv * ihd * (a.mref * swt + ma * double(f0));
+      if (lane == 0) {
+        cols[es_dtdx * ld + p] = a.mref * g0;
+        cols[es_dtdy * ld + p] = a.mref * g1;
+        cols[es_dtdz * ld + p] = a.mref * g2;
+        if (a.simple) {
+          // circuit1.f90:293-301
+          const double hnew = P.hfac * pow(ma / wsum, 1. / DIM);
+          a.dkp1[p] = wsum;
+          a.hkp1[p] = hnew;
+          a.okp1[p] = 1.;
+        } else {
+          const double osum = -P.wCv * ihd / ha * (a.mref * sot + ma * (DIM * double(f0)));
+          double rho, om, hn;
+          const double eps = newton_update<DIM>(ha, ha0, ma, P.hfac, wsum, osum, rho, om, hn);
+          if (hn <= 0.) raise_status(a.status, SPH_ERR_H_NEG);
+          a.eps[p] = eps;
+          a.dkp1[p] = rho;
+          a.okp1[p] = om;
+          a.hkp1[p] = hn;
+          active_left = eps > P.tol ? 1 : 0;
+        }
       }
     }
   }
@@ -314,13 +363,23 @@ __global__ void k_c1_finalize(int64_t nrows, int64_t nreal, double* __restrict__
 }
 
 template <int K, int DIM, class R>
-void dispatch_newton(const C1Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
-  k_c1_newton<K, DIM, R><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
+void dispatch_newton(int G, const C1Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
+  switch (G) {
+    case 4: k_c1_newton<K, DIM, R, 4><<<nblocks(a.nc * 4), TPB, 0, s>>>(a, pb, P); break;
+    case 8: k_c1_newton<K, DIM, R, 8><<<nblocks(a.nc * 8), TPB, 0, s>>>(a, pb, P); break;
+    case 16: k_c1_newton<K, DIM, R, 16><<<nblocks(a.nc * 16), TPB, 0, s>>>(a, pb, P); break;
+    default: k_c1_newton<K, DIM, R, 32><<<nblocks(a.nc * 32), TPB, 0, s>>>(a, pb, P); break;
+  }
   note_launch();
 }
 template <int K, int DIM, class R>
-void dispatch_sweep(const C1Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
-  k_c1_sweep<K, DIM, R><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
+void dispatch_sweep(int G, const C1Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
+  switch (G) {
+    case 4: k_c1_sweep<K, DIM, R, 4><<<nblocks(a.nc * 4), TPB, 0, s>>>(a, pb, P); break;
+    case 8: k_c1_sweep<K, DIM, R, 8><<<nblocks(a.nc * 8), TPB, 0, s>>>(a, pb, P); break;
+    case 16: k_c1_sweep<K, DIM, R, 16><<<nblocks(a.nc * 16), TPB, 0, s>>>(a, pb, P); break;
+    default: k_c1_sweep<K, DIM, R, 32><<<nblocks(a.nc * 32), TPB, 0, s>>>(a, pb, P); break;
+  }
   note_launch();
 }
 
@@ -328,8 +387,8 @@ void dispatch_sweep(const C1Args& a, const PackBufs& pb, const Params& P, cudaSt
   template <int K, int DIM>                                                          \
   void FN##_prec(int prec, const C1Args& a, const PackBufs& pb, const Params& P,    \
                  cudaStream_t s) {                                                   \
-    if (prec == SPH_PREC_FP64) FN<K, DIM, double>(a, pb, P, s);                      \
-    else FN<K, DIM, float>(a, pb, P, s);                                             \
+    if (prec == SPH_PREC_FP64) FN<K, DIM, double>(a.G, a, pb, P, s);                 \
+    else FN<K, DIM, float>(a.G, a, pb, P, s);                                        \
   }                                                                                  \
   template <int K>                                                                   \
   void FN##_dim(int prec, int dim, const C1Args& a, const PackBufs& pb,             \

@@ -85,10 +85,23 @@ __device__ __forceinline__ R fld_coef(R gnorm, R kappa, R rho, R T, R& lambda) {
   return R(kLightspeed) * lambda / kappa / rho;
 }
 
-template <int K, int DIM, class R, bool GENERAL>
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned gmask) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+  return v;
+}
+
+// G lanes per centre: lane l takes neighbours l, l+G, ... of the centre's
+// list row; per-lane two-sum partials are added over the group in FP64 and
+// lane 0 stores the result.
+template <int K, int DIM, class R, bool GENERAL, int G>
 __global__ void __launch_bounds__(TPB)
 k_c2(C2Args a, PackBufs pb, Params P) {
-  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
+  const int lane = threadIdx.x & (G - 1);
+  const int wl = threadIdx.x & 31;
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (wl & ~(G - 1)));
   unsigned long long pairs = 0;
   if (c < a.nc) {
     const int64_t k = a.centre_k[c];
@@ -130,7 +143,8 @@ k_c2(C2Args a, PackBufs pb, Params P) {
           R gn = my_sqrt<R>(AX.gx * AX.gx + AX.gy * AX.gy + AX.gz * AX.gz);
           R fd = fld_coef<R>(gn, AX.kappa, A.rho, AX.T, lam);
           kta[0][0] = kta[1][1] = kta[2][2] = fd;
-          cols[es_vfld * ld + p] = double(fd) / ((double(AX.T) * double(A.rho)) / double(gn));
+          if (lane == 0)
+            cols[es_vfld * ld + p] = double(fd) / ((double(AX.T) * double(A.rho)) / double(gn));
         } else if (P.difiso == 1) {
           R dc = R(P.difcond);
           kta[0][0] = kta[1][1] = kta[2][2] = dc;
@@ -150,8 +164,9 @@ k_c2(C2Args a, PackBufs pb, Params P) {
 
     bool bad = false;
     const int n = a.ncnt[c];
-    for (int l = 0; l < n; ++l) {
-      const int64_t j = a.nl[int64_t(l) * a.nc + c];
+    const int32_t* __restrict__ row = a.nl + c * int64_t(a.cap);
+    for (int l = lane; l < n; l += G) {
+      const int64_t j = row[l];
       Part<R> B;
       Loader<R>::hydro(pb, j, B);
       R rab[3];
@@ -184,15 +199,12 @@ k_c2(C2Args a, PackBufs pb, Params P) {
       if (adden) drho.add(mb * ga * vr);  // circuit2.f90:265-267
       R F = R(0);  // dv -= mb * F * r_ab
       if (artts) {
-        // circuit2.f90:294-336
+        // circuit2.f90:294-336; the Monaghan switch dvr < 0 as a clamp
         const R faba = Ka * dfa, fabb = Kb * dfb;
         const R dvr = vr * invr;
-        R qav = R(0), qbv = R(0);
-        if (dvr < R(0)) {
-          const R adv = fabs(dvr);
-          qav = R(-0.5) * A.rho * (alpha * A.c + beta * adv) * dvr;
-          qbv = R(-0.5) * B.rho * (alpha * B.c + beta * adv) * dvr;
-        }
+        const R dneg = dvr < R(0) ? dvr : R(0);
+        const R qav = R(-0.5) * A.rho * (alpha * A.c - beta * dneg) * dneg;
+        const R qbv = R(-0.5) * B.rho * (alpha * B.c - beta * dneg) * dneg;
         F += qav * ga * A.Pi + qbv * gb * B.Pi;
         R qc = R(0);
         if (use_au) {
@@ -269,34 +281,57 @@ k_c2(C2Args a, PackBufs pb, Params P) {
       }
       for (int d = 0; d < DIM; ++d) dv[d].add(-mb * F * rab[d]);
     }
-    pairs = n;
     if (bad) raise_status(a.status, SPH_ERR_Q_NAN);
     const double mref = a.mref;
-    cols[es_ax * ld + p] = mref * dv[0].dval();
-    cols[es_ay * ld + p] = mref * dv[1].dval();
-    cols[es_az * ld + p] = mref * dv[2].dval();
-    cols[es_du * ld + p] = mref * du.dval();
-    double dh = 0.;
-    if (adden) {  // circuit2.f90:468-470
-      const double ha = cols[es_h * ld + p];
-      dh = -double(DIM) * ha * double(A.rho) * double(A.Pi) * (mref * drho.dval());
+    const double ax = group_sum<G>(dv[0].dval(), gmask);
+    const double ay = DIM >= 2 || GENERAL ? group_sum<G>(dv[1].dval(), gmask) : 0.0;
+    const double az = DIM == 3 || GENERAL ? group_sum<G>(dv[2].dval(), gmask) : 0.0;
+    const double dus = group_sum<G>(du.dval(), gmask);
+    const double drs = group_sum<G>(drho.dval(), gmask);
+    double dts = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+    if constexpr (GENERAL) {
+      dts = group_sum<G>(ddt.dval(), gmask);
+      b0 = group_sum<G>(db[0].dval(), gmask);
+      b1 = group_sum<G>(db[1].dval(), gmask);
+      b2 = group_sum<G>(db[2].dval(), gmask);
     }
-    cols[es_dh * ld + p] = dh;
-    cols[es_ddt * ld + p] = mref * ddt.dval();
-    cols[es_dbx * ld + p] = mref * db[0].dval();
-    cols[es_dby * ld + p] = mref * db[1].dval();
-    cols[es_dbz * ld + p] = mref * db[2].dval();
+    if (lane == 0) {
+      pairs = n;
+      cols[es_ax * ld + p] = mref * ax;
+      cols[es_ay * ld + p] = mref * ay;
+      cols[es_az * ld + p] = mref * az;
+      cols[es_du * ld + p] = mref * dus;
+      double dh = 0.;
+      if (adden) {  // circuit2.f90:468-470
+        const double ha = cols[es_h * ld + p];
+        dh = -double(DIM) * ha * double(A.rho) * double(A.Pi) * (mref * drs);
+      }
+      cols[es_dh * ld + p] = dh;
+      cols[es_ddt * ld + p] = mref * dts;
+      cols[es_dbx * ld + p] = mref * b0;
+      cols[es_dby * ld + p] = mref * b1;
+      cols[es_dbz * ld + p] = mref * b2;
+    }
   }
   unsigned long long wp = pairs;
   for (int o = 16; o > 0; o >>= 1) wp += __shfl_xor_sync(0xffffffffu, wp, o);
-  if ((threadIdx.x & 31) == 0 && wp) atomicAdd(&a.dcnt[DC_C2_PAIRS], wp);
+  if (wl == 0 && wp) atomicAdd(&a.dcnt[DC_C2_PAIRS], wp);
 }
 
+template <int K, int DIM, class R, bool GEN>
+void run_g(const C2Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
+  switch (a.G) {
+    case 4: k_c2<K, DIM, R, GEN, 4><<<nblocks(a.nc * 4), TPB, 0, s>>>(a, pb, P); break;
+    case 8: k_c2<K, DIM, R, GEN, 8><<<nblocks(a.nc * 8), TPB, 0, s>>>(a, pb, P); break;
+    case 16: k_c2<K, DIM, R, GEN, 16><<<nblocks(a.nc * 16), TPB, 0, s>>>(a, pb, P); break;
+    default: k_c2<K, DIM, R, GEN, 32><<<nblocks(a.nc * 32), TPB, 0, s>>>(a, pb, P); break;
+  }
+}
 template <int K, int DIM, class R>
 void run(const C2Args& a, const PackBufs& pb, const Params& P, cudaStream_t s) {
   const bool general = P.eq_diff || P.eq_magneto;
-  if (general) k_c2<K, DIM, R, true><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
-  else k_c2<K, DIM, R, false><<<nblocks(a.nc), TPB, 0, s>>>(a, pb, P);
+  if (general) run_g<K, DIM, R, true>(a, pb, P, s);
+  else run_g<K, DIM, R, false>(a, pb, P, s);
   note_launch();
 }
 template <int K, int DIM>

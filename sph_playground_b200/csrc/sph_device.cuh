@@ -98,6 +98,48 @@ __device__ __forceinline__ void kshape_all(R q, R& f, R& df, R& ddf) {
   }
 }
 
+// FP32 f(q) that follows q below FP32 resolution, for the Newton iteration on
+// h.  q_lo is the rounding residual of q = r/h.  Each clamped piece
+// t_k = c_k - q is itself rounded; its exact residual (Fast2Sum, c_k >= q on
+// the live pieces) and q_lo enter f to first order through the piece's own
+// derivative.  The density sum then changes smoothly with h instead of in
+// steps of one FP32 ulp of q or t_k, so the Newton iterates settle.
+template <int K>
+__device__ __forceinline__ void kshape_f_df_res(float q, float q_lo, float& f, float& df) {
+  if constexpr (K == KM6 || K == KM4) {
+    constexpr int NP = (K == KM6) ? 3 : 2;
+    const float cs[3] = {K == KM6 ? 3.f : 2.f, K == KM6 ? 2.f : 1.f, 1.f};
+    const float as[3] = {K == KM6 ? 1.f : 0.25f, K == KM6 ? -6.f : -1.f, 15.f};
+    f = 0.f;
+    df = 0.f;
+    float corr = 0.f;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      float th = cs[k] - q;
+      float tl = (-q) - (th - cs[k]);
+      if (!(th > 0.f)) { th = 0.f; tl = 0.f; }
+      float s = th * th;
+      float d;
+      if constexpr (K == KM6) {
+        float q4 = s * s;
+        f = fmaf(as[k], q4 * th, f);
+        d = (-5.f * as[k]) * q4;  // d f_k / d q
+      } else {
+        f = fmaf(as[k], s * th, f);
+        d = (-3.f * as[k]) * s;
+      }
+      df += d;
+      corr = fmaf(-d, tl - q_lo, corr);
+    }
+    f += corr;
+  } else {
+    float e = expf(-q * q);
+    f = e;
+    df = -2.f * e * q;
+    f = fmaf(df, q_lo, f);
+  }
+}
+
 template <int K, class R>
 __device__ __forceinline__ R kshape_f(R q) {
   R f, df;

@@ -140,9 +140,9 @@ struct sph_handle {
   DevBuf gcount, goff, gx, gy, gz, gsrc, gcode, scan_tmp;
   int64_t nghost = 0;
   // sort + cells
-  DevBuf keys, keys_alt, vals, vals_alt, sort_tmp, cstart, cend;
+  DevBuf keys, keys_alt, vals, vals_alt, sort_tmp, cstart;
   // sorted arrays
-  DevBuf sx, sy, sz, ssrc, cflag, cpos, centre_k, centre_p;
+  DevBuf sx, sy, sz, s32, ssrc, cflag, cpos, centre_k, centre_p;
   DevBuf hk_s, dk_s, ok_s;
   DevBuf pk[11], qk[6];
   // neighbours
@@ -241,6 +241,15 @@ struct sph_handle {
     }
   }
   int dim() const { return ival(ec_dim); }
+  static int lanes_ok(int g) { return (g == 4 || g == 8 || g == 16 || g == 32) ? g : 0; }
+  int lanes_search() const {
+    int g = lanes_ok(int(st[SPH_P_LANES_SEARCH]));
+    return g ? g : (dim() == 3 ? 16 : 8);
+  }
+  int lanes_pair() const {
+    int g = lanes_ok(int(st[SPH_P_LANES_PAIR]));
+    return g ? g : (dim() == 3 ? 8 : 4);
+  }
 
   int params(Params& P) {
     eqset();
@@ -367,6 +376,7 @@ struct sph_handle {
     RC(sx.ensure(sizeof(double) * nall));
     RC(sy.ensure(sizeof(double) * nall));
     RC(sz.ensure(sizeof(double) * nall));
+    RC(s32.ensure(sizeof(float4) * nall));
     RC(ssrc.ensure(sizeof(int32_t) * nall));
     RC(cflag.ensure(sizeof(int32_t) * (nall + 1)));
     RC(cpos.ensure(sizeof(int32_t) * (nall + 1)));
@@ -481,7 +491,7 @@ struct sph_handle {
     if (!(hmin > 0) || !std::isfinite(hmin)) return fail(SPH_ERR_IC_H, "smoothing length <= 0");
     for (int k = 0; k < 3; ++k)
       if (!std::isfinite(lo[k]) || !std::isfinite(hi[k])) return fail(SPH_ERR_Q_NAN, "q is nan");
-    double cf = st[SPH_P_CELL_FACTOR] > 0 ? st[SPH_P_CELL_FACTOR] : 1.0;
+    double cf = st[SPH_P_CELL_FACTOR] > 0 ? st[SPH_P_CELL_FACTOR] : 0.5;
     double L = P.krad * hmin * cf;
     int64_t ncell = 0;
     int n3[3];
@@ -490,21 +500,21 @@ struct sph_handle {
       ncell = 1;
       for (int k = 0; k < 3; ++k) {
         double e = (hi[k] - lo[k]) / L;
-        if (!(e < 1023.0)) { ok = false; break; }
+        if (!(e < 1e9)) { ok = false; break; }
         n3[k] = int(std::floor(e)) + 1;
         ncell *= n3[k];
       }
-      if (ok && ncell <= std::max<int64_t>(8 * nall, 1 << 20)) break;
+      if (ok && ncell <= std::min<int64_t>(std::max<int64_t>(8 * nall, 1 << 20),
+                                           int64_t(1) << 31))
+        break;
       L *= 1.25;
       if (guard > 400) return fail(SPH_ERR_GRID, "cell grid would not fit");
     }
     grid.ox = lo[0]; grid.oy = lo[1]; grid.oz = lo[2];
     grid.L = L; grid.invL = 1.0 / L;
     grid.nx = n3[0]; grid.ny = n3[1]; grid.nz = n3[2];
-    int maxn = std::max(n3[0], std::max(n3[1], n3[2]));
-    int bits = 0;
-    while ((1 << bits) < maxn) ++bits;
-    int end_bit = std::max(1, 3 * bits);
+    int end_bit = 1;
+    while ((int64_t(1) << end_bit) < ncell) ++end_bit;
     // FP32 position packing: one binade [2^E, 2^(E+1)) over the whole extent
     double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
     double sh = 1.0;
@@ -521,16 +531,12 @@ struct sph_handle {
                   nghost, grid, keys.as<uint32_t>(), vals.as<int32_t>(), s);
       sort_pairs(sort_tmp.p, sort_tmp.bytes, keys.as<uint32_t>(), keys_alt.as<uint32_t>(),
                  vals.as<int32_t>(), vals_alt.as<int32_t>(), nall, end_bit, s);
-      RC(cstart.ensure(sizeof(int32_t) * ncell));
-      RC(cend.ensure(sizeof(int32_t) * ncell));
-      CK(cudaMemsetAsync(cstart.p, 0, sizeof(int32_t) * ncell, s));
-      CK(cudaMemsetAsync(cend.p, 0, sizeof(int32_t) * ncell, s));
-      launch_cell_ranges(keys_alt.as<uint32_t>(), nall, grid, cstart.as<int32_t>(),
-                         cend.as<int32_t>(), s);
+      RC(cstart.ensure(sizeof(int32_t) * (ncell + 1)));
+      launch_cell_starts(keys_alt.as<uint32_t>(), nall, ncell, cstart.as<int32_t>(), s);
       launch_sorted_gather(vals_alt.as<int32_t>(), nall, nrows, nreal, cols.as<double>(),
                            gx.as<double>(), gy.as<double>(), gz.as<double>(), gsrc.as<int32_t>(),
                            sx.as<double>(), sy.as<double>(), sz.as<double>(), ssrc.as<int32_t>(),
-                           cflag.as<int32_t>(), nullptr, nullptr, s);
+                           cflag.as<int32_t>(), s32.as<float4>(), pgeom, s);
       CK(cudaMemsetAsync(cflag.as<int32_t>() + nall, 0, sizeof(int32_t), s));
       exclusive_scan(scan_tmp.p, scan_tmp.bytes, cflag.as<int32_t>(), cpos.as<int32_t>(),
                      nall + 1, s);
@@ -539,10 +545,9 @@ struct sph_handle {
     }
     // neighbour lists, grown until every list fits
     if (cap <= 0) {
-      double sp = 1.0, kh = P.krad * P.hfac;
+      double kh = P.krad * P.hfac;
       double est = d == 3 ? 4.0 / 3.0 * kPi * kh * kh * kh : (d == 2 ? kPi * kh * kh : 2 * kh);
-      (void)sp;
-      cap = int(est * 1.5) + 32;
+      cap = int(est * 2.0) + 32;
       if (st[SPH_P_NEIB_CAP] > 0) cap = int(st[SPH_P_NEIB_CAP]);
     }
     for (int attempt = 0; attempt < 4; ++attempt) {
@@ -550,11 +555,11 @@ struct sph_handle {
       RC(nl.ensure(sizeof(int32_t) * size_t(cap) * std::max<int64_t>(nreal, 1)));
       RC(ncnt.ensure(sizeof(int32_t) * std::max<int64_t>(nreal, 1)));
       CK(cudaMemsetAsync(maxcnt.p, 0, sizeof(int32_t), s));
-      launch_neighbours(d, nreal, centre_k.as<int32_t>(), centre_p.as<int32_t>(), sx.as<double>(),
-                        sy.as<double>(), sz.as<double>(), col(es_h), P.krad, grid,
-                        cstart.as<int32_t>(), cend.as<int32_t>(), cap, nl.as<int32_t>(),
-                        ncnt.as<int32_t>(), maxcnt.as<int32_t>(), dcnt.as<unsigned long long>(),
-                        s);
+      launch_neighbours(d, lanes_search(), nreal, centre_k.as<int32_t>(), centre_p.as<int32_t>(),
+                        sx.as<double>(), sy.as<double>(), sz.as<double>(), s32.as<float4>(),
+                        pgeom.shift, col(es_h), P.krad, grid, cstart.as<int32_t>(), cap,
+                        nl.as<int32_t>(), ncnt.as<int32_t>(), maxcnt.as<int32_t>(),
+                        dcnt.as<unsigned long long>(), s);
       CK(cudaMemcpyAsync(h_i32, maxcnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       CK(cudaGetLastError());
@@ -562,7 +567,7 @@ struct sph_handle {
       if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc + 1 > kb.maxneib[d - 1])
         return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
       if (mc <= cap) break;
-      cap = int(mc * 1.15) + 8;
+      cap = int(mc * 1.5) + 16;
       if (attempt == 3) return fail(SPH_ERR_NEIB_OVERFLOW, "neighbour list capacity");
     }
     have_order = true;
@@ -590,6 +595,8 @@ struct sph_handle {
                 sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
     C1Args a{};
     a.nc = nreal;
+    a.cap = cap;
+    a.G = lanes_pair();
     a.centre_k = centre_k.as<int32_t>();
     a.centre_p = centre_p.as<int32_t>();
     a.nl = nl.as<int32_t>();
@@ -655,6 +662,8 @@ struct sph_handle {
                 sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
     C2Args a{};
     a.nc = nreal;
+    a.cap = cap;
+    a.G = lanes_pair();
     a.centre_k = centre_k.as<int32_t>();
     a.centre_p = centre_p.as<int32_t>();
     a.nl = nl.as<int32_t>();
@@ -908,7 +917,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
   h->st[SPH_P_AV_BETA] = 2.;
   h->st[SPH_P_NEWTON_TOL] = 1e-8;
   h->st[SPH_P_NEWTON_MAXITER] = 100;
-  h->st[SPH_P_CELL_FACTOR] = 1.;
+  h->st[SPH_P_CELL_FACTOR] = 0.5;
   h->st[SPH_P_REORDER_EVERY] = 8;
   h->nreal = int64_t(h->st[ec_realpn]);
   h->nfixed = std::max<int64_t>(0, int64_t(h->st[ec_fixedpn]));
@@ -1085,7 +1094,7 @@ int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs, int64_t 
     int64_t c = centre_of_orig[o];
     int64_t base = offsets[o];
     for (int l = 0; l < cnt[c]; ++l) {
-      int64_t q = nl[size_t(l) * nc + c];
+      int64_t q = nl[size_t(c) * h->cap + l];
       int64_t u = sidx[q];
       int64_t rj = og[ssrc[q]];
       int64_t code = u < h->nrows ? 13 : gcode[u - h->nrows];

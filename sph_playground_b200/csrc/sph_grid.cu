@@ -207,25 +207,12 @@ __global__ void k_ghost_write(const double* __restrict__ cols, int64_t ld, int64
 }
 
 // ---- cell keys ----------------------------------------------------------------------
-__device__ __forceinline__ uint32_t spread3(uint32_t x) {
-  x &= 0x3ffu;
-  x = (x | (x << 16)) & 0x030000FFu;
-  x = (x | (x << 8)) & 0x0300F00Fu;
-  x = (x | (x << 4)) & 0x030C30C3u;
-  x = (x | (x << 2)) & 0x09249249u;
-  return x;
-}
-__device__ __forceinline__ uint32_t compact3(uint32_t x) {
-  x &= 0x09249249u;
-  x = (x | (x >> 2)) & 0x030C30C3u;
-  x = (x | (x >> 4)) & 0x0300F00Fu;
-  x = (x | (x >> 8)) & 0x030000FFu;
-  x = (x | (x >> 16)) & 0x000003FFu;
-  return x;
-}
-// Cell index along one axis, clamped to [0, n-1].  NaN and -inf map to 0
-// and +inf to n-1 before any float-to-int conversion happens.
+// Cells are numbered row-major (x fastest), so the cells of one (y, z) row are
+// contiguous in the sorted particle order and a search visits one index range
+// per row instead of one per cell.
 __device__ __forceinline__ int cell_coord(double x, double o, double invL, int n) {
+  // clamped to [0, n-1]; NaN and -inf map to 0 and +inf to n-1 before any
+  // float-to-int conversion happens
   double f = floor((x - o) * invL);
   if (!(f >= 0.0)) return 0;
   if (f >= double(n - 1)) return n - 1;
@@ -248,22 +235,21 @@ __global__ void k_keys(const double* __restrict__ cols, int64_t ld, int64_t nrow
   uint32_t cx = cell_coord(x, g.ox, g.invL, g.nx);
   uint32_t cy = cell_coord(y, g.oy, g.invL, g.ny);
   uint32_t cz = cell_coord(z, g.oz, g.invL, g.nz);
-  keys[u] = spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
+  keys[u] = cx + uint32_t(g.nx) * (cy + uint32_t(g.ny) * cz);
   vals[u] = int32_t(u);
 }
 
-__global__ void k_cell_ranges(const uint32_t* __restrict__ keys, int64_t n, Grid g,
-                              int32_t* __restrict__ cstart, int32_t* __restrict__ cend) {
+// cstart[c] = number of particles in cells before c (ncell + 1 entries), from
+// the sorted keys: each key change fills the empty cells it skips.
+__global__ void k_cell_starts(const uint32_t* __restrict__ keys, int64_t n, int64_t ncell,
+                              int32_t* __restrict__ cstart) {
   int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (k >= n) return;
-  uint32_t key = keys[k];
-  bool first = (k == 0) || keys[k - 1] != key;
-  bool last = (k == n - 1) || keys[k + 1] != key;
-  if (!first && !last) return;
-  int cx = compact3(key), cy = compact3(key >> 1), cz = compact3(key >> 2);
-  int64_t d = cx + int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
-  if (first) cstart[d] = int32_t(k);
-  if (last) cend[d] = int32_t(k + 1);
+  if (k > n) return;
+  int64_t lo, hi;  // cells (lo, hi] start at k
+  if (k == 0) { lo = -1; hi = n > 0 ? int64_t(keys[0]) : ncell; }
+  else if (k == n) { lo = int64_t(keys[n - 1]); hi = ncell; }
+  else { lo = int64_t(keys[k - 1]); hi = int64_t(keys[k]); }
+  for (int64_t c = lo + 1; c <= hi; ++c) cstart[c] = int32_t(k);
 }
 
 // Sorted-order gather of positions and source rows; compaction of centres
@@ -274,20 +260,27 @@ __global__ void k_sorted_gather(const int32_t* __restrict__ sidx, int64_t n, int
                                 const double* __restrict__ gz, const int32_t* __restrict__ gsrc,
                                 double* __restrict__ sx, double* __restrict__ sy,
                                 double* __restrict__ sz, int32_t* __restrict__ ssrc,
-                                int32_t* __restrict__ centre_slot) {
+                                int32_t* __restrict__ centre_slot, float4* __restrict__ s32,
+                                PackGeom pg) {
   int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (k >= n) return;
   int64_t u = sidx[k];
+  double x, y, z;
   if (u < nrows) {
-    sx[k] = cols[es_rx * ld + u]; sy[k] = cols[es_ry * ld + u]; sz[k] = cols[es_rz * ld + u];
+    x = cols[es_rx * ld + u]; y = cols[es_ry * ld + u]; z = cols[es_rz * ld + u];
     ssrc[k] = int32_t(u);
     centre_slot[k] = (u < nreal) ? 1 : 0;
   } else {
     int64_t q = u - nrows;
-    sx[k] = gx[q]; sy[k] = gy[q]; sz[k] = gz[q];
+    x = gx[q]; y = gy[q]; z = gz[q];
     ssrc[k] = gsrc[q];
     centre_slot[k] = 0;
   }
+  sx[k] = x; sy[k] = y; sz[k] = z;
+  // FP32 image of the position, one binade for the whole extent (see PackGeom)
+  s32[k] = make_float4(__double2float_rn((x - pg.ox) + pg.shift),
+                       __double2float_rn((y - pg.oy) + pg.shift),
+                       __double2float_rn((z - pg.oz) + pg.shift), 0.f);
 }
 
 __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __restrict__ flag,
@@ -302,82 +295,122 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
 }
 
 // ---- neighbour search -------------------------------------------------------------------
-// One thread per centre.  Candidates come from the cells that overlap the
-// box [x - R, x + R]; cells whose nearest point lies beyond R are skipped.
+// A group of G lanes serves one centre.  For every (y, z) row of cells that
+// the sphere of radius R = krad*h reaches, the x-extent of the sphere at that
+// row's nearest point selects a run of cells, which is one contiguous range
+// of the sorted particles; the group walks it G candidates at a time
+// (coalesced loads) and appends hits to the centre's list with a ballot, so
+// list writes are contiguous too.
+//
 // Inclusion is the kd-tree's FP64 test, summed x, y, z in order without
 // fused multiply-adds: ((dx*dx + dy*dy) + dz*dz) <= (krad*h)^2
 // (kdtree2.f90:1673-1678, neighboursearch.f90:126), self excluded
-// (neighboursearch.f90:190).
-template <int DIM>
+// (neighboursearch.f90:190).  Most candidates are far from the sphere's
+// surface, so a FP32 test on the one-binade position images decides them
+// first: with per-axis image error e = 2^-23 * shift, the FP32 distance differs
+// from the exact one by less than 2 sqrt(3) e R + 3 e^2 (plus FP32 rounding)
+// near the surface, so delta = 8 e / R + 4 (e / R)^2 + 1e-6 bounds it.  Only
+// the candidates with |sd32 - R^2| <= delta R^2 are tested in FP64; the FP64
+// test alone decides membership, so the sets equal the FP64 predicate's.
+template <int DIM, int G>
 __global__ void __launch_bounds__(128)
 k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
              const int32_t* __restrict__ centre_p, const double* __restrict__ sx,
              const double* __restrict__ sy, const double* __restrict__ sz,
-             const double* __restrict__ hcol, double krad, Grid g,
-             const int32_t* __restrict__ cstart, const int32_t* __restrict__ cend, int cap,
+             const float4* __restrict__ s32, double shift, const double* __restrict__ hcol,
+             double krad, Grid g, const int32_t* __restrict__ cstart, int cap,
              int32_t* __restrict__ nl, int32_t* __restrict__ ncnt, int32_t* __restrict__ maxcnt,
              unsigned long long* __restrict__ dcnt) {
-  int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  unsigned int ncand = 0, nfound = 0;
-  if (c < nc) {
+  const int64_t gid = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
+  const int lane = threadIdx.x & (G - 1);
+  const int wl = threadIdx.x & 31;
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (wl & ~(G - 1)));
+  const unsigned below = (1u << wl) - 1u;
+  unsigned int ncand = 0, nexact = 0, nfound = 0;
+  if (gid < nc) {
+    const int64_t c = gid;
     const int32_t k = centre_k[c];
     const int32_t p = centre_p[c];
     const double xi = sx[k], yi = sy[k], zi = sz[k];
+    const float4 pi = s32[k];
     const double kh = __dmul_rn(krad, hcol[p]);
     const double R2 = __dmul_rn(kh, kh);
     const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
+    const double er = (shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
+    const double delta = 8.0 * er + 4.0 * er * er + 1e-6;
+    const float lo_thr = float(R2 * (1.0 - delta));
+    const float hi_thr = float(R2 * (1.0 + delta));
     const double tolc = 1e-9 * g.L;
-    int c0[3], c1[3];
-    const double xs[3] = {xi, yi, zi};
-    const double os[3] = {g.ox, g.oy, g.oz};
-    const int ns[3] = {g.nx, g.ny, g.nz};
-    for (int a = 0; a < 3; ++a) {
-      double sl = fabs(xs[a]) * 1e-15;
-      c0[a] = cell_coord(xs[a] - R - sl, os[a], g.invL, ns[a]);
-      c1[a] = cell_coord(xs[a] + R + sl, os[a], g.invL, ns[a]);
-    }
+    const double slx = fabs(xi) * 1e-15, sly = fabs(yi) * 1e-15, slz = fabs(zi) * 1e-15;
+    const int cy0 = DIM >= 2 ? cell_coord(yi - R - sly, g.oy, g.invL, g.ny) : 0;
+    const int cy1 = DIM >= 2 ? cell_coord(yi + R + sly, g.oy, g.invL, g.ny) : 0;
+    const int cz0 = DIM == 3 ? cell_coord(zi - R - slz, g.oz, g.invL, g.nz) : 0;
+    const int cz1 = DIM == 3 ? cell_coord(zi + R + slz, g.oz, g.invL, g.nz) : 0;
+    const int64_t base = c * int64_t(cap);
     int cnt = 0;
-    for (int cz = c0[2]; cz <= c1[2]; ++cz) {
+    for (int cz = cz0; cz <= cz1; ++cz) {
       double dzc = 0.0;
       if (DIM == 3) {
         double lo = g.oz + cz * g.L - tolc, hi = g.oz + (cz + 1) * g.L + tolc;
         dzc = zi < lo ? lo - zi : (zi > hi ? zi - hi : 0.0);
       }
-      for (int cy = c0[1]; cy <= c1[1]; ++cy) {
+      for (int cy = cy0; cy <= cy1; ++cy) {
         double dyc = 0.0;
         if (DIM >= 2) {
           double lo = g.oy + cy * g.L - tolc, hi = g.oy + (cy + 1) * g.L + tolc;
           dyc = yi < lo ? lo - yi : (yi > hi ? yi - hi : 0.0);
         }
-        for (int cx = c0[0]; cx <= c1[0]; ++cx) {
-          double lo = g.ox + cx * g.L - tolc, hi = g.ox + (cx + 1) * g.L + tolc;
-          double dxc = xi < lo ? lo - xi : (xi > hi ? xi - hi : 0.0);
-          if (dxc * dxc + dyc * dyc + dzc * dzc > R * R) continue;
-          int64_t d = cx + int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
-          int32_t s = cstart[d], e = cend[d];
-          for (int32_t q = s; q < e; ++q) {
+        const double rem = R * R - dyc * dyc - dzc * dzc;
+        if (rem < 0.0) continue;
+        const double w = sqrt(rem) * (1.0 + 1e-9);
+        const int cx0 = cell_coord(xi - w - slx, g.ox, g.invL, g.nx);
+        const int cx1 = cell_coord(xi + w + slx, g.ox, g.invL, g.nx);
+        const int64_t row = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+        const int32_t s = cstart[row + cx0], e = cstart[row + cx1 + 1];
+        for (int32_t q0 = s; q0 < e; q0 += G) {
+          const int32_t q = q0 + lane;
+          bool inside = false;
+          if (q < e) {
             ++ncand;
-            double d0 = __dadd_rn(sx[q], -xi);
-            double d1 = __dadd_rn(sy[q], -yi);
-            double d2 = __dadd_rn(sz[q], -zi);
-            double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
-                                  __dmul_rn(d2, d2));
-            if (sd > R2 || q == k) continue;
-            if (cnt < cap) nl[int64_t(cnt) * nc + c] = q;
-            ++cnt;
+            const float4 pj = s32[q];
+            const float fx = pj.x - pi.x, fy = pj.y - pi.y, fz = pj.z - pi.z;
+            const float sd32 = fx * fx + fy * fy + fz * fz;
+            if (!(sd32 > hi_thr) && q != k) {
+              if (sd32 < lo_thr) {
+                inside = true;
+              } else {
+                ++nexact;
+                double d0 = __dadd_rn(sx[q], -xi);
+                double d1 = __dadd_rn(sy[q], -yi);
+                double d2 = __dadd_rn(sz[q], -zi);
+                double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                      __dmul_rn(d2, d2));
+                inside = !(sd > R2);
+              }
+            }
           }
+          const unsigned bal = __ballot_sync(gmask, inside) & gmask;
+          if (inside) {
+            const int slot = cnt + __popc(bal & below);
+            if (slot < cap) nl[base + slot] = q;
+          }
+          cnt += __popc(bal);
         }
       }
     }
-    ncnt[c] = cnt;
-    nfound = unsigned(cnt);
-    atomicMax(maxcnt, cnt);
+    if (lane == 0) {
+      ncnt[c] = cnt;
+      atomicMax(maxcnt, cnt);
+      nfound = unsigned(cnt);
+    }
   }
   unsigned int wc = __reduce_add_sync(0xffffffffu, ncand);
   unsigned int wf = __reduce_add_sync(0xffffffffu, nfound);
-  if ((threadIdx.x & 31) == 0) {
+  unsigned int we = __reduce_add_sync(0xffffffffu, nexact);
+  if (wl == 0) {
     atomicAdd(&dcnt[DC_CANDIDATES], (unsigned long long)wc);
     atomicAdd(&dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
+    atomicAdd(&dcnt[DC_EXACT_TESTS], (unsigned long long)we);
   }
 }
 
@@ -650,44 +683,63 @@ void launch_keys(const double* cols, int64_t nrows, const double* gx, const doub
                                                  keys, vals);
   note_launch();
 }
-void launch_cell_ranges(const uint32_t* keys, int64_t n, Grid g, int32_t* cstart, int32_t* cend,
+void launch_cell_starts(const uint32_t* keys, int64_t n, int64_t ncell, int32_t* cstart,
                         cudaStream_t s) {
-  k_cell_ranges<<<nblocks(n), TPB, 0, s>>>(keys, n, g, cstart, cend);
+  k_cell_starts<<<nblocks(n + 1), TPB, 0, s>>>(keys, n, ncell, cstart);
   note_launch();
 }
 void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
                           const double* cols, const double* gx, const double* gy,
                           const double* gz, const int32_t* gsrc, double* sx, double* sy,
-                          double* sz, int32_t* ssrc, int32_t* centre_slot, int32_t* centre_k,
-                          int32_t* centre_p, cudaStream_t s) {
-  // centre_slot receives flags first; the exclusive scan of the flags is
-  // written into centre_k's tail scratch by the caller, see sph_engine.cu.
+                          double* sz, int32_t* ssrc, int32_t* centre_slot, float4* s32,
+                          PackGeom pg, cudaStream_t s) {
   k_sorted_gather<<<nblocks(n), TPB, 0, s>>>(sidx, n, nrows, nreal, cols, nrows, gx, gy, gz,
-                                             gsrc, sx, sy, sz, ssrc, centre_slot);
+                                             gsrc, sx, sy, sz, ssrc, centre_slot, s32, pg);
   note_launch();
-  (void)centre_k;
-  (void)centre_p;
 }
 void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
                     int32_t* centre_k, int32_t* centre_p, cudaStream_t s) {
   k_centres<<<nblocks(n), TPB, 0, s>>>(sidx, flag, pos, n, centre_k, centre_p);
   note_launch();
 }
-void launch_neighbours(int dim, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
-                       const double* sx, const double* sy, const double* sz, const double* hcol,
-                       double krad, Grid g, const int32_t* cstart, const int32_t* cend, int cap,
-                       int32_t* nl, int32_t* ncnt, int32_t* maxcnt, unsigned long long* dcnt,
-                       cudaStream_t s) {
+template <int DIM, int G>
+static void neighbours_g(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
+                         const double* sx, const double* sy, const double* sz, const float4* s32,
+                         double shift, const double* hcol, double krad, Grid g,
+                         const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt,
+                         int32_t* maxcnt, unsigned long long* dcnt, cudaStream_t s) {
   const int tpb = 128;
+  k_neighbours<DIM, G><<<nblocks(nc * G, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, s32,
+                                                            shift, hcol, krad, g, cstart, cap, nl,
+                                                            ncnt, maxcnt, dcnt);
+}
+template <int DIM>
+static void neighbours_dim(int G, int64_t nc, const int32_t* ck, const int32_t* cp,
+                           const double* sx, const double* sy, const double* sz, const float4* s32,
+                           double shift, const double* hcol, double krad, Grid g,
+                           const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt,
+                           int32_t* maxcnt, unsigned long long* dcnt, cudaStream_t s) {
+  switch (G) {
+    case 4: neighbours_g<DIM, 4>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
+    case 8: neighbours_g<DIM, 8>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
+    case 16: neighbours_g<DIM, 16>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
+    default: neighbours_g<DIM, 32>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
+  }
+}
+void launch_neighbours(int dim, int G, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
+                       const double* sx, const double* sy, const double* sz, const float4* s32,
+                       double shift, const double* hcol, double krad, Grid g,
+                       const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt, int32_t* maxcnt,
+                       unsigned long long* dcnt, cudaStream_t s) {
   if (dim == 3)
-    k_neighbours<3><<<nblocks(nc, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, hcol, krad,
-                                                     g, cstart, cend, cap, nl, ncnt, maxcnt, dcnt);
+    neighbours_dim<3>(G, nc, centre_k, centre_p, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap,
+                      nl, ncnt, maxcnt, dcnt, s);
   else if (dim == 2)
-    k_neighbours<2><<<nblocks(nc, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, hcol, krad,
-                                                     g, cstart, cend, cap, nl, ncnt, maxcnt, dcnt);
+    neighbours_dim<2>(G, nc, centre_k, centre_p, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap,
+                      nl, ncnt, maxcnt, dcnt, s);
   else
-    k_neighbours<1><<<nblocks(nc, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, hcol, krad,
-                                                     g, cstart, cend, cap, nl, ncnt, maxcnt, dcnt);
+    neighbours_dim<1>(G, nc, centre_k, centre_p, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap,
+                      nl, ncnt, maxcnt, dcnt, s);
   note_launch();
 }
 void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,

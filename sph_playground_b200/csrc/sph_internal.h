@@ -49,7 +49,7 @@ enum RedSlot : int {
 // Device counters (unsigned long long, cumulative).
 enum DevCnt : int {
   DC_NEIB_PAIRS = 0, DC_C1_PAIRS, DC_C2_PAIRS, DC_CANDIDATES,
-  DC_C1_CENTRE_SWEEPS, DC_C1_MAXSWEEPS, DC_TOTAL
+  DC_C1_CENTRE_SWEEPS, DC_C1_MAXSWEEPS, DC_EXACT_TESTS, DC_TOTAL
 };
 
 // Periodic geometry for the image builder (BC.f90:46-68, 196-475).
@@ -82,30 +82,30 @@ void launch_ghost_write(const double* cols, int64_t nrows, BoxGeom g, int dim,
 void launch_keys(const double* cols, int64_t nrows, const double* gx, const double* gy,
                  const double* gz, int64_t nghost, Grid g, uint32_t* keys, int32_t* vals,
                  cudaStream_t s);
-void launch_cell_ranges(const uint32_t* keys, int64_t n, Grid g, int32_t* cstart,
-                        int32_t* cend, cudaStream_t s);
+void launch_cell_starts(const uint32_t* keys, int64_t n, int64_t ncell, int32_t* cstart,
+                        cudaStream_t s);
+struct PackGeom {
+  double ox, oy, oz;  // origin subtracted before the binade shift
+  double shift;       // 2^E with every (x - origin) in [0, 2^E)
+  double mref;        // mass scale (packed m = m / mref)
+};
 void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
                           const double* cols, const double* gx, const double* gy,
                           const double* gz, const int32_t* gsrc, double* sx, double* sy,
-                          double* sz, int32_t* ssrc, int32_t* centre_slot,
-                          int32_t* centre_k, int32_t* centre_p, cudaStream_t s);
+                          double* sz, int32_t* ssrc, int32_t* centre_slot, float4* s32,
+                          PackGeom pg, cudaStream_t s);
 void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
                     int32_t* centre_k, int32_t* centre_p, cudaStream_t s);
-void launch_neighbours(int dim, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
-                       const double* sx, const double* sy, const double* sz,
-                       const double* hcol, double krad, Grid g, const int32_t* cstart,
-                       const int32_t* cend, int cap, int32_t* nl, int32_t* ncnt,
-                       int32_t* maxcnt, unsigned long long* dcnt, cudaStream_t s);
+void launch_neighbours(int dim, int G, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
+                       const double* sx, const double* sy, const double* sz, const float4* s32,
+                       double shift, const double* hcol, double krad, Grid g,
+                       const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt, int32_t* maxcnt,
+                       unsigned long long* dcnt, cudaStream_t s);
 // pack groups
 enum PackGroup : int { PACK_POS = 1, PACK_HYDRO = 2, PACK_EXTRA = 4 };
 struct PackBufs {
   double2* p[11];
   float4* q[6];
-};
-struct PackGeom {
-  double ox, oy, oz;  // origin subtracted before the binade shift
-  double shift;       // 2^E
-  double mref;        // mass scale (packed m = m / mref)
 };
 void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
                  const double* sy, const double* sz, const double* cols, int64_t ld,
@@ -139,6 +139,8 @@ void exclusive_scan(void* tmp, size_t tmp_bytes, const int32_t* in, int32_t* out
 // ---- circuit1 (sph_circuit1.cu) ---------------------------------------------------
 struct C1Args {
   int64_t nc;
+  int cap;  // neighbour slots per centre (row length of nl)
+  int G;    // lanes per centre
   const int32_t* centre_k;
   const int32_t* centre_p;
   const int32_t* nl;
@@ -173,6 +175,8 @@ void launch_c1_snapshot(int64_t n, const int32_t* ssrc, const double* hkp1,
 // ---- circuit2 (sph_circuit2.cu) ---------------------------------------------------
 struct C2Args {
   int64_t nc;
+  int cap;
+  int G;
   const int32_t* centre_k;
   const int32_t* centre_p;
   const int32_t* nl;

@@ -21,12 +21,13 @@ pytestmark = pytest.mark.gpu
 FP64, FP32 = abi.PREC_FP64, abi.PREC_FP32_COMP
 TOL = {FP64: dict(part=1e-12, field=1e-12), FP32: dict(part=1e-6, field=1e-5)}
 # The Jacobi path stores the temperature gradient of each particle's last
-# active sweep (circuit1.f90:207), so it depends on the sweep count.  With
-# the default tolerance 1e-8 the third Newton iterate of these lattices lands
-# at eps ~ 1e-8, where FP32 rounding can add or drop a sweep; the FP32 runs of
-# the diffusion cases therefore use the 1e-6 tolerance of the FP32-vs-FP64
-# density workload, at which both sides take the same sweeps.
-JACOBI_TOL = {FP64: 1e-8, FP32: 1e-6}
+# active sweep (circuit1.f90:207), so it depends on how many sweeps the
+# particle took, a decision made by comparing eps with the tolerance.  FP32
+# sums move eps by ~1e-9, which flips that decision for the few particles
+# whose eps lies that close to the tolerance; the FP32 runs of the diffusion
+# cases therefore cap the sweeps at 2 on both sides (every particle is still
+# active after the first sweep), which tests the pair arithmetic itself.
+JACOBI = {FP64: {}, FP32: {abi.P_NEWTON_MAXITER: 2}}
 
 
 def compare(ref, got, prec, part_fields=(), field_fields=()):
@@ -81,7 +82,7 @@ def test_sod_shock12_iterate(oracle_lib, engine_lib, cuda_ok, prec):
 @pytest.mark.parametrize("prec", [FP64, FP32])
 def test_diffusion_iterate(oracle_lib, engine_lib, cuda_ok, ddw, full, prec):
     st, store = ic.diffusion2d(24, ddw=ddw, full_tensor=full)
-    params = {abi.P_FULL_TENSOR: 1.0 if full else 0.0, abi.P_NEWTON_TOL: JACOBI_TOL[prec]}
+    params = {abi.P_FULL_TENSOR: 1.0 if full else 0.0, **JACOBI[prec]}
     ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate", params)
     got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate", params)
     assert neighbour_sets_equal(nb_got, nb_ref)
@@ -125,7 +126,7 @@ def _mhd_case(seed=7, n=20):
 @pytest.mark.parametrize("prec", [FP64, FP32])
 def test_mhd_iterate(oracle_lib, engine_lib, cuda_ok, prec):
     st, store = _mhd_case()
-    params = {abi.P_NEWTON_TOL: JACOBI_TOL[prec]}
+    params = dict(JACOBI[prec])
     ref, _, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate", params)
     got, _, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate", params)
     bad = compare(ref, got, prec, part_fields=("den", "h"),
@@ -141,7 +142,7 @@ def test_fld_iterate(oracle_lib, engine_lib, cuda_ok, prec):
     ic.set_state(st, "eqonsts", 0.0)
     store[:, COL["t"]] = 1.0 + 0.2 * np.sin(2 * np.pi * store[:, 0]) * np.cos(2 * np.pi * store[:, 1])
     store[:, COL["kappa"]] = 1e9
-    params = {abi.P_NEWTON_TOL: JACOBI_TOL[prec]}
+    params = dict(JACOBI[prec])
     ref, _, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate", params)
     got, _, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate", params)
     bad = compare(ref, got, prec, part_fields=("den", "h"),
@@ -182,7 +183,7 @@ def test_sedov_steps(oracle_lib, engine_lib, cuda_ok, prec):
 @pytest.mark.parametrize("prec", [FP64, FP32])
 def test_sts_steps(oracle_lib, engine_lib, cuda_ok, prec):
     st, store = ic.diffusion2d(16, ddw="2nw_ds", sts_stages=4, tfinish=1.0)
-    params = {abi.P_NEWTON_TOL: JACOBI_TOL[prec]}
+    params = dict(JACOBI[prec])
     ref, _, cref, sref = run_pass(oracle_lib, st, store, "m6", FP64, "steps", params, steps=2)
     got, _, cgot, sgot = run_pass(engine_lib, st, store, "m6", prec, "steps", params, steps=2)
     assert cgot["iterates"] == cref["iterates"]
