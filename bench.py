@@ -282,6 +282,10 @@ def main():
         e6, ms6, cnt6, tm6, _ = run(abi.PREC_FP64)
         e6.close()
         fp64 = {"value": ws * N * args.steps / (ms6 * 1e-3), "ms_per_step": ms6 / args.steps,
+                "work_per_step": {"c1_pairs": cnt6["c1_pairs"] / args.steps,
+                                  "c1_max_sweeps": cnt6["c1_sweeps"], "neib_max": cnt6["neib_max"],
+                                  "searches": cnt6["searches"] / args.steps,
+                                  "candidates": cnt6["candidates"] / args.steps},
                 "phases_ms_per_step": {k: v / args.steps for k, v in tm6.items()},
                 "peak_fp64_tflops": peak64 / 1e12}
 
@@ -313,6 +317,9 @@ def main():
                               "c1_pairs": cnt["c1_pairs"] / args.steps,
                               "c2_pairs": cnt["c2_pairs"] / args.steps,
                               "c1_max_sweeps": cnt["c1_sweeps"],
+                              "neib_max": cnt["neib_max"],
+                              "searches": cnt["searches"] / args.steps,
+                              "exact_tests": cnt["exact_tests"] / args.steps,
                               "candidates": cnt["candidates"] / args.steps},
             "fp64": fp64,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,

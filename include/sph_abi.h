@@ -104,7 +104,11 @@ extern "C" {
 #define SPH_CNT_CENTRES         8 /* real centres processed (sum)             */
 #define SPH_CNT_C1_CENTRE_SWEEPS 9 /* sum over particles of their sweeps      */
 #define SPH_CNT_LAUNCHES      10 /* kernels of this library launched         */
-#define SPH_CNT_TOTAL          11
+#define SPH_CNT_NEIB_MAX      11 /* longest neighbour list of the last search */
+#define SPH_CNT_SEARCHES      12 /* neighbour-search launches (incl. re-runs
+                                    after a list outgrew its slots)          */
+#define SPH_CNT_EXACT_TESTS   13 /* candidates decided by the FP64 test      */
+#define SPH_CNT_TOTAL          14
 
 /* ---- per-kernel timers (sph_get_timers, milliseconds, cumulative) ------- */
 #define SPH_T_PREDICT    0

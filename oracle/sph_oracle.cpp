@@ -572,6 +572,12 @@ struct Oracle {
     for (int64_t i = 0; i < realpn; ++i)
       std::copy(lists[i].begin(), lists[i].end(), nidx.begin() + noff[i]);
     cnt[SPH_CNT_NEIB_PAIRS] += noff[realpn];
+    cnt[SPH_CNT_SEARCHES]++;
+    {
+      int64_t mx = 0;
+      for (int64_t i = 0; i < realpn; ++i) mx = std::max(mx, noff[i + 1] - noff[i]);
+      cnt[SPH_CNT_NEIB_MAX] = mx;
+    }
     cnt[SPH_CNT_CANDIDATES] += cand;
     cnt[SPH_CNT_GHOSTS] = periodpn;
     timers[SPH_T_NEIGHBOURS] += 1e3 * (omp_get_wtime() - t0);

@@ -44,7 +44,8 @@ P_LANES_PAIR = 61
 
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",
-            "c1_centre_sweeps", "launches"]
+            "c1_centre_sweeps", "launches", "neib_max", "searches",
+            "exact_tests"]
 TIMERS = ["predict", "ghosts", "sort", "neighbours", "circuit1", "circuit2",
           "correct", "timestep", "sts", "step"]
 

@@ -54,9 +54,7 @@ template <> struct PosAccess<float> {
   }
 };
 
-template <class R> __device__ __forceinline__ R rsq(R x);
-template <> __device__ __forceinline__ double rsq<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float rsq<float>(float x) { return sqrtf(x); }
+template <class R> __device__ __forceinline__ R rsq(R x) { return fsqrt<R>(x); }
 
 // One Newton update from the summed density and dW/dh terms
 // (circuit1.f90:191-206).  Returns eps; writes rho, Omega, h_new.
@@ -258,13 +256,13 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
         if (dT) {
           const R tb = PosAccess<R>::temp(pb, j);
           // nabla W_a = wCv f'(q_a) r_ab / (h_a^(d+1) r)   (kernel.f90:189-197)
-          const R ga = R(Ka) * df / r;
+          const R ga = fdiv<R>(R(Ka) * df, r);
           R coef;
           if (P.ddw == esd_2nw_sd) {
             const double hb = a.hk_s[j], rhob = a.dk_s[j], omb = a.ok_s[j];
-            const R qb = r / R(hb);
+            const R qb = r * R(1.0 / hb);
             const R dfb = kshape_df<K, R>(qb);
-            const R gb = R(P.wCv / ipow<DIM + 1>(hb)) * dfb / r;
+            const R gb = fdiv<R>(R(P.wCv / ipow<DIM + 1>(hb)) * dfb, r);
             R ca, cb;
             if (a.simple) {  // circuit1.f90:289
               ca = rta / rrhoa / rrhoa;

@@ -134,7 +134,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
       R b2 = AX.bx * AX.bx + AX.by * AX.by + AX.bz * AX.bz;
       halfB2a = R(0.5) * b2;
       if (b2 != R(0)) {
-        R ib = R(1) / my_sqrt<R>(b2);
+        R ib = frsqrt<R>(b2);
         uba[0] = AX.bx * ib; uba[1] = AX.by * ib; uba[2] = AX.bz * ib;
       }
       if (P.eq_diff) {
@@ -174,8 +174,8 @@ k_c2(C2Args a, PackBufs pb, Params P) {
       R r2 = rab[0] * rab[0];
       if (DIM >= 2) r2 += rab[1] * rab[1];
       if (DIM == 3) r2 += rab[2] * rab[2];
-      const R r = my_sqrt<R>(r2);
-      const R invr = R(1) / r;
+      const R invr = frsqrt<R>(r2);
+      const R r = r2 * invr;
       const R vab[3] = {A.vx - B.vx, A.vy - B.vy, A.vz - B.vz};
       R vr = vab[0] * rab[0];
       if (DIM >= 2) vr += vab[1] * rab[1];
@@ -208,7 +208,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         F += qav * ga * A.Pi + qbv * gb * B.Pi;
         R qc = R(0);
         if (use_au) {
-          const R vsigu = my_sqrt<R>(fabs(A.P - B.P) / (R(0.5) * (A.rho + B.rho)));
+          const R vsigu = fsqrt<R>(fdiv<R>(fabs(A.P - B.P), R(0.5) * (A.rho + B.rho)));
           qc = au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + fabb * B.rho * B.Pi));
         }
         du.add(mb * (dvr * qav * faba * rPiA + qc));
@@ -232,7 +232,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
           } else if (P.difiso == 0) {
             R b2 = BX.bx * BX.bx + BX.by * BX.by + BX.bz * BX.bz;
             if (b2 != R(0)) {  // a zero B_b keeps the previous unit vector (:220-224)
-              R ib = R(1) / my_sqrt<R>(b2);
+              R ib = frsqrt<R>(b2);
               ubb[0] = BX.bx * ib; ubb[1] = BX.by * ib; ubb[2] = BX.bz * ib;
             }
             aniso_tensor<R>(R(P.difcond), ubb, P.full_tensor, ktb);
@@ -245,7 +245,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
               tr += R(0.5) * (kta[x][x] + ktb[x][x]);
               for (int y = 0; y < DIM; ++y) rr += R(0.5) * (kta[x][y] + ktb[x][y]) * rab[x] * rab[y];
             }
-            rr = rr / r2;
+            rr = rr * (invr * invr);
             R contr;
             if (ddw == esd_n2w) {
               contr = Ka * A.invh * ddfa * rr + ga * (tr - rr);
@@ -253,7 +253,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
               const R f2 = (ddw == esd_fab) ? -ga : R(0.5) * R(P.fwc) * Ka * A.invh * fa;
               contr = f2 * (R(DIM + 2) * rr - tr);
             }
-            ddt.add(mb / B.rho / A.rho * (BX.T * B.rho - AX.T * A.rho) * contr);
+            ddt.add(fdiv<R>(mb, B.rho * A.rho) * (BX.T * B.rho - AX.T * A.rho) * contr);
           } else {
             R kgb[3];
             const R gb3[3] = {BX.gx, BX.gy, BX.gz};

@@ -147,6 +147,21 @@ __device__ __forceinline__ R kshape_f(R q) {
   return f;
 }
 
+// Reciprocal square root, square root and division of the pair arithmetic.
+// FP64 keeps IEEE operations (the parity path); FP32 uses the MUFU
+// approximations (about 2 ulp), inside the FP32 path's error budget.
+template <class R> __device__ __forceinline__ R frsqrt(R x);
+template <> __device__ __forceinline__ double frsqrt<double>(double x) { return 1.0 / sqrt(x); }
+template <> __device__ __forceinline__ float frsqrt<float>(float x) { return rsqrtf(x); }
+template <class R> __device__ __forceinline__ R fsqrt(R x);
+template <> __device__ __forceinline__ double fsqrt<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float fsqrt<float>(float x) {
+  return x > 0.f ? x * rsqrtf(x) : 0.f;
+}
+template <class R> __device__ __forceinline__ R fdiv(R a, R b);
+template <> __device__ __forceinline__ double fdiv<double>(double a, double b) { return a / b; }
+template <> __device__ __forceinline__ float fdiv<float>(float a, float b) { return __fdividef(a, b); }
+
 // h^n for small non-negative n (the reference's h**dim, h**(dim+2)).
 template <int N, class R>
 __device__ __forceinline__ R ipow(R x) {

@@ -564,6 +564,8 @@ struct sph_handle {
       CK(cudaStreamSynchronize(s));
       CK(cudaGetLastError());
       int mc = h_i32[0];
+      cnt_host[SPH_CNT_NEIB_MAX] = mc;
+      cnt_host[SPH_CNT_SEARCHES]++;
       if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc + 1 > kb.maxneib[d - 1])
         return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
       if (mc <= cap) break;
@@ -1119,6 +1121,7 @@ int sph_get_counters(sph_handle* h, int64_t* out, int n) {
   all[SPH_CNT_CANDIDATES] = int64_t(d[DC_CANDIDATES]);
   all[SPH_CNT_C1_CENTRE_SWEEPS] = int64_t(d[DC_C1_CENTRE_SWEEPS]);
   all[SPH_CNT_LAUNCHES] = int64_t(launches_so_far() - h->launch_base);
+  all[SPH_CNT_EXACT_TESTS] = int64_t(d[DC_EXACT_TESTS]);
   for (int k = 0; k < n && k < SPH_CNT_TOTAL; ++k) out[k] = all[k];
   return SPH_OK;
 }

@@ -340,31 +340,37 @@ k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
     const double delta = 8.0 * er + 4.0 * er * er + 1e-6;
     const float lo_thr = float(R2 * (1.0 - delta));
     const float hi_thr = float(R2 * (1.0 + delta));
-    const double tolc = 1e-9 * g.L;
-    const double slx = fabs(xi) * 1e-15, sly = fabs(yi) * 1e-15, slz = fabs(zi) * 1e-15;
-    const int cy0 = DIM >= 2 ? cell_coord(yi - R - sly, g.oy, g.invL, g.ny) : 0;
-    const int cy1 = DIM >= 2 ? cell_coord(yi + R + sly, g.oy, g.invL, g.ny) : 0;
-    const int cz0 = DIM == 3 ? cell_coord(zi - R - slz, g.oz, g.invL, g.nz) : 0;
-    const int cz1 = DIM == 3 ? cell_coord(zi + R + slz, g.oz, g.invL, g.nz) : 0;
+    // Row selection in cell units and FP32: every quantity is widened by a
+    // margin far above its rounding, so the selected cells are a superset of
+    // the ones the sphere touches; membership is decided per candidate below.
+    const float ux = float((xi - g.ox) * g.invL), uy = float((yi - g.oy) * g.invL),
+                uz = float((zi - g.oz) * g.invL);
+    const float mrg = 1e-3f + 1e-6f * (fabsf(ux) + fabsf(uy) + fabsf(uz));
+    const float rc = float(R * g.invL) * (1.f + 1e-5f) + mrg;
+    const float rc2 = rc * rc;
+    auto clampc = [](float v, int n) {
+      float f = floorf(v);
+      if (!(f >= 0.f)) return 0;
+      if (f >= float(n - 1)) return n - 1;
+      return int(f);
+    };
+    const int cy0 = DIM >= 2 ? clampc(uy - rc, g.ny) : 0;
+    const int cy1 = DIM >= 2 ? clampc(uy + rc, g.ny) : 0;
+    const int cz0 = DIM == 3 ? clampc(uz - rc, g.nz) : 0;
+    const int cz1 = DIM == 3 ? clampc(uz + rc, g.nz) : 0;
     const int64_t base = c * int64_t(cap);
     int cnt = 0;
     for (int cz = cz0; cz <= cz1; ++cz) {
-      double dzc = 0.0;
-      if (DIM == 3) {
-        double lo = g.oz + cz * g.L - tolc, hi = g.oz + (cz + 1) * g.L + tolc;
-        dzc = zi < lo ? lo - zi : (zi > hi ? zi - hi : 0.0);
-      }
+      float dzc = 0.f;
+      if (DIM == 3) dzc = fmaxf(0.f, fmaxf(float(cz) - uz, uz - float(cz + 1)));
       for (int cy = cy0; cy <= cy1; ++cy) {
-        double dyc = 0.0;
-        if (DIM >= 2) {
-          double lo = g.oy + cy * g.L - tolc, hi = g.oy + (cy + 1) * g.L + tolc;
-          dyc = yi < lo ? lo - yi : (yi > hi ? yi - hi : 0.0);
-        }
-        const double rem = R * R - dyc * dyc - dzc * dzc;
-        if (rem < 0.0) continue;
-        const double w = sqrt(rem) * (1.0 + 1e-9);
-        const int cx0 = cell_coord(xi - w - slx, g.ox, g.invL, g.nx);
-        const int cx1 = cell_coord(xi + w + slx, g.ox, g.invL, g.nx);
+        float dyc = 0.f;
+        if (DIM >= 2) dyc = fmaxf(0.f, fmaxf(float(cy) - uy, uy - float(cy + 1)));
+        const float rem = rc2 - dyc * dyc - dzc * dzc;
+        if (rem < 0.f) continue;
+        const float w = sqrtf(rem) + mrg;
+        const int cx0 = clampc(ux - w, g.nx);
+        const int cx1 = clampc(ux + w, g.nx);
         const int64_t row = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
         const int32_t s = cstart[row + cx0], e = cstart[row + cx1 + 1];
         for (int32_t q0 = s; q0 < e; q0 += G) {
