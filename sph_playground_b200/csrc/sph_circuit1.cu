@@ -117,12 +117,12 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
     const double ma = cols[es_m * ld + p];
     const double ha0 = cols[es_h * ld + p];
     const int n = a.ncnt[c];
-    const int32_t* __restrict__ row = a.nl + c * int64_t(a.cap);
+    const int32_t* __restrict__ row = a.nl + a.rowoff[c];
     const double wcv = P.wCv;
     // kernel shape at q = 0 for the self term (circuit1.f90:191-194)
     R f0, df0;
     kshape_f_df<K, R>(R(0), f0, df0);
-    double ha = ha0, rho = 0., om = 1., hn = ha0;
+    double ha = ha0, rho = 0., om = 1., hn = ha0, eps_prev = 1e300;
     int it = 0;
     bool bad = false;
     for (;;) {
@@ -172,6 +172,13 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
         break;
       }
       if (!(eps > P.tol) || it >= P.maxiter) break;
+      if constexpr (sizeof(R) == 4) {
+        // FP32 sums carry a noise floor of a few 1e-9 in rho, i.e. ~1e-8 in
+        // the Newton step.  Once eps is below 1e-7 and no longer at least
+        // halves, further sweeps move h only within that noise: stop.
+        if (eps < 1e-7 && eps >= 0.5 * eps_prev) break;
+      }
+      eps_prev = eps;
       ha = hn;
     }
     if (bad) raise_status(a.status, (ha > 0.0) ? SPH_ERR_Q_NAN : SPH_ERR_Q_NEG);
@@ -223,7 +230,7 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
       const double ha = a.hk_s[k], rhoa = a.dk_s[k], oma = a.ok_s[k];
       const double ta = cols[es_t * ld + p];
       const int n = a.ncnt[c];
-      const int32_t* __restrict__ row = a.nl + c * int64_t(a.cap);
+      const int32_t* __restrict__ row = a.nl + a.rowoff[c];
       const bool dT = a.simple ? (P.eq_diff && (P.ddw == esd_2nw_ds || P.ddw == esd_2nw_sd))
                                : (P.eq_diff || P.eq_fld);
       const R ih = R(1.0 / ha);
@@ -308,8 +315,14 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
         } else {
           const double osum = -P.wCv * ihd / ha * (a.mref * sot + ma * (DIM * double(f0)));
           double rho, om, hn;
-          const double eps = newton_update<DIM>(ha, ha0, ma, P.hfac, wsum, osum, rho, om, hn);
+          double eps = newton_update<DIM>(ha, ha0, ma, P.hfac, wsum, osum, rho, om, hn);
           if (hn <= 0.) raise_status(a.status, SPH_ERR_H_NEG);
+          if constexpr (sizeof(R) == 4) {
+            // FP32 noise floor, as in k_c1_newton: a stagnating eps below 1e-7
+            // counts as converged
+            const double eps_prev = a.eps[p];
+            if (eps > P.tol && eps < 1e-7 && eps >= 0.5 * eps_prev) eps = 0.0;
+          }
           a.eps[p] = eps;
           a.dkp1[p] = rho;
           a.okp1[p] = om;

@@ -164,7 +164,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
 
     bool bad = false;
     const int n = a.ncnt[c];
-    const int32_t* __restrict__ row = a.nl + c * int64_t(a.cap);
+    const int32_t* __restrict__ row = a.nl + a.rowoff[c];
     for (int l = lane; l < n; l += G) {
       const int64_t j = row[l];
       Part<R> B;

@@ -97,7 +97,10 @@ struct DevBuf {
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
-    size_t nb = std::max<size_t>(b, 256);
+    // 25% headroom: sizes that follow the image count move by a few rows
+    // between steps and must not trigger a free/allocate (which would also
+    // synchronise the device) every time
+    size_t nb = std::max<size_t>(b + b / 4, 256);
     cudaError_t e = cudaMalloc(&p, nb);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -145,9 +148,11 @@ struct sph_handle {
   DevBuf sx, sy, sz, s32, ssrc, cflag, cpos, centre_k, centre_p;
   DevBuf hk_s, dk_s, ok_s;
   DevBuf pk[11], qk[6];
-  // neighbours
-  DevBuf nl, ncnt;
-  int cap = 0;
+  // neighbours: one row per centre inside nl, rows sized from each
+  // particle's previous count (CSR with slack)
+  DevBuf nl, ncnt, rowoff, rowcap, rowcap64, count_prev, scan64_tmp, overflow;
+  int64_t nl_size = 0;
+  int est_count = 0;
   // scalars
   DevBuf status, red, dcnt, maxcnt, ctrl, ciso;
   unsigned long long* h_red = nullptr;  // pinned
@@ -357,6 +362,13 @@ struct sph_handle {
     RC(red.ensure(sizeof(unsigned long long) * RED_TOTAL));
     RC(dcnt.ensure(sizeof(unsigned long long) * DC_TOTAL));
     RC(maxcnt.ensure(sizeof(int32_t)));
+    RC(overflow.ensure(sizeof(int32_t)));
+    RC(count_prev.ensure(sizeof(int32_t) * nrows));
+    RC(rowoff.ensure(sizeof(int64_t) * nreal));
+    RC(rowcap.ensure(sizeof(int32_t) * nreal));
+    RC(rowcap64.ensure(sizeof(int64_t) * nreal));
+    RC(ncnt.ensure(sizeof(int32_t) * nreal));
+    RC(scan64_tmp.ensure(scan64_temp_bytes(nreal)));
     RC(ctrl.ensure(sizeof(double) * 8));
     RC(ciso.ensure(sizeof(double)));
     CK(cudaMemsetAsync(status.p, 0, sizeof(int), s));
@@ -543,24 +555,66 @@ struct sph_handle {
       launch_centres(vals_alt.as<int32_t>(), cflag.as<int32_t>(), cpos.as<int32_t>(), nall,
                      centre_k.as<int32_t>(), centre_p.as<int32_t>(), s);
     }
-    // neighbour lists, grown until every list fits
-    if (cap <= 0) {
+    // neighbour lists: rows sized from each particle's previous count; a row
+    // that overflows (or a table that is too small) re-runs the search with
+    // the counts it just measured
+    if (est_count <= 0) {
       double kh = P.krad * P.hfac;
       double est = d == 3 ? 4.0 / 3.0 * kPi * kh * kh * kh : (d == 2 ? kPi * kh * kh : 2 * kh);
-      cap = int(est * 2.0) + 32;
-      if (st[SPH_P_NEIB_CAP] > 0) cap = int(st[SPH_P_NEIB_CAP]);
+      est_count = int(est * 1.3) + 8;
+      if (st[SPH_P_NEIB_CAP] > 0) est_count = int(st[SPH_P_NEIB_CAP]);
+      launch_fill_i32(count_prev.as<int32_t>(), nrows, est_count, s);
     }
     for (int attempt = 0; attempt < 4; ++attempt) {
       Phase ph(this, SPH_T_NEIGHBOURS);
-      RC(nl.ensure(sizeof(int32_t) * size_t(cap) * std::max<int64_t>(nreal, 1)));
-      RC(ncnt.ensure(sizeof(int32_t) * std::max<int64_t>(nreal, 1)));
+      launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(), count_prev.as<int32_t>(),
+                    1.2f, rowcap64.as<int64_t>(), rowcap.as<int32_t>(), s);
+      exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, rowcap64.as<int64_t>(), rowoff.as<int64_t>(),
+                       nreal, s);
+      if (nl_size <= 0) {
+        nl_size = (int64_t(est_count) * 12 / 10 + 8) * nreal * 5 / 4;
+        RC(nl.ensure(sizeof(int32_t) * nl_size));
+      }
+      if (attempt > 0) {
+        // a re-run: size the table for the rows computed from the new counts
+        CK(cudaMemcpyAsync(h_i32 + 2, rowcap.as<int32_t>() + (nreal - 1), sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(reinterpret_cast<int64_t*>(h_red + RED_TOTAL),
+                           rowoff.as<int64_t>() + (nreal - 1), sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        int64_t total = reinterpret_cast<int64_t*>(h_red + RED_TOTAL)[0] + h_i32[2];
+        if (total > nl_size) {
+          nl_size = total + total / 4;
+          RC(nl.ensure(sizeof(int32_t) * nl_size));
+        }
+      }
       CK(cudaMemsetAsync(maxcnt.p, 0, sizeof(int32_t), s));
-      launch_neighbours(d, lanes_search(), nreal, centre_k.as<int32_t>(), centre_p.as<int32_t>(),
-                        sx.as<double>(), sy.as<double>(), sz.as<double>(), s32.as<float4>(),
-                        pgeom.shift, col(es_h), P.krad, grid, cstart.as<int32_t>(), cap,
-                        nl.as<int32_t>(), ncnt.as<int32_t>(), maxcnt.as<int32_t>(),
-                        dcnt.as<unsigned long long>(), s);
+      CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
+      NeibArgs na{};
+      na.nc = nreal;
+      na.centre_k = centre_k.as<int32_t>();
+      na.centre_p = centre_p.as<int32_t>();
+      na.sx = sx.as<double>(); na.sy = sy.as<double>(); na.sz = sz.as<double>();
+      na.s32 = s32.as<float4>();
+      na.shift = pgeom.shift;
+      na.hcol = col(es_h);
+      na.krad = P.krad;
+      na.g = grid;
+      na.cstart = cstart.as<int32_t>();
+      na.rowoff = rowoff.as<int64_t>();
+      na.rowcap = rowcap.as<int32_t>();
+      na.nl_size = nl_size;
+      na.nl = nl.as<int32_t>();
+      na.ncnt = ncnt.as<int32_t>();
+      na.orig = orig.as<int32_t>();
+      na.count_prev = count_prev.as<int32_t>();
+      na.maxcnt = maxcnt.as<int32_t>();
+      na.overflow = overflow.as<int32_t>();
+      na.dcnt = dcnt.as<unsigned long long>();
+      launch_neighbours(d, lanes_search(), na, s);
       CK(cudaMemcpyAsync(h_i32, maxcnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(h_i32 + 1, overflow.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       CK(cudaGetLastError());
       int mc = h_i32[0];
@@ -568,8 +622,8 @@ struct sph_handle {
       cnt_host[SPH_CNT_SEARCHES]++;
       if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc + 1 > kb.maxneib[d - 1])
         return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
-      if (mc <= cap) break;
-      cap = int(mc * 1.5) + 16;
+      if (!h_i32[1]) break;
+      // count_prev now holds the exact counts, so the next attempt fits
       if (attempt == 3) return fail(SPH_ERR_NEIB_OVERFLOW, "neighbour list capacity");
     }
     have_order = true;
@@ -597,7 +651,7 @@ struct sph_handle {
                 sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
     C1Args a{};
     a.nc = nreal;
-    a.cap = cap;
+    a.rowoff = rowoff.as<int64_t>();
     a.G = lanes_pair();
     a.centre_k = centre_k.as<int32_t>();
     a.centre_p = centre_p.as<int32_t>();
@@ -664,7 +718,7 @@ struct sph_handle {
                 sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
     C2Args a{};
     a.nc = nreal;
-    a.cap = cap;
+    a.rowoff = rowoff.as<int64_t>();
     a.G = lanes_pair();
     a.centre_k = centre_k.as<int32_t>();
     a.centre_p = centre_p.as<int32_t>();
@@ -943,7 +997,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
     delete h;
     return fail(SPH_ERR_CUDA, "cudaStreamCreate failed");
   }
-  if (cudaMallocHost(&h->h_red, sizeof(unsigned long long) * RED_TOTAL) != cudaSuccess ||
+  if (cudaMallocHost(&h->h_red, sizeof(unsigned long long) * (RED_TOTAL + 2)) != cudaSuccess ||
       cudaMallocHost(&h->h_ctrl, sizeof(double) * 8) != cudaSuccess ||
       cudaMallocHost(&h->h_i32, sizeof(int32_t) * 8) != cudaSuccess) {
     cudaGetLastError();
@@ -978,7 +1032,7 @@ int sph_set_param(sph_handle* h, int index, double value) {
   if ((index == ec_realpn || index == ec_fixedpn) && value != h->st[index])
     return fail(SPH_ERR_ARG, "particle counts are fixed by the store");
   h->st[index] = value;
-  if (index == SPH_P_NEIB_CAP && value > 0) h->cap = int(value);
+  if (index == SPH_P_NEIB_CAP && value > 0) h->est_count = 0;
   return SPH_OK;
 }
 
@@ -1071,7 +1125,17 @@ int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs, int64_t 
   const int64_t nc = h->nreal, nall = h->nrows + h->nghost;
   std::vector<int32_t> cnt(nc), cp(nc), og(h->nrows), sidx(nall), ssrc(nall);
   std::vector<int8_t> gcode(std::max<int64_t>(h->nghost, 1));
-  std::vector<int32_t> nl(size_t(h->cap) * nc);
+  std::vector<int64_t> roff(nc);
+  CK(cudaMemcpyAsync(roff.data(), h->rowoff.p, sizeof(int64_t) * nc, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  int64_t nl_used = nc > 0 ? roff[nc - 1] + 1 : 1;
+  for (int64_t c = 0; c < nc; ++c) nl_used = std::max<int64_t>(nl_used, roff[c] + 1);
+  std::vector<int32_t> ncv(nc);
+  CK(cudaMemcpyAsync(ncv.data(), h->ncnt.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  for (int64_t c = 0; c < nc; ++c) nl_used = std::max<int64_t>(nl_used, roff[c] + ncv[c]);
+  nl_used = std::min<int64_t>(nl_used, h->nl_size);
+  std::vector<int32_t> nl(nl_used);
   cudaStream_t s = h->s;
   CK(cudaMemcpyAsync(cnt.data(), h->ncnt.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(cp.data(), h->centre_p.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, s));
@@ -1096,7 +1160,7 @@ int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs, int64_t 
     int64_t c = centre_of_orig[o];
     int64_t base = offsets[o];
     for (int l = 0; l < cnt[c]; ++l) {
-      int64_t q = nl[size_t(c) * h->cap + l];
+      int64_t q = nl[size_t(roff[c] + l)];
       int64_t u = sidx[q];
       int64_t rj = og[ssrc[q]];
       int64_t code = u < h->nrows ? 13 : gcode[u - h->nrows];

@@ -314,29 +314,25 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
 // test alone decides membership, so the sets equal the FP64 predicate's.
 template <int DIM, int G>
 __global__ void __launch_bounds__(128)
-k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
-             const int32_t* __restrict__ centre_p, const double* __restrict__ sx,
-             const double* __restrict__ sy, const double* __restrict__ sz,
-             const float4* __restrict__ s32, double shift, const double* __restrict__ hcol,
-             double krad, Grid g, const int32_t* __restrict__ cstart, int cap,
-             int32_t* __restrict__ nl, int32_t* __restrict__ ncnt, int32_t* __restrict__ maxcnt,
-             unsigned long long* __restrict__ dcnt) {
+k_neighbours(NeibArgs a) {
   const int64_t gid = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
   const int lane = threadIdx.x & (G - 1);
   const int wl = threadIdx.x & 31;
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (wl & ~(G - 1)));
   const unsigned below = (1u << wl) - 1u;
+  const int gbase = wl & ~(G - 1);
   unsigned int ncand = 0, nexact = 0, nfound = 0;
-  if (gid < nc) {
+  const Grid g = a.g;
+  if (gid < a.nc) {
     const int64_t c = gid;
-    const int32_t k = centre_k[c];
-    const int32_t p = centre_p[c];
-    const double xi = sx[k], yi = sy[k], zi = sz[k];
-    const float4 pi = s32[k];
-    const double kh = __dmul_rn(krad, hcol[p]);
+    const int32_t k = a.centre_k[c];
+    const int32_t p = a.centre_p[c];
+    const double xi = a.sx[k], yi = a.sy[k], zi = a.sz[k];
+    const float4 pi = a.s32[k];
+    const double kh = __dmul_rn(a.krad, a.hcol[p]);
     const double R2 = __dmul_rn(kh, kh);
     const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
-    const double er = (shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
+    const double er = (a.shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
     const double delta = 8.0 * er + 4.0 * er * er + 1e-6;
     const float lo_thr = float(R2 * (1.0 - delta));
     const float hi_thr = float(R2 * (1.0 + delta));
@@ -358,27 +354,41 @@ k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
     const int cy1 = DIM >= 2 ? clampc(uy + rc, g.ny) : 0;
     const int cz0 = DIM == 3 ? clampc(uz - rc, g.nz) : 0;
     const int cz1 = DIM == 3 ? clampc(uz + rc, g.nz) : 0;
-    const int64_t base = c * int64_t(cap);
+    const int ny_r = cy1 - cy0 + 1;
+    const int nrows_r = ny_r * (cz1 - cz0 + 1);
+    const int64_t off = a.rowoff[c];
+    const int rcap = a.rowcap[c];
     int cnt = 0;
-    for (int cz = cz0; cz <= cz1; ++cz) {
-      float dzc = 0.f;
-      if (DIM == 3) dzc = fmaxf(0.f, fmaxf(float(cz) - uz, uz - float(cz + 1)));
-      for (int cy = cy0; cy <= cy1; ++cy) {
-        float dyc = 0.f;
+    // rows are set up G at a time, one per lane, then walked in order with
+    // their ranges fetched by shuffle
+    for (int r0 = 0; r0 < nrows_r; r0 += G) {
+      int32_t my_s = 0, my_e = 0;
+      const int rr = r0 + lane;
+      if (rr < nrows_r) {
+        const int cy = cy0 + rr % ny_r, cz = cz0 + rr / ny_r;
+        float dzc = 0.f, dyc = 0.f;
+        if (DIM == 3) dzc = fmaxf(0.f, fmaxf(float(cz) - uz, uz - float(cz + 1)));
         if (DIM >= 2) dyc = fmaxf(0.f, fmaxf(float(cy) - uy, uy - float(cy + 1)));
         const float rem = rc2 - dyc * dyc - dzc * dzc;
-        if (rem < 0.f) continue;
-        const float w = sqrtf(rem) + mrg;
-        const int cx0 = clampc(ux - w, g.nx);
-        const int cx1 = clampc(ux + w, g.nx);
-        const int64_t row = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
-        const int32_t s = cstart[row + cx0], e = cstart[row + cx1 + 1];
+        if (rem >= 0.f) {
+          const float w = sqrtf(rem) + mrg;
+          const int cx0 = clampc(ux - w, g.nx);
+          const int cx1 = clampc(ux + w, g.nx);
+          const int64_t row = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+          my_s = a.cstart[row + cx0];
+          my_e = a.cstart[row + cx1 + 1];
+        }
+      }
+      const int nr = min(G, nrows_r - r0);
+      for (int t = 0; t < nr; ++t) {
+        const int32_t s = __shfl_sync(gmask, my_s, gbase + t);
+        const int32_t e = __shfl_sync(gmask, my_e, gbase + t);
         for (int32_t q0 = s; q0 < e; q0 += G) {
           const int32_t q = q0 + lane;
           bool inside = false;
           if (q < e) {
             ++ncand;
-            const float4 pj = s32[q];
+            const float4 pj = a.s32[q];
             const float fx = pj.x - pi.x, fy = pj.y - pi.y, fz = pj.z - pi.z;
             const float sd32 = fx * fx + fy * fy + fz * fz;
             if (!(sd32 > hi_thr) && q != k) {
@@ -386,9 +396,9 @@ k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
                 inside = true;
               } else {
                 ++nexact;
-                double d0 = __dadd_rn(sx[q], -xi);
-                double d1 = __dadd_rn(sy[q], -yi);
-                double d2 = __dadd_rn(sz[q], -zi);
+                double d0 = __dadd_rn(a.sx[q], -xi);
+                double d1 = __dadd_rn(a.sy[q], -yi);
+                double d2 = __dadd_rn(a.sz[q], -zi);
                 double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
                                       __dmul_rn(d2, d2));
                 inside = !(sd > R2);
@@ -398,15 +408,17 @@ k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
           const unsigned bal = __ballot_sync(gmask, inside) & gmask;
           if (inside) {
             const int slot = cnt + __popc(bal & below);
-            if (slot < cap) nl[base + slot] = q;
+            if (slot < rcap && off + slot < a.nl_size) a.nl[off + slot] = q;
           }
           cnt += __popc(bal);
         }
       }
     }
     if (lane == 0) {
-      ncnt[c] = cnt;
-      atomicMax(maxcnt, cnt);
+      a.ncnt[c] = cnt;
+      a.count_prev[a.orig[p]] = cnt;
+      atomicMax(a.maxcnt, cnt);
+      if (cnt > rcap || off + rcap > a.nl_size) atomicOr(a.overflow, 1);
       nfound = unsigned(cnt);
     }
   }
@@ -414,10 +426,23 @@ k_neighbours(int64_t nc, const int32_t* __restrict__ centre_k,
   unsigned int wf = __reduce_add_sync(0xffffffffu, nfound);
   unsigned int we = __reduce_add_sync(0xffffffffu, nexact);
   if (wl == 0) {
-    atomicAdd(&dcnt[DC_CANDIDATES], (unsigned long long)wc);
-    atomicAdd(&dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
-    atomicAdd(&dcnt[DC_EXACT_TESTS], (unsigned long long)we);
+    atomicAdd(&a.dcnt[DC_CANDIDATES], (unsigned long long)wc);
+    atomicAdd(&a.dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
+    atomicAdd(&a.dcnt[DC_EXACT_TESTS], (unsigned long long)we);
   }
+}
+
+// Row capacity of each centre's neighbour list: the particle's count from
+// the previous search plus 20% and 8 slots of slack (or the initial estimate).
+__global__ void k_rowcap(int64_t nc, const int32_t* __restrict__ centre_p,
+                         const int32_t* __restrict__ orig, const int32_t* __restrict__ count_prev,
+                         float slack, int64_t* __restrict__ rowcap64, int32_t* __restrict__ rowcap) {
+  int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= nc) return;
+  int prev = count_prev[orig[centre_p[c]]];
+  int cap = int(float(prev) * slack) + 8;
+  rowcap[c] = cap;
+  rowcap64[c] = cap;
 }
 
 // ---- pair-data packing (sorted order) --------------------------------------------------------
@@ -569,6 +594,11 @@ __global__ void k_timestep_reduce(const double* __restrict__ cols, int64_t ld,
   }
 }
 
+__global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
 __global__ void k_fill_u64(unsigned long long* p, int n, unsigned long long v) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
@@ -709,44 +739,39 @@ void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos
   note_launch();
 }
 template <int DIM, int G>
-static void neighbours_g(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
-                         const double* sx, const double* sy, const double* sz, const float4* s32,
-                         double shift, const double* hcol, double krad, Grid g,
-                         const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt,
-                         int32_t* maxcnt, unsigned long long* dcnt, cudaStream_t s) {
+static void neighbours_g(const NeibArgs& a, cudaStream_t s) {
   const int tpb = 128;
-  k_neighbours<DIM, G><<<nblocks(nc * G, tpb), tpb, 0, s>>>(nc, centre_k, centre_p, sx, sy, sz, s32,
-                                                            shift, hcol, krad, g, cstart, cap, nl,
-                                                            ncnt, maxcnt, dcnt);
+  k_neighbours<DIM, G><<<nblocks(a.nc * G, tpb), tpb, 0, s>>>(a);
 }
 template <int DIM>
-static void neighbours_dim(int G, int64_t nc, const int32_t* ck, const int32_t* cp,
-                           const double* sx, const double* sy, const double* sz, const float4* s32,
-                           double shift, const double* hcol, double krad, Grid g,
-                           const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt,
-                           int32_t* maxcnt, unsigned long long* dcnt, cudaStream_t s) {
+static void neighbours_dim(int G, const NeibArgs& a, cudaStream_t s) {
   switch (G) {
-    case 4: neighbours_g<DIM, 4>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
-    case 8: neighbours_g<DIM, 8>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
-    case 16: neighbours_g<DIM, 16>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
-    default: neighbours_g<DIM, 32>(nc, ck, cp, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap, nl, ncnt, maxcnt, dcnt, s); break;
+    case 4: neighbours_g<DIM, 4>(a, s); break;
+    case 8: neighbours_g<DIM, 8>(a, s); break;
+    case 16: neighbours_g<DIM, 16>(a, s); break;
+    default: neighbours_g<DIM, 32>(a, s); break;
   }
 }
-void launch_neighbours(int dim, int G, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
-                       const double* sx, const double* sy, const double* sz, const float4* s32,
-                       double shift, const double* hcol, double krad, Grid g,
-                       const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt, int32_t* maxcnt,
-                       unsigned long long* dcnt, cudaStream_t s) {
-  if (dim == 3)
-    neighbours_dim<3>(G, nc, centre_k, centre_p, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap,
-                      nl, ncnt, maxcnt, dcnt, s);
-  else if (dim == 2)
-    neighbours_dim<2>(G, nc, centre_k, centre_p, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap,
-                      nl, ncnt, maxcnt, dcnt, s);
-  else
-    neighbours_dim<1>(G, nc, centre_k, centre_p, sx, sy, sz, s32, shift, hcol, krad, g, cstart, cap,
-                      nl, ncnt, maxcnt, dcnt, s);
+void launch_neighbours(int dim, int G, const NeibArgs& a, cudaStream_t s) {
+  if (dim == 3) neighbours_dim<3>(G, a, s);
+  else if (dim == 2) neighbours_dim<2>(G, a, s);
+  else neighbours_dim<1>(G, a, s);
   note_launch();
+}
+void launch_rowcap(int64_t nc, const int32_t* centre_p, const int32_t* orig,
+                   const int32_t* count_prev, float slack, int64_t* rowcap64, int32_t* rowcap,
+                   cudaStream_t s) {
+  k_rowcap<<<nblocks(nc), TPB, 0, s>>>(nc, centre_p, orig, count_prev, slack, rowcap64, rowcap);
+  note_launch();
+}
+size_t scan64_temp_bytes(int64_t n) {
+  size_t b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (const int64_t*)nullptr, (int64_t*)nullptr, int(n));
+  return b;
+}
+void exclusive_scan64(void* tmp, size_t tmp_bytes, const int64_t* in, int64_t* out, int64_t n,
+                      cudaStream_t s) {
+  cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, int(n), s);
 }
 void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
                  const double* sy, const double* sz, const double* cols, int64_t ld, PackGeom pg,
@@ -767,6 +792,10 @@ void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows
 void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
                             int64_t n_ts, Params P, unsigned long long* red, cudaStream_t s) {
   k_timestep_reduce<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_ts, P, red);
+  note_launch();
+}
+void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s) {
+  k_fill_i32<<<nblocks(n), TPB, 0, s>>>(p, n, v);
   note_launch();
 }
 void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s) {

@@ -96,11 +96,37 @@ void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t
                           PackGeom pg, cudaStream_t s);
 void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
                     int32_t* centre_k, int32_t* centre_p, cudaStream_t s);
-void launch_neighbours(int dim, int G, int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
-                       const double* sx, const double* sy, const double* sz, const float4* s32,
-                       double shift, const double* hcol, double krad, Grid g,
-                       const int32_t* cstart, int cap, int32_t* nl, int32_t* ncnt, int32_t* maxcnt,
-                       unsigned long long* dcnt, cudaStream_t s);
+struct NeibArgs {
+  int64_t nc;
+  const int32_t* centre_k;
+  const int32_t* centre_p;
+  const double* sx;
+  const double* sy;
+  const double* sz;
+  const float4* s32;
+  double shift;
+  const double* hcol;
+  double krad;
+  Grid g;
+  const int32_t* cstart;
+  const int64_t* rowoff;  // start of each centre's row in nl
+  const int32_t* rowcap;  // slots of each row
+  int64_t nl_size;
+  int32_t* nl;
+  int32_t* ncnt;
+  const int32_t* orig;
+  int32_t* count_prev;  // per original row: neighbours found by the last search
+  int32_t* maxcnt;
+  int32_t* overflow;
+  unsigned long long* dcnt;
+};
+void launch_neighbours(int dim, int G, const NeibArgs& a, cudaStream_t s);
+void launch_rowcap(int64_t nc, const int32_t* centre_p, const int32_t* orig,
+                   const int32_t* count_prev, float slack, int64_t* rowcap64, int32_t* rowcap,
+                   cudaStream_t s);
+size_t scan64_temp_bytes(int64_t n);
+void exclusive_scan64(void* tmp, size_t tmp_bytes, const int64_t* in, int64_t* out, int64_t n,
+                      cudaStream_t s);
 // pack groups
 enum PackGroup : int { PACK_POS = 1, PACK_HYDRO = 2, PACK_EXTRA = 4 };
 struct PackBufs {
@@ -120,6 +146,7 @@ void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig,
                             int64_t nrows, int64_t n_ts, Params P,
                             unsigned long long* red, cudaStream_t s);
 void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s);
+void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s);
 void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, double a0,
                       double a1, double a2, double a3, double a4, const double* ctrl,
                       cudaStream_t s);
@@ -139,8 +166,8 @@ void exclusive_scan(void* tmp, size_t tmp_bytes, const int32_t* in, int32_t* out
 // ---- circuit1 (sph_circuit1.cu) ---------------------------------------------------
 struct C1Args {
   int64_t nc;
-  int cap;  // neighbour slots per centre (row length of nl)
-  int G;    // lanes per centre
+  const int64_t* rowoff;  // start of each centre's neighbour row in nl
+  int G;                  // lanes per centre
   const int32_t* centre_k;
   const int32_t* centre_p;
   const int32_t* nl;
@@ -175,7 +202,7 @@ void launch_c1_snapshot(int64_t n, const int32_t* ssrc, const double* hkp1,
 // ---- circuit2 (sph_circuit2.cu) ---------------------------------------------------
 struct C2Args {
   int64_t nc;
-  int cap;
+  const int64_t* rowoff;
   int G;
   const int32_t* centre_k;
   const int32_t* centre_p;
