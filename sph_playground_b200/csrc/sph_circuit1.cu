@@ -133,32 +133,43 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
       Acc<R> sw, so;
       sw.init();
       so.init();
-      for (int l = lane; l < n; l += G) {
-        const int64_t j = row[l];
-        R mj;
-        const PairPos<R> pj = PosAccess<R>::load(pb, j, mj);
-        R dx, dy, dz;
-        pos_delta(pi, pj, dx, dy, dz);
-        R r2 = dx * dx;
-        if (DIM >= 2) r2 += dy * dy;
-        if (DIM == 3) r2 += dz * dz;
-        const R r = rsq<R>(r2);
-        const R q = r * ih;
-        bad |= !(q >= R(0));
-        R f, df;
-        if constexpr (sizeof(R) == 4) {
-          // q carries the FP32 rounding of r/h; its residual (exact via FMA)
-          // and the residuals of the kernel pieces enter f to first order, so
-          // the density sum varies smoothly with h below FP32 resolution and
-          // the Newton iterates converge instead of cycling between
-          // neighbouring FP32 values (kshape_f_df_res).
-          const R q_lo = fmaf(r, ih, -q) + r * ih_lo;
-          kshape_f_df_res<K>(q, q_lo, f, df);
-        } else {
-          kshape_f_df<K, R>(q, f, df);
+      // U neighbours per lane per round: their list entries and pair data
+      // are all requested before the first is used, so the gathers overlap
+      constexpr int U = 4;
+      for (int l0 = lane; l0 < n; l0 += G * U) {
+        int64_t jj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) jj[u] = (l0 + u * G < n) ? int64_t(row[l0 + u * G]) : -1;
+        PairPos<R> pj[U];
+        R mj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) pj[u] = PosAccess<R>::load(pb, jj[u] >= 0 ? jj[u] : 0, mj[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (jj[u] < 0) continue;
+          R dx, dy, dz;
+          pos_delta(pi, pj[u], dx, dy, dz);
+          R r2 = dx * dx;
+          if (DIM >= 2) r2 += dy * dy;
+          if (DIM == 3) r2 += dz * dz;
+          const R r = rsq<R>(r2);
+          const R q = r * ih;
+          bad |= !(q >= R(0));
+          R f, df;
+          if constexpr (sizeof(R) == 4) {
+            // q carries the FP32 rounding of r/h; its residual (exact via FMA)
+            // and the residuals of the kernel pieces enter f to first order,
+            // so the density sum varies smoothly with h below FP32 resolution
+            // and the Newton iterates converge instead of cycling between
+            // neighbouring FP32 values (kshape_f_df_res).
+            const R q_lo = fmaf(r, ih, -q) + r * ih_lo;
+            kshape_f_df_res<K>(q, q_lo, f, df);
+          } else {
+            kshape_f_df<K, R>(q, f, df);
+          }
+          sw.add(mj[u] * f);
+          so.add(mj[u] * (R(DIM) * f + q * df));
         }
-        sw.add(mj * f);
-        so.add(mj * (R(DIM) * f + q * df));
       }
       const double swt = group_sum<G>(sw.dval(), gmask);
       const double sot = group_sum<G>(so.dval(), gmask);

@@ -165,10 +165,19 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     bool bad = false;
     const int n = a.ncnt[c];
     const int32_t* __restrict__ row = a.nl + a.rowoff[c];
-    for (int l = lane; l < n; l += G) {
-      const int64_t j = row[l];
-      Part<R> B;
-      Loader<R>::hydro(pb, j, B);
+    constexpr int U = 2;  // neighbours per lane per round, loads issued together
+    for (int l0 = lane; l0 < n; l0 += G * U) {
+    int64_t jj[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) jj[u] = (l0 + u * G < n) ? int64_t(row[l0 + u * G]) : -1;
+    Part<R> BB[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) Loader<R>::hydro(pb, jj[u] >= 0 ? jj[u] : 0, BB[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (jj[u] < 0) continue;
+      const int64_t j = jj[u];
+      const Part<R>& B = BB[u];
       R rab[3];
       pos_delta(A.pos, B.pos, rab[0], rab[1], rab[2]);
       R r2 = rab[0] * rab[0];
@@ -280,6 +289,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         }
       }
       for (int d = 0; d < DIM; ++d) dv[d].add(-mb * F * rab[d]);
+    }
     }
     if (bad) raise_status(a.status, SPH_ERR_Q_NAN);
     const double mref = a.mref;

@@ -249,7 +249,7 @@ struct sph_handle {
   static int lanes_ok(int g) { return (g == 4 || g == 8 || g == 16 || g == 32) ? g : 0; }
   int lanes_search() const {
     int g = lanes_ok(int(st[SPH_P_LANES_SEARCH]));
-    return g ? g : (dim() == 3 ? 16 : 8);
+    return g ? g : (dim() == 3 ? 8 : 8);
   }
   int lanes_pair() const {
     int g = lanes_ok(int(st[SPH_P_LANES_PAIR]));
