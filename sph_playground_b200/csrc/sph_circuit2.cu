@@ -165,7 +165,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     bool bad = false;
     const int n = a.ncnt[c];
     const int32_t* __restrict__ row = a.nl + a.rowoff[c];
-    constexpr int U = 2;  // neighbours per lane per round, loads issued together
+    constexpr int U = 1;  // neighbours per lane per round (U > 1 raised registers past the gain)
     for (int l0 = lane; l0 < n; l0 += G * U) {
     int64_t jj[U];
 #pragma unroll
