@@ -172,6 +172,26 @@ int sph_get_counters(sph_handle* h, int64_t* out, int n);
 int sph_reset_counters(sph_handle* h);
 int sph_get_timers(sph_handle* h, double* out_ms, int n);
 
+/* ---- allocation-free density ---------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a code running inside another application's fixed device-memory
+ * budget, e.g. an in-situ hook handed particle arrays by a host simulation,
+ * or a caller that must avoid the device synchronisation of cudaMalloc /
+ * cudaFree): rho_i = sum_{j != i, r_ij <= krad h_i} m_j W(r_ij, h_i)
+ * + m_i W(0, h_i) over n particles given as device arrays (x, y, z, m, h;
+ * y and z may be NULL below 3 dimensions), written to the device array rho.
+ * No periodic images.  All intermediate data lives in a fixed static device
+ * array of SPH_NOALLOC_SCRATCH_BYTES on every GPU that loads the library;
+ * n above SPH_NOALLOC_MAX_PARTICLES is rejected with SPH_ERR_ARG.  The first
+ * call on a device looks the array up (make it before any stream capture).
+ * Calls share the array: calls that overlap on the GPU race.  `stream` is a
+ * cudaStream_t (NULL = default stream); the call synchronises it. */
+#define SPH_NOALLOC_MAX_PARTICLES 262144
+#define SPH_NOALLOC_SCRATCH_BYTES (32u << 20)
+int sph_density_noalloc(const double* x, const double* y, const double* z,
+                        const double* m, const double* h, int64_t n, int dim,
+                        int kernel_id, double* rho, void* stream);
+
 /* Last error message (static storage, valid until the next call). */
 const char* sph_last_error(void);
 

@@ -123,6 +123,7 @@ struct Mode {
 }  // namespace
 
 namespace sph {
+int sph_fail(int code, const std::string& msg) { return fail(code, msg); }
 void note_launch(int n) { g_launches += n; }
 long long launches_so_far() { return g_launches; }
 }  // namespace sph

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "sph_device.cuh"
@@ -60,6 +61,9 @@ struct BoxGeom {
   int periodic[3];  // axes that get periodic images
   int reflect[3];   // axes whose real particles are wrapped
 };
+
+// Record an error message for sph_last_error and return `code`.
+int sph_fail(int code, const std::string& msg);
 
 // Count of this library's kernel launches (process-wide).
 void note_launch(int n = 1);
