@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-n", type=int, default=64, help="lattice per axis of the CPU sample")
+    ap.add_argument("--param", action="append", default=[],
+                    help="engine parameter NAME=VALUE (abi.P_* name or slot), for both arms")
     return ap.parse_args()
 
 
@@ -75,11 +77,18 @@ class Clocks:
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                   "-lms", "200"]
+                   "-lms", "20"]
             if self.uuid:
                 cmd += ["-i", self.uuid]
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+            # the timed region starts once the sampler is producing lines
+            t0 = time.time()
+            while time.time() - t0 < 10 and self.proc.poll() is None:
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.02)
+            self.skip = sum(1 for _ in open(self.path))
         except Exception:
             self.proc = None
         return self
@@ -98,7 +107,7 @@ class Clocks:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
         except Exception:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        rows = [[c.strip() for c in r] for r in rows[getattr(self, "skip", 0):] if len(r) >= 9]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -200,9 +209,16 @@ def main():
     N = store.shape[0]
     peak32, peak64 = measure_peak()
 
+    def engine(prec):
+        e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+        for kv in args.param:
+            k, v = kv.split("=")
+            e.set_param(int(k) if k.isdigit() else getattr(abi, k, k), float(v))
+        return e
+
     # FP32 vs FP64 density error on the bench input (the metric's rho bound)
-    e32 = abi.Engine(st, store, "m6", precision=abi.PREC_FP32_COMP, lib=lib)
-    e64 = abi.Engine(st, store, "m6", precision=abi.PREC_FP64, lib=lib)
+    e32 = engine(abi.PREC_FP32_COMP)
+    e64 = engine(abi.PREC_FP64)
     e32.density()
     e64.density()
     r32, r64 = e32.get_store(), e64.get_store()
@@ -215,7 +231,7 @@ def main():
     e64.close()
 
     def run(prec):
-        e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+        e = engine(prec)
         e.set_param(abi.consts.ec["tfinish"], 1.0)
         for _ in range(args.warmup):
             e.step(1)

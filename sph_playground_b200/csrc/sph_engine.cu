@@ -151,7 +151,7 @@ struct sph_handle {
   DevBuf pk[11], qk[6];
   // neighbours: one row per centre inside nl, rows sized from each
   // particle's previous count (CSR with slack)
-  DevBuf nl, ncnt, rowoff, rowcap, rowcap64, count_prev, scan64_tmp, overflow;
+  DevBuf nl, ncnt, rowoff, rowcap, rowcap64, count_prev, h_prev, scan64_tmp, overflow;
   int64_t nl_size = 0;
   int est_count = 0;
   // scalars
@@ -365,6 +365,7 @@ struct sph_handle {
     RC(maxcnt.ensure(sizeof(int32_t)));
     RC(overflow.ensure(sizeof(int32_t)));
     RC(count_prev.ensure(sizeof(int32_t) * nrows));
+    RC(h_prev.ensure(sizeof(float) * nrows));
     RC(rowoff.ensure(sizeof(int64_t) * nreal));
     RC(rowcap.ensure(sizeof(int32_t) * nreal));
     RC(rowcap64.ensure(sizeof(int64_t) * nreal));
@@ -565,11 +566,13 @@ struct sph_handle {
       est_count = int(est * 1.3) + 8;
       if (st[SPH_P_NEIB_CAP] > 0) est_count = int(st[SPH_P_NEIB_CAP]);
       launch_fill_i32(count_prev.as<int32_t>(), nrows, est_count, s);
+      CK(cudaMemsetAsync(h_prev.p, 0, sizeof(float) * nrows, s));
     }
     for (int attempt = 0; attempt < 4; ++attempt) {
       Phase ph(this, SPH_T_NEIGHBOURS);
       launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(), count_prev.as<int32_t>(),
-                    1.2f, rowcap64.as<int64_t>(), rowcap.as<int32_t>(), s);
+                    h_prev.as<float>(), col(es_h), d, 1.2f, rowcap64.as<int64_t>(),
+                    rowcap.as<int32_t>(), s);
       exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, rowcap64.as<int64_t>(), rowoff.as<int64_t>(),
                        nreal, s);
       if (nl_size <= 0) {
@@ -610,6 +613,7 @@ struct sph_handle {
       na.ncnt = ncnt.as<int32_t>();
       na.orig = orig.as<int32_t>();
       na.count_prev = count_prev.as<int32_t>();
+      na.h_prev = h_prev.as<float>();
       na.maxcnt = maxcnt.as<int32_t>();
       na.overflow = overflow.as<int32_t>();
       na.dcnt = dcnt.as<unsigned long long>();

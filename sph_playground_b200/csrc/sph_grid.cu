@@ -295,12 +295,18 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
 }
 
 // ---- neighbour search -------------------------------------------------------------------
-// A group of G lanes serves one centre.  For every (y, z) row of cells that
-// the sphere of radius R = krad*h reaches, the x-extent of the sphere at that
-// row's nearest point selects a run of cells, which is one contiguous range
-// of the sorted particles; the group walks it G candidates at a time
-// (coalesced loads) and appends hits to the centre's list with a ballot, so
-// list writes are contiguous too.
+// One lane per centre; a group of G consecutive centres (in cell order, so
+// neighbours in space) shares one stream of candidates.  The centres of a
+// group whose home cell lies in the same (y, z) row of cells form a segment
+// (almost always the whole group); for every row of cells that the segment's
+// spheres reach, the x-extent of the union of the spheres selects a run of
+// cells, which is one contiguous range of the sorted particles.  The group
+// stages up to 8G ranges in shared memory with a prefix of their lengths and
+// walks their concatenation G candidates at a time: every lane loads one
+// candidate (coalesced) into shared memory, then every lane tests all G of
+// them against its own centre and appends the hits to its centre's list.  A
+// candidate is fetched once for the G centres, and no lane computes a range
+// of cells for itself alone.
 //
 // Inclusion is the kd-tree's FP64 test, summed x, y, z in order without
 // fused multiply-adds: ((dx*dx + dy*dy) + dz*dz) <= (krad*h)^2
@@ -312,119 +318,298 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
 // near the surface, so delta = 8 e / R + 4 (e / R)^2 + 1e-6 bounds it.  Only
 // the candidates with |sd32 - R^2| <= delta R^2 are tested in FP64; the FP64
 // test alone decides membership, so the sets equal the FP64 predicate's.
+constexpr int kNeibRowsPerLane = 6;
+
+// minimum / maximum over the G lanes of a group (all lanes of the warp call)
+template <int G>
+__device__ __forceinline__ float group_min(float v) {
+#pragma unroll
+  for (int d = 1; d < G; d <<= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, d, G));
+  return v;
+}
+template <int G>
+__device__ __forceinline__ float group_max(float v) {
+#pragma unroll
+  for (int d = 1; d < G; d <<= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, d, G));
+  return v;
+}
+
 template <int DIM, int G>
 __global__ void __launch_bounds__(128)
 k_neighbours(NeibArgs a) {
-  const int64_t gid = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
+  constexpr int RPL = kNeibRowsPerLane;
+  constexpr int NG = 128 / G;
+  constexpr unsigned FULL = 0xffffffffu;
+  // Staged ranges per group, stored [entry of the lane][lane] so that the
+  // lanes' stores hit distinct banks.  Entry = (first sorted index of the
+  // range - its offset in the concatenation, end of the range in the
+  // concatenation).
+  __shared__ int2 ranges[NG][RPL * G];
+  // The batch of candidates: FP32 image and sorted index; one float4 of
+  // padding per group puts the groups of a warp on different banks.
+  __shared__ float4 batch[NG][G + 1];
+  // Each lane's hits wait in its own slice of `held` and go to its list in
+  // runs, written by the whole warp at once (coalesced), whenever a lane
+  // holds FLUSH_AT or more.  At most G hits arrive between two checks, so
+  // a slice of 33 words (a stride that spreads the slices over the banks)
+  // never overflows and a run never exceeds the warp's 32 lanes.
+  constexpr int FLUSH_AT = 33 - G;
+  __shared__ int32_t held[128][33];
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int lane = threadIdx.x & (G - 1);
   const int wl = threadIdx.x & 31;
-  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (wl & ~(G - 1)));
-  const unsigned below = (1u << wl) - 1u;
-  const int gbase = wl & ~(G - 1);
+  const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1u) << (wl & ~(G - 1)));
+  int2* rs = ranges[threadIdx.x / G];
+  float4* bt = batch[threadIdx.x / G];
   unsigned int ncand = 0, nexact = 0, nfound = 0;
   const Grid g = a.g;
-  if (gid < a.nc) {
-    const int64_t c = gid;
-    const int32_t k = a.centre_k[c];
-    const int32_t p = a.centre_p[c];
-    const double xi = a.sx[k], yi = a.sy[k], zi = a.sz[k];
-    const float4 pi = a.s32[k];
+  // Every loop below runs the same number of passes on all lanes of the warp
+  // (the maximum over its groups), so votes and shuffles take the full mask.
+  const bool active = c < a.nc;
+  int32_t k = -1, p = 0;
+  double xi = 0.0, yi = 0.0, zi = 0.0, R2 = 0.0;
+  float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+  float lo_thr = -1.f, hi_thr = -1.f, ux = 0.f, uy = 0.f, uz = 0.f, rc = 0.f, mrg = 0.f;
+  int rcap = 0, home = -1;
+  int64_t off = 0;
+  auto clampc = [](float v, int n) {
+    float f = floorf(v);
+    if (!(f >= 0.f)) return 0;
+    if (f >= float(n - 1)) return n - 1;
+    return int(f);
+  };
+  if (active) {
+    k = a.centre_k[c];
+    p = a.centre_p[c];
+    xi = a.sx[k]; yi = a.sy[k]; zi = a.sz[k];
+    pi = a.s32[k];
     const double kh = __dmul_rn(a.krad, a.hcol[p]);
-    const double R2 = __dmul_rn(kh, kh);
+    R2 = __dmul_rn(kh, kh);
     const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
     const double er = (a.shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
     const double delta = 8.0 * er + 4.0 * er * er + 1e-6;
-    const float lo_thr = float(R2 * (1.0 - delta));
-    const float hi_thr = float(R2 * (1.0 + delta));
+    lo_thr = float(R2 * (1.0 - delta));
+    hi_thr = float(R2 * (1.0 + delta));
     // Row selection in cell units and FP32: every quantity is widened by a
     // margin far above its rounding, so the selected cells are a superset of
-    // the ones the sphere touches; membership is decided per candidate below.
-    const float ux = float((xi - g.ox) * g.invL), uy = float((yi - g.oy) * g.invL),
-                uz = float((zi - g.oz) * g.invL);
-    const float mrg = 1e-3f + 1e-6f * (fabsf(ux) + fabsf(uy) + fabsf(uz));
-    const float rc = float(R * g.invL) * (1.f + 1e-5f) + mrg;
-    const float rc2 = rc * rc;
-    auto clampc = [](float v, int n) {
-      float f = floorf(v);
-      if (!(f >= 0.f)) return 0;
-      if (f >= float(n - 1)) return n - 1;
-      return int(f);
-    };
-    const int cy0 = DIM >= 2 ? clampc(uy - rc, g.ny) : 0;
-    const int cy1 = DIM >= 2 ? clampc(uy + rc, g.ny) : 0;
-    const int cz0 = DIM == 3 ? clampc(uz - rc, g.nz) : 0;
-    const int cz1 = DIM == 3 ? clampc(uz + rc, g.nz) : 0;
+    // the ones the spheres touch; membership is decided per candidate below.
+    ux = float((xi - g.ox) * g.invL); uy = float((yi - g.oy) * g.invL);
+    uz = float((zi - g.oz) * g.invL);
+    mrg = 1e-3f + 1e-6f * (fabsf(ux) + fabsf(uy) + fabsf(uz));
+    rc = float(R * g.invL) * (1.f + 1e-5f) + mrg;
+    home = (DIM >= 2 ? clampc(uy, g.ny) : 0) + (DIM == 3 ? clampc(uz, g.nz) : 0) * g.ny;
+    off = a.rowoff[c];
+    // slots usable without leaving the table; a shorter row is an overflow
+    const int rcap0 = a.rowcap[c];
+    const int64_t room = a.nl_size - off;
+    rcap = room <= 0 ? 0 : (room < int64_t(rcap0) ? int(room) : rcap0);
+  }
+  int cnt = 0;   // hits written to the list
+  int nheld = 0;  // hits waiting in held[threadIdx.x]
+  int32_t* const row = a.nl + off;
+  int32_t* const mine_held = held[threadIdx.x];
+  int32_t* const warp_held = held[threadIdx.x & ~31];
+  // writes the held hits of the lanes in `who` to their lists, all 32
+  // lanes of the warp carrying one lane's run at a time
+  auto flush = [&](unsigned who) {
+    __syncwarp();
+    while (who) {
+      const int L = __ffs(who) - 1;
+      who &= who - 1u;
+      const int nL = __shfl_sync(FULL, nheld, L);
+      const int baseL = __shfl_sync(FULL, cnt, L);
+      const int capL = __shfl_sync(FULL, rcap, L);
+      int32_t* const rowL = reinterpret_cast<int32_t*>(
+          __shfl_sync(FULL, reinterpret_cast<unsigned long long>(row), L));
+      if (wl < nL && baseL + wl < capL) rowL[baseL + wl] = warp_held[L * 33 + wl];
+    }
+    __syncwarp();
+  };
+  unsigned todo = __ballot_sync(FULL, active) & gmask;
+  while (__any_sync(FULL, todo != 0u)) {
+    // this pass: the centres that share the home row of the first one left
+    const int lead = todo ? __ffs(todo) - 1 : wl;
+    const int lead_home = __shfl_sync(FULL, home, lead);
+    const bool mine = ((todo >> wl) & 1u) && home == lead_home;
+    const unsigned seg = __ballot_sync(FULL, mine) & gmask;
+    todo &= ~seg;
+    // bounding box of the segment's centres and its largest radius (cells)
+    const float BIG = 3.0e38f;
+    const float bx0 = group_min<G>(mine ? ux : BIG), bx1 = group_max<G>(mine ? ux : -BIG);
+    const float by0 = group_min<G>(mine ? uy : BIG), by1 = group_max<G>(mine ? uy : -BIG);
+    const float bz0 = group_min<G>(mine ? uz : BIG), bz1 = group_max<G>(mine ? uz : -BIG);
+    const float rmax = group_max<G>(mine ? rc : 0.f);
+    const float bm = group_max<G>(mine ? mrg : 0.f);
+    int cy0 = 0, cy1 = -1, cz0 = 0, cz1 = 0;
+    if (seg) {
+      cy0 = DIM >= 2 ? clampc(by0 - rmax, g.ny) : 0;
+      cy1 = DIM >= 2 ? clampc(by1 + rmax, g.ny) : 0;
+      cz0 = DIM == 3 ? clampc(bz0 - rmax, g.nz) : 0;
+      cz1 = DIM == 3 ? clampc(bz1 + rmax, g.nz) : 0;
+    }
     const int ny_r = cy1 - cy0 + 1;
-    const int nrows_r = ny_r * (cz1 - cz0 + 1);
-    const int64_t off = a.rowoff[c];
-    const int rcap = a.rowcap[c];
-    int cnt = 0;
-    // rows are set up G at a time, one per lane, then walked in order with
-    // their ranges fetched by shuffle
-    for (int r0 = 0; r0 < nrows_r; r0 += G) {
-      int32_t my_s = 0, my_e = 0;
-      const int rr = r0 + lane;
-      if (rr < nrows_r) {
-        const int cy = cy0 + rr % ny_r, cz = cz0 + rr / ny_r;
-        float dzc = 0.f, dyc = 0.f;
-        if (DIM == 3) dzc = fmaxf(0.f, fmaxf(float(cz) - uz, uz - float(cz + 1)));
-        if (DIM >= 2) dyc = fmaxf(0.f, fmaxf(float(cy) - uy, uy - float(cy + 1)));
-        const float rem = rc2 - dyc * dyc - dzc * dzc;
-        if (rem >= 0.f) {
-          const float w = sqrtf(rem) + mrg;
-          const int cx0 = clampc(ux - w, g.nx);
-          const int cx1 = clampc(ux + w, g.nx);
-          const int64_t row = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
-          my_s = a.cstart[row + cx0];
-          my_e = a.cstart[row + cx1 + 1];
-        }
-      }
-      const int nr = min(G, nrows_r - r0);
-      for (int t = 0; t < nr; ++t) {
-        const int32_t s = __shfl_sync(gmask, my_s, gbase + t);
-        const int32_t e = __shfl_sync(gmask, my_e, gbase + t);
-        for (int32_t q0 = s; q0 < e; q0 += G) {
-          const int32_t q = q0 + lane;
-          bool inside = false;
-          if (q < e) {
-            ++ncand;
-            const float4 pj = a.s32[q];
-            const float fx = pj.x - pi.x, fy = pj.y - pi.y, fz = pj.z - pi.z;
-            const float sd32 = fx * fx + fy * fy + fz * fz;
-            if (!(sd32 > hi_thr) && q != k) {
-              if (sd32 < lo_thr) {
-                inside = true;
-              } else {
-                ++nexact;
-                double d0 = __dadd_rn(a.sx[q], -xi);
-                double d1 = __dadd_rn(a.sy[q], -yi);
-                double d2 = __dadd_rn(a.sz[q], -zi);
-                double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
-                                      __dmul_rn(d2, d2));
-                inside = !(sd > R2);
-              }
+    const int nrows_r = seg ? ny_r * (cz1 - cz0 + 1) : 0;
+    const float r2 = rmax * rmax;
+    const int nch = __reduce_max_sync(FULL, (nrows_r + RPL * G - 1) / (RPL * G));
+    for (int ch = 0; ch < nch; ++ch) {
+      // The chunk's rows go round-robin over the lanes (row rbase + i G is
+      // the lane's i-th); first each lane finds its rows' runs of cells,
+      // then issues all their cell-start loads at once.
+      const int rbase = ch * RPL * G + lane;
+      unsigned ia[RPL], ib[RPL];  // cstart indices of each run's ends
+#pragma unroll
+      for (int i = 0; i < RPL; ++i) ia[i] = ib[i] = 0u;
+      if (nrows_r > 0) {  // then ny_r >= 1
+        int cy = cy0 + rbase % ny_r, cz = cz0 + rbase / ny_r;
+        const int dq = G / ny_r, dr = G % ny_r;  // a step of G rows
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+          if (rbase + i * G < nrows_r) {
+            float dzc = 0.f, dyc = 0.f;
+            if (DIM == 3) dzc = fmaxf(0.f, fmaxf(float(cz) - bz1, bz0 - float(cz + 1)));
+            if (DIM >= 2) dyc = fmaxf(0.f, fmaxf(float(cy) - by1, by0 - float(cy + 1)));
+            const float rem = r2 - dyc * dyc - dzc * dzc;
+            if (rem >= 0.f) {
+              const float w = sqrtf(rem) + bm;
+              const int cx0 = clampc(bx0 - w, g.nx);
+              const int cx1 = clampc(bx1 + w, g.nx);
+              const int64_t rowc = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+              ia[i] = unsigned(rowc + cx0);
+              ib[i] = unsigned(rowc + cx1 + 1);
             }
           }
-          const unsigned bal = __ballot_sync(gmask, inside) & gmask;
-          if (inside) {
-            const int slot = cnt + __popc(bal & below);
-            if (slot < rcap && off + slot < a.nl_size) a.nl[off + slot] = q;
-          }
-          cnt += __popc(bal);
+          cy += dr;
+          cz += dq;
+          if (cy > cy1) { cy -= ny_r; ++cz; }
         }
       }
-    }
-    if (lane == 0) {
-      a.ncnt[c] = cnt;
-      a.count_prev[a.orig[p]] = cnt;
-      atomicMax(a.maxcnt, cnt);
-      if (cnt > rcap || off + rcap > a.nl_size) atomicOr(a.overflow, 1);
-      nfound = unsigned(cnt);
+      int mysum = 0;
+      {
+        int32_t sa[RPL], sb[RPL];
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+          sa[i] = __ldg(a.cstart + ia[i]);
+          sb[i] = __ldg(a.cstart + ib[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+          rs[i * G + lane] = make_int2(sa[i], sb[i] - sa[i]);
+          mysum += sb[i] - sa[i];
+        }
+      }
+      // exclusive prefix of the lanes' sums over the group
+      int incl = mysum;
+#pragma unroll
+      for (int d = 1; d < G; d <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, d, G);
+        if (lane >= d) incl += t;
+      }
+      const int total = __shfl_sync(FULL, incl, G - 1, G);
+      int run = incl - mysum;
+#pragma unroll
+      for (int i = 0; i < RPL; ++i) {
+        const int2 v = rs[i * G + lane];
+        rs[i * G + lane] = make_int2(v.x - run, run + v.y);
+        run += v.y;
+      }
+      __syncwarp();
+      if (mine) ncand += unsigned(total);
+      const int tmax = __reduce_max_sync(FULL, total);
+      // The walk: lane j of the group fetches candidate p0 + j of every
+      // batch, one batch ahead of the tests (software pipelining), past the
+      // end a far-away sentinel that no test accepts.
+      int r = 0;
+      int2 rw = rs[0];
+      const float4 far = make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.f);
+      float4 nxt = far;
+      int32_t nxt_q = -1;
+      if (lane < total) {
+        while (lane >= rw.y) {
+          ++r;
+          rw = rs[(r % RPL) * G + r / RPL];
+        }
+        nxt_q = lane + rw.x;
+        nxt = __ldg(a.s32 + nxt_q);
+      }
+      for (int p0 = 0; p0 < tmax; p0 += G) {
+        const float4 cur = make_float4(nxt.x, nxt.y, nxt.z, __int_as_float(nxt_q));
+        const int pos = p0 + G + lane;
+        nxt = far;
+        nxt_q = -1;
+        if (pos < total) {
+          // the range holding pos: ends are increasing and the last one is
+          // total, so the walk stays inside the chunk
+          while (pos >= rw.y) {
+            ++r;
+            rw = rs[(r % RPL) * G + r / RPL];
+          }
+          nxt_q = pos + rw.x;
+          nxt = __ldg(a.s32 + nxt_q);
+        }
+        bt[lane] = cur;
+        __syncwarp();
+        if (mine) {
+          // FP32 decisions for the batch; the candidates in the guard band
+          // are marked in `band` and decided in FP64 after it (rare)
+          unsigned band = 0u;
+#pragma unroll
+          for (int t = 0; t < G; ++t) {
+            const float4 pj = bt[t];
+            const float fx = pj.x - pi.x, fy = pj.y - pi.y, fz = pj.z - pi.z;
+            const float sd32 = fx * fx + fy * fy + fz * fz;
+            const int32_t q = __float_as_int(pj.w);
+            const bool in32 = sd32 < lo_thr;
+            band |= (!in32 && !(sd32 > hi_thr)) ? (1u << t) : 0u;
+            const bool take = in32 && q != k;
+            if (take) mine_held[nheld] = q;
+            nheld += take ? 1 : 0;
+          }
+          while (band) {
+            const int t = __ffs(band) - 1;
+            band &= band - 1u;
+            const float4 pj = bt[t];
+            const int32_t q = __float_as_int(pj.w);
+            ++nexact;
+            double d0 = __dadd_rn(a.sx[q], -xi);
+            double d1 = __dadd_rn(a.sy[q], -yi);
+            double d2 = __dadd_rn(a.sz[q], -zi);
+            double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                  __dmul_rn(d2, d2));
+            const bool take = !(sd > R2) && q != k;
+            if (take) mine_held[nheld] = q;
+            nheld += take ? 1 : 0;
+          }
+        }
+        __syncwarp();  // the next batch overwrites this one
+        const unsigned full = __ballot_sync(FULL, nheld >= FLUSH_AT);
+        if (full) {
+          flush(full);
+          if ((full >> wl) & 1u) {
+            cnt += nheld;
+            nheld = 0;
+          }
+        }
+      }
+      __syncwarp();  // the next chunk overwrites the ranges
     }
   }
-  unsigned int wc = __reduce_add_sync(0xffffffffu, ncand);
-  unsigned int wf = __reduce_add_sync(0xffffffffu, nfound);
-  unsigned int we = __reduce_add_sync(0xffffffffu, nexact);
+  {
+    const unsigned left = __ballot_sync(FULL, nheld > 0);
+    if (left) flush(left);
+    cnt += nheld;
+    nheld = 0;
+  }
+  if (active) {
+    a.ncnt[c] = cnt;
+    a.count_prev[a.orig[p]] = cnt;
+    a.h_prev[a.orig[p]] = float(a.hcol[p]);
+    atomicMax(a.maxcnt, cnt);
+    if (cnt > rcap) atomicOr(a.overflow, 1);
+    nfound = unsigned(cnt);
+  }
+  unsigned int wc = __reduce_add_sync(FULL, ncand);
+  unsigned int wf = __reduce_add_sync(FULL, nfound);
+  unsigned int we = __reduce_add_sync(FULL, nexact);
   if (wl == 0) {
     atomicAdd(&a.dcnt[DC_CANDIDATES], (unsigned long long)wc);
     atomicAdd(&a.dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
@@ -433,14 +618,26 @@ k_neighbours(NeibArgs a) {
 }
 
 // Row capacity of each centre's neighbour list: the particle's count from
-// the previous search plus 20% and 8 slots of slack (or the initial estimate).
+// the previous search, scaled by (h / h_then)^dim for the change of its
+// search radius since, plus 20% and 8 slots of slack (or the initial
+// estimate, which comes with h_then = 0).
 __global__ void k_rowcap(int64_t nc, const int32_t* __restrict__ centre_p,
                          const int32_t* __restrict__ orig, const int32_t* __restrict__ count_prev,
-                         float slack, int64_t* __restrict__ rowcap64, int32_t* __restrict__ rowcap) {
+                         const float* __restrict__ h_prev, const double* __restrict__ hcol,
+                         int dim, float slack, int64_t* __restrict__ rowcap64,
+                         int32_t* __restrict__ rowcap) {
   int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (c >= nc) return;
-  int prev = count_prev[orig[centre_p[c]]];
-  int cap = int(float(prev) * slack) + 8;
+  const int32_t p = centre_p[c];
+  const int32_t o = orig[p];
+  float est = float(count_prev[o]);
+  const float hp = h_prev[o];
+  if (hp > 0.f) {
+    float g = float(hcol[p]) / hp;
+    g = fminf(fmaxf(g, 0.5f), 4.f);
+    est *= dim == 3 ? g * g * g : (dim == 2 ? g * g : g);
+  }
+  const int cap = int(fminf(est * slack, 1.0e9f)) + 8;
   rowcap[c] = cap;
   rowcap64[c] = cap;
 }
@@ -741,7 +938,7 @@ void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos
 template <int DIM, int G>
 static void neighbours_g(const NeibArgs& a, cudaStream_t s) {
   const int tpb = 128;
-  k_neighbours<DIM, G><<<nblocks(a.nc * G, tpb), tpb, 0, s>>>(a);
+  k_neighbours<DIM, G><<<nblocks(a.nc, tpb), tpb, 0, s>>>(a);
 }
 template <int DIM>
 static void neighbours_dim(int G, const NeibArgs& a, cudaStream_t s) {
@@ -759,9 +956,11 @@ void launch_neighbours(int dim, int G, const NeibArgs& a, cudaStream_t s) {
   note_launch();
 }
 void launch_rowcap(int64_t nc, const int32_t* centre_p, const int32_t* orig,
-                   const int32_t* count_prev, float slack, int64_t* rowcap64, int32_t* rowcap,
+                   const int32_t* count_prev, const float* h_prev, const double* hcol,
+                   int dim, float slack, int64_t* rowcap64, int32_t* rowcap,
                    cudaStream_t s) {
-  k_rowcap<<<nblocks(nc), TPB, 0, s>>>(nc, centre_p, orig, count_prev, slack, rowcap64, rowcap);
+  k_rowcap<<<nblocks(nc), TPB, 0, s>>>(nc, centre_p, orig, count_prev, h_prev, hcol, dim, slack,
+                                       rowcap64, rowcap);
   note_launch();
 }
 size_t scan64_temp_bytes(int64_t n) {

@@ -120,13 +120,15 @@ struct NeibArgs {
   int32_t* ncnt;
   const int32_t* orig;
   int32_t* count_prev;  // per original row: neighbours found by the last search
+  float* h_prev;        // per original row: h of that search
   int32_t* maxcnt;
   int32_t* overflow;
   unsigned long long* dcnt;
 };
 void launch_neighbours(int dim, int G, const NeibArgs& a, cudaStream_t s);
 void launch_rowcap(int64_t nc, const int32_t* centre_p, const int32_t* orig,
-                   const int32_t* count_prev, float slack, int64_t* rowcap64, int32_t* rowcap,
+                   const int32_t* count_prev, const float* h_prev, const double* hcol,
+                   int dim, float slack, int64_t* rowcap64, int32_t* rowcap,
                    cudaStream_t s);
 size_t scan64_temp_bytes(int64_t n);
 void exclusive_scan64(void* tmp, size_t tmp_bytes, const int64_t* in, int64_t* out, int64_t n,
