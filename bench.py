@@ -28,6 +28,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from sph_playground_b200 import abi  # noqa: E402  (ctypes only; no CUDA at import)
+
 METRIC = "particle-steps/s, 2.1M 3D: FP32-comp vs FP64 on B200 at rho err<=1e-6"
 UNIT = "particle-steps/s"
 # per-pair algorithmic FLOP weights (circuit1 per pair per Newton sweep,
@@ -133,7 +135,7 @@ def measure_peak():
 def cpu_baseline(n):
     """The oracle (CPU FP64 OpenMP restatement) on a bounded sample: one
     leapfrog step of the same Sedov set-up at n^3 after its start-up iterate."""
-    from sph_playground_b200 import abi, ic
+    from sph_playground_b200 import ic
     lib = abi.load(os.path.join(ROOT, "oracle", "liboracle.so"))
     st, store = ic.sedov3d(n=n)
     e = abi.Engine(st, store, "m6", lib=lib)
@@ -151,7 +153,7 @@ def cpu_baseline(n):
 def run_reference(args, ws, rank):
     if rank != 0:
         return
-    from sph_playground_b200 import abi, ic
+    from sph_playground_b200 import ic
     lib = abi.load(os.path.join(ROOT, "oracle", "liboracle.so"))
     n = args.cpu_n
     st, store = ic.sedov3d(n=n)
@@ -183,12 +185,16 @@ def run_reference(args, ws, rank):
 
 
 def timed_steps(e, K):
-    """Run K steps; returns (device ms from the engine's stream events,
-    counters delta, per-phase ms delta)."""
+    """Run K steps timed by CUDA events on the engine's stream: one pair
+    around the call (the step time) and one per phase (SPH_P_TIMING = 1);
+    returns (device ms of the K steps, counters of the K steps, per-phase ms
+    per step)."""
     e.reset_counters()
-    e.set_param(58, 1)  # SPH_P_TIMING
+    e.set_param(abi.P_TIMING, 1)
     e.step(K)
-    return e.timers()["step"], e.counters(), e.timers()
+    t = e.timers()
+    e.set_param(abi.P_TIMING, 0)
+    return t["step"], e.counters(), {k: v / K for k, v in t.items()}
 
 
 def main():
@@ -202,33 +208,55 @@ def main():
     torch.cuda.set_device(local)
     if ws > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    from sph_playground_b200 import abi, ic
+    from sph_playground_b200 import ic
 
     lib = abi.load()
     st, store = ic.sedov3d(n=args.n)
     N = store.shape[0]
     peak32, peak64 = measure_peak()
 
-    def engine(prec):
-        e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+    def engine(prec, st_=None, store_=None):
+        e = abi.Engine(st if st_ is None else st_, store if store_ is None else store_, "m6",
+                       precision=prec, lib=lib)
         for kv in args.param:
             k, v = kv.split("=")
             e.set_param(int(k) if k.isdigit() else getattr(abi, k, k), float(v))
         return e
 
-    # FP32 vs FP64 density error on the bench input (the metric's rho bound)
-    e32 = engine(abi.PREC_FP32_COMP)
+    def field_errors(st_, store_):
+        """FP32-comp vs FP64: one iterate on the same state; rho and h per
+        particle, a / du/dt / dh/dt per particle relative to the field's
+        largest magnitude (a lattice at rest has a ~ 0 almost everywhere)."""
+        e32, e64 = engine(abi.PREC_FP32_COMP, st_, store_), engine(abi.PREC_FP64, st_, store_)
+        e32.iterate()
+        e64.iterate()
+        r32, r64 = e32.get_store(), e64.get_store()
+        e32.close()
+        e64.close()
+        C = {k: v - 1 for k, v in abi.consts.es.items()}
+        out = {}
+        for name in ("den", "h"):
+            rel = np.abs(r32[:, C[name]] - r64[:, C[name]]) / np.abs(r64[:, C[name]])
+            out["rho" if name == "den" else name] = {"max": float(rel.max()),
+                                                     "p99.9": float(np.quantile(rel, 0.999))}
+        for name, cols in (("a", [C["ax"], C["ay"], C["az"]]), ("du", [C["du"]]),
+                           ("dh", [C["dh"]])):
+            d = np.linalg.norm(r32[:, cols] - r64[:, cols], axis=1)
+            ref = np.linalg.norm(r64[:, cols], axis=1).max()
+            rel = d / ref if ref > 0 else d
+            out[name + "_rel_field_max"] = {"max": float(rel.max()),
+                                            "p99.9": float(np.quantile(rel, 0.999))}
+        return out
+
+    # FP32 vs FP64 errors on the bench input and after the warm-up steps
+    errs = {"t0": field_errors(st, store)}
     e64 = engine(abi.PREC_FP64)
-    e32.density()
-    e64.density()
-    r32, r64 = e32.get_store(), e64.get_store()
-    col = abi.consts.es["den"] - 1
-    rel = np.abs(r32[:, col] - r64[:, col]) / np.abs(r64[:, col])
-    rho_err = {"max": float(rel.max()), "p99.9": float(np.quantile(rel, 0.999))}
-    hcol = abi.consts.es["h"] - 1
-    relh = np.abs(r32[:, hcol] - r64[:, hcol]) / np.abs(r64[:, hcol])
-    e32.close()
+    e64.set_param(abi.consts.ec["tfinish"], 1.0)
+    e64.step(max(args.warmup, 1))
+    mid_store, mid_st = e64.get_store(), e64.get_state()
     e64.close()
+    errs[f"after_{max(args.warmup, 1)}_steps"] = field_errors(mid_st, mid_store)
+    rho_err = max((v["rho"] for v in errs.values()), key=lambda x: x["max"])
 
     def run(prec):
         e = engine(prec)
@@ -259,7 +287,8 @@ def main():
     # roofline of the dominant pair kernel: algorithmic FLOPs / its event time
     c1_flops = cnt["c1_pairs"] * F1_C1
     c2_flops = cnt["c2_pairs"] * F2_C2
-    kern = {"circuit1": (c1_flops, tm["circuit1"]), "circuit2": (c2_flops, tm["circuit2"])}
+    kern = {"circuit1": (c1_flops / args.steps, tm["circuit1"]),
+            "circuit2": (c2_flops / args.steps, tm["circuit2"])}
     dom = max(kern, key=lambda k: kern[k][1])
     ach = kern[dom][0] / (kern[dom][1] * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": peak32 / 1e12,
@@ -302,7 +331,7 @@ def main():
                                   "c1_max_sweeps": cnt6["c1_sweeps"], "neib_max": cnt6["neib_max"],
                                   "searches": cnt6["searches"] / args.steps,
                                   "candidates": cnt6["candidates"] / args.steps},
-                "phases_ms_per_step": {k: v / args.steps for k, v in tm6.items()},
+                "phases_ms_per_step": tm6,
                 "peak_fp64_tflops": peak64 / 1e12}
 
     cpu = None
@@ -327,8 +356,8 @@ def main():
             "gpu_launches": cnt["launches"],
             "clocks": clocks,
             "rho_rel_err_fp32_vs_fp64": rho_err,
-            "h_rel_err_fp32_vs_fp64": {"max": float(relh.max())},
-            "phases_ms_per_step": {k: v / args.steps for k, v in tm.items()},
+            "errors_fp32_vs_fp64": errs,
+            "phases_ms_per_step": tm,
             "work_per_step": {"neib_pairs": cnt["neib_pairs"] / args.steps,
                               "c1_pairs": cnt["c1_pairs"] / args.steps,
                               "c2_pairs": cnt["c2_pairs"] / args.steps,

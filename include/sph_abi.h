@@ -61,7 +61,8 @@ extern "C" {
                                     when n_i+1 > maxneibnum; default 0       */
 #define SPH_P_CELL_FACTOR     56 /* cell edge / (krad*h_min), default 0.5    */
 #define SPH_P_REORDER_EVERY   57 /* physical re-sort interval in steps (8)   */
-#define SPH_P_TIMING          58 /* 1: record per-kernel CUDA-event times    */
+#define SPH_P_TIMING          58 /* 1: CUDA-event times per phase and per
+                                       call (sph_get_timers); 2: per call only */
 #define SPH_P_NEIB_CAP        59 /* neighbour slots per centre (0 = auto)    */
 #define SPH_P_LANES_SEARCH    60 /* lanes per centre in the neighbour search
                                     (4, 8, 16, 32; 0 = auto)                  */
@@ -121,7 +122,9 @@ extern "C" {
 #define SPH_T_TIMESTEP   7
 #define SPH_T_STS        8
 #define SPH_T_STEP       9 /* whole sph_step / sph_run_to calls */
-#define SPH_T_TOTAL      10
+#define SPH_T_PACK      10 /* pair-data packing before circuit1 and circuit2
+                              (not part of SPH_T_CIRCUIT1 / SPH_T_CIRCUIT2) */
+#define SPH_T_TOTAL      11
 
 typedef struct sph_handle sph_handle;
 

@@ -47,7 +47,7 @@ COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c1_centre_sweeps", "launches", "neib_max", "searches",
             "exact_tests"]
 TIMERS = ["predict", "ghosts", "sort", "neighbours", "circuit1", "circuit2",
-          "correct", "timestep", "sts", "step"]
+          "correct", "timestep", "sts", "step", "pack"]
 
 # every symbol include/sph_abi.h declares
 ABI_SYMBOLS = [

@@ -201,7 +201,8 @@ struct sph_handle {
     int slot;
     cudaEvent_t a = nullptr, b = nullptr;
     Phase(sph_handle* hh, int sl) : h(hh), slot(sl) {
-      if (h->st[SPH_P_TIMING] != 0) {
+      const double mode = h->st[SPH_P_TIMING];
+      if (mode == 1 || (mode == 2 && sl == SPH_T_STEP)) {
         a = h->get_event();
         b = h->get_event();
         cudaEventRecord(a, h->s);
@@ -467,9 +468,13 @@ struct sph_handle {
       Phase ph(this, SPH_T_GHOSTS);
       if (m.ghosts) launch_reflect(cols.as<double>(), nrows, nreal, g, s);
       // reduction slots: lo (min), hi (max), hmin
-      launch_fill_u64(red.as<unsigned long long>() + RED_LO_X, 3, dkey(1e308), s);
-      launch_fill_u64(red.as<unsigned long long>() + RED_HI_X, 3, dkey(-1e308), s);
-      launch_fill_u64(red.as<unsigned long long>() + RED_HMIN, 1, dkey(1e308), s);
+      SlotInit si{};
+      for (int k = 0; k < 3; ++k) {
+        si.off[si.n] = RED_LO_X + k; si.val[si.n++] = dkey(1e308);
+        si.off[si.n] = RED_HI_X + k; si.val[si.n++] = dkey(-1e308);
+      }
+      si.off[si.n] = RED_HMIN; si.val[si.n++] = dkey(1e308);
+      launch_init_slots(red.as<unsigned long long>(), si, s);
       BoxGeom gg = g;
       if (!m.ghosts) for (int k = 0; k < 3; ++k) gg.periodic[k] = 0;
       launch_ghost_count(cols.as<double>(), nrows, nreal, gg, d, gcount.as<int32_t>(),
@@ -638,7 +643,6 @@ struct sph_handle {
 
   // ---- circuit1 + EOS ----------------------------------------------------------------------
   int circuit1(const Mode& m, Params& P) {
-    Phase ph(this, SPH_T_CIRCUIT1);
     const int64_t nall = nrows + nghost;
     PackBufs pb = packs();
     P.eos_kind = m.eos_kind;
@@ -652,8 +656,12 @@ struct sph_handle {
       CK(cudaStreamSynchronize(s));
       P.c_iso = h_ctrl[7];
     }
-    launch_pack(prec, PACK_POS, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
-                sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+    {
+      Phase pk(this, SPH_T_PACK);
+      launch_pack(prec, PACK_POS, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+                  sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+    }
+    Phase ph(this, SPH_T_CIRCUIT1);
     C1Args a{};
     a.nc = nreal;
     a.rowoff = rowoff.as<int64_t>();
@@ -715,12 +723,15 @@ struct sph_handle {
   }
 
   int circuit2(const Mode& m, const Params& P) {
-    Phase ph(this, SPH_T_CIRCUIT2);
     const int64_t nall = nrows + nghost;
     PackBufs pb = packs();
     int groups = PACK_POS | PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
-    launch_pack(prec, groups, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
-                sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+    {
+      Phase pk(this, SPH_T_PACK);
+      launch_pack(prec, groups, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+                  sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+    }
+    Phase ph(this, SPH_T_CIRCUIT2);
     C2Args a{};
     a.nc = nreal;
     a.rowoff = rowoff.as<int64_t>();
@@ -803,14 +814,13 @@ struct sph_handle {
     Params P{};
     RC(params(P));
     unsigned long long* r = red.as<unsigned long long>();
-    launch_fill_u64(r + RED_TS_HMIN, 1, dkey(1e308), s);
-    launch_fill_u64(r + RED_TS_CMAX, 1, dkey(-1e308), s);
-    launch_fill_u64(r + RED_TS_DENMIN, 1, dkey(1e308), s);
-    launch_fill_u64(r + RED_TS_CMIN, 1, dkey(1e308), s);
-    launch_fill_u64(r + RED_TS_KAPMAX, 1, dkey(-1e308), s);
-    launch_fill_u64(r + RED_TS_BMAX, 1, dkey(-1e308), s);
-    launch_fill_u64(r + RED_TS_KAPMIN, 1, dkey(1e308), s);
-    launch_fill_u64(r + RED_TS_LAMMAX, 1, dkey(-1e308), s);
+    SlotInit si{};
+    const int slot[8] = {RED_TS_HMIN, RED_TS_CMAX, RED_TS_DENMIN, RED_TS_CMIN,
+                         RED_TS_KAPMAX, RED_TS_BMAX, RED_TS_KAPMIN, RED_TS_LAMMAX};
+    const double init[8] = {1e308, -1e308, 1e308, 1e308, -1e308, -1e308, 1e308, -1e308};
+    for (int k = 0; k < 8; ++k) { si.off[k] = slot[k]; si.val[k] = dkey(init[k]); }
+    si.n = 8;
+    launch_init_slots(r, si, s);
     launch_timestep_reduce(cols.as<double>(), nrows, orig.as<int32_t>(), nrows,
                            int64_t(st[ec_realpn]), P, r, s);
     CK(cudaMemcpyAsync(h_red + RED_TS_HMIN, r + RED_TS_HMIN,
@@ -818,7 +828,9 @@ struct sph_handle {
                        cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     CK(cudaGetLastError());
-    collect_timers();  // every earlier phase has completed at this point
+    // every earlier phase has completed at this point; the event pairs are
+    // read at the end of the call unless many have piled up
+    if (pending_ev.size() > 4096) collect_timers();
     double hmin = dkey_inv(h_red[RED_TS_HMIN]), cmax = dkey_inv(h_red[RED_TS_CMAX]);
     double denmin = dkey_inv(h_red[RED_TS_DENMIN]), cmin = dkey_inv(h_red[RED_TS_CMIN]);
     double kapmax = dkey_inv(h_red[RED_TS_KAPMAX]), bmax = dkey_inv(h_red[RED_TS_BMAX]);

@@ -1001,6 +1001,14 @@ void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStr
   k_fill_u64<<<nblocks(n), TPB, 0, s>>>(p, n, v);
   note_launch();
 }
+__global__ void k_init_slots(unsigned long long* p, SlotInit in) {
+  const int i = threadIdx.x;
+  if (i < in.n) p[in.off[i]] = in.val[i];
+}
+void launch_init_slots(unsigned long long* p, const SlotInit& in, cudaStream_t s) {
+  k_init_slots<<<1, 32, 0, s>>>(p, in);
+  note_launch();
+}
 void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, double a0,
                       double a1, double a2, double a3, double a4, const double* ctrl,
                       cudaStream_t s) {

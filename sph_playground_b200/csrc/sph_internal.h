@@ -152,6 +152,13 @@ void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig,
                             int64_t nrows, int64_t n_ts, Params P,
                             unsigned long long* red, cudaStream_t s);
 void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s);
+// up to 8 single reduction slots set in one launch: p[off[i]] = val[i]
+struct SlotInit {
+  int n;
+  int off[8];
+  unsigned long long val[8];
+};
+void launch_init_slots(unsigned long long* p, const SlotInit& in, cudaStream_t s);
 void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s);
 void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, double a0,
                       double a1, double a2, double a3, double a4, const double* ctrl,
