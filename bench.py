@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-errors", action="store_true",
+                    help="skip the FP32-vs-FP64 error check (profiling runs)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-n", type=int, default=64, help="lattice per axis of the CPU sample")
     ap.add_argument("--param", action="append", default=[],
@@ -249,14 +251,16 @@ def main():
         return out
 
     # FP32 vs FP64 errors on the bench input and after the warm-up steps
-    errs = {"t0": field_errors(st, store)}
-    e64 = engine(abi.PREC_FP64)
-    e64.set_param(abi.consts.ec["tfinish"], 1.0)
-    e64.step(max(args.warmup, 1))
-    mid_store, mid_st = e64.get_store(), e64.get_state()
-    e64.close()
-    errs[f"after_{max(args.warmup, 1)}_steps"] = field_errors(mid_st, mid_store)
-    rho_err = max((v["rho"] for v in errs.values()), key=lambda x: x["max"])
+    errs, rho_err = None, None
+    if not args.no_errors:
+        errs = {"t0": field_errors(st, store)}
+        e64 = engine(abi.PREC_FP64)
+        e64.set_param(abi.consts.ec["tfinish"], 1.0)
+        e64.step(max(args.warmup, 1))
+        mid_store, mid_st = e64.get_store(), e64.get_state()
+        e64.close()
+        errs[f"after_{max(args.warmup, 1)}_steps"] = field_errors(mid_st, mid_store)
+        rho_err = max((v["rho"] for v in errs.values()), key=lambda x: x["max"])
 
     def run(prec):
         e = engine(prec)

@@ -40,23 +40,41 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 // ---- store transposes -----------------------------------------------------------
-__global__ void k_upload(const double* __restrict__ rm, double* __restrict__ cols,
-                         int32_t* __restrict__ orig, int64_t n) {
-  int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (t >= n * NCOL) return;
-  int64_t i = t / NCOL;
-  int f = int(t - i * NCOL);
-  cols[f * n + i] = rm[t];
-  if (f == 0) orig[i] = int32_t(i);
+// Row-major (n x NCOL) table <-> column store, through 32 x 32 tiles in
+// shared memory so that both the row reads / writes and the column writes /
+// reads are contiguous runs of 256 bytes.  Block (32, 8): tile of 32 rows.
+static_assert(NCOL == 32, "the tile transposes assume 32 fields");
+__global__ void __launch_bounds__(256)
+k_upload(const double* __restrict__ rm, double* __restrict__ cols, int32_t* __restrict__ orig,
+         int64_t n) {
+  __shared__ double tile[32][33];
+  const int64_t r0 = int64_t(blockIdx.x) * 32;
+  for (int k = threadIdx.y; k < 32; k += 8) {  // row r0 + k, field threadIdx.x
+    const int64_t i = r0 + k;
+    if (i < n) tile[k][threadIdx.x] = rm[i * NCOL + threadIdx.x];
+  }
+  __syncthreads();
+  for (int f = threadIdx.y; f < NCOL; f += 8) {  // field f, row r0 + threadIdx.x
+    const int64_t i = r0 + threadIdx.x;
+    if (i < n) cols[f * n + i] = tile[threadIdx.x][f];
+  }
+  if (threadIdx.y == 0 && r0 + threadIdx.x < n) orig[r0 + threadIdx.x] = int32_t(r0 + threadIdx.x);
 }
 
-__global__ void k_download(const double* __restrict__ cols, const int32_t* __restrict__ orig,
-                           double* __restrict__ rm, int64_t n) {
-  int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (t >= n * NCOL) return;
-  int64_t i = t / NCOL;
-  int f = int(t - i * NCOL);
-  rm[int64_t(orig[i]) * NCOL + f] = cols[f * n + i];
+__global__ void __launch_bounds__(256)
+k_download(const double* __restrict__ cols, const int32_t* __restrict__ orig,
+           double* __restrict__ rm, int64_t n) {
+  __shared__ double tile[32][33];
+  const int64_t r0 = int64_t(blockIdx.x) * 32;
+  for (int f = threadIdx.y; f < NCOL; f += 8) {  // field f of physical row r0 + threadIdx.x
+    const int64_t i = r0 + threadIdx.x;
+    if (i < n) tile[threadIdx.x][f] = cols[f * n + i];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {  // physical row r0 + k to its original row
+    const int64_t i = r0 + k;
+    if (i < n) rm[int64_t(orig[i]) * NCOL + threadIdx.x] = tile[k][threadIdx.x];
+  }
 }
 
 __global__ void k_reorder(const double* __restrict__ cin, double* __restrict__ cout,
@@ -146,40 +164,70 @@ __device__ __forceinline__ double image_coord(double x, int sign, double emin, d
   return x;
 }
 
-__global__ void k_ghost_count(const double* __restrict__ cols, int64_t ld, int64_t nrows,
-                              int64_t nreal, BoxGeom g, int dim, int32_t* __restrict__ count,
-                              unsigned long long* __restrict__ red) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  double hmin = 1e300;
-  int c = 0;
-  if (i < nrows) {
+// Reduction of per-thread partial minima / maxima over the block: one value
+// per slot leaves the block (then one atomic per block and slot, so that the
+// slots see a few thousand atomics per launch rather than one per warp).
+template <int K>
+__device__ __forceinline__ void block_minmax(double (&v)[K], const bool (&is_max)[K]) {
+  __shared__ double part[TPB / 32][K];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < K; ++j) v[j] = is_max[j] ? warp_max(v[j]) : warp_min(v[j]);
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) part[warp][j] = v[j];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      double x = lane < int(blockDim.x >> 5) ? part[lane][j] : (is_max[j] ? -1e308 : 1e308);
+      v[j] = is_max[j] ? warp_max(x) : warp_min(x);
+    }
+  }
+}
+// grid of the reduction kernels: a few blocks per SM, each thread striding
+// over the rows
+inline int reduce_blocks(int64_t n) {
+  const int64_t b = (n + TPB - 1) / TPB;
+  return int(b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8);
+}
+
+__global__ void __launch_bounds__(TPB)
+k_ghost_count(const double* __restrict__ cols, int64_t ld, int64_t nrows, int64_t nreal,
+              BoxGeom g, int dim, int32_t* __restrict__ count,
+              unsigned long long* __restrict__ red) {
+  // slots: lo x, y, z (min), hi x, y, z (max), hmin (min)
+  double v[7] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 1e300};
+  const bool is_max[7] = {false, false, false, true, true, true, false};
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nrows;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    int c = 0;
     double r[3] = {cols[es_rx * ld + i], cols[es_ry * ld + i], cols[es_rz * ld + i]};
-    for (int k = 0; k < 3; ++k) { lo[k] = r[k]; hi[k] = r[k]; }
-    if (i < nreal) hmin = cols[es_h * ld + i];
+    for (int k = 0; k < 3; ++k) { v[k] = fmin(v[k], r[k]); v[3 + k] = fmax(v[3 + k], r[k]); }
+    if (i < nreal) v[6] = fmin(v[6], cols[es_h * ld + i]);
     if (ghost_source(cols[es_type * ld + i])) {
-      AxisSigns s = axis_signs(r, g, dim);
+      AxisSigns sg_ = axis_signs(r, g, dim);
       for (int mask = 1; mask < 8; ++mask) {
         int sg[3];
-        if (!image_of(s, mask, sg)) continue;
+        if (!image_of(sg_, mask, sg)) continue;
         ++c;
         for (int k = 0; k < 3; ++k) {
-          double v = image_coord(r[k], sg[k], g.emin[k], g.emax[k]);
-          lo[k] = fmin(lo[k], v);
-          hi[k] = fmax(hi[k], v);
+          double x = image_coord(r[k], sg[k], g.emin[k], g.emax[k]);
+          v[k] = fmin(v[k], x);
+          v[3 + k] = fmax(v[3 + k], x);
         }
       }
     }
     count[i] = c;
   }
-  for (int k = 0; k < 3; ++k) { lo[k] = warp_min(lo[k]); hi[k] = warp_max(hi[k]); }
-  hmin = warp_min(hmin);
-  if ((threadIdx.x & 31) == 0) {
+  block_minmax<7>(v, is_max);
+  if (threadIdx.x == 0) {
     for (int k = 0; k < 3; ++k) {
-      if (lo[k] < 1e300) red_min(&red[RED_LO_X + k], lo[k]);
-      if (hi[k] > -1e300) red_max(&red[RED_HI_X + k], hi[k]);
+      if (v[k] < 1e300) red_min(&red[RED_LO_X + k], v[k]);
+      if (v[3 + k] > -1e300) red_max(&red[RED_HI_X + k], v[3 + k]);
     }
-    if (hmin < 1e300) red_min(&red[RED_HMIN], hmin);
+    if (v[6] < 1e300) red_min(&red[RED_HMIN], v[6]);
   }
 }
 
@@ -758,36 +806,42 @@ __global__ void k_correct(double* __restrict__ cols, int64_t ld, const int32_t* 
 
 // ---- timestep reductions (timestep.f90:40-166) -----------------------------------------------
 // Over the first realpn rows in original order.
-__global__ void k_timestep_reduce(const double* __restrict__ cols, int64_t ld,
-                                  const int32_t* __restrict__ orig, int64_t nrows, int64_t n_ts,
-                                  Params P, unsigned long long* __restrict__ red) {
-  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  double hmin = 1e308, cmax = -1e308, dmin = 1e308, cmin = 1e308, kmax = -1e308,
-         bmax = -1e308, kmin = 1e308, lmax = -1e308;
-  if (i < nrows && orig[i] < n_ts) {
+__global__ void __launch_bounds__(TPB)
+k_timestep_reduce(const double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
+                  int64_t nrows, int64_t n_ts, Params P, unsigned long long* __restrict__ red) {
+  // slots: hmin, cmax, denmin, cmin, kapmax, bmax, kapmin, lammax
+  double v[8] = {1e308, -1e308, 1e308, 1e308, -1e308, -1e308, 1e308, -1e308};
+  const bool is_max[8] = {false, true, false, false, true, true, false, true};
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nrows;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    if (orig[i] >= n_ts) continue;
     double h = cols[es_h * ld + i], c = cols[es_c * ld + i], d = cols[es_den * ld + i];
     double ka = cols[es_kappa * ld + i];
-    hmin = h; cmax = c; dmin = d; cmin = c; kmax = ka; kmin = ka;
-    bmax = fmax(fmax(cols[es_bx * ld + i], cols[es_by * ld + i]), cols[es_bz * ld + i]);
+    v[0] = fmin(v[0], h);
+    v[1] = fmax(v[1], c);
+    v[2] = fmin(v[2], d);
+    v[3] = fmin(v[3], c);
+    v[4] = fmax(v[4], ka);
+    v[5] = fmax(v[5], fmax(fmax(cols[es_bx * ld + i], cols[es_by * ld + i]), cols[es_bz * ld + i]));
+    v[6] = fmin(v[6], ka);
     if (P.eq_fld) {
       double n0 = cols[es_dtdx * ld + i], n1 = cols[es_dtdy * ld + i], n2 = cols[es_dtdz * ld + i];
       double ta = cols[es_t * ld + i];
-      double g = sqrt(((0.0 + n0 * n0) + n1 * n1) + n2 * n2);
-      double fr = g / (ka * d * d * ta);
-      lmax = (2. + fr) / (6. + 3 * fr + fr * fr);
+      double gr = sqrt(((0.0 + n0 * n0) + n1 * n1) + n2 * n2);
+      double fr = gr / (ka * d * d * ta);
+      v[7] = fmax(v[7], (2. + fr) / (6. + 3 * fr + fr * fr));
     }
   }
-  hmin = warp_min(hmin); cmax = warp_max(cmax); dmin = warp_min(dmin); cmin = warp_min(cmin);
-  kmax = warp_max(kmax); bmax = warp_max(bmax); kmin = warp_min(kmin); lmax = warp_max(lmax);
-  if ((threadIdx.x & 31) == 0) {
-    red_min(&red[RED_TS_HMIN], hmin);
-    red_max(&red[RED_TS_CMAX], cmax);
-    red_min(&red[RED_TS_DENMIN], dmin);
-    red_min(&red[RED_TS_CMIN], cmin);
-    red_max(&red[RED_TS_KAPMAX], kmax);
-    red_max(&red[RED_TS_BMAX], bmax);
-    red_min(&red[RED_TS_KAPMIN], kmin);
-    red_max(&red[RED_TS_LAMMAX], lmax);
+  block_minmax<8>(v, is_max);
+  if (threadIdx.x == 0) {
+    red_min(&red[RED_TS_HMIN], v[0]);
+    red_max(&red[RED_TS_CMAX], v[1]);
+    red_min(&red[RED_TS_DENMIN], v[2]);
+    red_min(&red[RED_TS_CMIN], v[3]);
+    red_max(&red[RED_TS_KAPMAX], v[4]);
+    red_max(&red[RED_TS_BMAX], v[5]);
+    red_min(&red[RED_TS_KAPMIN], v[6]);
+    red_max(&red[RED_TS_LAMMAX], v[7]);
   }
 }
 
@@ -878,12 +932,14 @@ __global__ void k_set(double* col, int64_t n, double v) {
 
 // ---- launchers ------------------------------------------------------------------------------
 void launch_upload_store(const double* rm, double* cols, int32_t* orig, int64_t n, cudaStream_t s) {
-  k_upload<<<nblocks(n * NCOL), TPB, 0, s>>>(rm, cols, orig, n);
+  if (n <= 0) return;
+  k_upload<<<unsigned((n + 31) / 32), dim3(32, 8), 0, s>>>(rm, cols, orig, n);
   note_launch();
 }
 void launch_download_store(const double* cols, const int32_t* orig, double* rm, int64_t n,
                            cudaStream_t s) {
-  k_download<<<nblocks(n * NCOL), TPB, 0, s>>>(cols, orig, rm, n);
+  if (n <= 0) return;
+  k_download<<<unsigned((n + 31) / 32), dim3(32, 8), 0, s>>>(cols, orig, rm, n);
   note_launch();
 }
 void launch_reorder(const double* cin, double* cout, const int32_t* oin, int32_t* oout,
@@ -899,7 +955,8 @@ void launch_reflect(double* cols, int64_t ld, int64_t nreal, BoxGeom g, cudaStre
 }
 void launch_ghost_count(const double* cols, int64_t nrows, int64_t nreal, BoxGeom g, int dim,
                         int32_t* count, unsigned long long* red, cudaStream_t s) {
-  k_ghost_count<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, nreal, g, dim, count, red);
+  k_ghost_count<<<reduce_blocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, nreal, g, dim, count,
+                                                     red);
   note_launch();
 }
 void launch_ghost_write(const double* cols, int64_t nrows, BoxGeom g, int dim,
@@ -990,7 +1047,7 @@ void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows
 }
 void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
                             int64_t n_ts, Params P, unsigned long long* red, cudaStream_t s) {
-  k_timestep_reduce<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_ts, P, red);
+  k_timestep_reduce<<<reduce_blocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_ts, P, red);
   note_launch();
 }
 void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s) {
