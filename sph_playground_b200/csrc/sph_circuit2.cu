@@ -118,7 +118,8 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     const bool artts = P.artts == 1, adden = P.adden == 1, hydro = P.eq_hydro != 0;
     const bool use_au = P.au != -1.0;
     const R rPiA = A.rho * A.Pi;  // 1 / (rho_a Omega_a)
-    Acc<R> dv[3], du, drho, ddt, db[3];
+    // force-type sums: plain per lane (a few tens of terms), FP64 over lanes
+    SumAcc<R> dv[3], du, drho, ddt, db[3];
     for (int d = 0; d < 3; ++d) { dv[d].init(); db[d].init(); }
     du.init(); drho.init(); ddt.init();
 

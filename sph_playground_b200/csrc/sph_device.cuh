@@ -190,6 +190,17 @@ template <class R> struct Acc {
   __device__ __forceinline__ R val() const { return s + c; }
   __device__ __forceinline__ double dval() const { return double(s) + double(c); }
 };
+// Plain running sum in R with the same interface: a lane's share of a pair
+// loop (n terms) carries at most gamma_n * sum|t| of rounding, about 2e-6
+// sum|t| in FP32 for the n ~ 30 terms of a force lane; the lanes are then
+// added in FP64.
+template <class R> struct SumAcc {
+  R s;
+  __device__ __forceinline__ void init() { s = R(0); }
+  __device__ __forceinline__ void add(R x) { s += x; }
+  __device__ __forceinline__ R val() const { return s; }
+  __device__ __forceinline__ double dval() const { return double(s); }
+};
 // Plain FP64 accumulator with the same interface.
 template <> struct Acc<double> {
   double s;
