@@ -175,6 +175,28 @@ int sph_get_counters(sph_handle* h, int64_t* out, int n);
 int sph_reset_counters(sph_handle* h);
 int sph_get_timers(sph_handle* h, double* out_ms, int n);
 
+/* ---- batches of instances -----------------------------------------------
+ * Many independent runs stepped together (the resolution x method sweeps
+ * of the experiment runners, e.g. runner/anisotropic/
+ * 000_anisopaper_v1_gls_kxx.py, which run one Context after another through
+ * CleanRun / ContinueRun, core.py:152-156).  Each instance keeps its own
+ * handle, stream and time loop; a batch runs the instances' steps from one
+ * host worker per instance, so their kernels and their host round trips
+ * (dt, image counts, list sizes) overlap on the device instead of queueing
+ * one run behind the other.  The handles stay owned by the caller and must
+ * not be used elsewhere while a batch call runs.  Results equal those of
+ * the instances stepped one by one. */
+typedef struct sph_batch sph_batch;
+int sph_batch_create(int n_inst, sph_handle* const* handles, sph_batch** out);
+/* sph_step(h_i, nsteps) for every instance */
+int sph_batch_step(sph_batch* b, int nsteps);
+/* sph_run_to(h_i, tfinish) for every instance */
+int sph_batch_run_to(sph_batch* b, double tfinish);
+/* status of every instance's last batch call (0 = ok); the call itself
+ * returns the first non-zero status, its message in sph_last_error */
+int sph_batch_status(sph_batch* b, int* status, int n);
+void sph_batch_destroy(sph_batch* b);
+
 /* ---- allocation-free density ---------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a code running inside another application's fixed device-memory

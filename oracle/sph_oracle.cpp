@@ -42,6 +42,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -1441,5 +1442,58 @@ int sph_get_timers(sph_handle* h, double* out_ms, int n) {
 }
 
 void sph_destroy(sph_handle* h) { delete h; }
+
+// Batches: the reference runs the instances of a sweep one after another
+// (runner/anisotropic/000_anisopaper_v1_gls_kxx.py through CleanRun /
+// ContinueRun, core.py:152-156), and so does the oracle.
+struct sph_batch {
+  std::vector<sph_handle*> h;
+  std::vector<int> status;
+};
+
+int sph_batch_create(int n_inst, sph_handle* const* handles, sph_batch** out) {
+  if (!out || !handles || n_inst <= 0) return fail(SPH_ERR_ARG, "bad batch arguments");
+  for (int i = 0; i < n_inst; ++i) {
+    if (!handles[i]) return fail(SPH_ERR_ARG, "null handle in batch");
+    for (int j = 0; j < i; ++j)
+      if (handles[j] == handles[i]) return fail(SPH_ERR_ARG, "handle twice in batch");
+  }
+  auto* b = new sph_batch();
+  b->h.assign(handles, handles + n_inst);
+  b->status.assign(n_inst, 0);
+  *out = b;
+  return SPH_OK;
+}
+
+static int batch_each(sph_batch* b, const std::function<int(sph_handle*)>& fn) {
+  int first = SPH_OK;
+  std::string msg;
+  for (size_t i = 0; i < b->h.size(); ++i) {
+    b->status[i] = fn(b->h[i]);
+    if (b->status[i] && !first) {
+      first = b->status[i];
+      msg = "instance " + std::to_string(i) + ": " + g_err;
+    }
+  }
+  return first ? fail(first, msg) : SPH_OK;
+}
+
+int sph_batch_step(sph_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return fail(SPH_ERR_ARG, "bad argument");
+  return batch_each(b, [nsteps](sph_handle* h) { return sph_step(h, nsteps); });
+}
+
+int sph_batch_run_to(sph_batch* b, double tfinish) {
+  if (!b) return fail(SPH_ERR_ARG, "null batch");
+  return batch_each(b, [tfinish](sph_handle* h) { return sph_run_to(h, tfinish); });
+}
+
+int sph_batch_status(sph_batch* b, int* status, int n) {
+  if (!b || !status) return fail(SPH_ERR_ARG, "null argument");
+  for (int i = 0; i < n && i < int(b->status.size()); ++i) status[i] = b->status[i];
+  return SPH_OK;
+}
+
+void sph_batch_destroy(sph_batch* b) { delete b; }
 
 }  // extern "C"

@@ -55,6 +55,8 @@ ABI_SYMBOLS = [
     "sph_iterate", "sph_density", "sph_step", "sph_run_to", "sph_get_store",
     "sph_get_state", "sph_get_neighbours", "sph_get_counters",
     "sph_reset_counters", "sph_get_timers", "sph_last_error", "sph_destroy",
+    "sph_batch_create", "sph_batch_step", "sph_batch_run_to", "sph_batch_status",
+    "sph_batch_destroy",
 ]
 
 
@@ -101,8 +103,14 @@ def load(path=None):
     lib.sph_last_error.restype = ctypes.c_char_p
     lib.sph_destroy.argtypes = [vp]
     lib.sph_destroy.restype = None
+    lib.sph_batch_create.argtypes = [c_int, P(vp), P(vp)]
+    lib.sph_batch_step.argtypes = [vp, c_int]
+    lib.sph_batch_run_to.argtypes = [vp, d]
+    lib.sph_batch_status.argtypes = [vp, P(c_int), c_int]
+    lib.sph_batch_destroy.argtypes = [vp]
+    lib.sph_batch_destroy.restype = None
     for name in ABI_SYMBOLS:
-        if name not in ("sph_last_error", "sph_destroy"):
+        if name not in ("sph_last_error", "sph_destroy", "sph_batch_destroy"):
             getattr(lib, name).restype = c_int
     _libs[path] = lib
     return lib
@@ -224,3 +232,53 @@ class Engine:
         out = np.zeros(len(TIMERS), dtype=np.float64)
         self._check(self.lib.sph_get_timers(self.h, _dptr(out), len(TIMERS)))
         return dict(zip(TIMERS, (float(x) for x in out)))
+
+
+class Batch:
+    """Several Engine instances stepped together (sph_batch_*): every
+    instance runs its own time loop, the instances overlap on the device.
+    The engines stay usable after the batch is closed."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        if not self.engines:
+            raise ValueError("empty batch")
+        self.lib = self.engines[0].lib
+        if any(e.lib is not self.lib for e in self.engines):
+            raise ValueError("all engines of a batch must use the same library")
+        arr = (ctypes.c_void_p * len(self.engines))(*[e.h.value for e in self.engines])
+        b = ctypes.c_void_p()
+        self._check(self.lib.sph_batch_create(len(self.engines), arr, ctypes.byref(b)))
+        self.b = b
+
+    def _check(self, rc):
+        if rc != 0:
+            raise SphError(rc, self.lib.sph_last_error().decode(errors="replace"))
+
+    def step(self, nsteps=1):
+        self._check(self.lib.sph_batch_step(self.b, int(nsteps)))
+
+    def run_to(self, tfinish):
+        self._check(self.lib.sph_batch_run_to(self.b, float(tfinish)))
+
+    def status(self):
+        out = (ctypes.c_int * len(self.engines))()
+        self._check(self.lib.sph_batch_status(self.b, out, len(self.engines)))
+        return list(out)
+
+    def close(self):
+        if getattr(self, "b", None) is not None and self.b.value:
+            self.lib.sph_batch_destroy(self.b)
+            self.b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

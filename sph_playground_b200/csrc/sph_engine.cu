@@ -10,6 +10,7 @@
 // count, the Newton "still active" flag on the Jacobi path, the timestep
 // reductions) and nothing else.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,7 +25,7 @@ using namespace sph;
 namespace {
 
 thread_local std::string g_err;
-long long g_launches = 0;
+std::atomic<long long> g_launches{0};
 
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -129,6 +130,7 @@ long long launches_so_far() { return g_launches; }
 }  // namespace sph
 
 struct sph_handle {
+  int dev = 0;  // the device current at sph_create
   int kernel_id = SPH_KERNEL_M6;
   int prec = SPH_PREC_FP64;
   KBase kb;
@@ -510,7 +512,7 @@ struct sph_handle {
     if (!(hmin > 0) || !std::isfinite(hmin)) return fail(SPH_ERR_IC_H, "smoothing length <= 0");
     for (int k = 0; k < 3; ++k)
       if (!std::isfinite(lo[k]) || !std::isfinite(hi[k])) return fail(SPH_ERR_Q_NAN, "q is nan");
-    double cf = st[SPH_P_CELL_FACTOR] > 0 ? st[SPH_P_CELL_FACTOR] : 0.5;
+    double cf = st[SPH_P_CELL_FACTOR] > 0 ? st[SPH_P_CELL_FACTOR] : 0.4;
     double L = P.krad * hmin * cf;
     int64_t ncell = 0;
     int n3[3];
@@ -981,6 +983,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
     return fail(SPH_ERR_CUDA, "no CUDA device");
   }
   auto* h = new sph_handle();
+  cudaGetDevice(&h->dev);
   h->kernel_id = kernel_id;
   h->prec = precision_mode;
   h->kb = kbase(kernel_id);
@@ -990,7 +993,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
   h->st[SPH_P_AV_BETA] = 2.;
   h->st[SPH_P_NEWTON_TOL] = 1e-8;
   h->st[SPH_P_NEWTON_MAXITER] = 100;
-  h->st[SPH_P_CELL_FACTOR] = 0.5;
+  h->st[SPH_P_CELL_FACTOR] = 0.4;
   h->st[SPH_P_REORDER_EVERY] = 8;
   h->nreal = int64_t(h->st[ec_realpn]);
   h->nfixed = std::max<int64_t>(0, int64_t(h->st[ec_fixedpn]));
@@ -1232,3 +1235,7 @@ void sph_destroy(sph_handle* h) {
 }
 
 }  // extern "C"
+
+namespace sph {
+int handle_device(const sph_handle* h) { return h->dev; }
+}  // namespace sph

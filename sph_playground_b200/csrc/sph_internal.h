@@ -64,6 +64,8 @@ struct BoxGeom {
 
 // Record an error message for sph_last_error and return `code`.
 int sph_fail(int code, const std::string& msg);
+// The device a handle was created on.
+int handle_device(const sph_handle* h);
 
 // Count of this library's kernel launches (process-wide).
 void note_launch(int n = 1);
