@@ -67,7 +67,8 @@ extern "C" {
 #define SPH_P_LANES_SEARCH    60 /* lanes per centre in the neighbour search
                                     (4, 8, 16, 32; 0 = auto)                  */
 #define SPH_P_LANES_PAIR      61 /* lanes per centre in circuit1/circuit2     */
-#define SPH_P_LAST            61
+#define SPH_P_FIXED_DT        62 /* dt of sph_adjoint_forward's steps (> 0)   */
+#define SPH_P_LAST            62
 
 /* ---- status codes --------------------------------------------------------- */
 #define SPH_OK                     0
@@ -174,6 +175,34 @@ int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs,
 int sph_get_counters(sph_handle* h, int64_t* out, int n);
 int sph_reset_counters(sph_handle* h);
 int sph_get_timers(sph_handle* h, double* out_ms, int n);
+
+/* ---- adjoint (gradients of a final-state misfit) ------------------------
+ * No counterpart in the reference (its Fortran computes no derivatives).
+ * sph_adjoint_forward runs nsteps leapfrog steps of fixed dt
+ * (SPH_P_FIXED_DT; main.f90:323-362 without the timestep and output logic)
+ * from the handle's state, keeping a copy of the particle table every
+ * `every` steps; on a handle that has not stepped yet the initial force
+ * pass (main.f90:216-225) is part of the differentiated map.  It lowers the
+ * Newton tolerance (SPH_P_NEWTON_TOL) to 1e-12 and stops the physical
+ * re-ordering of rows (SPH_P_REORDER_EVERY = 0) on the handle: the
+ * differentiated density pass is the converged one.
+ * sph_adjoint_backward takes dL/dv, dL/du, dL/dr at the final state (caller
+ * row order, n_rows x 3 / n_rows / n_rows x 3; NULL = zero) and returns
+ * dL/dr0, dL/dv0 (n_rows x 3), dL/du0 (n_rows) at the initial state and
+ * dL/d(alpha, beta) (2 values; SPH_P_AV_ALPHA / SPH_P_AV_BETA), NULL
+ * outputs skipped.  It replays each segment from its copy and runs the
+ * hand-written adjoint kernels of the force pass (circuit2.f90:294-345), of
+ * the Newton-h density pass (circuit1.f90:76-224, by the implicit function
+ * theorem at convergence), of the EOS (eos.f90:21-33) and of the
+ * integrator.  Differentiated subset: equations = hydro, adden = yes
+ * (Newton h), artificial viscosity on or off with au = 0 or -1 (no
+ * artificial conductivity), adiabatic EOS,
+ * no fixed particles; other set-ups return SPH_ERR_UNSUPPORTED.  The handle
+ * is left at the final state of the forward run. */
+int sph_adjoint_forward(sph_handle* h, int nsteps, int every);
+int sph_adjoint_backward(sph_handle* h, const double* dl_dv, const double* dl_du,
+                         const double* dl_dr, double* g_r0, double* g_v0, double* g_u0,
+                         double* g_par);
 
 /* ---- batches of instances -----------------------------------------------
  * Many independent runs stepped together (the resolution x method sweeps

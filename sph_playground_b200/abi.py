@@ -41,6 +41,7 @@ P_TIMING = 58
 P_NEIB_CAP = 59
 P_LANES_SEARCH = 60
 P_LANES_PAIR = 61
+P_FIXED_DT = 62
 
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",
@@ -109,6 +110,11 @@ def load(path=None):
     lib.sph_batch_status.argtypes = [vp, P(c_int), c_int]
     lib.sph_batch_destroy.argtypes = [vp]
     lib.sph_batch_destroy.restype = None
+    if hasattr(lib, "sph_adjoint_forward"):  # the CUDA engine only
+        lib.sph_adjoint_forward.argtypes = [vp, c_int, c_int]
+        lib.sph_adjoint_forward.restype = c_int
+        lib.sph_adjoint_backward.argtypes = [vp, P(d), P(d), P(d), P(d), P(d), P(d), P(d)]
+        lib.sph_adjoint_backward.restype = c_int
     for name in ABI_SYMBOLS:
         if name not in ("sph_last_error", "sph_destroy", "sph_batch_destroy"):
             getattr(lib, name).restype = c_int
@@ -207,6 +213,33 @@ class Engine:
     def get_state(self):
         out = np.empty(consts.EC_TOTAL, dtype=np.float64)
         self._check(self.lib.sph_get_state(self.h, _dptr(out)))
+        return out
+
+    # ---- adjoint (CUDA engine only) -----------------------------------------
+    def adjoint_forward(self, nsteps, every):
+        """nsteps fixed-dt steps (P_FIXED_DT) with a table copy every `every`
+        steps, for adjoint_backward."""
+        self._check(self.lib.sph_adjoint_forward(self.h, int(nsteps), int(every)))
+
+    def adjoint_backward(self, dl_dv=None, dl_du=None, dl_dr=None):
+        """Gradients at the initial state of the last adjoint_forward run from
+        dL/dv, dL/du, dL/dr at its final state (caller row order): dict with
+        g_r0 (n x 3), g_v0 (n x 3), g_u0 (n), g_par (d/d alpha, d/d beta)."""
+        n = self.n_rows
+
+        def inp(a, shape):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+            return a
+        iv, iu, ir = inp(dl_dv, (n, 3)), inp(dl_du, (n,)), inp(dl_dr, (n, 3))
+        out = {"g_r0": np.zeros((n, 3)), "g_v0": np.zeros((n, 3)), "g_u0": np.zeros(n),
+               "g_par": np.zeros(2)}
+        nul = ctypes.POINTER(ctypes.c_double)()
+        ptr = lambda a: _dptr(a) if a is not None else nul  # noqa: E731
+        self._check(self.lib.sph_adjoint_backward(
+            self.h, ptr(iv), ptr(iu), ptr(ir), _dptr(out["g_r0"]), _dptr(out["g_v0"]),
+            _dptr(out["g_u0"]), _dptr(out["g_par"])))
         return out
 
     def get_neighbours(self):

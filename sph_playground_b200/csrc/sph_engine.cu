@@ -154,6 +154,13 @@ struct sph_handle {
   // neighbours: one row per centre inside nl, rows sized from each
   // particle's previous count (CSR with slack)
   DevBuf nl, ncnt, rowoff, rowcap, rowcap64, count_prev, h_prev, scan64_tmp, overflow;
+  // adjoint: per-row adjoint columns, d/d(alpha, beta), checkpoints of the
+  // particle table (the run's initial state, every k-th step, the final one)
+  // and the states of the segment being replayed
+  DevBuf adj, adj_par, adj_ckpt, adj_seg, adj_io;
+  int adj_nsteps = -1, adj_every = 0, adj_ncp = 0;
+  bool adj_initial_force = false;
+  double adj_dt = 0., adj_t0 = 0.;
   int64_t nl_size = 0;
   int est_count = 0;
   // scalars
@@ -892,6 +899,190 @@ struct sph_handle {
     return SPH_OK;
   }
 
+  // One leapfrog step with a given dt (main.f90:323-362 without the
+  // timestep and output logic): the differentiated forward map.  With
+  // `stop_before_correct` the step ends after the force pass, leaving the
+  // buffers of that pass for the adjoint kernels.
+  int fixed_step(double dt, bool stop_before_correct = false) {
+    h_ctrl[0] = dt;
+    CK(cudaMemcpyAsync(ctrl.p, h_ctrl, sizeof(double), cudaMemcpyHostToDevice, s));
+    {
+      Phase ph(this, SPH_T_PREDICT);
+      launch_predict(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
+                     ctrl.as<double>(), false, s);
+    }
+    RC(iterate(true));
+    if (stop_before_correct) return SPH_OK;
+    {
+      Phase ph(this, SPH_T_CORRECT);
+      launch_correct(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
+                     ctrl.as<double>(), false, s);
+    }
+    st[ec_time] += dt;
+    cnt_host[SPH_CNT_STEPS]++;
+    return SPH_OK;
+  }
+  size_t table_bytes() const { return sizeof(double) * NCOL * size_t(nrows); }
+  int copy_table(void* dst, const void* src) {
+    CK(cudaMemcpyAsync(dst, src, table_bytes(), cudaMemcpyDeviceToDevice, s));
+    return SPH_OK;
+  }
+  double* ckpt(int i) { return adj_ckpt.as<double>() + size_t(i) * NCOL * nrows; }
+  double* seg(int i) { return adj_seg.as<double>() + size_t(i) * NCOL * nrows; }
+
+  // the hydro subset the adjoint kernels differentiate
+  int adjoint_supported() {
+    eqset();
+    if (ival(ec_eqs) != eeq_hydro || eq_magneto || eq_diff || eq_fld || eq_sts || eq_radexch)
+      return fail(SPH_ERR_UNSUPPORTED, "adjoint: equations must be hydro");
+    if (ival(ec_adden) != 1)
+      return fail(SPH_ERR_UNSUPPORTED, "adjoint: needs the Newton h-iteration (adden = yes)");
+    if (ival(ec_artts) == 1 && st[ec_au] != -1.0 && st[ec_au] != 0.0)
+      return fail(SPH_ERR_UNSUPPORTED,
+                  "adjoint: artificial conductivity (au) is not differentiated; set au = 0 or -1");
+    if (nfixed > 0) return fail(SPH_ERR_UNSUPPORTED, "adjoint: fixed particles");
+    Mode m;
+    RC(mode(m));
+    if (m.eos_kind != 1 || m.mti) return fail(SPH_ERR_UNSUPPORTED, "adjoint: adiabatic EOS only");
+    if (!(st[SPH_P_FIXED_DT] > 0)) return fail(SPH_ERR_ARG, "adjoint: set SPH_P_FIXED_DT > 0");
+    return SPH_OK;
+  }
+
+  int adjoint_forward(int nsteps, int every) {
+    RC(adjoint_supported());
+    if (nsteps < 1 || every < 1) return fail(SPH_ERR_ARG, "adjoint: nsteps and every must be >= 1");
+    st[SPH_P_REORDER_EVERY] = 0;  // rows stay put: checkpoints are row images
+    // The adjoint differentiates the converged density pass (h a function of
+    // the positions alone).  The stored rho and Omega are those of the last
+    // Newton iterate before its update of h, so with the parity tolerance
+    // (one sweep from the predicted h) they would still depend, to first
+    // order, on that starting h; a tolerance of 1e-12 adds the sweep that
+    // makes the dependence second order (Newton converges quadratically).
+    st[SPH_P_NEWTON_TOL] = std::min(st[SPH_P_NEWTON_TOL], 1e-12);
+    adj_dt = st[SPH_P_FIXED_DT];
+    adj_nsteps = nsteps;
+    adj_every = every;
+    adj_ncp = (nsteps - 1) / every + 1;  // states at 0, k, 2k, ... below nsteps
+    // slots: [0] before the initial force pass, [1 + i] at step i k, [ncp + 1] final
+    RC(adj_ckpt.ensure(table_bytes() * size_t(adj_ncp + 2)));
+    RC(adj_seg.ensure(table_bytes() * size_t(every)));
+    adj_initial_force = !started;
+    RC(copy_table(ckpt(0), cols.p));
+    if (!started) {
+      eqset();
+      dtout = 0.;
+      RC(check_vars_ready());
+      RC(iterate(true));
+      ltout = 0.;
+      stopped = false;
+      started = true;
+    }
+    adj_t0 = st[ec_time];
+    for (int n = 0; n < nsteps; ++n) {
+      if (n % every == 0) RC(copy_table(ckpt(1 + n / every), cols.p));
+      RC(fixed_step(adj_dt));
+    }
+    RC(copy_table(ckpt(adj_ncp + 1), cols.p));
+    CK(cudaStreamSynchronize(s));
+    return SPH_OK;
+  }
+
+  AdjArgs adj_args() {
+    Params P{};
+    params(P);
+    AdjArgs a{};
+    a.nc = nreal;
+    a.nreal = nreal;
+    a.centre_k = centre_k.as<int32_t>();
+    a.centre_p = centre_p.as<int32_t>();
+    a.nl = nl.as<int32_t>();
+    a.rowoff = rowoff.as<int64_t>();
+    a.ncnt = ncnt.as<int32_t>();
+    a.ssrc = ssrc.as<int32_t>();
+    a.sx = sx.as<double>();
+    a.sy = sy.as<double>();
+    a.sz = sz.as<double>();
+    a.cols = cols.as<double>();
+    a.ld = nrows;
+    a.adj = adj.as<double>();
+    a.gpar = adj_par.as<double>();
+    a.wcv = P.wCv;
+    a.alpha = P.alpha;
+    a.beta = P.beta;
+    a.gamma = P.gamma;
+    a.artts = P.artts == 1;
+    a.hydro = P.eq_hydro != 0;
+    return a;
+  }
+
+  // dL/dv(T), dL/du(T), dL/dr(T) (original row order; NULL = 0) -> dL/d(r0,
+  // v0, u0) and dL/d(alpha, beta) by the checkpointed adjoint sweep
+  int adjoint_backward(const double* dl_dv, const double* dl_du, const double* dl_dr,
+                       double* g_r0, double* g_v0, double* g_u0, double* g_par) {
+    if (adj_nsteps < 1) return fail(SPH_ERR_ARG, "adjoint: no forward run recorded");
+    const int d = dim();
+    RC(adj.ensure(sizeof(double) * AJ_TOTAL * size_t(nrows)));
+    RC(adj_par.ensure(sizeof(double) * 2));
+    RC(adj_io.ensure(sizeof(double) * 3 * size_t(nrows)));
+    CK(cudaMemsetAsync(adj.p, 0, sizeof(double) * AJ_TOTAL * size_t(nrows), s));
+    CK(cudaMemsetAsync(adj_par.p, 0, sizeof(double) * 2, s));
+    auto load = [&](const double* host, int col, int ncomp) -> int {
+      if (!host) return SPH_OK;
+      CK(cudaMemcpyAsync(adj_io.p, host, sizeof(double) * ncomp * nrows, cudaMemcpyHostToDevice, s));
+      launch_adj_gather(adj_io.as<double>(), ncomp, orig.as<int32_t>(), nrows,
+                        adj.as<double>() + size_t(col) * nrows, nrows, s);
+      return SPH_OK;
+    };
+    RC(load(dl_dv, AJ_LV, 3));
+    RC(load(dl_du, AJ_LU, 1));
+    RC(load(dl_dr, AJ_LR, 3));
+    const int G = lanes_pair();
+    for (int sgi = adj_ncp - 1; sgi >= 0; --sgi) {
+      const int n0 = sgi * adj_every, n1 = std::min(adj_nsteps, n0 + adj_every);
+      // replay the segment, keeping the state before every step
+      RC(copy_table(cols.p, ckpt(1 + sgi)));
+      for (int n = n0; n < n1; ++n) {
+        RC(copy_table(seg(n - n0), cols.p));
+        st[ec_time] = adj_t0 + n * adj_dt;
+        RC(fixed_step(adj_dt));
+      }
+      for (int n = n1 - 1; n >= n0; --n) {
+        RC(copy_table(cols.p, seg(n - n0)));
+        st[ec_time] = adj_t0 + n * adj_dt;
+        RC(fixed_step(adj_dt, true));
+        launch_adj_step(kernel_id, d, G, adj_args(), adj_dt, 0, s);
+      }
+    }
+    if (adj_initial_force) {
+      RC(copy_table(cols.p, ckpt(0)));
+      RC(iterate(true));
+      launch_adj_step(kernel_id, d, G, adj_args(), adj_dt, 1, s);
+    }
+    auto store = [&](double* host, int col, int ncomp) -> int {
+      if (!host) return SPH_OK;
+      launch_adj_scatter(adj.as<double>() + size_t(col) * nrows, nrows, orig.as<int32_t>(), nrows,
+                         adj_io.as<double>(), ncomp, s);
+      CK(cudaMemcpyAsync(host, adj_io.p, sizeof(double) * ncomp * nrows, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      return SPH_OK;
+    };
+    RC(store(g_v0, AJ_LV, 3));
+    RC(store(g_u0, AJ_LU, 1));
+    RC(store(g_r0, AJ_LR, 3));
+    if (g_par) {
+      CK(cudaMemcpyAsync(h_ctrl + 1, adj_par.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      g_par[0] = h_ctrl[1];
+      g_par[1] = h_ctrl[2];
+    }
+    // back to the state at the end of the forward run
+    RC(copy_table(cols.p, ckpt(adj_ncp + 1)));
+    st[ec_time] = adj_t0 + adj_nsteps * adj_dt;
+    RC(check_status());
+    CK(cudaStreamSynchronize(s));
+    return SPH_OK;
+  }
+
   int one_step(double tfinish, bool& done) {
     double t = st[ec_time];
     if (!((t < tfinish + std::numeric_limits<double>::epsilon()) && !stopped)) {
@@ -1226,6 +1417,22 @@ int sph_get_timers(sph_handle* h, double* out_ms, int n) {
   h->collect_timers();
   for (int k = 0; k < n && k < SPH_T_TOTAL; ++k) out_ms[k] = h->timers[k];
   return SPH_OK;
+}
+
+int sph_adjoint_forward(sph_handle* h, int nsteps, int every) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  int rc = h->adjoint_forward(nsteps, every);
+  h->collect_timers();
+  return rc;
+}
+
+int sph_adjoint_backward(sph_handle* h, const double* dl_dv, const double* dl_du,
+                         const double* dl_dr, double* g_r0, double* g_v0, double* g_u0,
+                         double* g_par) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  int rc = h->adjoint_backward(dl_dv, dl_du, dl_dr, g_r0, g_v0, g_u0, g_par);
+  h->collect_timers();
+  return rc;
 }
 
 void sph_destroy(sph_handle* h) {

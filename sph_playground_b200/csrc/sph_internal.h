@@ -232,4 +232,44 @@ struct C2Args {
 void launch_c2(int prec, int kernel, int dim, const C2Args& a, PackBufs pb, Params P,
                cudaStream_t s);
 
+// ---- adjoint of the hydro step (sph_adjoint.cu) ----
+// columns of the per-row adjoint buffer (ld = rows of the particle table):
+// state adjoints LR (r), LV (v), LU (u), LAS (a), LDUS (du); the adjoints
+// LA, LDU of the new a, du fed to the force VJP; its results GR, GV (r', v'),
+// GH, GRHO, GOM, GP, GC, GU (h, rho, Omega, P, c, u); S' (d2 rho^/dh2) and
+// the Newton-h coefficients MU, WC.
+enum AdjCol : int {
+  AJ_LR = 0, AJ_LV = 3, AJ_LU = 6, AJ_LAS = 7, AJ_LDUS = 10, AJ_LA = 11, AJ_LDU = 14,
+  AJ_GR = 15, AJ_GV = 18, AJ_GH = 21, AJ_GRHO = 22, AJ_GOM = 23, AJ_GP = 24, AJ_GC = 25,
+  AJ_GU = 26, AJ_SP = 27, AJ_MU = 28, AJ_WC = 29, AJ_TOTAL = 30
+};
+struct AdjArgs {
+  int64_t nc, nreal;
+  const int32_t* centre_k;
+  const int32_t* centre_p;
+  const int32_t* nl;
+  const int64_t* rowoff;
+  const int32_t* ncnt;
+  const int32_t* ssrc;
+  const double* sx;
+  const double* sy;
+  const double* sz;
+  const double* cols;
+  int64_t ld;
+  double* adj;   // AJ_TOTAL columns of ld rows
+  double* gpar;  // d/d alpha, d/d beta
+  double wcv, alpha, beta, gamma;
+  int artts, hydro;
+};
+// one step's adjoint: prep, force VJP (circuit2, Newton-h density, EOS) and
+// the integrator's adjoint; first = 1 for the force evaluation of the
+// initial state (no integrator step)
+void launch_adj_step(int kernel, int dim, int G, const AdjArgs& a, double dt, int first,
+                     cudaStream_t s);
+// caller-order rows (ncomp per row) to ncomp columns of ld physical rows, and back
+void launch_adj_gather(const double* in, int ncomp, const int32_t* orig, int64_t n, double* out,
+                       int64_t ld, cudaStream_t s);
+void launch_adj_scatter(const double* in, int64_t ld, const int32_t* orig, int64_t n,
+                        double* out, int ncomp, cudaStream_t s);
+
 }  // namespace sph
