@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint cost / gradient check (2D shear 256^2)")
     ap.add_argument("--no-errors", action="store_true",
                     help="skip the FP32-vs-FP64 error check (profiling runs)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -184,6 +186,45 @@ def run_reference(args, ws, rank):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def adjoint_block(lib, n=256, n_ref=64, nsteps=200, every=20, dt=5e-4):
+    """The adjoint workload: 2D periodic shear flow (n^2 particles, M6,
+    alpha = 1, beta = 2), nsteps fixed-dt leapfrog steps with a checkpoint
+    every `every` steps; forward and backward timed on the host around the
+    synchronous C-ABI calls.  Also the FP32-comp gradient against the FP64
+    gradient at n_ref^2."""
+    from sph_playground_b200 import ic
+    V = [abi.consts.es["vx"] - 1, abi.consts.es["vy"] - 1, abi.consts.es["vz"] - 1]
+
+    def grads(nn, prec, steps):
+        st, store = ic.shear2d(n=nn)
+        target = store[:, V] * 1.2
+        target[:, 2] = 0.0
+        e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+        e.set_param(abi.P_FIXED_DT, dt)
+        t0 = time.perf_counter()
+        e.adjoint_forward(steps, every)
+        t1 = time.perf_counter()
+        vT = e.get_store()[:, V]
+        t2 = time.perf_counter()
+        g = e.adjoint_backward(dl_dv=2.0 * (vT - target))
+        t3 = time.perf_counter()
+        e.close()
+        return g, (t1 - t0) * 1e3 / steps, (t3 - t2) * 1e3 / steps
+
+    grads(64, abi.PREC_FP64, 4)  # warm-up
+    _, fwd, bwd = grads(n, abi.PREC_FP64, nsteps)
+    g64, _, _ = grads(n_ref, abi.PREC_FP64, nsteps)
+    g32, _, _ = grads(n_ref, abi.PREC_FP32_COMP, nsteps)
+    rel = float(np.linalg.norm(g32["g_v0"] - g64["g_v0"]) / np.linalg.norm(g64["g_v0"]))
+    return {"workload": f"shear2d {n}^2 ({n * n} particles), M6, alpha 1, beta 2, {nsteps} steps "
+                        f"of dt {dt}, checkpoint every {every}, FP64",
+            "forward_ms_per_step": fwd, "backward_ms_per_step": bwd,
+            "backward_over_forward": bwd / fwd,
+            "grad_v0_fp32_vs_fp64_rel": rel,
+            "grad_reference": f"FP64 adjoint gradient at {n_ref}^2",
+            "timing": "host clock around synchronous C-ABI calls"}
 
 
 def timed_steps(e, K):
@@ -338,6 +379,10 @@ def main():
                 "phases_ms_per_step": tm6,
                 "peak_fp64_tflops": peak64 / 1e12}
 
+    adj = None
+    if not args.no_adjoint:
+        adj = adjoint_block(lib)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_n)
@@ -371,6 +416,7 @@ def main():
                               "exact_tests": cnt["exact_tests"] / args.steps,
                               "candidates": cnt["candidates"] / args.steps},
             "fp64": fp64,
+            "adjoint": adj,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "peak_fp32_tflops": peak32 / 1e12,
         }
