@@ -93,6 +93,7 @@ extern "C" {
 #define SPH_ERR_OOM               19  /* device allocation failed             */
 #define SPH_ERR_TIMEOUT           20  /* a bounded device wait gave up        */
 #define SPH_ERR_STATE             21  /* call not valid in this handle state  */
+#define SPH_ERR_RAD_NEGATIVE      22  /* rad_exchange.f90:61-64               */
 
 /* ---- work counters (sph_get_counters, cumulative since create/reset) ----- */
 #define SPH_CNT_ITERATES        0 /* calls of iterate (iterator.f90:44)       */

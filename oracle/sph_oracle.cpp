@@ -89,8 +89,8 @@ enum : int { ests_auto = 0, ests_fixeds = 1 };
 const double pi = 4.0 * std::atan(1.0);             // const.f90:4
 const double eps0 = std::numeric_limits<double>::epsilon();  // const.f90:5
 const double lightspeed = 2.997924e10;              // const.f90:6
-const double sigmaB = 5.67051e-5;                   // const.f90:8
 const double Rg = 8.314e7;                          // const.f90:7
+const double sigmaB = 5.67051e-5;                   // const.f90:8
 
 thread_local std::string g_err;
 
@@ -1140,6 +1140,38 @@ struct Oracle {
   }
   // one pass of the while loop body; returns SPH_OK and sets `done` when the
   // loop condition fails.
+  // update_radenergy (rad_exchange.f90:9-68) with the implicit solve of
+  // :111-126: Newton on the gas energy at fixed u + xi
+  int update_radenergy(int64_t n, double dt) {
+    const double gamma = st[ec_gamma], gmw = st[ec_molecularmass];
+    const double a = 4. * sigmaB / lightspeed;
+    const double cv1 = (gamma - 1.) * gmw / Rg;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int64_t i = 0; i < n; ++i) {
+      const double kappa = S(i, es_kappa);
+      const double ack = 4. * sigmaB * kappa;
+      const double rhoi = S(i, es_den), ui = S(i, es_u), dudt = S(i, es_du), xii = S(i, es_t);
+      const double etot = ui + xii;
+      double unew = ui, uold = 2. * ui;
+      for (int iter = 0; std::fabs(unew - uold) > 1e-16 && iter < 10; ++iter) {
+        uold = unew;
+        const double uc = unew * cv1;
+        const double uc2 = uc * uc;
+        const double u3 = (unew * unew) * unew;
+        const double cv2 = cv1 * cv1;
+        const double fu = ((unew / dt - ui / dt) - dudt) - ack * (rhoi * (etot - unew) / a - uc2 * uc2);
+        const double dfu = 1. / dt + ack * (rhoi / a + 4. * (u3 * (cv2 * cv2)));
+        unew = unew - fu / dfu;
+      }
+      S(i, es_u) = unew;
+      S(i, es_t) = etot - unew;
+      if (!(S(i, es_t) > 0.) || !(S(i, es_u) > 0.)) bad = 1;
+    }
+    if (bad) return fail(SPH_ERR_RAD_NEGATIVE, "radiation or thermal energy is negative after exchange");
+    return SPH_OK;
+  }
+
   int one_step(double tfinish, bool& done) {
     double t = st[ec_time];
     if (!((t < tfinish + eps0) && !stopped)) { done = true; return SPH_OK; }
@@ -1214,7 +1246,10 @@ struct Oracle {
       rc = sts_integrate(sts_s, dt);
       if (rc) return rc;
     }
-    if (eq_radexch) return fail(SPH_ERR_UNSUPPORTED, "radiation exchange (rad_exchange.f90) is not part of this engine");
+    if (eq_radexch) {  // main.f90:367-369
+      rc = update_radenergy(n, dt);
+      if (rc) return rc;
+    }
     st[ec_time] = t + dt;
     ++iterc;
     cnt[SPH_CNT_STEPS]++;

@@ -23,7 +23,7 @@ STATUS = {
     12: "SPH_ERR_IC_MUZERO", 13: "SPH_ERR_IC_DIFFCOND",
     14: "SPH_ERR_UNSUPPORTED", 15: "SPH_ERR_FLD_ANISO", 16: "SPH_ERR_DDW",
     17: "SPH_ERR_PROCESS", 18: "SPH_ERR_GRID", 19: "SPH_ERR_OOM",
-    20: "SPH_ERR_TIMEOUT", 21: "SPH_ERR_STATE",
+    20: "SPH_ERR_TIMEOUT", 21: "SPH_ERR_STATE", 22: "SPH_ERR_RAD_NEGATIVE",
 }
 
 PREC_FP64 = 0

@@ -24,6 +24,8 @@ enum : int {
 };
 constexpr int NCOL = SPH_ES_TOTAL;
 constexpr double kLightspeed = 2.997924e10;  // const.f90:6
+constexpr double kRg = 8.314e7;              // const.f90:7
+constexpr double kSigmaB = 5.67051e-5;       // const.f90:8
 
 // ---- kernel shapes ------------------------------------------------------------
 // The reference evaluates f(q), f'(q), f''(q) piecewise (kernel/base_m6.f90:36-97,

@@ -54,6 +54,7 @@ enum : int {
   ec_realpn = 25, ec_fixedpn = 26, ec_gamma = 27, ec_dtprint = 30,
   ec_process = 31, ec_au = 32, ec_eqonhydro = 34, ec_eqondiff = 35,
   ec_eqonfluxlim = 36, ec_eqonradexch = 37, ec_eqonsts = 38, ec_time = 46,
+  ec_molecularmass = 47,
   ec_ststype = 48, ec_stsfixeds = 49
 };
 enum : int { eeq_hydro = 300, eeq_diffusion = 301, eeq_magnetohydro = 302,
@@ -437,6 +438,7 @@ struct sph_handle {
         case SPH_ERR_Q_NAN: msg = "q is nan"; break;
         case SPH_ERR_Q_NEG: msg = "q is negative"; break;
         case SPH_ERR_H_NEG: msg = "Negative smoothing length in c1 advanced"; break;
+        case SPH_ERR_RAD_NEGATIVE: msg = "radiation or thermal energy is negative after exchange"; break;
         default: break;
       }
       return fail(code, msg);
@@ -1134,8 +1136,11 @@ struct sph_handle {
                      ctrl.as<double>(), do_sts, s);
     }
     if (do_sts) RC(sts_integrate(sts_s, dt));
-    if (eq_radexch)
-      return fail(SPH_ERR_UNSUPPORTED, "radiation exchange (rad_exchange.f90) is not part of this engine");
+    if (eq_radexch) {  // main.f90:367-369
+      launch_radexch(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, dt,
+                     st[ec_gamma], st[ec_molecularmass], status.as<int>(), s);
+      RC(check_status());
+    }
     st[ec_time] = t + dt;
     cnt_host[SPH_CNT_STEPS]++;
     steps_since_reorder++;

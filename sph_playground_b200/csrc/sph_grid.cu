@@ -845,6 +845,45 @@ k_timestep_reduce(const double* __restrict__ cols, int64_t ld, const int32_t* __
   }
 }
 
+// ---- radiation - gas energy exchange (rad_exchange.f90:9-118) ---------------------------------
+// Per integrated row: the gas energy u and the radiation energy xi = T
+// exchange at fixed total e = u + xi; the new u solves, by at most 10 Newton
+// steps from u0 until two iterates agree to 1e-16,
+//   u/dt - u0/dt - du - 4 sigma kappa (rho (e - u) / a - (u cv1)^4) = 0,
+// a = 4 sigma / c, cv1 = (gamma - 1) mu / Rg (rad_exchange.f90:111-126).
+// Integer powers as repeated products, no fused multiply-adds.
+__global__ void k_radexch(double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
+                          int64_t nrows, int64_t n_int, double dt, double gamma, double gmw,
+                          int* __restrict__ status) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nrows || orig[i] >= n_int) return;
+  auto C = [&](int f) -> double& { return cols[f * ld + i]; };
+  const double a = __ddiv_rn(__dmul_rn(4., kSigmaB), kLightspeed);
+  const double cv1 = __ddiv_rn(__dmul_rn(gamma - 1., gmw), kRg);
+  const double ack = __dmul_rn(__dmul_rn(4., kSigmaB), C(es_kappa));
+  const double rho = C(es_den), u0 = C(es_u), dudt = C(es_du), xi = C(es_t);
+  const double etot = __dadd_rn(u0, xi);
+  double unew = u0, uold = __dmul_rn(2., u0);
+  for (int iter = 0; fabs(__dadd_rn(unew, -uold)) > 1e-16 && iter < 10; ++iter) {
+    uold = unew;
+    const double uc = __dmul_rn(unew, cv1);
+    const double uc2 = __dmul_rn(uc, uc);
+    const double u3 = __dmul_rn(__dmul_rn(unew, unew), unew);
+    const double cv2 = __dmul_rn(cv1, cv1);
+    const double fu = __dadd_rn(
+        __dadd_rn(__dadd_rn(__ddiv_rn(unew, dt), -__ddiv_rn(u0, dt)), -dudt),
+        -__dmul_rn(ack, __dadd_rn(__ddiv_rn(__dmul_rn(rho, __dadd_rn(etot, -unew)), a),
+                                  -__dmul_rn(uc2, uc2))));
+    const double dfu = __dadd_rn(
+        __ddiv_rn(1., dt),
+        __dmul_rn(ack, __dadd_rn(__ddiv_rn(rho, a), __dmul_rn(4., __dmul_rn(u3, __dmul_rn(cv2, cv2))))));
+    unew = __dadd_rn(unew, -__ddiv_rn(fu, dfu));
+  }
+  C(es_u) = unew;
+  C(es_t) = __dadd_rn(etot, -unew);
+  if (!(C(es_t) > 0.) || !(C(es_u) > 0.)) atomicCAS(status, 0, SPH_ERR_RAD_NEGATIVE);
+}
+
 __global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i < n) p[i] = v;
@@ -1048,6 +1087,11 @@ void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows
 void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
                             int64_t n_ts, Params P, unsigned long long* red, cudaStream_t s) {
   k_timestep_reduce<<<reduce_blocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_ts, P, red);
+  note_launch();
+}
+void launch_radexch(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
+                    double dt, double gamma, double gmw, int* status, cudaStream_t s) {
+  k_radexch<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, dt, gamma, gmw, status);
   note_launch();
 }
 void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s) {

@@ -154,6 +154,9 @@ void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig,
                             int64_t nrows, int64_t n_ts, Params P,
                             unsigned long long* red, cudaStream_t s);
 void launch_fill_u64(unsigned long long* p, int n, unsigned long long v, cudaStream_t s);
+// radiation - gas exchange after the corrector (rad_exchange.f90:9-118)
+void launch_radexch(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
+                    double dt, double gamma, double gmw, int* status, cudaStream_t s);
 // up to 8 single reduction slots set in one launch: p[off[i]] = val[i]
 struct SlotInit {
   int n;

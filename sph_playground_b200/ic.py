@@ -357,3 +357,50 @@ def shear2d(n=256, amp=0.1, seed=4, noise_seed=5, noise=1e-3, rho=1.0,
     store[:, col("c")] = math.sqrt(gamma * P / rho)
     store[:, col("type")] = ept["real"]
     return st, store
+
+
+def hyrad1d(resolution=128, kernel="gauss", T_gas=1500.0, T_rad=2000.0, rho=1e-10,
+            kappa=4e-3, mu=2.0, gamma=5.0 / 3.0, csound=3.2e5, ststype="auto",
+            exchange_only=False):
+    """Radiating shock tube (runner/004.3_fluxlimdif_shock.py): 1D uniform
+    particles on x in [-1e15, 1e15], periodic (the runner closes the tube
+    with periodic fixed particles instead), rho = 1e-10, gas at T_gas,
+    radiation energy xi = 4 sigma T_rad^4 / (c rho), flows of +-csound
+    towards x = 0; hydro + flux-limited diffusion (fab, isotropic) +
+    radiation exchange, STS.  With `exchange_only` the gas is at rest and
+    only the exchange acts (hydro, diffusion and STS off)."""
+    RG, STEBOLTZ, C = 8.314e7, 5.67051e-5, 2.997924e10  # const.f90:6-8
+    st = make_state(1, "manual", ddw="fab", hfac=1.0, tfinish=1e9, adden="yes",
+                    artts="yes", au=1.0, disotropic="yes", process="fullyperiodic",
+                    xmin=-1e15, xmax=1e15, resolution=resolution)
+    store = place_uniform(st, kernel)
+    N = store.shape[0]
+    sp = get_state(st, "spacing")
+    set_state(st, "gamma", gamma)
+    set_state(st, "molecularmass", mu)
+    set_state(st, "dcondconst", kappa)
+    set_state(st, "time", 0.0)
+    set_state(st, "dtprint", 1e9)
+    set_state(st, "eqonhydro", 0.0 if exchange_only else consts.eif["yes"])
+    set_state(st, "eqondiff", 0.0 if exchange_only else consts.eif["yes"])
+    set_state(st, "eqonfluxlim", 0.0 if exchange_only else consts.eif["yes"])
+    set_state(st, "eqonradexch", consts.eif["yes"])
+    set_state(st, "eqonsts", 0.0 if exchange_only else consts.eif["yes"])
+    set_state(st, "ststype", consts.ests[ststype])
+    set_state(st, "muzero", 1.0)
+    ksi = 4.0 * STEBOLTZ * T_rad ** 4 / C / rho
+    u = T_gas * RG / (gamma - 1.0) / mu
+    store[:, col("m")] = rho * sp  # CalcUniformMass in 1D
+    store[:, col("den")] = rho
+    store[:, col("h")] = get_state(st, "hfac") * sp
+    store[:, col("om")] = 1.0
+    store[:, col("u")] = u
+    store[:, col("p")] = u * rho * (gamma - 1.0)
+    store[:, col("c")] = csound
+    store[:, col("kappa")] = kappa
+    store[:, col("t")] = ksi
+    if not exchange_only:
+        x = store[:, col("rx")]
+        store[:, col("vx")] = np.where(x <= 0.0, csound, -csound)
+    return st, store
+

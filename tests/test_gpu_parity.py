@@ -192,6 +192,24 @@ def test_sts_steps(oracle_lib, engine_lib, cuda_ok, prec):
     assert e <= (1e-11 if prec == FP64 else 1e-5), e
 
 
+@pytest.mark.parametrize("exchange_only", [True, False])
+def test_radiation_exchange_steps(oracle_lib, engine_lib, cuda_ok, exchange_only):
+    # hydro + flux-limited diffusion + STS + radiation exchange
+    # (rad_exchange.f90, main.f90:367-369), FP64, 4 steps
+    st, store = ic.hyrad1d(64, kernel="m6", exchange_only=exchange_only)
+    ref, _, cref, sref = run_pass(oracle_lib, st, store, "m6", FP64, "steps", steps=4)
+    got, _, cgot, sgot = run_pass(engine_lib, st, store, "m6", FP64, "steps", steps=4)
+    assert cgot["steps"] == cref["steps"]
+    t_ref = sref[consts.ec["time"] - 1]
+    assert abs(sgot[consts.ec["time"] - 1] - t_ref) <= 1e-11 * t_ref
+    bad = {}
+    for f in ("u", "t", "vx", "den", "h"):
+        e = rel_field(got[:, COL[f]], ref[:, COL[f]])
+        if not e <= 1e-10:
+            bad[f] = e
+    assert not bad, bad
+
+
 def test_borderless_and_fixed(oracle_lib, engine_lib, cuda_ok):
     st, store = ic.sedov3d(n=10)
     ic.set_state(st, "process", consts.epc["borderless"])

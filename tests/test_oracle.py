@@ -345,3 +345,19 @@ def test_oracle_diffusion_decay(oracle_lib):
     l2 = float(np.sqrt(np.mean((out[:, COL["t"]] - exact) ** 2)))
     assert t == pytest.approx(0.01, abs=1e-12)
     assert l2 < 0.02, l2
+
+
+def test_radiation_exchange_conserves_energy(oracle_lib):
+    # rad_exchange.f90:9-126: gas and radiation trade energy at fixed u + xi;
+    # with T_rad > T_gas the gas heats and the radiation cools
+    st, store = ic.hyrad1d(32, kernel="m6", exchange_only=True)
+    C = {k: v - 1 for k, v in consts.es.items()}
+    e0 = store[:, C["u"]] + store[:, C["t"]]
+    with abi.Engine(st, store, "m6", lib=oracle_lib) as e:
+        e.set_param("tfinish", 2e8)
+        e.step(1)
+        s = e.get_store()
+    assert np.max(np.abs(s[:, C["u"]] + s[:, C["t"]] - e0) / e0) <= 1e-15
+    assert np.all(s[:, C["u"]] > store[:, C["u"]])
+    assert np.all(s[:, C["t"]] < store[:, C["t"]])
+
