@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the default launch shapes instead of autotuning them")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint cost / gradient check (2D shear 256^2)")
     ap.add_argument("--no-errors", action="store_true",
@@ -258,9 +260,20 @@ def main():
     N = store.shape[0]
     peak32, peak64 = measure_peak()
 
+    # launch shapes (lanes per centre, cell edge) picked by the autotuner on
+    # this workload, per precision (sph_playground_b200/tune.py)
+    tuned = {abi.PREC_FP32_COMP: {}, abi.PREC_FP64: {}}
+    if not args.no_autotune:
+        from sph_playground_b200 import tune
+        for prec in tuned:
+            r = tune.autotune(st, store, "m6", prec, lib=lib, cache=None)
+            tuned[prec] = {k: v for k, v in r.items() if k.startswith("P_")}
+
     def engine(prec, st_=None, store_=None):
         e = abi.Engine(st if st_ is None else st_, store if store_ is None else store_, "m6",
                        precision=prec, lib=lib)
+        for k, v in tuned[prec].items():
+            e.set_param(getattr(abi, k), float(v))
         for kv in args.param:
             k, v = kv.split("=")
             e.set_param(int(k) if k.isdigit() else getattr(abi, k, k), float(v))
@@ -398,7 +411,11 @@ def main():
                        "particles": N, "kernel": "m6", "precision": "fp32_comp",
                        "l2": "inputs larger than L2 (particle table "
                              f"{N * 32 * 8 / 1e6:.0f} MB + pair streams)",
-                       "parallelism": f"replicas x{ws}"},
+                       "parallelism": f"replicas x{ws}",
+                       "launch_shapes": {"fp32_comp": tuned[abi.PREC_FP32_COMP],
+                                         "fp64": tuned[abi.PREC_FP64],
+                                         "source": "autotuned on this workload" if not
+                                         args.no_autotune else "defaults"}},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
