@@ -386,6 +386,7 @@ def main():
         e6.close()
         fp64 = {"value": ws * N * args.steps / (ms6 * 1e-3), "ms_per_step": ms6 / args.steps,
                 "work_per_step": {"c1_pairs": cnt6["c1_pairs"] / args.steps,
+                                  "device_allocations_in_timed_steps": cnt6["allocs"],
                                   "c1_max_sweeps": cnt6["c1_sweeps"], "neib_max": cnt6["neib_max"],
                                   "searches": cnt6["searches"] / args.steps,
                                   "candidates": cnt6["candidates"] / args.steps},
@@ -431,6 +432,7 @@ def main():
                               "neib_max": cnt["neib_max"],
                               "searches": cnt["searches"] / args.steps,
                               "exact_tests": cnt["exact_tests"] / args.steps,
+                              "device_allocations_in_timed_steps": cnt["allocs"],
                               "candidates": cnt["candidates"] / args.steps},
             "fp64": fp64,
             "adjoint": adj,

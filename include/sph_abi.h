@@ -111,7 +111,8 @@ extern "C" {
 #define SPH_CNT_SEARCHES      12 /* neighbour-search launches (incl. re-runs
                                     after a list outgrew its slots)          */
 #define SPH_CNT_EXACT_TESTS   13 /* candidates decided by the FP64 test      */
-#define SPH_CNT_TOTAL          14
+#define SPH_CNT_ALLOCS        14 /* device allocations made by this handle    */
+#define SPH_CNT_TOTAL          15
 
 /* ---- per-kernel timers (sph_get_timers, milliseconds, cumulative) ------- */
 #define SPH_T_PREDICT    0

@@ -46,7 +46,7 @@ P_FIXED_DT = 62
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",
             "c1_centre_sweeps", "launches", "neib_max", "searches",
-            "exact_tests"]
+            "exact_tests", "allocs"]
 TIMERS = ["predict", "ghosts", "sort", "neighbours", "circuit1", "circuit2",
           "correct", "timestep", "sts", "step", "pack"]
 

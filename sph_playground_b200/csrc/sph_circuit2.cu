@@ -93,7 +93,7 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
 }
 
 // G lanes per centre: lane l takes neighbours l, l+G, ... of the centre's
-// list row; per-lane two-sum partials are added over the group in FP64 and
+// list row; per-lane partial sums are added over the group in FP64 and
 // lane 0 stores the result.
 template <int K, int DIM, class R, bool GENERAL, int G>
 __global__ void __launch_bounds__(TPB)
@@ -116,7 +116,10 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     Ka *= wcv;  // wCv / h_a^(d+1)
     const R alpha = R(P.alpha), beta = R(P.beta), au = R(P.au);
     const bool artts = P.artts == 1, adden = P.adden == 1, hydro = P.eq_hydro != 0;
-    const bool use_au = P.au != -1.0;
+    // the artificial conductivity term (circuit2.f90:316-331) is scaled by
+    // au: au = -1 switches it off in the reference, and au = 0 makes it
+    // vanish, so it is skipped for both
+    const bool use_au = P.au != -1.0 && P.au != 0.0;
     const R rPiA = A.rho * A.Pi;  // 1 / (rho_a Omega_a)
     // force-type sums: plain per lane (a few tens of terms), FP64 over lanes
     SumAcc<R> dv[3], du, drho, ddt, db[3];

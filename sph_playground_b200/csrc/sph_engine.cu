@@ -13,6 +13,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -88,6 +89,9 @@ KBase kbase(int id) {
   return k;
 }
 
+// device allocations made by DevBuf::ensure on this thread's current handle
+thread_local int64_t* t_alloc_count = nullptr;
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -103,6 +107,9 @@ struct DevBuf {
     // between steps and must not trigger a free/allocate (which would also
     // synchronise the device) every time
     size_t nb = std::max<size_t>(b + b / 4, 256);
+    if (t_alloc_count) ++*t_alloc_count;
+    static const bool log_allocs = std::getenv("SPH_ALLOC_LOG") != nullptr;
+    if (log_allocs) std::fprintf(stderr, "sph: device allocation of %zu bytes\n", nb);
     cudaError_t e = cudaMalloc(&p, nb);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -524,6 +531,8 @@ struct sph_handle {
     double cf = st[SPH_P_CELL_FACTOR] > 0 ? st[SPH_P_CELL_FACTOR] : 0.4;
     double L = P.krad * hmin * cf;
     int64_t ncell = 0;
+    const int64_t ncell_cap = std::min<int64_t>(std::max<int64_t>(8 * nall, 1 << 20),
+                                                int64_t(1) << 31);
     int n3[3];
     for (int guard = 0;; ++guard) {
       bool ok = true;
@@ -534,9 +543,7 @@ struct sph_handle {
         n3[k] = int(std::floor(e)) + 1;
         ncell *= n3[k];
       }
-      if (ok && ncell <= std::min<int64_t>(std::max<int64_t>(8 * nall, 1 << 20),
-                                           int64_t(1) << 31))
-        break;
+      if (ok && ncell <= ncell_cap) break;
       L *= 1.25;
       if (guard > 400) return fail(SPH_ERR_GRID, "cell grid would not fit");
     }
@@ -561,7 +568,12 @@ struct sph_handle {
                   nghost, grid, keys.as<uint32_t>(), vals.as<int32_t>(), s);
       sort_pairs(sort_tmp.p, sort_tmp.bytes, keys.as<uint32_t>(), keys_alt.as<uint32_t>(),
                  vals.as<int32_t>(), vals_alt.as<int32_t>(), nall, end_bit, s);
-      RC(cstart.ensure(sizeof(int32_t) * (ncell + 1)));
+      // the cell count follows 1 / h_min^d, which drifts from step to step:
+      // room for four times the current count (at most the cap) keeps the
+      // reallocation out of the steady state
+      if (sizeof(int32_t) * size_t(ncell + 1) > cstart.bytes)
+        RC(cstart.ensure(sizeof(int32_t) *
+                         size_t(std::min<int64_t>(4 * (ncell + 1), ncell_cap + 1))));
       launch_cell_starts(keys_alt.as<uint32_t>(), nall, ncell, cstart.as<int32_t>(), s);
       launch_sorted_gather(vals_alt.as<int32_t>(), nall, nrows, nreal, cols.as<double>(),
                            gx.as<double>(), gy.as<double>(), gz.as<double>(), gsrc.as<int32_t>(),
@@ -1164,6 +1176,12 @@ struct sph_handle {
 
 extern "C" {
 
+// counts the device allocations of one C-ABI call on its handle
+struct AllocScope {
+  explicit AllocScope(sph_handle* h) { t_alloc_count = h ? &h->cnt_host[SPH_CNT_ALLOCS] : nullptr; }
+  ~AllocScope() { t_alloc_count = nullptr; }
+};
+
 const char* sph_last_error(void) { return g_err.c_str(); }
 
 int sph_create(const double* state49, const double* store, int64_t n_rows, int kernel_id,
@@ -1269,6 +1287,7 @@ int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
 }
 
 int sph_iterate(sph_handle* h) {
+  AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   RC(h->reorder_rows());
   int rc = h->iterate(true);
@@ -1277,6 +1296,7 @@ int sph_iterate(sph_handle* h) {
 }
 
 int sph_density(sph_handle* h) {
+  AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   RC(h->reorder_rows());
   int rc = h->iterate(false);
@@ -1285,6 +1305,7 @@ int sph_density(sph_handle* h) {
 }
 
 int sph_step(sph_handle* h, int nsteps) {
+  AllocScope alloc_scope(h);
   if (!h || nsteps < 0) return fail(SPH_ERR_ARG, "bad argument");
   int rc = SPH_OK;
   {
@@ -1302,6 +1323,7 @@ int sph_step(sph_handle* h, int nsteps) {
 }
 
 int sph_run_to(sph_handle* h, double tfinish) {
+  AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   h->st[ec_tfinish] = tfinish;
   int rc = SPH_OK;
@@ -1425,6 +1447,7 @@ int sph_get_timers(sph_handle* h, double* out_ms, int n) {
 }
 
 int sph_adjoint_forward(sph_handle* h, int nsteps, int every) {
+  AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   int rc = h->adjoint_forward(nsteps, every);
   h->collect_timers();
@@ -1434,6 +1457,7 @@ int sph_adjoint_forward(sph_handle* h, int nsteps, int every) {
 int sph_adjoint_backward(sph_handle* h, const double* dl_dv, const double* dl_du,
                          const double* dl_dr, double* g_r0, double* g_v0, double* g_u0,
                          double* g_par) {
+  AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   int rc = h->adjoint_backward(dl_dv, dl_du, dl_dr, g_r0, g_v0, g_u0, g_par);
   h->collect_timers();
