@@ -37,6 +37,12 @@ UNIT = "particle-steps/s"
 # reference formulas with sqrt/div each as one FLOP
 F1_C1 = 50.0
 F2_C2 = 150.0
+# DRAM bytes per in-support pair of the FP32-comp circuit2 launch:
+# dram__bytes_read.sum + dram__bytes_write.sum = 846.06 MB + 67.74 MB over
+# 157.49M pairs of the 96^3 capture in profiles/k_c2_fp32_sedov3d_96.md (the
+# neighbour index, 4 B, plus the gathered pair data that misses L2); the
+# traffic scales with the pairs a launch processes
+C2_DRAM_BYTES_PER_PAIR = (846.06e6 + 67.74e6) / 157.49e6
 
 
 def parse():
@@ -349,8 +355,11 @@ def main():
             "circuit2": (c2_flops / args.steps, tm["circuit2"])}
     dom = max(kern, key=lambda k: kern[k][1])
     ach = kern[dom][0] / (kern[dom][1] * 1e-3) / 1e12
+    traffic = C2_DRAM_BYTES_PER_PAIR * cnt["c2_pairs"] / args.steps if dom == "circuit2" else None
     roofline = {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": peak32 / 1e12,
-                "unit": "TFLOP/s", "frac": ach / (peak32 / 1e12), "traffic": None,
+                "unit": "TFLOP/s", "frac": ach / (peak32 / 1e12), "traffic": traffic,
+                "traffic_source": "ncu DRAM bytes of the 96^3 capture (profiles/k_c2_fp32_sedov3d_96.md) "
+                                  "per pair, times this launch's pairs",
                 "peak_source": "live FFMA-chain probe (libsph_peak.so) on this GPU; "
                                "MEASURED_PEAKS.json holds no non-tensor FP32 figure"}
 
