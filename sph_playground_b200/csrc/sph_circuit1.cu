@@ -130,7 +130,11 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
       const double ihd_full = 1.0 / ha;
       const R ih = R(ihd_full);
       const R ih_lo = R(ihd_full - double(ih));
-      Acc<R> sw, so;
+      // the density sum keeps its two-sum partials (its smoothness in h is
+      // what the Newton iteration needs); the d rho / dh sum only scales the
+      // Newton step and Omega, so a plain per-lane sum suffices
+      Acc<R> sw;
+      SumAcc<R> so;
       sw.init();
       so.init();
       // U neighbours per lane per round: their list entries and pair data

@@ -383,7 +383,7 @@ __device__ __forceinline__ float group_max(float v) {
 }
 
 template <int DIM, int G>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 7)
 k_neighbours(NeibArgs a) {
   constexpr int RPL = kNeibRowsPerLane;
   constexpr int NG = 128 / G;
