@@ -100,7 +100,7 @@ __device__ __forceinline__ unsigned group_mask() {
 // row of the neighbour list (coalesced), the group adds its lanes' two-sum
 // partials in FP64, and every lane takes the same FP64 Newton step.
 template <int K, int DIM, class R, int G>
-__global__ void __launch_bounds__(TPB)
+__global__ void __launch_bounds__(TPB, 8)
 k_c1_newton(C1Args a, PackBufs pb, Params P) {
   const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
   const int lane = threadIdx.x & (G - 1);
