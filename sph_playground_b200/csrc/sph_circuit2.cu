@@ -96,7 +96,7 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
 // list row; per-lane partial sums are added over the group in FP64 and
 // lane 0 stores the result.
 template <int K, int DIM, class R, bool GENERAL, int G>
-__global__ void __launch_bounds__(TPB)
+__global__ void __launch_bounds__(TPB, sizeof(R) == 8 ? 5 : 8)
 k_c2(C2Args a, PackBufs pb, Params P) {
   const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
   const int lane = threadIdx.x & (G - 1);
