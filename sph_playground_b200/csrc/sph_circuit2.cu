@@ -121,6 +121,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     // vanish, so it is skipped for both
     const bool use_au = P.au != -1.0 && P.au != 0.0;
     const R rPiA = A.rho * A.Pi;  // 1 / (rho_a Omega_a)
+    const R hrhoa = R(-0.5) * A.rho, alpha_ca = alpha * A.c;
     // force-type sums: plain per lane (a few tens of terms), FP64 over lanes
     SumAcc<R> dv[3], du, drho, ddt, db[3];
     for (int d = 0; d < 3; ++d) { dv[d].init(); db[d].init(); }
@@ -206,31 +207,40 @@ k_c2(C2Args a, PackBufs pb, Params P) {
       R Kb = B.invh;
       for (int d = 0; d < DIM; ++d) Kb *= B.invh;
       Kb *= wcv;
-      const R ga = Ka * dfa * invr;  // nabla W_a = ga * r_ab
-      const R gb = Kb * dfb * invr;  // nabla W_b = gb * r_ab
+      const R ga = (Ka * invr) * dfa;  // nabla W_a = ga * r_ab
+      const R gb = (Kb * invr) * dfb;  // nabla W_b = gb * r_ab
       const R mb = B.m;
-      if (adden) drho.add(mb * ga * vr);  // circuit2.f90:265-267
-      R F = R(0);  // dv -= mb * F * r_ab
+      const R mgv = mb * ga * vr;      // m_b nabla W_a . v_ab
+      if (adden) drho.add(mgv);        // circuit2.f90:265-267
+      // F = ga Pi_a Fa + gb Pi_b Fb (dv -= mb F r_ab); du += mgv Pi_a Da.
+      // With faba = Ka f'_a = ga r the viscous heating
+      // mb dvr qav faba / (rho_a Omega_a) of circuit2.f90:329-334 is
+      // mgv Pi_a (qav rho_a), and the pressure work of :343-344 is
+      // mgv Pi_a P_a.
+      R Fa = R(0), Fb = R(0), Da = R(0);
       if (artts) {
         // circuit2.f90:294-336; the Monaghan switch dvr < 0 as a clamp
-        const R faba = Ka * dfa, fabb = Kb * dfb;
         const R dvr = vr * invr;
         const R dneg = dvr < R(0) ? dvr : R(0);
-        const R qav = R(-0.5) * A.rho * (alpha * A.c - beta * dneg) * dneg;
-        const R qbv = R(-0.5) * B.rho * (alpha * B.c - beta * dneg) * dneg;
-        F += qav * ga * A.Pi + qbv * gb * B.Pi;
-        R qc = R(0);
+        const R qav = hrhoa * (alpha_ca - beta * dneg) * dneg;
+        const R qbv = (R(-0.5) * B.rho) * (alpha * B.c - beta * dneg) * dneg;
+        Fa = qav;
+        Fb = qbv;
+        Da = qav * A.rho;
         if (use_au) {
+          const R faba = Ka * dfa, fabb = Kb * dfb;
           const R vsigu = fsqrt<R>(fdiv<R>(fabs(A.P - B.P), R(0.5) * (A.rho + B.rho)));
-          qc = au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + fabb * B.rho * B.Pi));
+          du.add(mb * (au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + fabb * B.rho * B.Pi))));
         }
-        du.add(mb * (dvr * qav * faba * rPiA + qc));
       }
       if (hydro) {
         // circuit2.f90:338-345
-        F += A.P * ga * A.Pi + B.P * gb * B.Pi;
-        du.add(mb * A.P * A.Pi * ga * vr);
+        Fa += A.P;
+        Fb += B.P;
+        Da += A.P;
       }
+      const R F = ga * A.Pi * Fa + gb * B.Pi * Fb;
+      du.add(mgv * A.Pi * Da);
       if constexpr (GENERAL) {
         PartX<R> BX;
         Loader<R>::extra(pb, j, BX);

@@ -117,9 +117,11 @@ __device__ __forceinline__ void kshape_f_df_res(float q, float q_lo, float& f, f
     float corr = 0.f;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      float th = cs[k] - q;
-      float tl = (-q) - (th - cs[k]);
-      if (!(th > 0.f)) { th = 0.f; tl = 0.f; }
+      const float traw = cs[k] - q;
+      const float tl = (-q) - (traw - cs[k]);
+      // a piece outside its support has th = 0, hence d = 0, and its
+      // residual tl then drops out of the correction by itself
+      const float th = fmaxf(traw, 0.f);
       float s = th * th;
       float d;
       if constexpr (K == KM6) {
