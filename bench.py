@@ -235,6 +235,24 @@ def adjoint_block(lib, n=256, n_ref=64, nsteps=200, every=20, dt=5e-4):
             "timing": "host clock around synchronous C-ABI calls"}
 
 
+def max_over_ranks(x, device="cuda"):
+    """The largest of every rank's x (every rank calls this at the same
+    point); x itself without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(ws, n_particles, steps, ms_max):
+    """Whole-job particle-steps/s of ws independent replicas of n_particles
+    each, `steps` steps, timed as the slowest rank's ms."""
+    return ws * n_particles * steps / (ms_max * 1e-3)
+
+
 def timed_steps(e, K):
     """Run K steps timed by CUDA events on the engine's stream: one pair
     around the call (the step time) and one per phase (SPH_P_TIMING = 1);
@@ -338,15 +356,13 @@ def main():
         with Clocks(uuid) as ck:
             ms, cnt, tm = timed_steps(e, args.steps)
             torch.cuda.synchronize()
+        ms = max_over_ranks(ms)
         if ws > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
             dist.barrier()
         return e, ms, cnt, tm, ck.summary()
 
     e, ms, cnt, tm, clocks = run(abi.PREC_FP32_COMP)
-    value = ws * N * args.steps / (ms * 1e-3)
+    value = replica_throughput(ws, N, args.steps, ms)
 
     # roofline of the dominant pair kernel: algorithmic FLOPs / its event time
     c1_flops = cnt["c1_pairs"] * F1_C1
@@ -379,11 +395,8 @@ def main():
             host_in, host_out = host_out, host_in
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
-        if ws > 1:
-            t = torch.tensor([el], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": ws * N * args.e2e_steps / el, "unit": UNIT,
+        el = max_over_ranks(el)
+        e2e = {"value": replica_throughput(ws, N, args.e2e_steps, el * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": N * 32 * 8, "d2h_bytes_per_step": N * 32 * 8,
                "steps": args.e2e_steps,
                "timing": "host clock around synchronous C-ABI calls (set_store, step, get_store)"}
@@ -393,7 +406,7 @@ def main():
     if not args.no_fp64:
         e6, ms6, cnt6, tm6, _ = run(abi.PREC_FP64)
         e6.close()
-        fp64 = {"value": ws * N * args.steps / (ms6 * 1e-3), "ms_per_step": ms6 / args.steps,
+        fp64 = {"value": replica_throughput(ws, N, args.steps, ms6), "ms_per_step": ms6 / args.steps,
                 "work_per_step": {"c1_pairs": cnt6["c1_pairs"] / args.steps,
                                   "device_allocations_in_timed_steps": cnt6["allocs"],
                                   "c1_max_sweeps": cnt6["c1_sweeps"], "neib_max": cnt6["neib_max"],
