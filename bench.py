@@ -370,7 +370,8 @@ def main():
     kern = {"circuit1": (c1_flops / args.steps, tm["circuit1"]),
             "circuit2": (c2_flops / args.steps, tm["circuit2"])}
     dom = max(kern, key=lambda k: kern[k][1])
-    ach = kern[dom][0] / (kern[dom][1] * 1e-3) / 1e12
+    # (no per-phase events inside a device-resident graph step)
+    ach = kern[dom][0] / (kern[dom][1] * 1e-3) / 1e12 if kern[dom][1] > 0 else 0.0
     traffic = C2_DRAM_BYTES_PER_PAIR * cnt["c2_pairs"] / args.steps if dom == "circuit2" else None
     roofline = {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": peak32 / 1e12,
                 "unit": "TFLOP/s", "frac": ach / (peak32 / 1e12), "traffic": traffic,

@@ -68,7 +68,11 @@ extern "C" {
                                     (4, 8, 16, 32; 0 = auto)                  */
 #define SPH_P_LANES_PAIR      61 /* lanes per centre in circuit1/circuit2     */
 #define SPH_P_FIXED_DT        62 /* dt of sph_adjoint_forward's steps (> 0)   */
-#define SPH_P_LAST            62
+#define SPH_P_GRAPH           63 /* 1: sph_step / sph_run_to run each step as a
+                                      replayed CUDA graph with no host round trip
+                                      inside (a step that cannot be planned on
+                                      the device is redone on the host path)   */
+#define SPH_P_LAST            63
 
 /* ---- status codes --------------------------------------------------------- */
 #define SPH_OK                     0
@@ -112,7 +116,9 @@ extern "C" {
                                     after a list outgrew its slots)          */
 #define SPH_CNT_EXACT_TESTS   13 /* candidates decided by the FP64 test      */
 #define SPH_CNT_ALLOCS        14 /* device allocations made by this handle    */
-#define SPH_CNT_TOTAL          15
+#define SPH_CNT_GRAPH_STEPS   15 /* steps run as a device-resident graph      */
+#define SPH_CNT_GRAPH_REDOS   16 /* device-resident steps redone on the host  */
+#define SPH_CNT_TOTAL          17
 
 /* ---- per-kernel timers (sph_get_timers, milliseconds, cumulative) ------- */
 #define SPH_T_PREDICT    0

@@ -42,11 +42,12 @@ P_NEIB_CAP = 59
 P_LANES_SEARCH = 60
 P_LANES_PAIR = 61
 P_FIXED_DT = 62
+P_GRAPH = 63
 
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",
             "c1_centre_sweeps", "launches", "neib_max", "searches",
-            "exact_tests", "allocs"]
+            "exact_tests", "allocs", "graph_steps", "graph_redos"]
 TIMERS = ["predict", "ghosts", "sort", "neighbours", "circuit1", "circuit2",
           "correct", "timestep", "sts", "step", "pack"]
 

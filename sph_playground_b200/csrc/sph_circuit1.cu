@@ -227,6 +227,7 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
 template <int K, int DIM, class R, int G>
 __global__ void __launch_bounds__(TPB)
 k_c1_sweep(C1Args a, PackBufs pb, Params P) {
+  if (a.gate && *a.gate == 0ull) return;  // the previous sweep left no particle active
   const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
   const int lane = threadIdx.x & (G - 1);
   const unsigned gmask = group_mask<G>();
@@ -356,15 +357,19 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
   if ((threadIdx.x & 31) == 0) {
     if (wp) atomicAdd(&a.dcnt[DC_C1_PAIRS], wp);
     if (ws) atomicAdd(&a.dcnt[DC_C1_CENTRE_SWEEPS], ws);
-    if (active_left) atomicOr(&a.red[RED_C1_ACTIVE], 1ull);
+    if (active_left) atomicOr(&a.red[a.active_slot], 1ull);
   }
 }
 
 __global__ void k_c1_snapshot(int64_t n, const int32_t* __restrict__ ssrc,
                               const double* __restrict__ hkp1, const double* __restrict__ dkp1,
                               const double* __restrict__ okp1, double* __restrict__ hk_s,
-                              double* __restrict__ dk_s, double* __restrict__ ok_s) {
+                              double* __restrict__ dk_s, double* __restrict__ ok_s,
+                              const DevPlan* __restrict__ plan,
+                              const unsigned long long* __restrict__ gate) {
+  if (gate && *gate == 0ull) return;
   int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (plan) n = plan->nall;  // launched over the capacity
   if (k >= n) return;
   int64_t p = ssrc[k];
   hk_s[k] = hkp1[p];
@@ -452,8 +457,9 @@ void launch_c1_finalize(int64_t nrows, int64_t nreal, double* cols, int64_t ld, 
 }
 void launch_c1_snapshot(int64_t n, const int32_t* ssrc, const double* hkp1, const double* dkp1,
                         const double* okp1, double* hk_s, double* dk_s, double* ok_s,
-                        cudaStream_t s) {
-  k_c1_snapshot<<<nblocks(n, 256), 256, 0, s>>>(n, ssrc, hkp1, dkp1, okp1, hk_s, dk_s, ok_s);
+                        cudaStream_t s, const DevPlan* plan, const unsigned long long* gate) {
+  k_c1_snapshot<<<nblocks(n, 256), 256, 0, s>>>(n, ssrc, hkp1, dkp1, okp1, hk_s, dk_s, ok_s,
+                                                plan, gate);
   note_launch();
 }
 

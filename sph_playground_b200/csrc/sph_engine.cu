@@ -137,6 +137,10 @@ void note_launch(int n) { g_launches += n; }
 long long launches_so_far() { return g_launches; }
 }  // namespace sph
 
+// Jacobi sweeps of circuit1 that a device-resident step runs before it asks
+// the host (a step whose particles need more is redone on the host path)
+constexpr int kDrsSweeps = 6;
+
 struct sph_handle {
   int dev = 0;  // the device current at sph_create
   int kernel_id = SPH_KERNEL_M6;
@@ -166,6 +170,19 @@ struct sph_handle {
   // particle table (the run's initial state, every k-th step, the final one)
   // and the states of the segment being replayed
   DevBuf adj, adj_par, adj_ckpt, adj_seg, adj_io;
+  // device-resident steps (SPH_P_GRAPH): the per-step plan, clock and error
+  // word on the device, the table saved at the start of a step (restored
+  // when the step has to be redone on the host path), the capacities the
+  // step is planned for, and the captured CUDA graph of one step
+  DevBuf drs_plan, drs_clock, drs_err, drs_save;
+  const DevPlan* dplan = nullptr;  // set while a device-resident step is built
+  int64_t nghost_cap = 0, nall_cap = 0;
+  int end_bit_cap = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool graph_dirty = true;
+  int64_t graph_alloc_mark = -1;  // allocations seen when the graph was captured
+  DevPlan* h_plan = nullptr;      // pinned read-back of the last device plan
   int adj_nsteps = -1, adj_every = 0, adj_ncp = 0;
   bool adj_initial_force = false;
   double adj_dt = 0., adj_t0 = 0.;
@@ -219,7 +236,7 @@ struct sph_handle {
     cudaEvent_t a = nullptr, b = nullptr;
     Phase(sph_handle* hh, int sl) : h(hh), slot(sl) {
       const double mode = h->st[SPH_P_TIMING];
-      if (mode == 1 || (mode == 2 && sl == SPH_T_STEP)) {
+      if (!h->dplan && (mode == 1 || (mode == 2 && sl == SPH_T_STEP))) {
         a = h->get_event();
         b = h->get_event();
         cudaEventRecord(a, h->s);
@@ -468,6 +485,7 @@ struct sph_handle {
     }
     launch_reorder(cols.as<double>(), cols_alt.as<double>(), orig.as<int32_t>(),
                    orig_alt.as<int32_t>(), perm, nrows, nrows, nrows, s);
+    graph_dirty = true;  // a captured step holds the old table pointers
     std::swap(cols.p, cols_alt.p);
     std::swap(cols.bytes, cols_alt.bytes);
     std::swap(orig.p, orig_alt.p);
@@ -681,8 +699,12 @@ struct sph_handle {
     }
     {
       Phase pk(this, SPH_T_PACK);
-      launch_pack(prec, PACK_POS, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
-                  sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+      if (dplan)
+        launch_pack_dev(prec, PACK_POS, nall_cap, ssrc.as<int32_t>(), sx.as<double>(),
+                        sy.as<double>(), sz.as<double>(), cols.as<double>(), nrows, dplan, pb, s);
+      else
+        launch_pack(prec, PACK_POS, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+                    sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
     }
     Phase ph(this, SPH_T_CIRCUIT1);
     C1Args a{};
@@ -706,6 +728,8 @@ struct sph_handle {
     a.status = status.as<int>();
     a.dcnt = dcnt.as<unsigned long long>();
     a.red = red.as<unsigned long long>();
+    a.active_slot = RED_C1_ACTIVE;
+    a.gate = nullptr;
     const bool advanced = ival(ec_adden) == 1;
     if (advanced && P.maxiter == 0) {  // zero sweeps: h, rho, Omega stay (circuit1.f90:114)
       launch_eos(cols.as<double>(), nrows, nreal, P, s);
@@ -724,6 +748,32 @@ struct sph_handle {
     CK(cudaMemcpyAsync(okp1.p, col(es_om), sizeof(double) * nrows, cudaMemcpyDeviceToDevice, s));
     launch_set_col(epsb.as<double>(), nrows, 1.0, s);
     int iter = 0;
+    if (dplan) {
+      // device-resident step: a fixed number of sweeps without looking at
+      // the host; a particle that converged skips the later sweeps, so the
+      // result equals the host loop's as long as all converge within them
+      // (otherwise the error word sends the step back to the host path)
+      // (sweep k marks slot k % 2; sweep k + 1 and its snapshot do nothing
+      // once that slot stays zero)
+      const int sweeps = a.simple ? 1 : std::max(1, std::min(P.maxiter, kDrsSweeps));
+      unsigned long long* rb = red.as<unsigned long long>();
+      for (iter = 1; iter <= sweeps; ++iter) {
+        const unsigned long long* gate =
+            iter == 1 ? nullptr : rb + ((iter - 1) % 2 ? RED_C1_ACTIVE : RED_C1_ACTIVE2);
+        a.active_slot = iter % 2 ? RED_C1_ACTIVE : RED_C1_ACTIVE2;
+        a.gate = gate;
+        launch_c1_snapshot(nall_cap, ssrc.as<int32_t>(), hkp1.as<double>(), dkp1.as<double>(),
+                           okp1.as<double>(), hk_s.as<double>(), dk_s.as<double>(),
+                           ok_s.as<double>(), s, dplan, gate);
+        launch_fill_u64(rb + a.active_slot, 1, 0ull, s);
+        launch_c1_sweep(prec, kernel_id, P.dim, a, pb, P, s);
+      }
+      --iter;
+      if (!a.simple && sweeps < P.maxiter)
+        launch_flag_if_nonzero(rb + a.active_slot, drs_err.as<int>(), SPH_ERR_STATE, s);
+      a.active_slot = RED_C1_ACTIVE;
+      a.gate = nullptr;
+    } else
     for (;;) {
       ++iter;
       launch_c1_snapshot(nall, ssrc.as<int32_t>(), hkp1.as<double>(), dkp1.as<double>(),
@@ -751,8 +801,12 @@ struct sph_handle {
     int groups = PACK_POS | PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
     {
       Phase pk(this, SPH_T_PACK);
-      launch_pack(prec, groups, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
-                  sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
+      if (dplan)
+        launch_pack_dev(prec, groups, nall_cap, ssrc.as<int32_t>(), sx.as<double>(),
+                        sy.as<double>(), sz.as<double>(), cols.as<double>(), nrows, dplan, pb, s);
+      else
+        launch_pack(prec, groups, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+                    sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
     }
     Phase ph(this, SPH_T_CIRCUIT2);
     C2Args a{};
@@ -777,6 +831,7 @@ struct sph_handle {
 
   // iterate() (iterator.f90:44-179); full = false stops after circuit1 + EOS
   int iterate(bool full) {
+    if (dplan) return iterate_dev(full);
     Params P{};
     RC(params(P));
     Mode m;
@@ -787,6 +842,271 @@ struct sph_handle {
     RC(check_status());
     cnt_host[SPH_CNT_ITERATES] += full ? 1 : 0;
     cnt_host[SPH_CNT_CENTRES] += nreal;
+    return SPH_OK;
+  }
+
+  // ---- device-resident step ------------------------------------------------------------------
+  // The classic step asks the host four or five times per iterate (image
+  // count and bounding box, list overflow, Newton sweeps, status) and once
+  // per step (dt).  The device-resident step plans all of that on the device
+  // (k_plan, k_dt), runs the sort and the passes over capacities fixed on the
+  // host, and reports problems through one error word read after the step:
+  // a capacity that was too small, a list row that overflowed, or Newton
+  // sweeps beyond kDrsSweeps send the step back to the host path from the
+  // table saved at its start.  With no host round trip inside, one step is
+  // captured as a CUDA graph and replayed.
+
+  int neighbour_phase_dev(const Mode& m, const Params& P) {
+    const int d = P.dim;
+    BoxGeom g = box(m);
+    if (m.ghosts) launch_reflect(cols.as<double>(), nrows, nreal, g, s);
+    SlotInit si{};
+    for (int k = 0; k < 3; ++k) {
+      si.off[si.n] = RED_LO_X + k; si.val[si.n++] = dkey(1e308);
+      si.off[si.n] = RED_HI_X + k; si.val[si.n++] = dkey(-1e308);
+    }
+    si.off[si.n] = RED_HMIN; si.val[si.n++] = dkey(1e308);
+    launch_init_slots(red.as<unsigned long long>(), si, s);
+    BoxGeom gg = g;
+    if (!m.ghosts) for (int k = 0; k < 3; ++k) gg.periodic[k] = 0;
+    launch_ghost_count(cols.as<double>(), nrows, nreal, gg, d, gcount.as<int32_t>(),
+                       red.as<unsigned long long>(), s);
+    CK(cudaMemsetAsync(gcount.as<int32_t>() + nrows, 0, sizeof(int32_t), s));
+    exclusive_scan(scan_tmp.p, scan_tmp.bytes, gcount.as<int32_t>(), goff.as<int32_t>(),
+                   nrows + 1, s);
+    PlanIn pin{};
+    pin.nrows = nrows;
+    pin.nghost_cap = nghost_cap;
+    pin.nall_cap = nall_cap;
+    pin.krad = P.krad;
+    pin.cf = st[SPH_P_CELL_FACTOR] > 0 ? st[SPH_P_CELL_FACTOR] : 0.4;
+    pin.mref = mref;
+    pin.end_bit_cap = end_bit_cap;
+    DevPlan* plan = drs_plan.as<DevPlan>();
+    launch_plan(red.as<unsigned long long>(), goff.as<int32_t>() + nrows, pin, plan,
+                drs_err.as<int>(), s);
+    launch_ghost_write_cap(cols.as<double>(), nrows, gg, d, goff.as<int32_t>(), nghost_cap,
+                           gx.as<double>(), gy.as<double>(), gz.as<double>(),
+                           gsrc.as<int32_t>(), gcode.as<int8_t>(), s);
+    launch_keys_dev(cols.as<double>(), nrows, gx.as<double>(), gy.as<double>(), gz.as<double>(),
+                    plan, nall_cap, keys.as<uint32_t>(), vals.as<int32_t>(), s);
+    sort_pairs(sort_tmp.p, sort_tmp.bytes, keys.as<uint32_t>(), keys_alt.as<uint32_t>(),
+               vals.as<int32_t>(), vals_alt.as<int32_t>(), nall_cap, end_bit_cap, s);
+    launch_cell_starts_dev(keys_alt.as<uint32_t>(), nall_cap, plan, cstart.as<int32_t>(), s);
+    launch_sorted_gather_dev(vals_alt.as<int32_t>(), nall_cap, nrows, nreal, cols.as<double>(),
+                             gx.as<double>(), gy.as<double>(), gz.as<double>(),
+                             gsrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+                             sz.as<double>(), ssrc.as<int32_t>(), cflag.as<int32_t>(),
+                             s32.as<float4>(), plan, s);
+    exclusive_scan(scan_tmp.p, scan_tmp.bytes, cflag.as<int32_t>(), cpos.as<int32_t>(),
+                   nall_cap + 1, s);
+    launch_centres(vals_alt.as<int32_t>(), cflag.as<int32_t>(), cpos.as<int32_t>(), nall_cap,
+                   centre_k.as<int32_t>(), centre_p.as<int32_t>(), s);
+    launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(), count_prev.as<int32_t>(),
+                  h_prev.as<float>(), col(es_h), d, 1.2f, rowcap64.as<int64_t>(),
+                  rowcap.as<int32_t>(), s);
+    exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, rowcap64.as<int64_t>(), rowoff.as<int64_t>(),
+                     nreal, s);
+    NeibArgs na{};
+    na.plan = plan;
+    na.nc = nreal;
+    na.centre_k = centre_k.as<int32_t>();
+    na.centre_p = centre_p.as<int32_t>();
+    na.sx = sx.as<double>(); na.sy = sy.as<double>(); na.sz = sz.as<double>();
+    na.s32 = s32.as<float4>();
+    na.hcol = col(es_h);
+    na.krad = P.krad;
+    na.cstart = cstart.as<int32_t>();
+    na.rowoff = rowoff.as<int64_t>();
+    na.rowcap = rowcap.as<int32_t>();
+    na.nl_size = nl_size;
+    na.nl = nl.as<int32_t>();
+    na.ncnt = ncnt.as<int32_t>();
+    na.orig = orig.as<int32_t>();
+    na.count_prev = count_prev.as<int32_t>();
+    na.h_prev = h_prev.as<float>();
+    na.maxcnt = maxcnt.as<int32_t>();
+    na.overflow = overflow.as<int32_t>();
+    na.dcnt = dcnt.as<unsigned long long>();
+    launch_neighbours(d, lanes_search(), na, s);
+    CK(cudaGetLastError());
+    return SPH_OK;
+  }
+
+  int iterate_dev(bool full) {
+    Params P{};
+    RC(params(P));
+    Mode m;
+    RC(mode(m));
+    RC(neighbour_phase_dev(m, P));
+    RC(circuit1(m, P));
+    if (full) RC(circuit2(m, P));
+    return SPH_OK;
+  }
+
+  // can this handle's step run without the host?  (sets the reason when not)
+  bool drs_eligible(const char** why) {
+    eqset();
+    Mode m;
+    if (mode(m) != SPH_OK) { *why = "mode"; return false; }
+    if (!started) { *why = "not started"; return false; }
+    if (eq_radexch) { *why = "radiation exchange"; return false; }
+    if (eq_sts && ival(ec_ststype) != 1) { *why = "STS with automatic stages"; return false; }
+    if (m.eos_kind == 2) { *why = "isothermal EOS"; return false; }
+    if (st[SPH_P_NEIB_CAP_CHECK] != 0) { *why = "neighbour cap check"; return false; }
+    if (nl_size <= 0 || nghost < 0) { *why = "no search yet"; return false; }
+    return true;
+  }
+
+  // capacities of the device-resident step, from the last host-planned one
+  int drs_prepare() {
+    const int64_t want_ghost = nghost + nghost / 4 + 1024;
+    if (want_ghost > nghost_cap || nall_cap != nrows + nghost_cap) {
+      nghost_cap = std::max(want_ghost, nghost_cap);
+      nall_cap = nrows + nghost_cap;
+      graph_dirty = true;
+    }
+    RC(gx.ensure(sizeof(double) * nghost_cap));
+    RC(gy.ensure(sizeof(double) * nghost_cap));
+    RC(gz.ensure(sizeof(double) * nghost_cap));
+    RC(gsrc.ensure(sizeof(int32_t) * nghost_cap));
+    RC(gcode.ensure(sizeof(int8_t) * nghost_cap));
+    RC(alloc_all(nall_cap));
+    const int64_t cap = std::min<int64_t>(std::max<int64_t>(8 * nall_cap, 1 << 20),
+                                          int64_t(1) << 31);
+    RC(cstart.ensure(sizeof(int32_t) * size_t(cap + 1)));
+    int eb = 1;
+    while (eb < 32 && (int64_t(1) << eb) <= cap) ++eb;
+    if (eb != end_bit_cap) { end_bit_cap = eb; graph_dirty = true; }
+    RC(drs_plan.ensure(sizeof(DevPlan)));
+    RC(drs_clock.ensure(sizeof(DevClock)));
+    RC(drs_err.ensure(sizeof(int)));
+    RC(drs_save.ensure(sizeof(double) * NCOL * size_t(nrows)));
+    if (eq_sts) RC(stsY.ensure(sizeof(double) * 6 * nrows));
+    return SPH_OK;
+  }
+
+  // the work of one step, with every size and decision on the device
+  int step_body_dev() {
+    CK(cudaMemsetAsync(drs_err.p, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
+    Params P{};
+    RC(params(P));
+    unsigned long long* r = red.as<unsigned long long>();
+    SlotInit si{};
+    const int slot[8] = {RED_TS_HMIN, RED_TS_CMAX, RED_TS_DENMIN, RED_TS_CMIN,
+                         RED_TS_KAPMAX, RED_TS_BMAX, RED_TS_KAPMIN, RED_TS_LAMMAX};
+    const double init[8] = {1e308, -1e308, 1e308, 1e308, -1e308, -1e308, 1e308, -1e308};
+    for (int k = 0; k < 8; ++k) { si.off[k] = slot[k]; si.val[k] = dkey(init[k]); }
+    si.n = 8;
+    launch_init_slots(r, si, s);
+    launch_timestep_reduce(cols.as<double>(), nrows, orig.as<int32_t>(), nrows,
+                           int64_t(st[ec_realpn]), P, r, s);
+    DtIn di{};
+    di.eq_hydro = eq_hydro; di.eq_magneto = eq_magneto; di.eq_diff = eq_diff; di.eq_fld = eq_fld;
+    di.sts_fixed = eq_sts ? 1 : 0;
+    di.sts_s = ival(ec_stsfixeds);
+    di.cn_hydro = kb.cn_hydro;
+    di.cnd2 = cnd2();
+    launch_dt(r, di, drs_clock.as<DevClock>(), ctrl.as<double>(), s);
+    const bool do_sts = eq_sts;
+    launch_predict(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
+                   ctrl.as<double>(), do_sts, s);
+    RC(iterate(true));
+    launch_correct(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
+                   ctrl.as<double>(), do_sts, s);
+    if (do_sts) RC(sts_integrate(ival(ec_stsfixeds), 0.0));
+    launch_clock_advance(drs_clock.as<DevClock>(), s);
+    return SPH_OK;
+  }
+
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+    graph_dirty = true;
+  }
+
+  // one step of the time loop without host round trips (falls back to
+  // one_step when the handle does not qualify or the step must be redone)
+  int one_step_graph(double tfinish, bool& done) {
+    double t = st[ec_time];
+    if (!((t < tfinish + std::numeric_limits<double>::epsilon()) && !stopped)) {
+      done = true;
+      return SPH_OK;
+    }
+    const char* why = nullptr;
+    if (!drs_eligible(&why)) {
+      static const bool log = std::getenv("SPH_GRAPH_LOG") != nullptr;
+      if (log) std::fprintf(stderr, "sph: step on the host path: %s\n", why);
+      return one_step(tfinish, done);
+    }
+    done = false;
+    int reorder_every = int(st[SPH_P_REORDER_EVERY]);
+    if (reorder_every > 0 && steps_since_reorder >= reorder_every) RC(reorder_rows());
+    RC(drs_prepare());
+    // buffers the graph was captured with may have moved since
+    if (cnt_host[SPH_CNT_ALLOCS] != graph_alloc_mark) graph_dirty = true;
+    RC(copy_table(drs_save.p, cols.p));
+    DevClock clk{};
+    clk.t = t;
+    clk.ltout = ltout;
+    clk.dtout = dtout;
+    clk.tfinish = tfinish;
+    clk.stopped = stopped ? 1 : 0;
+    std::memcpy(h_ctrl + 1, &clk, sizeof(DevClock));
+    CK(cudaMemcpyAsync(drs_clock.p, h_ctrl + 1, sizeof(DevClock), cudaMemcpyHostToDevice, s));
+    if (graph_dirty || !graph_exec) {
+      drop_graph();
+      dplan = drs_plan.as<DevPlan>();
+      cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      int rc = e == cudaSuccess ? step_body_dev() : SPH_ERR_CUDA;
+      cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      dplan = nullptr;
+      if (rc || e != cudaSuccess || e2 != cudaSuccess) {
+        cudaGetLastError();
+        drop_graph();
+        if (!rc) rc = fail(SPH_ERR_CUDA, "step capture failed");
+        return rc;
+      }
+      if (cudaGraphInstantiate(&graph_exec, graph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        drop_graph();
+        return fail(SPH_ERR_CUDA, "graph instantiation failed");
+      }
+      graph_dirty = false;
+      graph_alloc_mark = cnt_host[SPH_CNT_ALLOCS];
+    }
+    CK(cudaGraphLaunch(graph_exec, s));
+    // one read-back per step: the clock, the error words
+    CK(cudaMemcpyAsync(h_ctrl + 1, drs_clock.p, sizeof(DevClock), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h_i32 + 4, drs_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h_i32 + 5, overflow.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h_i32 + 6, status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h_plan, drs_plan.p, sizeof(DevPlan), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaGetLastError());
+    std::memcpy(&clk, h_ctrl + 1, sizeof(DevClock));
+    if (h_i32[4] || h_i32[5] || h_i32[6]) {
+      // redo this step on the host path from the saved table
+      RC(copy_table(cols.p, drs_save.p));
+      CK(cudaMemsetAsync(status.p, 0, sizeof(int), s));
+      cnt_host[SPH_CNT_GRAPH_REDOS]++;
+      return one_step(tfinish, done);
+    }
+    st[ec_time] = clk.t;
+    ltout = clk.ltout;
+    stopped = clk.stopped != 0;
+    have_order = true;
+    nghost = h_plan->nghost;  // the host view of the last search, as after a host step
+    grid = h_plan->grid;
+    pgeom = h_plan->pg;
+    cnt_host[SPH_CNT_STEPS]++;
+    cnt_host[SPH_CNT_ITERATES] += eq_sts ? 1 + ival(ec_stsfixeds) : 1;
+    cnt_host[SPH_CNT_SEARCHES] += eq_sts ? 1 + ival(ec_stsfixeds) : 1;
+    steps_since_reorder++;
+    cnt_host[SPH_CNT_GRAPH_STEPS]++;
     return SPH_OK;
   }
 
@@ -1167,6 +1487,8 @@ struct sph_handle {
       cudaEventDestroy(pe.second.second);
     }
     for (auto e : ev_pool) cudaEventDestroy(e);
+    drop_graph();
+    if (h_plan) cudaFreeHost(h_plan);
     if (h_red) cudaFreeHost(h_red);
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (h_i32) cudaFreeHost(h_i32);
@@ -1232,7 +1554,8 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
     return fail(SPH_ERR_CUDA, "cudaStreamCreate failed");
   }
   if (cudaMallocHost(&h->h_red, sizeof(unsigned long long) * (RED_TOTAL + 2)) != cudaSuccess ||
-      cudaMallocHost(&h->h_ctrl, sizeof(double) * 8) != cudaSuccess ||
+      cudaMallocHost(&h->h_ctrl, sizeof(double) * 16) != cudaSuccess ||
+      cudaMallocHost(&h->h_plan, sizeof(DevPlan)) != cudaSuccess ||
       cudaMallocHost(&h->h_i32, sizeof(int32_t) * 8) != cudaSuccess) {
     cudaGetLastError();
     h->destroy();
@@ -1265,6 +1588,7 @@ int sph_set_param(sph_handle* h, int index, double value) {
   if (!h || index < 1 || index > SPH_P_LAST) return fail(SPH_ERR_ARG, "bad param index");
   if ((index == ec_realpn || index == ec_fixedpn) && value != h->st[index])
     return fail(SPH_ERR_ARG, "particle counts are fixed by the store");
+  if (h->st[index] != value) h->graph_dirty = true;  // a captured step holds the old value
   h->st[index] = value;
   if (index == SPH_P_NEIB_CAP && value > 0) h->est_count = 0;
   return SPH_OK;
@@ -1312,9 +1636,10 @@ int sph_step(sph_handle* h, int nsteps) {
     sph_handle::Phase ph(h, SPH_T_STEP);
     if (!h->started) rc = h->start_run();
     if (!rc && h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
+    const bool graph = h->st[SPH_P_GRAPH] != 0;
     for (int i = 0; !rc && i < nsteps; ++i) {
       bool done = false;
-      rc = h->one_step(h->st[ec_tfinish], done);
+      rc = graph ? h->one_step_graph(h->st[ec_tfinish], done) : h->one_step(h->st[ec_tfinish], done);
       if (done) break;
     }
   }
@@ -1331,9 +1656,10 @@ int sph_run_to(sph_handle* h, double tfinish) {
     sph_handle::Phase ph(h, SPH_T_STEP);
     if (!h->started) rc = h->start_run();
     if (!rc && h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
+    const bool graph = h->st[SPH_P_GRAPH] != 0;
     while (!rc) {
       bool done = false;
-      rc = h->one_step(tfinish, done);
+      rc = graph ? h->one_step_graph(tfinish, done) : h->one_step(tfinish, done);
       if (done) break;
     }
   }

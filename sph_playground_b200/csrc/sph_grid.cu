@@ -232,7 +232,7 @@ k_ghost_count(const double* __restrict__ cols, int64_t ld, int64_t nrows, int64_
 }
 
 __global__ void k_ghost_write(const double* __restrict__ cols, int64_t ld, int64_t nrows,
-                              BoxGeom g, int dim, const int32_t* __restrict__ offset,
+                              BoxGeom g, int dim, const int32_t* __restrict__ offset, int64_t cap,
                               double* __restrict__ gx, double* __restrict__ gy,
                               double* __restrict__ gz, int32_t* __restrict__ gsrc,
                               int8_t* __restrict__ gcode) {
@@ -245,6 +245,7 @@ __global__ void k_ghost_write(const double* __restrict__ cols, int64_t ld, int64
   for (int mask = 1; mask < 8; ++mask) {
     int sg[3];
     if (!image_of(s, mask, sg)) continue;
+    if (o >= cap) return;  // a device-resident step found more images than room
     gx[o] = image_coord(r[0], sg[0], g.emin[0], g.emax[0]);
     gy[o] = image_coord(r[1], sg[1], g.emin[1], g.emax[1]);
     gz[o] = image_coord(r[2], sg[2], g.emin[2], g.emax[2]);
@@ -267,12 +268,26 @@ __device__ __forceinline__ int cell_coord(double x, double o, double invL, int n
   return int(f);
 }
 
+// With a device plan the particle count and grid come from it, and the
+// slots up to the capacity ncap get the padding key (sorted behind every
+// cell) so that the sort can run over a size fixed on the host.
 __global__ void k_keys(const double* __restrict__ cols, int64_t ld, int64_t nrows,
                        const double* __restrict__ gx, const double* __restrict__ gy,
                        const double* __restrict__ gz, int64_t nghost, Grid g,
-                       uint32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+                       uint32_t* __restrict__ keys, int32_t* __restrict__ vals,
+                       const DevPlan* __restrict__ plan, int64_t ncap) {
   int64_t u = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (u >= nrows + nghost) return;
+  int64_t n = nrows + nghost;
+  if (plan) {
+    n = plan->nall;
+    g = plan->grid;
+    if (u >= n && u < ncap) {
+      keys[u] = plan->pad_key;
+      vals[u] = int32_t(u);
+      return;
+    }
+  }
+  if (u >= n) return;
   double x, y, z;
   if (u < nrows) {
     x = cols[es_rx * ld + u]; y = cols[es_ry * ld + u]; z = cols[es_rz * ld + u];
@@ -290,8 +305,12 @@ __global__ void k_keys(const double* __restrict__ cols, int64_t ld, int64_t nrow
 // cstart[c] = number of particles in cells before c (ncell + 1 entries), from
 // the sorted keys: each key change fills the empty cells it skips.
 __global__ void k_cell_starts(const uint32_t* __restrict__ keys, int64_t n, int64_t ncell,
-                              int32_t* __restrict__ cstart) {
+                              int32_t* __restrict__ cstart, const DevPlan* __restrict__ plan) {
   int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (plan) {
+    n = plan->nall;
+    ncell = plan->ncell;
+  }
   if (k > n) return;
   int64_t lo, hi;  // cells (lo, hi] start at k
   if (k == 0) { lo = -1; hi = n > 0 ? int64_t(keys[0]) : ncell; }
@@ -309,8 +328,16 @@ __global__ void k_sorted_gather(const int32_t* __restrict__ sidx, int64_t n, int
                                 double* __restrict__ sx, double* __restrict__ sy,
                                 double* __restrict__ sz, int32_t* __restrict__ ssrc,
                                 int32_t* __restrict__ centre_slot, float4* __restrict__ s32,
-                                PackGeom pg) {
+                                PackGeom pg, const DevPlan* __restrict__ plan, int64_t ncap) {
   int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (plan) {
+    n = plan->nall;
+    pg = plan->pg;
+    if (k >= n && k <= ncap) {  // no centres past the particles (the scan covers ncap + 1)
+      centre_slot[k] = 0;
+      return;
+    }
+  }
   if (k >= n) return;
   int64_t u = sidx[k];
   double x, y, z;
@@ -410,7 +437,12 @@ k_neighbours(NeibArgs a) {
   int2* rs = ranges[threadIdx.x / G];
   float4* bt = batch[threadIdx.x / G];
   unsigned int ncand = 0, nexact = 0, nfound = 0;
-  const Grid g = a.g;
+  Grid g = a.g;
+  double shift = a.shift;
+  if (a.plan) {
+    g = a.plan->grid;
+    shift = a.plan->pg.shift;
+  }
   // Every loop below runs the same number of passes on all lanes of the warp
   // (the maximum over its groups), so votes and shuffles take the full mask.
   const bool active = c < a.nc;
@@ -434,7 +466,7 @@ k_neighbours(NeibArgs a) {
     const double kh = __dmul_rn(a.krad, a.hcol[p]);
     R2 = __dmul_rn(kh, kh);
     const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
-    const double er = (a.shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
+    const double er = (shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
     const double delta = 8.0 * er + 4.0 * er * er + 1e-6;
     lo_thr = float(R2 * (1.0 - delta));
     hi_thr = float(R2 * (1.0 + delta));
@@ -694,8 +726,12 @@ __global__ void k_rowcap(int64_t nc, const int32_t* __restrict__ centre_p,
 __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restrict__ ssrc,
                        const double* __restrict__ sx, const double* __restrict__ sy,
                        const double* __restrict__ sz, const double* __restrict__ cols, int64_t ld,
-                       PackGeom pg, PackBufs pb) {
+                       PackGeom pg, PackBufs pb, const DevPlan* __restrict__ plan) {
   int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (plan) {
+    n = plan->nall;
+    pg = plan->pg;
+  }
   if (k >= n) return;
   const int64_t p = ssrc[k];
   auto C = [&](int f) { return cols[f * ld + p]; };
@@ -884,6 +920,133 @@ __global__ void k_radexch(double* __restrict__ cols, int64_t ld, const int32_t* 
   if (!(C(es_t) > 0.) || !(C(es_u) > 0.)) atomicCAS(status, 0, SPH_ERR_RAD_NEGATIVE);
 }
 
+// ---- device-resident step: the host's per-step arithmetic on the device ------------------
+// k_plan repeats the host code between the image count and the sort (grid
+// edge krad h_min f widened by 1.25 until the cell count fits, the FP32
+// binade of the extent), with the same FP64 operations in the same order
+// and no contraction, so a step planned here equals the host-planned one.
+__global__ void k_plan(const unsigned long long* __restrict__ red,
+                       const int32_t* __restrict__ nghost_dev, PlanIn in,
+                       DevPlan* __restrict__ plan, int* __restrict__ err_out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  DevPlan P{};
+  P.err = 0;
+  int64_t ng = nghost_dev[0];
+  if (ng > in.nghost_cap || in.nrows + ng > in.nall_cap) {
+    P.err = SPH_ERR_STATE;  // more images than room: redo on the host path
+    ng = min(ng, in.nghost_cap);
+    if (in.nrows + ng > in.nall_cap) ng = in.nall_cap - in.nrows;
+  }
+  P.nghost = ng;
+  P.nall = in.nrows + ng;
+  P.pad_key = in.end_bit_cap >= 32 ? 0xffffffffu : ((1u << in.end_bit_cap) - 1u);
+  double lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = dkey_inv(red[RED_LO_X + k]);
+    hi[k] = dkey_inv(red[RED_HI_X + k]);
+  }
+  const double hmin = dkey_inv(red[RED_HMIN]);
+  bool ok_in = true;
+  if (!(hmin > 0) || !isfinite(hmin)) { P.err = P.err ? P.err : SPH_ERR_IC_H; ok_in = false; }
+  for (int k = 0; k < 3; ++k)
+    if (!isfinite(lo[k]) || !isfinite(hi[k])) { P.err = P.err ? P.err : SPH_ERR_Q_NAN; ok_in = false; }
+  double L = __dmul_rn(__dmul_rn(in.krad, hmin), in.cf);
+  const int64_t ncap = min(max(int64_t(8) * P.nall, int64_t(1) << 20), int64_t(1) << 31);
+  int n3[3] = {1, 1, 1};
+  int64_t ncell = 1;
+  bool fits = ok_in;
+  for (int guard = 0; fits; ++guard) {
+    bool ok = true;
+    ncell = 1;
+    for (int k = 0; k < 3; ++k) {
+      const double e = __ddiv_rn(__dadd_rn(hi[k], -lo[k]), L);
+      if (!(e < 1e9)) { ok = false; break; }
+      n3[k] = int(floor(e)) + 1;
+      ncell *= n3[k];
+    }
+    if (ok && ncell <= ncap) break;
+    L = __dmul_rn(L, 1.25);
+    if (guard > 400) { fits = false; P.err = P.err ? P.err : SPH_ERR_GRID; }
+  }
+  if (!fits) {  // an error: a one-cell grid keeps every later launch in bounds
+    n3[0] = n3[1] = n3[2] = 1;
+    ncell = 1;
+    L = 1.0;
+    for (int k = 0; k < 3; ++k) lo[k] = hi[k] = 0.0;
+  }
+  P.ncell = ncell;
+  P.grid.ox = lo[0]; P.grid.oy = lo[1]; P.grid.oz = lo[2];
+  P.grid.L = L;
+  P.grid.invL = __ddiv_rn(1.0, L);
+  P.grid.nx = n3[0]; P.grid.ny = n3[1]; P.grid.nz = n3[2];
+  const double e0 = __dadd_rn(hi[0], -lo[0]), e1 = __dadd_rn(hi[1], -lo[1]),
+               e2 = __dadd_rn(hi[2], -lo[2]);
+  const double ext = e0 < (e2 > e1 ? e2 : e1) ? (e2 > e1 ? e2 : e1) : e0;
+  double sh = 1.0;
+  if (ext > 0) {
+    const double lim = __dmul_rn(ext, 1.0001);
+    while (sh < lim) sh = __dmul_rn(sh, 2.0);
+    while (__dmul_rn(sh, 0.5) >= lim) sh = __dmul_rn(sh, 0.5);
+  }
+  P.pg.ox = lo[0]; P.pg.oy = lo[1]; P.pg.oz = lo[2];
+  P.pg.shift = sh;
+  P.pg.mref = in.mref;
+  *plan = P;
+  if (P.err) atomicCAS(err_out, 0, P.err);
+}
+__global__ void k_flag_if_nonzero(const unsigned long long* __restrict__ v, int* __restrict__ err,
+                                  int code) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *v != 0ull) atomicCAS(err, 0, code);
+}
+
+// dt of timestep.f90:40-166 and the clipping to tfinish / the next output
+// time of main.f90:241-320, as the host does them (same operations, no
+// contraction); writes dt to ctrl[0] for the predictor and corrector.
+__device__ __forceinline__ double dmin_host(double a, double b) { return b < a ? b : a; }
+__global__ void k_dt(const unsigned long long* __restrict__ red, DtIn in,
+                     DevClock* __restrict__ clk, double* __restrict__ ctrl) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const double hmin = dkey_inv(red[RED_TS_HMIN]), cmax = dkey_inv(red[RED_TS_CMAX]);
+  const double denmin = dkey_inv(red[RED_TS_DENMIN]), cmin = dkey_inv(red[RED_TS_CMIN]);
+  const double kapmax = dkey_inv(red[RED_TS_KAPMAX]), bmax = dkey_inv(red[RED_TS_BMAX]);
+  const double kapmin = dkey_inv(red[RED_TS_KAPMIN]), lammax = dkey_inv(red[RED_TS_LAMMAX]);
+  double dt = 1.7976931348623157e308;
+  double dtdiff = __longlong_as_double(0x7ff0000000000000LL), dtfld = dtdiff;
+  if (in.eq_hydro) dt = dmin_host(dt, __ddiv_rn(__dmul_rn(in.cn_hydro, hmin), cmax));
+  if (in.eq_magneto)
+    dt = dmin_host(dt, __ddiv_rn(__ddiv_rn(__dmul_rn(.1, hmin), cmax), bmax));
+  if (in.eq_diff) {
+    dtdiff = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(in.cnd2, denmin), cmin), __dmul_rn(hmin, hmin)),
+                       kapmax);
+    dt = dmin_host(dt, dtdiff);
+  }
+  if (in.eq_fld) {
+    dtfld = __ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(in.cnd2, hmin), hmin),
+                                                    denmin), kapmin), kLightspeed), lammax);
+    dt = dmin_host(dt, dtfld);
+  }
+  if (in.sts_fixed) {
+    const double sts_dt_min = dmin_host(dtdiff, dtfld);
+    dt = __dmul_rn(__dmul_rn(double(in.sts_s * in.sts_s + in.sts_s) - 2., 0.25), sts_dt_min);
+  }
+  DevClock c = *clk;
+  const double t = c.t;
+  if (__dadd_rn(t, dt) > c.tfinish) { dt = __dadd_rn(c.tfinish, -t); c.stopped = 1; }
+  if (c.dtout > 0) {
+    if (t >= c.ltout) { while (c.ltout <= t) c.ltout = __dadd_rn(c.ltout, c.dtout); }
+    if (__dadd_rn(t, dt) > c.ltout) {
+      if (c.dtout < dt) c.ltout = __dadd_rn(__dadd_rn(c.ltout, -c.dtout), dt);
+      else dt = __dadd_rn(c.ltout, -t);
+    }
+  }
+  c.dt = dt;
+  *clk = c;
+  ctrl[0] = dt;
+}
+__global__ void k_clock_advance(DevClock* __restrict__ clk) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) clk->t = __dadd_rn(clk->t, clk->dt);
+}
+
 __global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i < n) p[i] = v;
@@ -1001,7 +1164,14 @@ void launch_ghost_count(const double* cols, int64_t nrows, int64_t nreal, BoxGeo
 void launch_ghost_write(const double* cols, int64_t nrows, BoxGeom g, int dim,
                         const int32_t* offset, double* gx, double* gy, double* gz,
                         int32_t* gsrc, int8_t* gcode, unsigned long long*, cudaStream_t s) {
-  k_ghost_write<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, g, dim, offset, gx, gy, gz,
+  k_ghost_write<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, g, dim, offset, INT64_MAX, gx,
+                                               gy, gz, gsrc, gcode);
+  note_launch();
+}
+void launch_ghost_write_cap(const double* cols, int64_t nrows, BoxGeom g, int dim,
+                            const int32_t* offset, int64_t cap, double* gx, double* gy,
+                            double* gz, int32_t* gsrc, int8_t* gcode, cudaStream_t s) {
+  k_ghost_write<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, g, dim, offset, cap, gx, gy, gz,
                                                gsrc, gcode);
   note_launch();
 }
@@ -1009,12 +1179,24 @@ void launch_keys(const double* cols, int64_t nrows, const double* gx, const doub
                  const double* gz, int64_t nghost, Grid g, uint32_t* keys, int32_t* vals,
                  cudaStream_t s) {
   k_keys<<<nblocks(nrows + nghost), TPB, 0, s>>>(cols, nrows, nrows, gx, gy, gz, nghost, g,
-                                                 keys, vals);
+                                                 keys, vals, nullptr, 0);
+  note_launch();
+}
+void launch_keys_dev(const double* cols, int64_t nrows, const double* gx, const double* gy,
+                     const double* gz, const DevPlan* plan, int64_t ncap, uint32_t* keys,
+                     int32_t* vals, cudaStream_t s) {
+  k_keys<<<nblocks(ncap), TPB, 0, s>>>(cols, nrows, nrows, gx, gy, gz, 0, Grid{}, keys, vals, plan,
+                                       ncap);
   note_launch();
 }
 void launch_cell_starts(const uint32_t* keys, int64_t n, int64_t ncell, int32_t* cstart,
                         cudaStream_t s) {
-  k_cell_starts<<<nblocks(n + 1), TPB, 0, s>>>(keys, n, ncell, cstart);
+  k_cell_starts<<<nblocks(n + 1), TPB, 0, s>>>(keys, n, ncell, cstart, nullptr);
+  note_launch();
+}
+void launch_cell_starts_dev(const uint32_t* keys, int64_t ncap, const DevPlan* plan,
+                            int32_t* cstart, cudaStream_t s) {
+  k_cell_starts<<<nblocks(ncap + 1), TPB, 0, s>>>(keys, ncap, 0, cstart, plan);
   note_launch();
 }
 void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
@@ -1023,7 +1205,18 @@ void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t
                           double* sz, int32_t* ssrc, int32_t* centre_slot, float4* s32,
                           PackGeom pg, cudaStream_t s) {
   k_sorted_gather<<<nblocks(n), TPB, 0, s>>>(sidx, n, nrows, nreal, cols, nrows, gx, gy, gz,
-                                             gsrc, sx, sy, sz, ssrc, centre_slot, s32, pg);
+                                             gsrc, sx, sy, sz, ssrc, centre_slot, s32, pg,
+                                             nullptr, 0);
+  note_launch();
+}
+void launch_sorted_gather_dev(const int32_t* sidx, int64_t ncap, int64_t nrows, int64_t nreal,
+                              const double* cols, const double* gx, const double* gy,
+                              const double* gz, const int32_t* gsrc, double* sx, double* sy,
+                              double* sz, int32_t* ssrc, int32_t* centre_slot, float4* s32,
+                              const DevPlan* plan, cudaStream_t s) {
+  k_sorted_gather<<<nblocks(ncap + 1), TPB, 0, s>>>(sidx, ncap, nrows, nreal, cols, nrows, gx, gy,
+                                                    gz, gsrc, sx, sy, sz, ssrc, centre_slot, s32,
+                                                    PackGeom{}, plan, ncap);
   note_launch();
 }
 void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
@@ -1071,7 +1264,14 @@ void exclusive_scan64(void* tmp, size_t tmp_bytes, const int64_t* in, int64_t* o
 void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
                  const double* sy, const double* sz, const double* cols, int64_t ld, PackGeom pg,
                  PackBufs pb, cudaStream_t s) {
-  k_pack<<<nblocks(n), TPB, 0, s>>>(prec, groups, n, ssrc, sx, sy, sz, cols, ld, pg, pb);
+  k_pack<<<nblocks(n), TPB, 0, s>>>(prec, groups, n, ssrc, sx, sy, sz, cols, ld, pg, pb, nullptr);
+  note_launch();
+}
+void launch_pack_dev(int prec, int groups, int64_t ncap, const int32_t* ssrc, const double* sx,
+                     const double* sy, const double* sz, const double* cols, int64_t ld,
+                     const DevPlan* plan, PackBufs pb, cudaStream_t s) {
+  k_pack<<<nblocks(ncap), TPB, 0, s>>>(prec, groups, ncap, ssrc, sx, sy, sz, cols, ld, PackGeom{},
+                                       pb, plan);
   note_launch();
 }
 void launch_predict(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
@@ -1092,6 +1292,23 @@ void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig,
 void launch_radexch(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
                     double dt, double gamma, double gmw, int* status, cudaStream_t s) {
   k_radexch<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, dt, gamma, gmw, status);
+  note_launch();
+}
+void launch_plan(const unsigned long long* red, const int32_t* nghost_dev, PlanIn in,
+                 DevPlan* plan, int* err_out, cudaStream_t s) {
+  k_plan<<<1, 32, 0, s>>>(red, nghost_dev, in, plan, err_out);
+  note_launch();
+}
+void launch_flag_if_nonzero(const unsigned long long* v, int* err, int code, cudaStream_t s) {
+  k_flag_if_nonzero<<<1, 32, 0, s>>>(v, err, code);
+  note_launch();
+}
+void launch_dt(const unsigned long long* red, DtIn in, DevClock* clk, double* ctrl, cudaStream_t s) {
+  k_dt<<<1, 32, 0, s>>>(red, in, clk, ctrl);
+  note_launch();
+}
+void launch_clock_advance(DevClock* clk, cudaStream_t s) {
+  k_clock_advance<<<1, 32, 0, s>>>(clk);
   note_launch();
 }
 void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s) {

@@ -44,7 +44,7 @@ __host__ __device__ inline double dkey_inv(unsigned long long u) {
 enum RedSlot : int {
   RED_LO_X = 0, RED_LO_Y, RED_LO_Z, RED_HI_X, RED_HI_Y, RED_HI_Z, RED_HMIN,
   RED_TS_HMIN, RED_TS_CMAX, RED_TS_DENMIN, RED_TS_CMIN, RED_TS_KAPMAX,
-  RED_TS_BMAX, RED_TS_KAPMIN, RED_TS_LAMMAX, RED_C1_ACTIVE, RED_TOTAL
+  RED_TS_BMAX, RED_TS_KAPMIN, RED_TS_LAMMAX, RED_C1_ACTIVE, RED_C1_ACTIVE2, RED_TOTAL
 };
 
 // Device counters (unsigned long long, cumulative).
@@ -95,6 +95,52 @@ struct PackGeom {
   double shift;       // 2^E with every (x - origin) in [0, 2^E)
   double mref;        // mass scale (packed m = m / mref)
 };
+// ---- device-resident step (no host round trip inside a step) ----
+// What the host computes between the image count and the sort in the
+// classic step, computed by k_plan on the device instead: the image count,
+// the cell grid, the FP32 packing frame and the padding key of the
+// capacity-sized sort.  err is 0 or an SPH_ERR_* code (SPH_ERR_STATE for a
+// capacity that was too small: the step is then redone on the host path).
+struct DevPlan {
+  int64_t nghost, nall, ncell;
+  Grid grid;
+  PackGeom pg;
+  uint32_t pad_key;
+  int err;
+};
+// the time-loop state of main.f90:241-373 on the device
+struct DevClock {
+  double t, ltout, dtout, tfinish, dt;
+  int stopped;
+};
+struct PlanIn {
+  int64_t nrows, nghost_cap, nall_cap;
+  double krad, cf, mref;
+  int end_bit_cap;
+};
+void launch_plan(const unsigned long long* red, const int32_t* nghost_dev, PlanIn in,
+                 DevPlan* plan, int* err_out, cudaStream_t s);
+// err := code (first error wins) if *v != 0
+void launch_flag_if_nonzero(const unsigned long long* v, int* err, int code, cudaStream_t s);
+struct DtIn {
+  int eq_hydro, eq_magneto, eq_diff, eq_fld, sts_fixed, sts_s;
+  double cn_hydro, cnd2;
+};
+void launch_dt(const unsigned long long* red, DtIn in, DevClock* clk, double* ctrl, cudaStream_t s);
+void launch_clock_advance(DevClock* clk, cudaStream_t s);
+void launch_keys_dev(const double* cols, int64_t nrows, const double* gx, const double* gy,
+                     const double* gz, const DevPlan* plan, int64_t ncap, uint32_t* keys,
+                     int32_t* vals, cudaStream_t s);
+void launch_cell_starts_dev(const uint32_t* keys, int64_t ncap, const DevPlan* plan,
+                            int32_t* cstart, cudaStream_t s);
+void launch_sorted_gather_dev(const int32_t* sidx, int64_t ncap, int64_t nrows, int64_t nreal,
+                              const double* cols, const double* gx, const double* gy,
+                              const double* gz, const int32_t* gsrc, double* sx, double* sy,
+                              double* sz, int32_t* ssrc, int32_t* centre_slot, float4* s32,
+                              const DevPlan* plan, cudaStream_t s);
+void launch_ghost_write_cap(const double* cols, int64_t nrows, BoxGeom g, int dim,
+                            const int32_t* offset, int64_t cap, double* gx, double* gy,
+                            double* gz, int32_t* gsrc, int8_t* gcode, cudaStream_t s);
 void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
                           const double* cols, const double* gx, const double* gy,
                           const double* gz, const int32_t* gsrc, double* sx, double* sy,
@@ -103,6 +149,7 @@ void launch_sorted_gather(const int32_t* sidx, int64_t n, int64_t nrows, int64_t
 void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
                     int32_t* centre_k, int32_t* centre_p, cudaStream_t s);
 struct NeibArgs {
+  const DevPlan* plan;  // if set: grid and shift from the device plan
   int64_t nc;
   const int32_t* centre_k;
   const int32_t* centre_p;
@@ -141,6 +188,9 @@ struct PackBufs {
   double2* p[11];
   float4* q[6];
 };
+void launch_pack_dev(int prec, int groups, int64_t ncap, const int32_t* ssrc, const double* sx,
+                     const double* sy, const double* sz, const double* cols, int64_t ld,
+                     const DevPlan* plan, PackBufs pb, cudaStream_t s);
 void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
                  const double* sy, const double* sz, const double* cols, int64_t ld,
                  PackGeom pg, PackBufs pb, cudaStream_t s);
@@ -205,6 +255,8 @@ struct C1Args {
   int* status;
   unsigned long long* dcnt;
   unsigned long long* red;
+  int active_slot;                  // red slot the sweep marks when a particle stays active
+  const unsigned long long* gate;   // if set and zero, the sweep has nothing to do
 };
 void launch_c1_newton(int prec, int kernel, int dim, const C1Args& a, PackBufs pb, Params P,
                       cudaStream_t s);
@@ -215,7 +267,8 @@ void launch_c1_finalize(int64_t nrows, int64_t nreal, double* cols, int64_t ld, 
                         cudaStream_t s);
 void launch_c1_snapshot(int64_t n, const int32_t* ssrc, const double* hkp1,
                         const double* dkp1, const double* okp1, double* hk_s, double* dk_s,
-                        double* ok_s, cudaStream_t s);
+                        double* ok_s, cudaStream_t s, const DevPlan* plan = nullptr,
+                        const unsigned long long* gate = nullptr);
 
 // ---- circuit2 (sph_circuit2.cu) ---------------------------------------------------
 struct C2Args {
