@@ -178,9 +178,17 @@ struct sph_handle {
   const DevPlan* dplan = nullptr;  // set while a device-resident step is built
   int64_t nghost_cap = 0, nall_cap = 0;
   int end_bit_cap = 0;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-  bool graph_dirty = true;
+  // captured steps, one per table pointer pair: a row reorder swaps the
+  // table with its spare, so two captures serve a reordering run
+  struct GraphSlot {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    const void* k_cols = nullptr;
+    const void* k_orig = nullptr;
+  };
+  GraphSlot gslot[2];
+  int gslot_next = 0;
+  bool graph_dirty = true;        // every capture is stale (parameters, sizes, buffers)
   int64_t graph_alloc_mark = -1;  // allocations seen when the graph was captured
   DevPlan* h_plan = nullptr;      // pinned read-back of the last device plan
   int adj_nsteps = -1, adj_every = 0, adj_ncp = 0;
@@ -485,7 +493,6 @@ struct sph_handle {
     }
     launch_reorder(cols.as<double>(), cols_alt.as<double>(), orig.as<int32_t>(),
                    orig_alt.as<int32_t>(), perm, nrows, nrows, nrows, s);
-    graph_dirty = true;  // a captured step holds the old table pointers
     std::swap(cols.p, cols_alt.p);
     std::swap(cols.bytes, cols_alt.bytes);
     std::swap(orig.p, orig_alt.p);
@@ -1020,11 +1027,14 @@ struct sph_handle {
     return SPH_OK;
   }
 
+  static void drop_slot(GraphSlot& q) {
+    if (q.x) cudaGraphExecDestroy(q.x);
+    if (q.g) cudaGraphDestroy(q.g);
+    q = GraphSlot{};
+  }
+
   void drop_graph() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
-    if (graph) cudaGraphDestroy(graph);
-    graph_exec = nullptr;
-    graph = nullptr;
+    for (auto& q : gslot) drop_slot(q);
     graph_dirty = true;
   }
 
@@ -1048,6 +1058,11 @@ struct sph_handle {
     RC(drs_prepare());
     // buffers the graph was captured with may have moved since
     if (cnt_host[SPH_CNT_ALLOCS] != graph_alloc_mark) graph_dirty = true;
+    if (graph_dirty) {
+      drop_graph();
+      graph_dirty = false;
+      graph_alloc_mark = cnt_host[SPH_CNT_ALLOCS];
+    }
     RC(copy_table(drs_save.p, cols.p));
     DevClock clk{};
     clk.t = t;
@@ -1057,12 +1072,17 @@ struct sph_handle {
     clk.stopped = stopped ? 1 : 0;
     std::memcpy(h_ctrl + 1, &clk, sizeof(DevClock));
     CK(cudaMemcpyAsync(drs_clock.p, h_ctrl + 1, sizeof(DevClock), cudaMemcpyHostToDevice, s));
-    if (graph_dirty || !graph_exec) {
-      drop_graph();
+    GraphSlot* gs = nullptr;
+    for (auto& q : gslot)
+      if (q.x && q.k_cols == cols.p && q.k_orig == orig.p) gs = &q;
+    if (!gs) {
+      gs = &gslot[gslot_next];
+      gslot_next ^= 1;
+      drop_slot(*gs);
       dplan = drs_plan.as<DevPlan>();
       cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
       int rc = e == cudaSuccess ? step_body_dev() : SPH_ERR_CUDA;
-      cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      cudaError_t e2 = cudaStreamEndCapture(s, &gs->g);
       dplan = nullptr;
       if (rc || e != cudaSuccess || e2 != cudaSuccess) {
         cudaGetLastError();
@@ -1070,15 +1090,15 @@ struct sph_handle {
         if (!rc) rc = fail(SPH_ERR_CUDA, "step capture failed");
         return rc;
       }
-      if (cudaGraphInstantiate(&graph_exec, graph, 0) != cudaSuccess) {
+      if (cudaGraphInstantiate(&gs->x, gs->g, 0) != cudaSuccess) {
         cudaGetLastError();
         drop_graph();
         return fail(SPH_ERR_CUDA, "graph instantiation failed");
       }
-      graph_dirty = false;
-      graph_alloc_mark = cnt_host[SPH_CNT_ALLOCS];
+      gs->k_cols = cols.p;
+      gs->k_orig = orig.p;
     }
-    CK(cudaGraphLaunch(graph_exec, s));
+    CK(cudaGraphLaunch(gs->x, s));
     // one read-back per step: the clock, the error words
     CK(cudaMemcpyAsync(h_ctrl + 1, drs_clock.p, sizeof(DevClock), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(h_i32 + 4, drs_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -63,3 +63,32 @@ def test_graph_falls_back_where_not_eligible(engine_lib, cuda_ok):
     s1, t1, c1 = _run(engine_lib, st, store, FP64, 2, graph=True)
     assert c1["graph_steps"] == 0
     assert np.array_equal(s0, s1)
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_graph_reorder_every_two_steps(engine_lib, cuda_ok, prec):
+    # the table alternates between two buffers: each buffer's capture is
+    # replayed again after the next reordering
+    st, store = ic.sedov3d(n=12, tfinish=1.0)
+    params = {abi.P_REORDER_EVERY: 2}
+    s0, t0, _ = _run(engine_lib, st, store, prec, 12, graph=False, params=params)
+    s1, t1, c1 = _run(engine_lib, st, store, prec, 12, graph=True, params=params)
+    assert c1["graph_steps"] >= 10
+    assert np.array_equal(t0, t1)
+    assert np.array_equal(s0, s1)
+
+
+def test_graph_parameter_change_mid_run(engine_lib, cuda_ok):
+    # a parameter set between steps must reach the next replayed step
+    st, store = ic.diffusion2d(16, ddw="fab", sts_stages=4, tfinish=1.0)
+    out = []
+    for graph in (False, True):
+        with abi.Engine(st, store, "m6", precision=FP64, lib=engine_lib) as e:
+            e.set_param(abi.P_GRAPH, 1.0 if graph else 0.0)
+            e.step(4)
+            e.set_param(abi.P_NEWTON_TOL, 1e-6)
+            e.step(4)
+            out.append((e.get_store(), e.get_state(), e.counters()))
+    assert out[1][2]["graph_steps"] >= 6
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][0], out[1][0])
