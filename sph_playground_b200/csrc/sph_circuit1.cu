@@ -137,17 +137,26 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
       SumAcc<R> so;
       sw.init();
       so.init();
-      // U neighbours per lane per round: their list entries and pair data
-      // are all requested before the first is used, so the gathers overlap
-      constexpr int U = 4;
+      // U neighbours per lane per round: their pair data are all requested
+      // before the first is used, so the gathers overlap; the list entries
+      // of the next round are read one round ahead
+      constexpr int U = sizeof(R) == 4 ? 4 : 2;
+      int32_t jn[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) jn[u] = (lane + u * G < n) ? row[lane + u * G] : -1;
       for (int l0 = lane; l0 < n; l0 += G * U) {
         int64_t jj[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) jj[u] = (l0 + u * G < n) ? int64_t(row[l0 + u * G]) : -1;
+        for (int u = 0; u < U; ++u) jj[u] = jn[u];
         PairPos<R> pj[U];
         R mj[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) pj[u] = PosAccess<R>::load(pb, jj[u] >= 0 ? jj[u] : 0, mj[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int l = l0 + (U + u) * G;
+          jn[u] = l < n ? row[l] : -1;
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (jj[u] < 0) continue;
@@ -259,10 +268,12 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
       g[0].init(); g[1].init(); g[2].init();
       bool bad = false;
       const R rta = R(ta), rrhoa = R(rhoa), roma = R(oma);
+      int32_t jnext = lane < n ? row[lane] : 0;  // list entry read one round ahead
       for (int l = lane; l < n; l += G) {
-        const int64_t j = row[l];
+        const int64_t j = jnext;
         R mj;
         const PairPos<R> pj = PosAccess<R>::load(pb, j, mj);
+        if (l + G < n) jnext = row[l + G];
         R dx, dy, dz;
         pos_delta(pi, pj, dx, dy, dz);
         R r2 = dx * dx;

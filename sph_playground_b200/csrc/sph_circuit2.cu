@@ -170,19 +170,15 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     bool bad = false;
     const int n = a.ncnt[c];
     const int32_t* __restrict__ row = a.nl + a.rowoff[c];
-    constexpr int U = 1;  // neighbours per lane per round (U > 1 raised registers past the gain)
-    for (int l0 = lane; l0 < n; l0 += G * U) {
-    int64_t jj[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) jj[u] = (l0 + u * G < n) ? int64_t(row[l0 + u * G]) : -1;
-    Part<R> BB[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) Loader<R>::hydro(pb, jj[u] >= 0 ? jj[u] : 0, BB[u]);
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (jj[u] < 0) continue;
-      const int64_t j = jj[u];
-      const Part<R>& B = BB[u];
+    // the next neighbour's index is read one round ahead, so that a round
+    // waits on one dependent load (the neighbour's streams), not two
+    int32_t jnext = lane < n ? row[lane] : 0;
+    for (int l0 = lane; l0 < n; l0 += G) {
+    {
+      const int64_t j = jnext;
+      Part<R> B;
+      Loader<R>::hydro(pb, j, B);
+      if (l0 + G < n) jnext = row[l0 + G];
       R rab[3];
       pos_delta(A.pos, B.pos, rab[0], rab[1], rab[2]);
       R r2 = rab[0] * rab[0];
