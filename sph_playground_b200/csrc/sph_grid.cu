@@ -409,6 +409,13 @@ __device__ __forceinline__ float group_max(float v) {
   return v;
 }
 
+// squared distance of two FP32 images, rounded the same way wherever it is
+// computed (the guard-band pass recomputes it bit for bit)
+__device__ __forceinline__ float dist2_f32(const float4& b, const float4& a) {
+  const float fx = __fsub_rn(b.x, a.x), fy = __fsub_rn(b.y, a.y), fz = __fsub_rn(b.z, a.z);
+  return __fmaf_rn(fz, fz, __fmaf_rn(fy, fy, __fmul_rn(fx, fx)));
+}
+
 template <int DIM, int G>
 __global__ void __launch_bounds__(128, 7)
 k_neighbours(NeibArgs a) {
@@ -629,35 +636,39 @@ k_neighbours(NeibArgs a) {
         bt[lane] = cur;
         __syncwarp();
         if (mine) {
-          // FP32 decisions for the batch; the candidates in the guard band
-          // are marked in `band` and decided in FP64 after it (rare)
-          unsigned band = 0u;
+          // FP32 decisions for the batch: 0 < sd32 < lo is inside for sure.
+          // The guard band and sd32 = 0 (the centre itself, or a particle
+          // closer than the FP32 images resolve) are decided in FP64 after
+          // the batch, which recomputes sd32 bit for bit to find them (rare:
+          // about once per centre)
+          bool anyband = false;
 #pragma unroll
           for (int t = 0; t < G; ++t) {
             const float4 pj = bt[t];
-            const float fx = pj.x - pi.x, fy = pj.y - pi.y, fz = pj.z - pi.z;
-            const float sd32 = fx * fx + fy * fy + fz * fz;
-            const int32_t q = __float_as_int(pj.w);
-            const bool in32 = sd32 < lo_thr;
-            band |= (!in32 && !(sd32 > hi_thr)) ? (1u << t) : 0u;
-            const bool take = in32 && q != k;
-            if (take) mine_held[nheld] = q;
-            nheld += take ? 1 : 0;
+            const float sd32 = dist2_f32(pj, pi);
+            const bool in32 = sd32 < lo_thr && sd32 > 0.f;
+            anyband |= !in32 && !(sd32 > hi_thr);
+            if (in32) mine_held[nheld] = __float_as_int(pj.w);
+            nheld += in32 ? 1 : 0;
           }
-          while (band) {
-            const int t = __ffs(band) - 1;
-            band &= band - 1u;
+          if (anyband) {
+#pragma unroll 1
+          for (int t = 0; t < G; ++t) {
             const float4 pj = bt[t];
+            const float sd32 = dist2_f32(pj, pi);
+            if ((sd32 < lo_thr && sd32 > 0.f) || sd32 > hi_thr) continue;
             const int32_t q = __float_as_int(pj.w);
+            if (q == k) continue;
             ++nexact;
             double d0 = __dadd_rn(a.sx[q], -xi);
             double d1 = __dadd_rn(a.sy[q], -yi);
             double d2 = __dadd_rn(a.sz[q], -zi);
             double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
                                   __dmul_rn(d2, d2));
-            const bool take = !(sd > R2) && q != k;
+            const bool take = !(sd > R2);
             if (take) mine_held[nheld] = q;
             nheld += take ? 1 : 0;
+          }
           }
         }
         __syncwarp();  // the next batch overwrites this one
