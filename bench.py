@@ -38,11 +38,11 @@ UNIT = "particle-steps/s"
 F1_C1 = 50.0
 F2_C2 = 150.0
 # DRAM bytes per in-support pair of the FP32-comp circuit2 launch:
-# dram__bytes_read.sum + dram__bytes_write.sum = 845.72 MB + 66.78 MB over
+# dram__bytes_read.sum + dram__bytes_write.sum = 848.70 MB + 69.45 MB over
 # 157.49M pairs of the 96^3 capture in profiles/k_c2_fp32_sedov3d_96.md (the
 # neighbour index, 4 B, plus the gathered pair data that misses L2); the
 # traffic scales with the pairs a launch processes
-C2_DRAM_BYTES_PER_PAIR = (845.72e6 + 66.78e6) / 157.49e6
+C2_DRAM_BYTES_PER_PAIR = (848.70e6 + 69.45e6) / 157.49e6
 
 
 def parse():
