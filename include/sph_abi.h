@@ -212,6 +212,20 @@ int sph_adjoint_backward(sph_handle* h, const double* dl_dv, const double* dl_du
                          const double* dl_dr, double* g_r0, double* g_v0, double* g_u0,
                          double* g_par);
 
+/* ---- end-of-run error (main.f90:374-402, errcalc.f90) --------------------
+ * Replaces the engine's closing error evaluation: for the run's initial
+ * condition type (state slot ics) at the handle's current time, err_i of
+ * every real particle (errcalc.f90: shock12 :140-170 erf profile of T,
+ * ring :99-138, pulse :46-97, sin3 :172-197, soundwave :220-236 density,
+ * hydroshock :26-44 Sod density of the exact Riemann solution with the
+ * reference's fixed gamma 1.4, alfvenwave :198-218) and
+ * L1 = sum_i err_i / realpn (main.f90:401-402).  Types without a
+ * calculator there (mti, mtilowres, OTvortex, boilingtank, none) give
+ * err = 0, L1 = 0; fld_gauss and equations = kd2 (the chi error) return
+ * SPH_ERR_UNSUPPORTED.  err_out (cap >= realpn doubles, original row order)
+ * may be NULL. */
+int sph_errcalc(sph_handle* h, double* err_out, int64_t cap, double* l1_out);
+
 /* ---- batches of instances -----------------------------------------------
  * Many independent runs stepped together (the resolution x method sweeps
  * of the experiment runners, e.g. runner/anisotropic/

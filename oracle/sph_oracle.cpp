@@ -1257,6 +1257,128 @@ struct Oracle {
   }
 };
 
+// ---- closing error evaluation (main.f90:374-402, errcalc.f90) -----------
+// Exact Sod density for errcalc.f90:26-44 (the reference calls SPLASH's
+// exact_shock there); restated from the Riemann problem's equations
+// (Toro ch. 4): p* by bisection of f_L(p) + f_R(p) + (u_R - u_L) = 0, then
+// the wave pattern sampled at (x - x0) / t.
+double sod_density(double x, double t, double g, double rl, double pl, double rr, double pr) {
+  const double ul = 0.0, ur = 0.0, x0 = 0.0;
+  if (!(t > 0.0)) return x < x0 ? rl : rr;
+  const double cl = std::sqrt(g * pl / rl), cr = std::sqrt(g * pr / rr);
+  const double z = (g - 1.0) / (2.0 * g);
+  auto fk = [&](double p, double rk, double pk, double ck) {
+    if (p > pk) {
+      const double A = 2.0 / ((g + 1.0) * rk), B = (g - 1.0) / (g + 1.0) * pk;
+      return (p - pk) * std::sqrt(A / (p + B));
+    }
+    return 2.0 * ck / (g - 1.0) * (std::pow(p / pk, z) - 1.0);
+  };
+  double lo = 0.0, hi = 10.0 * std::max(pl, pr);
+  for (int it = 0; it < 200; ++it) {
+    const double pm = 0.5 * (lo + hi);
+    if (fk(pm, rl, pl, cl) + fk(pm, rr, pr, cr) + (ur - ul) > 0.0) hi = pm;
+    else lo = pm;
+  }
+  const double p = 0.5 * (lo + hi);
+  const double u = 0.5 * (ul + ur) + 0.5 * (fk(p, rr, pr, cr) - fk(p, rl, pl, cl));
+  const double gg = (g - 1.0) / (g + 1.0);
+  const double s = (x - x0) / t;
+  if (s <= u) {
+    if (p > pl) {
+      const double sl = ul - cl * std::sqrt((g + 1.0) / (2.0 * g) * p / pl + z);
+      return s <= sl ? rl : rl * ((p / pl + gg) / (gg * p / pl + 1.0));
+    }
+    if (s <= ul - cl) return rl;
+    if (s <= u - cl * std::pow(p / pl, z))
+      return rl * std::pow(2.0 / (g + 1.0) + (g - 1.0) / ((g + 1.0) * cl) * (ul - s),
+                           2.0 / (g - 1.0));
+    return rl * std::pow(p / pl, 1.0 / g);
+  }
+  if (p > pr) {
+    const double sr = ur + cr * std::sqrt((g + 1.0) / (2.0 * g) * p / pr + z);
+    return s >= sr ? rr : rr * ((p / pr + gg) / (gg * p / pr + 1.0));
+  }
+  if (s >= ur + cr) return rr;
+  if (s >= u + cr * std::pow(p / pr, z))
+    return rr * std::pow(2.0 / (g + 1.0) - (g - 1.0) / ((g + 1.0) * cr) * (ur - s),
+                         2.0 / (g - 1.0));
+  return rr * std::pow(p / pr, 1.0 / g);
+}
+
+// err_i of the real particles for the run's initial condition type, and
+// L1 = sum err / realpn, summed in row order as Fortran's sum() does
+int errcalc(const Oracle& o, double* err, double* l1) {
+  const int64_t n = o.realpn;
+  const int dim = o.ival(ec_dim), diso = o.ival(ec_disotropic), ivt = o.ival(ec_ics);
+  const double t = o.st[ec_time];
+  if (o.ival(ec_eqs) == eeq_kd2)
+    return fail(SPH_ERR_UNSUPPORTED, "the Taylor (chi) error of equations = kd2 is not built");
+  std::vector<double> e(size_t(n), 0.0);  // main.f90:202
+  switch (ivt) {
+    case ett_shock12:  // errcalc.f90:140-170
+      for (int64_t i = 0; i < n; ++i) {
+        const double tt = (diso == 1 || o.S(i, es_bx) == 1.) ? t : 1e-15;
+        const double tr = 2., tl = 1.;
+        const double exact = (tr + tl) / 2. + (tr - tl) / 2. * std::erf(o.S(i, es_rx) / std::sqrt(4 * tt));
+        e[i] = std::fabs(exact - o.S(i, es_t));
+      }
+      break;
+    case ett_ring:  // errcalc.f90:99-138
+      for (int64_t i = 0; i < n; ++i) {
+        const double x1 = o.S(i, es_rx), x2 = o.S(i, es_ry);
+        const double rho = std::sqrt(x1 * x1 + x2 * x2);
+        const double phi = std::atan2(x2, x1);
+        const double exact = std::exp(-0.5 * ((rho - 0.3) * (rho - 0.3) / (0.05 * 0.05) +
+                                              (phi * phi) / (0.5 * 0.5 + 2. * 1. * t / rho / rho)));
+        e[i] = std::fabs(exact - o.S(i, es_t));
+      }
+      break;
+    case ett_pulse: {  // errcalc.f90:46-97
+      const double eps = 0.1, dcnd = o.st[ec_dcondconst];
+      const double pifac = std::pow(2 * pi, -dim / 2.);
+      const double ekt = eps * eps + 2 * dcnd * t;
+      const double ektd2 = std::pow(ekt, dim / 2.);
+      const double ektsq = std::pow(ekt, 1. / 2.);
+      const double epsdm1 = powi(eps, dim - 1);
+      for (int64_t i = 0; i < n; ++i) {
+        const double x1 = o.S(i, es_rx), x2 = o.S(i, es_ry), x3 = o.S(i, es_rz);
+        double exact;
+        if (diso == 1) exact = pifac / ektd2 * std::exp(-0.5 * ((x1 * x1 + x2 * x2 + x3 * x3) / ekt));
+        else exact = pifac / epsdm1 / ektsq * std::exp(-0.5 * (x1 * x1 / ekt + (x2 * x2 + x3 * x3) / eps / eps));
+        e[i] = std::fabs(exact - o.S(i, es_t));
+      }
+      break;
+    }
+    case ett_sin3:  // errcalc.f90:172-197: filled only when ivt == 1, never for sin3
+      break;
+    case ett_soundwave:  // errcalc.f90:220-236
+      for (int64_t i = 0; i < n; ++i)
+        e[i] = std::fabs(1. + 0.005 * std::sin(pi * (o.S(i, es_rx) - t)) - o.S(i, es_den));
+      break;
+    case ett_hydroshock:  // errcalc.f90:26-44
+      for (int64_t i = 0; i < n; ++i)
+        e[i] = std::fabs(o.S(i, es_den) - sod_density(o.S(i, es_rx), t, 1.4, 1., 1., 1. / 8., 0.1));
+      break;
+    case ett_alfvenwave:  // errcalc.f90:198-218
+      for (int64_t i = 0; i < n; ++i) {
+        const double x1 = (o.S(i, es_rx) + 2 * o.S(i, es_ry) + 2 * o.S(i, es_rz)) / 3.;
+        const double b2 = (o.S(i, es_by) - 2 * o.S(i, es_bx)) / std::sqrt(5.);
+        e[i] = std::fabs(0.1 * std::sin(2. * pi * (x1 - t)) - b2);
+      }
+      break;
+    case ett_OTvortex: case ett_mti: case ett_boilingtank: case ett_mtilowres: case -1:
+      break;  // main.f90:377, 394-395
+    default:
+      return fail(SPH_ERR_UNSUPPORTED, "Task type was not sen in L2 error evaluation");
+  }
+  double sum = 0.0;
+  for (int64_t i = 0; i < n; ++i) sum += e[i];
+  if (err) std::copy(e.begin(), e.end(), err);
+  if (l1) *l1 = n > 0 ? sum / double(n) : 0.0;
+  return SPH_OK;
+}
+
 }  // namespace
 
 struct sph_handle {
@@ -1367,6 +1489,12 @@ int sph_get_store(sph_handle* h, double* out, int64_t cap_rows) {
   if (!h || !out || cap_rows < h->o.nrows) return fail(SPH_ERR_ARG, "buffer too small");
   std::copy(h->o.store.begin(), h->o.store.begin() + h->o.nrows * ES, out);
   return SPH_OK;
+}
+
+int sph_errcalc(sph_handle* h, double* err_out, int64_t cap, double* l1_out) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  if (err_out && cap < h->o.realpn) return fail(SPH_ERR_ARG, "err_out holds fewer than realpn values");
+  return errcalc(h->o, err_out, l1_out);
 }
 
 int sph_get_state(sph_handle* h, double* out49) {

@@ -58,7 +58,7 @@ ABI_SYMBOLS = [
     "sph_get_state", "sph_get_neighbours", "sph_get_counters",
     "sph_reset_counters", "sph_get_timers", "sph_last_error", "sph_destroy",
     "sph_batch_create", "sph_batch_step", "sph_batch_run_to", "sph_batch_status",
-    "sph_batch_destroy",
+    "sph_batch_destroy", "sph_errcalc",
 ]
 
 
@@ -111,6 +111,7 @@ def load(path=None):
     lib.sph_batch_status.argtypes = [vp, P(c_int), c_int]
     lib.sph_batch_destroy.argtypes = [vp]
     lib.sph_batch_destroy.restype = None
+    lib.sph_errcalc.argtypes = [vp, P(d), i64, P(d)]
     if hasattr(lib, "sph_adjoint_forward"):  # the CUDA engine only
         lib.sph_adjoint_forward.argtypes = [vp, c_int, c_int]
         lib.sph_adjoint_forward.restype = c_int
@@ -242,6 +243,15 @@ class Engine:
             self.h, ptr(iv), ptr(iu), ptr(ir), _dptr(out["g_r0"]), _dptr(out["g_v0"]),
             _dptr(out["g_u0"]), _dptr(out["g_par"])))
         return out
+
+    def errcalc(self):
+        """(err per real particle in original row order, L1): the closing
+        error evaluation of main.f90:374-402 for the run's initial
+        condition type at the handle's time."""
+        err = np.zeros(self.n_real, dtype=np.float64)
+        l1 = np.zeros(1, dtype=np.float64)
+        self._check(self.lib.sph_errcalc(self.h, _dptr(err), err.shape[0], _dptr(l1)))
+        return err, float(l1[0])
 
     def get_neighbours(self):
         """(offsets[n_real+1], pairs) with pairs = (rj << 5) | image code."""

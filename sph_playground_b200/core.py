@@ -92,6 +92,7 @@ class Context:
         self.env = os.environ.copy()
         self.setup = Setup()
         self.store = None
+        self.result = None  # the last run's result.info line (resolution, realpn, L1, chi, hfac)
         self.state = None
         self.precision = precision
         self.constf90 = constf90
@@ -216,7 +217,30 @@ class Context:
                 if t >= tfinish - 1e-15 * max(1.0, abs(tfinish)) or dtout <= 0:
                     break
                 nxt = t + dtout
+            if tfinish > 0:
+                self._write_result(e)
         self.__tolog__("CMD [./execute] EXECUTED")
+
+    def _write_result(self, e):
+        """The closing error evaluation of main.f90:374-435: err per real
+        particle for the run's initial condition type (sph_errcalc, on the
+        device), the line (resolution, realpn, L1, chi = 0, hfac) appended
+        to result.info in the working directory, and the L1 line of the
+        engine's output in the stdout log.  Where the reference stops with an
+        error instead (a type without an error calculator, main.f90:396-397)
+        the message goes to the stderr log and no line is written."""
+        try:
+            _, l1 = e.errcalc()
+        except abi.SphError as ex:
+            self._log("stderrfile", str(ex))
+            return
+        st = e.get_state()
+        row = [st[consts.ec["resolution"] - 1], st[consts.ec["realpn"] - 1], l1, 0.0,
+               st[consts.ec["hfac"] - 1]]
+        with open(os.path.join(self.pwd, "result.info"), "a") as f:
+            f.write(" " + "  ".join("%.17G" % v for v in row) + "\n")
+        self._log("stdoutfile", " # #   L1-error: %20.10f" % l1)
+        self.result = row
 
     def PrintCell(self, file, row, column):
         with open(file.split()[0]) as f:

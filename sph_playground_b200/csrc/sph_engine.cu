@@ -62,9 +62,9 @@ enum : int { eeq_hydro = 300, eeq_diffusion = 301, eeq_magnetohydro = 302,
              eeq_magnetohydrodiffusion = 303, eeq_hydrodiffusion = 304,
              eeq_kd2 = 305, eeq_hyrad = 306, eeq_manual = 307 };
 enum : int { epc_backcompatibility = 600, epc_fullyperiodic = 601, epc_borderless = 602 };
-enum : int { ett_mti = 101, ett_shock12 = 102, ett_pulse = 103, ett_ring = 104,
-             ett_soundwave = 105, ett_hydroshock = 106, ett_OTvortex = 108,
-             ett_mtilowres = 110, ett_fld_gauss = 111 };
+enum : int { ett_sin3 = 100, ett_mti = 101, ett_shock12 = 102, ett_pulse = 103, ett_ring = 104,
+             ett_soundwave = 105, ett_hydroshock = 106, ett_alfvenwave = 107, ett_OTvortex = 108,
+             ett_boilingtank = 109, ett_mtilowres = 110, ett_fld_gauss = 111, e_none = -1 };
 
 const double kPi = 4.0 * std::atan(1.0);
 
@@ -1130,6 +1130,67 @@ struct sph_handle {
     return SPH_OK;
   }
 
+  // ---- closing error evaluation (main.f90:374-402) ---------------------------------------------
+  DevBuf errb, errpart;
+  int errcalc(double* err_out, int64_t cap, double* l1) {
+    if (err_out && cap < nreal) return fail(SPH_ERR_ARG, "err_out holds fewer than realpn values");
+    if (ival(ec_eqs) == eeq_kd2)
+      return fail(SPH_ERR_UNSUPPORTED, "the Taylor (chi) error of equations = kd2 is not built");
+    ErrCalcIn in{};
+    in.dim = dim();
+    in.diso = ival(ec_disotropic);
+    in.t = st[ec_time];
+    switch (ival(ec_ics)) {
+      case ett_shock12: in.kind = EK_SHOCK12; break;
+      case ett_ring: in.kind = EK_RING; break;
+      case ett_pulse: {
+        // the constants of errcalc.f90:66-71, in its operation order
+        in.kind = EK_PULSE;
+        const double eps = 0.1, dcnd = st[ec_dcondconst];
+        in.pifac = std::pow(2.0 * kPi, -in.dim / 2.0);
+        in.ekt = eps * eps + 2.0 * dcnd * in.t;
+        in.ektd2 = std::pow(in.ekt, in.dim / 2.0);
+        in.ektsq = std::pow(in.ekt, 1.0 / 2.0);
+        in.epsdm1 = 1.0;
+        for (int k = 1; k < in.dim; ++k) in.epsdm1 *= eps;
+        break;
+      }
+      // err_sinxet fills err only when the type equals 1 (errcalc.f90:185),
+      // which ett_sin3 (100) never does: err stays 0
+      case ett_sin3: in.kind = EK_ZERO; break;
+      case ett_soundwave: in.kind = EK_SOUNDWAVE; break;
+      case ett_hydroshock:
+        // exact_shock(1, t, 1.4, 0., 1., 1./8., 1., 0.1, 0., 0., ...)
+        // (errcalc.f90:38): the standard Sod states, gamma 1.4 whatever
+        // the run's gamma
+        in.kind = EK_HYDROSHOCK;
+        in.fan = riemann_fan(1.4, 1.0, 0.0, 1.0, 1.0 / 8.0, 0.0, 0.1, 0.0);
+        break;
+      case ett_alfvenwave: in.kind = EK_ALFVEN; break;
+      case ett_OTvortex: case ett_mti: case ett_boilingtank: case ett_mtilowres: case e_none:
+        in.kind = EK_ZERO;  // no calculator: err as allocated, zero
+        break;
+      default:
+        return fail(SPH_ERR_UNSUPPORTED, "Task type was not sen in L2 error evaluation");
+    }
+    const int64_t np = errcalc_parts(nreal);
+    RC(errb.ensure(sizeof(double) * nreal));
+    RC(errpart.ensure(sizeof(double) * (np + 1)));
+    double* part = errpart.as<double>();
+    double* sum = part + np;
+    launch_errcalc(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, nreal, in,
+                   errb.as<double>(), part, sum, s);
+    CK(cudaGetLastError());
+    double total = 0.0;
+    CK(cudaMemcpyAsync(h_ctrl + 15, sum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (err_out)
+      CK(cudaMemcpyAsync(err_out, errb.p, sizeof(double) * nreal, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    total = h_ctrl[15];
+    if (l1) *l1 = nreal > 0 ? total / double(nreal) : 0.0;
+    return SPH_OK;
+  }
+
   // ---- pre-run check (preruncheck.f90:13-60) -------------------------------------------------
   int check_vars_ready() {
     int s_tt = ival(ec_eqs);
@@ -1790,6 +1851,12 @@ int sph_get_timers(sph_handle* h, double* out_ms, int n) {
   h->collect_timers();
   for (int k = 0; k < n && k < SPH_T_TOTAL; ++k) out_ms[k] = h->timers[k];
   return SPH_OK;
+}
+
+int sph_errcalc(sph_handle* h, double* err_out, int64_t cap, double* l1_out) {
+  AllocScope alloc_scope(h);
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  return h->errcalc(err_out, cap, l1_out);
 }
 
 int sph_adjoint_forward(sph_handle* h, int nsteps, int every) {

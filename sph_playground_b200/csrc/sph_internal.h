@@ -328,4 +328,33 @@ void launch_adj_gather(const double* in, int ncomp, const int32_t* orig, int64_t
 void launch_adj_scatter(const double* in, int64_t ld, const int32_t* orig, int64_t n,
                         double* out, int ncomp, cudaStream_t s);
 
+// ---- end-of-run error calculators (errcalc.f90, main.f90:374-402) ---------
+enum ErrKind : int { EK_ZERO = 0, EK_SHOCK12, EK_RING, EK_PULSE, EK_SOUNDWAVE,
+                     EK_HYDROSHOCK, EK_ALFVEN };
+// Exact solution of a 1-D Riemann problem: the star state and the wave
+// speeds, solved once on the host; sampled per particle on the device.
+struct RiemannFan {
+  double gamma, x0;
+  double rl, ul, pl, cl, rr, ur, pr, cr;
+  double ps, us, rsl, rsr;  // star pressure, velocity, densities left / right of the contact
+  int shock_l, shock_r;     // 1: shock, 0: rarefaction
+  double sl, sr;            // shock speeds
+  double hl, tl, hr, tr;    // rarefaction head / tail speeds
+};
+RiemannFan riemann_fan(double gamma, double rl, double ul, double pl, double rr, double ur,
+                       double pr, double x0);
+struct ErrCalcIn {
+  int kind, dim, diso;
+  double t;
+  double pifac, ekt, ektd2, ektsq, epsdm1;  // pulse constants (errcalc.f90:66-71)
+  RiemannFan fan;                           // hydroshock (errcalc.f90:38)
+};
+// err[orig[i]] for the real rows (orig < nreal) of the table; sum of err
+// over [0, nreal) in a fixed order into *sum (part: scratch of
+// errcalc_parts(nreal) doubles)
+int64_t errcalc_parts(int64_t nreal);
+void launch_errcalc(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                    int64_t nreal, const ErrCalcIn& in, double* err, double* part, double* sum,
+                    cudaStream_t s);
+
 }  // namespace sph
