@@ -26,7 +26,7 @@ import shutil
 
 import numpy as np
 
-from . import abi, consts, ic
+from . import abi, consts, ic, icsetup
 
 try:  # optional: the reference's dump format
     import h5py  # noqa: F401
@@ -161,10 +161,16 @@ class Context:
             ymin=float(get("ymin", 0.0)), ymax=float(get("ymax", 1.0)),
             zmin=float(get("zmin", 0.0)), zmax=float(get("zmax", 1.0)),
             placement=get("placement", "uniform") or "uniform",
+            ics=get("ics", "none") if isinstance(get("ics"), str) and get("ics") else "none",
             resolution=int(float(get("resolution", 0) or 0)),
             spacing=float(get("spacing", 0.0) or 0.0))
         kernel = str(self.setup.kernel)
-        store = ic.place_uniform(state, kernel)
+        # main.f90:133-139: place() without an initial-condition type,
+        # setupV2 with one
+        if int(ic.get_state(state, "ics")) == consts.ICS["none"]:
+            store = icsetup.place(state, kernel)
+        else:
+            store = icsetup.setup_v2(state, kernel, cv=1.0)
         tf = ic.get_state(state, "tfinish")
         npics = max(int(ic.get_state(state, "npics")), 1)
         ic.set_state(state, "dtprint", tf / npics if tf > 0 else 1.0)
