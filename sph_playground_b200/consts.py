@@ -91,3 +91,34 @@ KERNELS = {"m4": 0, "m6": 1, "gauss": 2}
 # support radius krad of each kernel (base_m4.f90:18, base_m6.f90:17,
 # base_gauss.f90:19)
 KRAD = {"m4": 2.0, "m6": 3.0, "gauss": 10.0}
+
+
+# ---- const.f90 parsing (core.py:235-319) ------------------------------------------
+CONST_PREFIXES = ["ec_", "es_", "ept_", "ett_", "ebc_", "eeq_", "esd_", "edi_", "eqs_",
+                  "epc_", "eif_", "ests_"]
+
+
+def parse_const_f90(path):
+    """The reference driver's rule for reading src/const.f90: split each line
+    into whitespace tokens and keep `name = value,&` triples; ec_/es_ entries
+    only with the trailing ",&", es_total skipped.  Returns one dictionary
+    per prefix, keyed by the name without the prefix."""
+    out = {p[:-1]: {} for p in CONST_PREFIXES}
+    with open(path) as f:
+        for line in f:
+            tok = line.split()
+            if len(tok) != 3:
+                continue
+            name, val = tok[0], tok[2]
+            for p in CONST_PREFIXES:
+                if not name.startswith(p):
+                    continue
+                key = name[len(p):]
+                if val.endswith(",&"):
+                    val = val[:-2]
+                elif p in ("ec_", "es_"):
+                    continue
+                if p == "es_" and key == "total":
+                    continue
+                out[p[:-1]][key] = float(val) if p in ("eif_", "ests_") else int(val)
+    return out

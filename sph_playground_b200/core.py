@@ -259,8 +259,7 @@ class Context:
                      "eif", "ests"):
             setattr(self, name, dict(getattr(consts, name)))
         if self.constf90 and os.path.exists(self.constf90):
-            from tests.golden.make_const_fixture import parse  # same splitting rule
-            parsed = parse(self.constf90)
+            parsed = consts.parse_const_f90(self.constf90)
             for k, v in parsed.items():
                 setattr(self, k, v)
         for name in ("ec", "es", "ept", "ett", "ebc", "eeq", "esd", "edi", "eqs", "epc",

@@ -12,31 +12,8 @@ import json
 import os
 import sys
 
-PREFIXES = ["ec_", "es_", "ept_", "ett_", "ebc_", "eeq_", "esd_", "edi_", "eqs_",
-            "epc_", "eif_", "ests_"]
-
-
-def parse(path):
-    out = {p[:-1]: {} for p in PREFIXES}
-    with open(path) as f:
-        for line in f:
-            tok = line.split()
-            if len(tok) != 3:
-                continue
-            name, val = tok[0], tok[2]
-            for p in PREFIXES:
-                if not name.startswith(p):
-                    continue
-                key = name[len(p):]
-                if val.endswith(",&"):
-                    val = val[:-2]
-                elif p in ("ec_", "es_"):
-                    continue  # core.py keeps ec_/es_ only with a trailing ",&"
-                if p == "es_" and key == "total":
-                    continue
-                num = float(val) if p in ("eif_", "ests_") else int(val)
-                out[p[:-1]][key] = num
-    return out
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", ".."))
+from sph_playground_b200.consts import parse_const_f90 as parse  # noqa: E402
 
 
 if __name__ == "__main__":
