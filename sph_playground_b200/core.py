@@ -16,8 +16,10 @@ process on the GPU engine instead of spawning ``./execute``:
   runs the time loop to tfinish, writing a dump at every output time
   (main.f90:241-373, printer.f90:19-38, dumper.f90:14-42).
 
-Dumps are HDF5 (``state`` (49,) and ``store`` (N, 32), dumper.f90:26-34) when
-h5py is importable, otherwise ``.npz`` files with the same two arrays.
+Dumps are HDF5 files with the reference's two chunked, resizable datasets
+(``state`` (49,) and ``store`` (N, 32), dumper.f90:26-34): through h5py when
+it is importable, otherwise through this package's own HDF5 writer and
+reader (sph_playground_b200/h5dump.py).
 """
 import copy
 import datetime
@@ -26,7 +28,7 @@ import shutil
 
 import numpy as np
 
-from . import abi, consts, ic, icsetup
+from . import abi, consts, h5dump, ic, icsetup
 
 try:  # optional: the reference's dump format
     import h5py  # noqa: F401
@@ -50,15 +52,8 @@ class Setup:
         return args
 
 
-def _dump_path(path):
-    if HAVE_H5PY or path.endswith(".npz"):
-        return path
-    return os.path.splitext(path)[0] + ".npz"
-
-
 def write_dump(path, state, store):
     """dumper.f90:14-42: write state and the real+fixed rows of store."""
-    path = _dump_path(path)
     os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
     tmp = path + ".new"
     if HAVE_H5PY:
@@ -68,19 +63,18 @@ def write_dump(path, state, store):
             f.create_dataset("store", data=store, maxshape=(None, consts.ES_TOTAL),
                              chunks=store.shape)
     else:
-        with open(tmp, "wb") as f:
-            np.savez(f, state=state, store=store)
+        h5dump.write(tmp, {"state": np.asarray(state, dtype=np.float64),
+                           "store": np.asarray(store, dtype=np.float64)})
     os.replace(tmp, path)  # atomic rename, dumper.f90:36
     return path
 
 
 def read_dump(path):
-    path = _dump_path(path)
-    if HAVE_H5PY and not path.endswith(".npz"):
+    if HAVE_H5PY:
         import h5py
         with h5py.File(path, "r") as f:
             return np.array(f["state"]), np.array(f["store"])
-    d = np.load(path)
+    d = h5dump.read(path)
     return np.array(d["state"]), np.array(d["store"])
 
 
@@ -217,8 +211,8 @@ class Context:
                 e.set_param("lastprint", st[consts.ec["lastprint"] - 1])
                 self.state, self.store = st, e.get_store()
                 write_dump(self._out("dump_full.h5"), self.state, self.store)
-                shutil.copyfile(_dump_path(self._out("dump_full.h5")),
-                                _dump_path(self._out("dump_%05d.h5" % int(st[consts.ec["lastprint"] - 1]))))
+                shutil.copyfile(self._out("dump_full.h5"),
+                                self._out("dump_%05d.h5" % int(st[consts.ec["lastprint"] - 1])))
                 t = st[consts.ec["time"] - 1]
                 if t >= tfinish - 1e-15 * max(1.0, abs(tfinish)) or dtout <= 0:
                     break
@@ -309,7 +303,7 @@ class Context:
                         dirs_exist_ok=True)
 
     def BackupDump(self, file):
-        p = _dump_path(os.path.join(self.pwd, file))
+        p = os.path.join(self.pwd, file)
         if os.path.exists(p):
             shutil.copyfile(p, p + ".bck")
 
