@@ -1,0 +1,64 @@
+"""Edge cases of the search and density pass against the oracle: coincident
+particles (distance 0 between distinct rows, decided by the FP64 predicate
+in the guard-band pass), a box so small that a particle sees several images
+of itself and of its neighbours, and a neighbour-list overflow (a particle
+set clustered after the capacities were sized for the spread one) that the
+engine must detect and redo with larger rows."""
+import numpy as np
+import pytest
+
+from sph_playground_b200 import abi, ic
+from tests.parity import COL, neighbour_sets_equal, rel_particle, run_pass
+
+pytestmark = pytest.mark.gpu
+
+FP64, FP32 = abi.PREC_FP64, abi.PREC_FP32_COMP
+TOL = {FP64: 1e-12, FP32: 1e-6}
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_coincident_particles(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = ic.density3d(n=10, seed=3)
+    # rows 1, 2 and 3 placed exactly on row 0 (and row 50 on row 51)
+    store[1:4, COL["rx"]:COL["rz"] + 1] = store[0, COL["rx"]:COL["rz"] + 1]
+    store[50, COL["rx"]:COL["rz"] + 1] = store[51, COL["rx"]:COL["rz"] + 1]
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "density")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "density")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    for f in ("den", "h", "om"):
+        assert rel_particle(got[:, COL[f]], ref[:, COL[f]]) <= TOL[prec], f
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_tiny_periodic_box(oracle_lib, engine_lib, cuda_ok, prec):
+    """4^3 particles with a support radius of 3.6 spacings: the strips are
+    the whole box, so every particle meets images of itself."""
+    st, store = ic.density3d(n=4, seed=5)
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "density")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "density")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    for f in ("den", "h", "om"):
+        assert rel_particle(got[:, COL[f]], ref[:, COL[f]]) <= TOL[prec], f
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_list_overflow_is_redone(oracle_lib, engine_lib, cuda_ok, prec):
+    """The row capacities follow the previous search's counts; after the
+    particles are squeezed into an eighth of the box (8x the neighbours at
+    the same h) the rows overflow and the search must be redone."""
+    st, store = ic.density3d(n=12, seed=4)
+    squeezed = store.copy()
+    squeezed[:, COL["rx"]:COL["rz"] + 1] *= 0.5
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, squeezed, "m6", FP64, "density")
+    with abi.Engine(st, store, "m6", precision=prec, lib=engine_lib) as e:
+        e.density()
+        before = e.get_neighbours()[0][-1]
+        e.set_store(squeezed)
+        e.reset_counters()
+        e.density()
+        got, nb_got, cnt = e.get_store(), e.get_neighbours(), e.counters()
+    assert nb_got[0][-1] > 3 * before
+    assert cnt["searches"] >= 2  # the overflowing search was redone
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    for f in ("den", "h", "om"):
+        assert rel_particle(got[:, COL[f]], ref[:, COL[f]]) <= TOL[prec], f
