@@ -211,6 +211,13 @@ int sph_adjoint_forward(sph_handle* h, int nsteps, int every);
 int sph_adjoint_backward(sph_handle* h, const double* dl_dv, const double* dl_du,
                          const double* dl_dr, double* g_r0, double* g_v0, double* g_u0,
                          double* g_par);
+/* The diffusion adjoint: after sph_adjoint_forward on a run with equations
+ * = diffusion (fixed positions: v = 0; ddw = fab, fw or n2w; isotropic,
+ * diagonal or full b b^T conductivity tensor, circuit2.f90:347-397), maps
+ * dL/dT(T) (realpn values, original row order) to dL/dT0 (g_T0) and
+ * dL/d difcond (one value, state slot dcondconst), NULL outputs skipped. */
+int sph_adjoint_backward_diffusion(sph_handle* h, const double* dl_dT, double* g_T0,
+                                   double* g_difcond);
 
 /* ---- end-of-run error (main.f90:374-402, errcalc.f90) --------------------
  * Replaces the engine's closing error evaluation: for the run's initial

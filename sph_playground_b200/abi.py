@@ -117,6 +117,8 @@ def load(path=None):
         lib.sph_adjoint_forward.restype = c_int
         lib.sph_adjoint_backward.argtypes = [vp, P(d), P(d), P(d), P(d), P(d), P(d), P(d)]
         lib.sph_adjoint_backward.restype = c_int
+        lib.sph_adjoint_backward_diffusion.argtypes = [vp, P(d), P(d), P(d)]
+        lib.sph_adjoint_backward_diffusion.restype = c_int
     for name in ABI_SYMBOLS:
         if name not in ("sph_last_error", "sph_destroy", "sph_batch_destroy"):
             getattr(lib, name).restype = c_int
@@ -252,6 +254,16 @@ class Engine:
         l1 = np.zeros(1, dtype=np.float64)
         self._check(self.lib.sph_errcalc(self.h, _dptr(err), err.shape[0], _dptr(l1)))
         return err, float(l1[0])
+
+    def adjoint_backward_diffusion(self, dl_dT):
+        """(dL/dT0 per real particle, dL/d difcond) after adjoint_forward on
+        a diffusion run, for dL/dT(T) per real particle (original order)."""
+        g = np.zeros(self.n_real, dtype=np.float64)
+        gd = np.zeros(1, dtype=np.float64)
+        lt = np.ascontiguousarray(dl_dT, dtype=np.float64)
+        assert lt.shape == (self.n_real,)
+        self._check(self.lib.sph_adjoint_backward_diffusion(self.h, _dptr(lt), _dptr(g), _dptr(gd)))
+        return g, float(gd[0])
 
     def get_neighbours(self):
         """(offsets[n_real+1], pairs) with pairs = (rj << 5) | image code."""

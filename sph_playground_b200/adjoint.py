@@ -12,6 +12,12 @@ the front end: the numbers come from the CUDA engine.
     vT = Rollout.apply(v0, alpha, beta, setup)
     loss = ((vT - v_target) ** 2).sum()
     loss.backward()            # v0.grad, alpha.grad, beta.grad
+
+For a diffusion run (fixed positions, leapfrog on T) the same setup drives
+DiffusionRollout: T(T) from the initial temperatures and the conductivity
+(state slot dcondconst), gradients by sph_adjoint_backward_diffusion.
+
+    TT = DiffusionRollout.apply(T0, difcond, setup)
 """
 from dataclasses import dataclass, field
 
@@ -87,3 +93,47 @@ class Rollout(torch.autograd.Function):
             ctx.engine = None
         t = lambda a: torch.as_tensor(a, dtype=ctx.dtype, device=ctx.dev)  # noqa: E731
         return t(res["g_v0"]), t(res["g_par"][0]), t(res["g_par"][1]), None
+
+
+_T = consts.es["t"] - 1
+
+
+def _diffusion_engine(setup, T0, difcond):
+    store = np.array(setup.store, dtype=np.float64, copy=True)
+    store[:, _T] = np.asarray(T0, dtype=np.float64).reshape(-1)
+    state = np.array(setup.state, dtype=np.float64, copy=True)
+    state[consts.ec["dcondconst"] - 1] = float(difcond)
+    e = abi.Engine(state, store, setup.kernel, precision=setup.precision, lib=setup.lib)
+    for k, v in setup.params.items():
+        e.set_param(k, v)
+    e.set_param(abi.P_FIXED_DT, float(setup.dt))
+    return e
+
+
+class DiffusionRollout(torch.autograd.Function):
+    """T(T) = rollout(T0, difcond) of a diffusion run; gradients by the
+    engine's adjoint of the diffusion term."""
+
+    @staticmethod
+    def forward(ctx, T0, difcond, setup):
+        e = _diffusion_engine(setup, T0.detach().cpu().numpy(), difcond.item())
+        try:
+            e.adjoint_forward(setup.nsteps, setup.every)
+            TT = e.get_store()[: e.n_real, _T]
+        except Exception:
+            e.close()
+            raise
+        ctx.engine = e
+        ctx.dev, ctx.dtype = T0.device, T0.dtype
+        return torch.as_tensor(TT, dtype=T0.dtype, device=T0.device)
+
+    @staticmethod
+    def backward(ctx, g_TT):
+        e = ctx.engine
+        try:
+            g_T0, g_dc = e.adjoint_backward_diffusion(g_TT.detach().cpu().numpy())
+        finally:
+            e.close()
+            ctx.engine = None
+        t = lambda a: torch.as_tensor(a, dtype=ctx.dtype, device=ctx.dev)  # noqa: E731
+        return t(g_T0), t(g_dc), None

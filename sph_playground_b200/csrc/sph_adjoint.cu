@@ -1,6 +1,8 @@
 // Adjoint (vector-Jacobian products) of one leapfrog step of the hydro path,
 // for the gradient of a final-state misfit with respect to the initial
-// velocities, energies, positions and the artificial-viscosity parameters.
+// velocities, energies, positions and the artificial-viscosity parameters;
+// and of the diffusion path (fixed positions), with respect to the initial
+// temperatures and the conductivity.
 // No counterpart in the reference (its Fortran has no derivatives); the
 // forward map differentiated here is exactly the engine's FP64 step for
 // equations = hydro with the artificial viscosity of circuit2.f90:294-336
@@ -301,6 +303,105 @@ k_adj_c1_scatter(AdjArgs a) {
     for (int d = 0; d < DIM; ++d) atomicAdd(&a.adj[int64_t(AJ_GR + d) * ld + pa], gr[d]);
 }
 
+// ---- VJP of the diffusion term (circuit2.f90:347-397, fab / fw / n2w) -----------------------
+// dT_a/dt = sum_b w_ab (T_b rho_b - T_a rho_a),  w_ab = m_b / (rho_a rho_b) c_ab,
+// c_ab the kernel.f90:377-539 contraction K_bar : Hessian_a, linear in the
+// conductivity (K = difcond I, or difcond times the b-field's diagonal or
+// full b b^T).  With positions fixed the map T -> dT/dt is linear, so
+//   dT_a/dt's adjoint mu_a adds  -mu_a rho_a sum_b w_ab  to T_a and
+//   mu_a w_ab rho_b  to T_b (the source row of an image), and
+//   mu_a dT_a/dt / difcond  to the conductivity.
+__device__ __forceinline__ void tensor3(double dc, const double* ub, int full, double K[3][3]) {
+  for (int x = 0; x < 3; ++x)
+    for (int y = 0; y < 3; ++y) K[x][y] = (x == y || full) ? dc * ub[x] * ub[y] : 0.0;
+}
+
+template <int K, int DIM, int G>
+__global__ void __launch_bounds__(TPB)
+k_adj_diff(AdjArgs a) {
+  const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
+  const int lane = threadIdx.x & (G - 1);
+  double gdc = 0.0;
+  if (c < a.nc) {
+    const int64_t k = a.centre_k[c];
+    const int64_t pa = a.centre_p[c];
+    const double* cols = a.cols;
+    const int64_t ld = a.ld;
+    auto CA = [&](int f) { return cols[f * ld + pa]; };
+    const double xa[3] = {a.sx[k], a.sy[k], a.sz[k]};
+    const double iha = 1.0 / CA(es_h), rhoa = CA(es_den);
+    double Ka = iha;
+    for (int d = 0; d < DIM; ++d) Ka *= iha;
+    Ka *= a.wcv;
+    const double mu = AJ(a, AJ_LDT, pa);
+    const double dc = a.difcond;
+    double kta[3][3], ktb[3][3], uba[3] = {0, 0, 0}, ubb[3] = {0, 0, 0};
+    const double Ba[3] = {CA(es_bx), CA(es_by), CA(es_bz)};
+    const double b2a = Ba[0] * Ba[0] + Ba[1] * Ba[1] + Ba[2] * Ba[2];
+    if (b2a != 0.0) {
+      const double ib = 1.0 / sqrt(b2a);
+      for (int x = 0; x < 3; ++x) uba[x] = Ba[x] * ib;
+    }
+    const double one[3] = {1.0, 1.0, 1.0};
+    if (a.difiso == 1) {
+      tensor3(dc, one, 0, kta);
+      tensor3(dc, one, 0, ktb);
+    } else {
+      tensor3(dc, uba, a.full_tensor, kta);
+    }
+    double diag = 0.0;
+    const int n = a.ncnt[c];
+    const int32_t* __restrict__ row = a.nl + a.rowoff[c];
+    for (int l = lane; l < n; l += G) {
+      const int64_t j = row[l];
+      const int64_t pb = a.ssrc[j];
+      auto CB = [&](int f) { return cols[f * ld + pb]; };
+      const double x[3] = {xa[0] - a.sx[j], xa[1] - a.sy[j], xa[2] - a.sz[j]};
+      double r2 = x[0] * x[0];
+      if (DIM >= 2) r2 += x[1] * x[1];
+      if (DIM == 3) r2 += x[2] * x[2];
+      const double invr = 1.0 / sqrt(r2);
+      const double r = r2 * invr;
+      double fa, dfa, ddfa;
+      kshape_all<K, double>(r * iha, fa, dfa, ddfa);
+      const double ga = (Ka * invr) * dfa;
+      if (a.difiso == 0) {
+        const double Bb[3] = {CB(es_bx), CB(es_by), CB(es_bz)};
+        const double b2 = Bb[0] * Bb[0] + Bb[1] * Bb[1] + Bb[2] * Bb[2];
+        if (b2 != 0.0) {  // a zero B_b keeps the previous unit vector (circuit2.f90:220-224)
+          const double ib = 1.0 / sqrt(b2);
+          for (int q = 0; q < 3; ++q) ubb[q] = Bb[q] * ib;
+        }
+        tensor3(dc, ubb, a.full_tensor, ktb);
+      }
+      double rr = 0.0, tr = 0.0;
+      for (int p = 0; p < DIM; ++p) {
+        tr += 0.5 * (kta[p][p] + ktb[p][p]);
+        for (int q = 0; q < DIM; ++q) rr += 0.5 * (kta[p][q] + ktb[p][q]) * x[p] * x[q];
+      }
+      rr = rr * (invr * invr);
+      double contr;
+      if (a.ddw == esd_n2w) {
+        contr = Ka * iha * ddfa * rr + ga * (tr - rr);
+      } else {
+        const double f2 = (a.ddw == esd_fab) ? -ga : 0.5 * a.fwc * Ka * iha * fa;
+        contr = f2 * (double(DIM + 2) * rr - tr);
+      }
+      const double rhob = CB(es_den);
+      const double w = CB(es_m) / (rhob * rhoa) * contr;
+      diag += w;
+      atomicAdd(&AJ(a, AJ_GT, pb), mu * w * rhob);
+    }
+    diag = gsum<G>(diag);
+    if (lane == 0) {
+      atomicAdd(&AJ(a, AJ_GT, pa), -mu * rhoa * diag);
+      if (dc != 0.0) gdc = mu * CA(es_ddt) / dc;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) gdc += __shfl_xor_sync(0xffffffffu, gdc, o);
+  if ((threadIdx.x & 31) == 0 && gdc != 0.0) atomicAdd(&a.gpar[2], gdc);
+}
+
 // ---- step adjoints -------------------------------------------------------------------------
 // before the force VJP: the adjoints of the new a, du and zeroed sums
 __global__ void k_adj_prep(AdjArgs a, double dt, int first) {
@@ -311,6 +412,10 @@ __global__ void k_adj_prep(AdjArgs a, double dt, int first) {
     AJ(a, AJ_LA + d, p) = AJ(a, AJ_LAS + d, p) + (first ? 0.0 : hdt * AJ(a, AJ_LV + d, p));
   AJ(a, AJ_LDU, p) = AJ(a, AJ_LDUS, p) + (first ? 0.0 : hdt * AJ(a, AJ_LU, p));
   for (int col = AJ_GR; col <= AJ_GU; ++col) AJ(a, col, p) = 0.0;
+  if (a.diff) {  // T follows u's integrator (main.f90:323-362)
+    AJ(a, AJ_LDT, p) = AJ(a, AJ_LDTS, p) + (first ? 0.0 : hdt * AJ(a, AJ_LT, p));
+    AJ(a, AJ_GT, p) = 0.0;
+  }
 }
 
 // after it: back through the corrector and the predictor (main.f90:323-362)
@@ -328,6 +433,10 @@ __global__ void k_adj_integrate(AdjArgs a, double dt, int first) {
     }
     AJ(a, AJ_LU, p) += AJ(a, AJ_GU, p);
     AJ(a, AJ_LDUS, p) = 0.0;
+    if (a.diff) {
+      AJ(a, AJ_LT, p) += AJ(a, AJ_GT, p);
+      AJ(a, AJ_LDTS, p) = 0.0;
+    }
     return;
   }
   const double hdt = 0.5 * dt;
@@ -343,11 +452,22 @@ __global__ void k_adj_integrate(AdjArgs a, double dt, int first) {
   const double lu1 = lu0 + AJ(a, AJ_GU, p);
   AJ(a, AJ_LU, p) = lu1;
   AJ(a, AJ_LDUS, p) = -hdt * lu0 + dt * lu1;
+  if (a.diff) {
+    const double lt0 = AJ(a, AJ_LT, p);
+    const double lt1 = lt0 + AJ(a, AJ_GT, p);
+    AJ(a, AJ_LT, p) = lt1;
+    AJ(a, AJ_LDTS, p) = -hdt * lt0 + dt * lt1;
+  }
 }
 
 template <int K, int DIM, int G>
 void adj_pairs_g(const AdjArgs& a, cudaStream_t s) {
   const int nb = nblocks(a.nc * G);
+  if (a.diff) {  // positions fixed: only the diffusion term depends on the state
+    k_adj_diff<K, DIM, G><<<nb, TPB, 0, s>>>(a);
+    note_launch();
+    return;
+  }
   k_adj_c2<K, DIM, G><<<nb, TPB, 0, s>>>(a);
   k_adj_c1_sum<K, DIM, G><<<nb, TPB, 0, s>>>(a);
   k_adj_particle<<<nblocks(a.nreal), TPB, 0, s>>>(a, DIM);

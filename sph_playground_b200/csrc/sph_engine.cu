@@ -1346,10 +1346,32 @@ struct sph_handle {
   double* seg(int i) { return adj_seg.as<double>() + size_t(i) * NCOL * nrows; }
 
   // the hydro subset the adjoint kernels differentiate
+  // which adjoint applies: the hydro one, or (adj_diff) the diffusion one
+  bool adj_diff = false;
   int adjoint_supported() {
     eqset();
+    adj_diff = false;
+    if (eq_diff && !eq_hydro) {
+      // pure diffusion: positions stay where they are (v = 0, no force), so
+      // dT/dt is linear in T and in the conductivity
+      if (eq_fld || eq_sts || eq_radexch || eq_magneto)
+        return fail(SPH_ERR_UNSUPPORTED, "adjoint: diffusion without FLD, STS or MHD");
+      const int ddw = ival(ec_ddw);
+      if (ddw != esd_fab && ddw != esd_fw && ddw != esd_n2w)
+        return fail(SPH_ERR_UNSUPPORTED, "adjoint: diffusion with ddw = fab, fw or n2w");
+      if (nfixed > 0) return fail(SPH_ERR_UNSUPPORTED, "adjoint: fixed particles");
+      if (!(st[SPH_P_FIXED_DT] > 0)) return fail(SPH_ERR_ARG, "adjoint: set SPH_P_FIXED_DT > 0");
+      std::vector<double> v(3 * size_t(nrows));
+      CK(cudaMemcpyAsync(v.data(), cols.as<double>() + size_t(es_vx) * nrows,
+                         sizeof(double) * 3 * nrows, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (double x : v)
+        if (x != 0.0) return fail(SPH_ERR_UNSUPPORTED, "adjoint: diffusion needs v = 0 (fixed positions)");
+      adj_diff = true;
+      return SPH_OK;
+    }
     if (ival(ec_eqs) != eeq_hydro || eq_magneto || eq_diff || eq_fld || eq_sts || eq_radexch)
-      return fail(SPH_ERR_UNSUPPORTED, "adjoint: equations must be hydro");
+      return fail(SPH_ERR_UNSUPPORTED, "adjoint: equations must be hydro or diffusion");
     if (ival(ec_adden) != 1)
       return fail(SPH_ERR_UNSUPPORTED, "adjoint: needs the Newton h-iteration (adden = yes)");
     if (ival(ec_artts) == 1 && st[ec_au] != -1.0 && st[ec_au] != 0.0)
@@ -1427,20 +1449,29 @@ struct sph_handle {
     a.gamma = P.gamma;
     a.artts = P.artts == 1;
     a.hydro = P.eq_hydro != 0;
+    a.diff = adj_diff ? 1 : 0;
+    a.ddw = P.ddw;
+    a.difiso = P.difiso;
+    a.full_tensor = P.full_tensor;
+    a.difcond = P.difcond;
+    a.fwc = P.fwc;
     return a;
   }
 
   // dL/dv(T), dL/du(T), dL/dr(T) (original row order; NULL = 0) -> dL/d(r0,
   // v0, u0) and dL/d(alpha, beta) by the checkpointed adjoint sweep
+  // (and dL/dT(T) -> dL/dT0, dL/d difcond for the diffusion adjoint; g_par
+  // then has npar = 3 slots: alpha, beta, difcond)
   int adjoint_backward(const double* dl_dv, const double* dl_du, const double* dl_dr,
-                       double* g_r0, double* g_v0, double* g_u0, double* g_par) {
+                       double* g_r0, double* g_v0, double* g_u0, double* g_par,
+                       const double* dl_dT = nullptr, double* g_T0 = nullptr, int npar = 2) {
     if (adj_nsteps < 1) return fail(SPH_ERR_ARG, "adjoint: no forward run recorded");
     const int d = dim();
     RC(adj.ensure(sizeof(double) * AJ_TOTAL * size_t(nrows)));
-    RC(adj_par.ensure(sizeof(double) * 2));
+    RC(adj_par.ensure(sizeof(double) * 3));
     RC(adj_io.ensure(sizeof(double) * 3 * size_t(nrows)));
     CK(cudaMemsetAsync(adj.p, 0, sizeof(double) * AJ_TOTAL * size_t(nrows), s));
-    CK(cudaMemsetAsync(adj_par.p, 0, sizeof(double) * 2, s));
+    CK(cudaMemsetAsync(adj_par.p, 0, sizeof(double) * 3, s));
     auto load = [&](const double* host, int col, int ncomp) -> int {
       if (!host) return SPH_OK;
       CK(cudaMemcpyAsync(adj_io.p, host, sizeof(double) * ncomp * nrows, cudaMemcpyHostToDevice, s));
@@ -1451,6 +1482,7 @@ struct sph_handle {
     RC(load(dl_dv, AJ_LV, 3));
     RC(load(dl_du, AJ_LU, 1));
     RC(load(dl_dr, AJ_LR, 3));
+    RC(load(dl_dT, AJ_LT, 1));
     const int G = lanes_pair();
     for (int sgi = adj_ncp - 1; sgi >= 0; --sgi) {
       const int n0 = sgi * adj_every, n1 = std::min(adj_nsteps, n0 + adj_every);
@@ -1484,11 +1516,11 @@ struct sph_handle {
     RC(store(g_v0, AJ_LV, 3));
     RC(store(g_u0, AJ_LU, 1));
     RC(store(g_r0, AJ_LR, 3));
+    RC(store(g_T0, AJ_LT, 1));
     if (g_par) {
-      CK(cudaMemcpyAsync(h_ctrl + 1, adj_par.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(h_ctrl + 1, adj_par.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      g_par[0] = h_ctrl[1];
-      g_par[1] = h_ctrl[2];
+      for (int k = 0; k < npar && k < 3; ++k) g_par[k] = h_ctrl[1 + k];
     }
     // back to the state at the end of the forward run
     RC(copy_table(cols.p, ckpt(adj_ncp + 1)));
@@ -1873,6 +1905,19 @@ int sph_adjoint_backward(sph_handle* h, const double* dl_dv, const double* dl_du
   AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   int rc = h->adjoint_backward(dl_dv, dl_du, dl_dr, g_r0, g_v0, g_u0, g_par);
+  h->collect_timers();
+  return rc;
+}
+
+int sph_adjoint_backward_diffusion(sph_handle* h, const double* dl_dT, double* g_T0,
+                                   double* g_difcond) {
+  AllocScope alloc_scope(h);
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  if (!h->adj_diff) return fail(SPH_ERR_STATE, "adjoint: the recorded forward run is not a diffusion run");
+  double g[3] = {0, 0, 0};
+  int rc = h->adjoint_backward(nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, g, dl_dT,
+                               g_T0, 3);
+  if (g_difcond) *g_difcond = g[2];
   h->collect_timers();
   return rc;
 }

@@ -293,11 +293,13 @@ void launch_c2(int prec, int kernel, int dim, const C2Args& a, PackBufs pb, Para
 // state adjoints LR (r), LV (v), LU (u), LAS (a), LDUS (du); the adjoints
 // LA, LDU of the new a, du fed to the force VJP; its results GR, GV (r', v'),
 // GH, GRHO, GOM, GP, GC, GU (h, rho, Omega, P, c, u); S' (d2 rho^/dh2) and
-// the Newton-h coefficients MU, WC.
+// the Newton-h coefficients MU, WC.  The diffusion adjoint adds LT (T),
+// LDTS (the stored dT/dt), LDT (the new dT/dt fed to its VJP) and GT (T').
 enum AdjCol : int {
   AJ_LR = 0, AJ_LV = 3, AJ_LU = 6, AJ_LAS = 7, AJ_LDUS = 10, AJ_LA = 11, AJ_LDU = 14,
   AJ_GR = 15, AJ_GV = 18, AJ_GH = 21, AJ_GRHO = 22, AJ_GOM = 23, AJ_GP = 24, AJ_GC = 25,
-  AJ_GU = 26, AJ_SP = 27, AJ_MU = 28, AJ_WC = 29, AJ_TOTAL = 30
+  AJ_GU = 26, AJ_SP = 27, AJ_MU = 28, AJ_WC = 29, AJ_LT = 30, AJ_LDTS = 31, AJ_LDT = 32,
+  AJ_GT = 33, AJ_TOTAL = 34
 };
 struct AdjArgs {
   int64_t nc, nreal;
@@ -313,9 +315,13 @@ struct AdjArgs {
   const double* cols;
   int64_t ld;
   double* adj;   // AJ_TOTAL columns of ld rows
-  double* gpar;  // d/d alpha, d/d beta
+  double* gpar;  // d/d alpha, d/d beta, d/d difcond
   double wcv, alpha, beta, gamma;
   int artts, hydro;
+  // the diffusion adjoint (diff = 1): equations = diffusion with fixed
+  // positions, second-derivative method fab / fw / n2w
+  int diff, ddw, difiso, full_tensor;
+  double difcond, fwc;
 };
 // one step's adjoint: prep, force VJP (circuit2, Newton-h density, EOS) and
 // the integrator's adjoint; first = 1 for the force evaluation of the

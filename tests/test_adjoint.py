@@ -188,3 +188,102 @@ def test_adjoint_rejects_other_equations(engine_lib, cuda_ok):
         with pytest.raises(abi.SphError) as ex:
             e.adjoint_forward(2, 1)
         assert ex.value.status == "SPH_ERR_UNSUPPORTED"
+
+
+# ---- the diffusion adjoint: dL/dT0 and dL/d difcond ---------------------------------------
+T_COL = consts.es["t"] - 1
+D_STEPS, D_EVERY, D_DT = 10, 4, 2e-4
+
+
+def _diff_setup(ddw, full):
+    st, store = ic.diffusion2d(16, ddw=ddw, full_tensor=full)
+    ic.set_state(st, "eqonsts", 0.0)  # leapfrog on T (the differentiated integrator)
+    return st, store
+
+
+def _diff_run(lib, st, store, full, prec=abi.PREC_FP64):
+    e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+    e.set_param(abi.P_FULL_TENSOR, 1.0 if full else 0.0)
+    e.set_param(abi.P_FIXED_DT, D_DT)
+    e.adjoint_forward(D_STEPS, D_EVERY)
+    return e
+
+
+def _diff_loss(T, target):
+    return float(np.sum((T - target) ** 2))
+
+
+@pytest.mark.parametrize("ddw,full", [("fab", False), ("fw", False), ("n2w", False),
+                                      ("fab", True)])
+def test_diffusion_gradients_match_fd(engine_lib, cuda_ok, ddw, full):
+    """dL/dT0 along a random direction and dL/d difcond against central
+    differences (the map is linear in T0 and in difcond, so the differences
+    are exact up to rounding): relative 1e-6."""
+    st, store = _diff_setup(ddw, full)
+    target = 0.9 * store[:, T_COL]
+    e = _diff_run(engine_lib, st, store, full)
+    T = e.get_store()[:, T_COL]
+    gT0, gdc = e.adjoint_backward_diffusion(2.0 * (T - target))
+    e.close()
+    rng = np.random.default_rng(7)
+    d = rng.normal(size=store.shape[0])
+    eps = 1e-6
+
+    def loss_at(T0=None, dc=None):
+        s2, st2 = store.copy(), st.copy()
+        if T0 is not None:
+            s2[:, T_COL] = T0
+        if dc is not None:
+            ic.set_state(st2, "dcondconst", dc)
+        e2 = _diff_run(engine_lib, st2, s2, full)
+        try:
+            return _diff_loss(e2.get_store()[:, T_COL], target)
+        finally:
+            e2.close()
+    fd_T = (loss_at(T0=store[:, T_COL] + eps * d) - loss_at(T0=store[:, T_COL] - eps * d)) / (2 * eps)
+    assert float(gT0 @ d) == pytest.approx(fd_T, rel=1e-6)
+    dc0 = ic.get_state(st, "dcondconst")
+    fd_dc = (loss_at(dc=dc0 + eps) - loss_at(dc=dc0 - eps)) / (2 * eps)
+    assert gdc == pytest.approx(fd_dc, rel=1e-6)
+
+
+def test_diffusion_gradient_fp32_near_fp64(engine_lib, cuda_ok):
+    st, store = _diff_setup("fab", False)
+    target = 0.9 * store[:, T_COL]
+    out = []
+    for prec in (abi.PREC_FP64, abi.PREC_FP32_COMP):
+        e = _diff_run(engine_lib, st, store, False, prec)
+        T = e.get_store()[:, T_COL]
+        out.append(e.adjoint_backward_diffusion(2.0 * (T - target)))
+        e.close()
+    (g64, d64), (g32, d32) = out
+    assert np.linalg.norm(g32 - g64) <= 1e-4 * np.linalg.norm(g64)
+    assert d32 == pytest.approx(d64, rel=1e-4)
+
+
+def test_diffusion_adjoint_rejects_sts(engine_lib, cuda_ok):
+    st, store = ic.diffusion2d(16, ddw="fab")  # fixed-stage STS integrator
+    e = abi.Engine(st, store, "m6", lib=engine_lib)
+    e.set_param(abi.P_FIXED_DT, D_DT)
+    with pytest.raises(abi.SphError) as ex:
+        e.adjoint_forward(2, 1)
+    assert ex.value.status == "SPH_ERR_UNSUPPORTED"
+    e.close()
+
+
+def test_diffusion_torch_function(engine_lib, cuda_ok):
+    import torch
+    from sph_playground_b200.adjoint import DiffusionRollout, RolloutSetup
+    st, store = _diff_setup("fab", False)
+    target = 0.9 * store[:, T_COL]
+    setup = RolloutSetup(st, store, D_STEPS, D_EVERY, D_DT, lib=engine_lib)
+    T0 = torch.tensor(store[:, T_COL], dtype=torch.float64, requires_grad=True)
+    dc = torch.tensor(ic.get_state(st, "dcondconst"), dtype=torch.float64, requires_grad=True)
+    TT = DiffusionRollout.apply(T0, dc, setup)
+    ((TT - torch.as_tensor(target)) ** 2).sum().backward()
+    e = _diff_run(engine_lib, st, store, False)
+    T = e.get_store()[:, T_COL]
+    gT0, gdc = e.adjoint_backward_diffusion(2.0 * (T - target))
+    e.close()
+    assert np.allclose(T0.grad.numpy(), gT0, rtol=1e-12, atol=1e-14)
+    assert dc.grad.item() == pytest.approx(gdc, rel=1e-12)
