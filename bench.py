@@ -59,6 +59,8 @@ def parse():
                     help="use the default launch shapes instead of autotuning them")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint cost / gradient check (2D shear 256^2)")
+    ap.add_argument("--no-density", action="store_true",
+                    help="skip the density-only pass (3D perturbed lattice 128^3, FP32 vs FP64)")
     ap.add_argument("--no-errors", action="store_true",
                     help="skip the FP32-vs-FP64 error check (profiling runs)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -233,6 +235,41 @@ def adjoint_block(lib, n=256, n_ref=64, nsteps=200, every=20, dt=5e-4):
             "grad_v0_fp32_vs_fp64_rel": rel,
             "grad_reference": f"FP64 adjoint gradient at {n_ref}^2",
             "timing": "host clock around synchronous C-ABI calls"}
+
+
+def density_block(lib, n=128, tol=1e-6, reps=5):
+    """The density-only workload: one density + Newton-h pass over a 3D
+    periodic n^3 lattice perturbed by uniform(-0.1, 0.1) dx (seed 2), M6,
+    hfac 1.2, Newton tolerance `tol`; FP32-comp against FP64: device time of
+    the pass (CUDA events of the neighbour and circuit1 phases, averaged
+    over `reps` passes after one warm-up) and the per-particle relative
+    error of rho and h."""
+    from sph_playground_b200 import ic
+    st, store = ic.density3d(n=n, seed=2)
+    out, res = {}, {}
+    for prec, name in ((abi.PREC_FP64, "fp64"), (abi.PREC_FP32_COMP, "fp32_comp")):
+        e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+        e.set_param(abi.P_NEWTON_TOL, tol)
+        e.density()
+        res[name] = e.get_store()
+        e.reset_counters()
+        e.set_param(abi.P_TIMING, 1)
+        for _ in range(reps):
+            e.set_store(store)
+            e.density()
+        t = e.timers()
+        e.close()
+        ms = sum(t[k] for k in ("ghosts", "sort", "neighbours", "pack", "circuit1")) / reps
+        out[name] = {"ms_per_pass": ms, "particle_passes_per_s": store.shape[0] / (ms * 1e-3)}
+    C = {k: v - 1 for k, v in abi.consts.es.items()}
+    for f in ("den", "h"):
+        rel = np.abs(res["fp32_comp"][:, C[f]] - res["fp64"][:, C[f]]) / np.abs(res["fp64"][:, C[f]])
+        out[("rho" if f == "den" else f) + "_rel_err"] = {"max": float(rel.max()),
+                                                        "p99.9": float(np.quantile(rel, 0.999))}
+    out["fp32_over_fp64_speed"] = out["fp64"]["ms_per_pass"] / out["fp32_comp"]["ms_per_pass"]
+    out["workload"] = (f"density3d {n}^3 ({store.shape[0]} particles), perturbed lattice, M6 hfac 1.2, "
+                       f"Newton tolerance {tol}, one density pass (images, sort, search, circuit1)")
+    return out
 
 
 def max_over_ranks(x, device="cuda"):
@@ -419,6 +456,9 @@ def main():
     adj = None
     if not args.no_adjoint:
         adj = adjoint_block(lib)
+    dens = None
+    if not args.no_density:
+        dens = density_block(lib)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -459,6 +499,7 @@ def main():
                               "candidates": cnt["candidates"] / args.steps},
             "fp64": fp64,
             "adjoint": adj,
+            "density_pass": dens,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "peak_fp32_tflops": peak32 / 1e12,
         }
