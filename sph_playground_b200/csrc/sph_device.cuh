@@ -101,41 +101,37 @@ __device__ __forceinline__ void kshape_all(R q, R& f, R& df, R& ddf) {
 }
 
 // FP32 f(q) that follows q below FP32 resolution, for the Newton iteration on
-// h.  q_lo is the rounding residual of q = r/h.  Each clamped piece
-// t_k = c_k - q is itself rounded; its exact residual (Fast2Sum, c_k >= q on
-// the live pieces) and q_lo enter f to first order through the piece's own
-// derivative.  The density sum then changes smoothly with h instead of in
-// steps of one FP32 ulp of q or t_k, so the Newton iterates settle.
+// h.  q_lo is the rounding residual of q = r/h.  q is split as qh + dq with
+// qh on the 2^-21 grid (for q < 4, q + 4 carries an ulp of 2^-21, so the add
+// rounds q to it and the subtraction back is exact), which makes every piece
+// t_k = c_k - qh exact; dq = (q - qh) + q_lo (the first difference exact)
+// enters f to first order, f(q) = f(qh) + f'(qh) dq, the second-order term
+// being below 1e-12 of f.  The density sum then changes smoothly with h
+// instead of in steps of one FP32 ulp of q, so the Newton iterates settle.
 template <int K>
 __device__ __forceinline__ void kshape_f_df_res(float q, float q_lo, float& f, float& df) {
   if constexpr (K == KM6 || K == KM4) {
+    const float qh = __fsub_rn(__fadd_rn(q, 4.0f), 4.0f);
+    const float dq = __fadd_rn(__fsub_rn(q, qh), q_lo);
     constexpr int NP = (K == KM6) ? 3 : 2;
     const float cs[3] = {K == KM6 ? 3.f : 2.f, K == KM6 ? 2.f : 1.f, 1.f};
     const float as[3] = {K == KM6 ? 1.f : 0.25f, K == KM6 ? -6.f : -1.f, 15.f};
     f = 0.f;
     df = 0.f;
-    float corr = 0.f;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      const float traw = cs[k] - q;
-      const float tl = (-q) - (traw - cs[k]);
-      // a piece outside its support has th = 0, hence d = 0, and its
-      // residual tl then drops out of the correction by itself
-      const float th = fmaxf(traw, 0.f);
-      float s = th * th;
-      float d;
+      const float th = fmaxf(cs[k] - qh, 0.f);  // exact: both on the 2^-21 grid
+      const float s = th * th;
       if constexpr (K == KM6) {
-        float q4 = s * s;
+        const float q4 = s * s;
         f = fmaf(as[k], q4 * th, f);
-        d = (-5.f * as[k]) * q4;  // d f_k / d q
+        df = fmaf(-5.f * as[k], q4, df);
       } else {
         f = fmaf(as[k], s * th, f);
-        d = (-3.f * as[k]) * s;
+        df = fmaf(-3.f * as[k], s, df);
       }
-      df += d;
-      corr = fmaf(-d, tl - q_lo, corr);
     }
-    f += corr;
+    f = fmaf(df, dq, f);
   } else {
     float e = expf(-q * q);
     f = e;
