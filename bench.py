@@ -38,11 +38,11 @@ UNIT = "particle-steps/s"
 F1_C1 = 50.0
 F2_C2 = 150.0
 # DRAM bytes per in-support pair of the FP32-comp circuit2 launch:
-# dram__bytes_read.sum + dram__bytes_write.sum = 848.70 MB + 69.45 MB over
+# dram__bytes_read.sum + dram__bytes_write.sum = 849.04 MB + 73.09 MB over
 # 157.49M pairs of the 96^3 capture in profiles/k_c2_fp32_sedov3d_96.md (the
 # neighbour index, 4 B, plus the gathered pair data that misses L2); the
 # traffic scales with the pairs a launch processes
-C2_DRAM_BYTES_PER_PAIR = (848.70e6 + 69.45e6) / 157.49e6
+C2_DRAM_BYTES_PER_PAIR = (849.04e6 + 73.09e6) / 157.49e6
 
 
 def parse():
@@ -237,7 +237,7 @@ def adjoint_block(lib, n=256, n_ref=64, nsteps=200, every=20, dt=5e-4):
             "timing": "host clock around synchronous C-ABI calls"}
 
 
-def density_block(lib, n=128, tol=1e-6, reps=5):
+def density_block(lib, shapes, n=128, tol=1e-6, reps=5):
     """The density-only workload: one density + Newton-h pass over a 3D
     periodic n^3 lattice perturbed by uniform(-0.1, 0.1) dx (seed 2), M6,
     hfac 1.2, Newton tolerance `tol`; FP32-comp against FP64: device time of
@@ -249,6 +249,8 @@ def density_block(lib, n=128, tol=1e-6, reps=5):
     out, res = {}, {}
     for prec, name in ((abi.PREC_FP64, "fp64"), (abi.PREC_FP32_COMP, "fp32_comp")):
         e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+        for k, v in shapes.get(prec, {}).items():  # the launch shapes of the step arms
+            e.set_param(getattr(abi, k), float(v))
         e.set_param(abi.P_NEWTON_TOL, tol)
         e.density()
         res[name] = e.get_store()
@@ -458,7 +460,8 @@ def main():
         adj = adjoint_block(lib)
     dens = None
     if not args.no_density:
-        dens = density_block(lib)
+        extra = dict(kv.split("=") for kv in args.param if not kv.split("=")[0].isdigit())
+        dens = density_block(lib, {p: {**tuned[p], **extra} for p in tuned})
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
