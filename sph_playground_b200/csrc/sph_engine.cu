@@ -805,7 +805,9 @@ struct sph_handle {
   int circuit2(const Mode& m, const Params& P) {
     const int64_t nall = nrows + nghost;
     PackBufs pb = packs();
-    int groups = PACK_POS | PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
+    // the positions (PACK_POS) were packed for circuit1 in this iterate and
+    // have not moved; h, rho, Omega, P, c and grad T are new
+    int groups = PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
     {
       Phase pk(this, SPH_T_PACK);
       if (dplan)
