@@ -838,6 +838,12 @@ struct sph_handle {
     return SPH_OK;
   }
 
+  // the integrator's mode: which of B and T an equation moves this run
+  int lf_mode(bool do_sts) {
+    eqset();
+    return (do_sts ? LF_STS : 0) | (eq_magneto ? 0 : LF_NO_B) | ((eq_diff || eq_fld) ? 0 : LF_NO_T);
+  }
+
   // iterate() (iterator.f90:44-179); full = false stops after circuit1 + EOS
   int iterate(bool full) {
     if (dplan) return iterate_dev(full);
@@ -1020,10 +1026,10 @@ struct sph_handle {
     launch_dt(r, di, drs_clock.as<DevClock>(), ctrl.as<double>(), s);
     const bool do_sts = eq_sts;
     launch_predict(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
-                   ctrl.as<double>(), do_sts, s);
+                   ctrl.as<double>(), lf_mode(do_sts), s);
     RC(iterate(true));
     launch_correct(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
-                   ctrl.as<double>(), do_sts, s);
+                   ctrl.as<double>(), lf_mode(do_sts), s);
     if (do_sts) RC(sts_integrate(ival(ec_stsfixeds), 0.0));
     launch_clock_advance(drs_clock.as<DevClock>(), s);
     return SPH_OK;
@@ -1326,14 +1332,14 @@ struct sph_handle {
     {
       Phase ph(this, SPH_T_PREDICT);
       launch_predict(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
-                     ctrl.as<double>(), false, s);
+                     ctrl.as<double>(), lf_mode(false), s);
     }
     RC(iterate(true));
     if (stop_before_correct) return SPH_OK;
     {
       Phase ph(this, SPH_T_CORRECT);
       launch_correct(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
-                     ctrl.as<double>(), false, s);
+                     ctrl.as<double>(), lf_mode(false), s);
     }
     st[ec_time] += dt;
     cnt_host[SPH_CNT_STEPS]++;
@@ -1574,13 +1580,13 @@ struct sph_handle {
     {
       Phase ph(this, SPH_T_PREDICT);
       launch_predict(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
-                     ctrl.as<double>(), do_sts, s);
+                     ctrl.as<double>(), lf_mode(do_sts), s);
     }
     RC(iterate(true));
     {
       Phase ph(this, SPH_T_CORRECT);
       launch_correct(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
-                     ctrl.as<double>(), do_sts, s);
+                     ctrl.as<double>(), lf_mode(do_sts), s);
     }
     if (do_sts) RC(sts_integrate(sts_s, dt));
     if (eq_radexch) {  // main.f90:367-369

@@ -802,14 +802,17 @@ __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restric
 // Integrated rows: the reals and the fixedreal rows that follow them
 // (main.f90:181-184), selected by original row index.  Arithmetic in the
 // reference's evaluation order without contraction, so the update is bitwise
-// reproducible by the CPU oracle.
+// reproducible by the CPU oracle.  B (T) is left as it is when no equation
+// gives it a derivative (dB/dt = 0, dT/dt = 0 every step): x + dt 0 = x,
+// except that a stored -0 would become +0.
 enum SaveSlot : int { SV_AX = 0, SV_AY, SV_AZ, SV_DU, SV_DH, SV_DDT, SV_DBX, SV_DBY, SV_DBZ, SV_N };
 
 __global__ void k_predict(double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
                           int64_t nrows, int64_t n_int, double* __restrict__ save,
-                          const double* __restrict__ ctrl, int do_sts) {
+                          const double* __restrict__ ctrl, int mode) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= nrows || orig[i] >= n_int) return;
+  const bool do_b = !(mode & LF_NO_B), do_t = !(mode & (LF_STS | LF_NO_T));
   const double dt = ctrl[0];
   const double hdt2 = __dmul_rn(__dmul_rn(0.5, dt), dt);
   auto C = [&](int f) -> double& { return cols[f * ld + i]; };
@@ -818,37 +821,41 @@ __global__ void k_predict(double* __restrict__ cols, int64_t ld, const int32_t* 
     ta[k] = C(es_ax + k);
     tv[k] = C(es_vx + k);
     save[(SV_AX + k) * ld + i] = ta[k];
-    save[(SV_DBX + k) * ld + i] = C(es_dbx + k);
+    if (do_b) save[(SV_DBX + k) * ld + i] = C(es_dbx + k);
   }
-  double tdu = C(es_du), tdh = C(es_dh), tddt = C(es_ddt);
+  double tdu = C(es_du), tdh = C(es_dh);
   save[SV_DU * ld + i] = tdu;
   save[SV_DH * ld + i] = tdh;
-  if (!do_sts) save[SV_DDT * ld + i] = tddt;
+  const double tddt = do_t ? C(es_ddt) : 0.0;
+  if (do_t) save[SV_DDT * ld + i] = tddt;
   for (int k = 0; k < 3; ++k) {
     C(es_rx + k) = __dadd_rn(__dadd_rn(C(es_rx + k), __dmul_rn(dt, tv[k])), __dmul_rn(hdt2, ta[k]));
     C(es_vx + k) = __dadd_rn(tv[k], __dmul_rn(dt, ta[k]));
   }
   C(es_u) = __dadd_rn(C(es_u), __dmul_rn(dt, tdu));
   C(es_h) = __dadd_rn(C(es_h), __dmul_rn(dt, tdh));
-  if (!do_sts) C(es_t) = __dadd_rn(C(es_t), __dmul_rn(dt, tddt));
-  for (int k = 0; k < 3; ++k)
-    C(es_bx + k) = __dadd_rn(C(es_bx + k), __dmul_rn(dt, save[(SV_DBX + k) * ld + i]));
+  if (do_t) C(es_t) = __dadd_rn(C(es_t), __dmul_rn(dt, tddt));
+  if (do_b)
+    for (int k = 0; k < 3; ++k)
+      C(es_bx + k) = __dadd_rn(C(es_bx + k), __dmul_rn(dt, save[(SV_DBX + k) * ld + i]));
 }
 
 __global__ void k_correct(double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
                           int64_t nrows, int64_t n_int, const double* __restrict__ save,
-                          const double* __restrict__ ctrl, int do_sts) {
+                          const double* __restrict__ ctrl, int mode) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= nrows || orig[i] >= n_int) return;
+  const bool do_b = !(mode & LF_NO_B), do_t = !(mode & (LF_STS | LF_NO_T));
   const double hdt = __dmul_rn(0.5, ctrl[0]);
   auto C = [&](int f) -> double& { return cols[f * ld + i]; };
   for (int k = 0; k < 3; ++k)
     C(es_vx + k) = __dadd_rn(C(es_vx + k), __dmul_rn(hdt, __dadd_rn(C(es_ax + k), -save[(SV_AX + k) * ld + i])));
   C(es_u) = __dadd_rn(C(es_u), __dmul_rn(hdt, __dadd_rn(C(es_du), -save[SV_DU * ld + i])));
   C(es_h) = __dadd_rn(C(es_h), __dmul_rn(hdt, __dadd_rn(C(es_dh), -save[SV_DH * ld + i])));
-  for (int k = 0; k < 3; ++k)
-    C(es_bx + k) = __dadd_rn(C(es_bx + k), __dmul_rn(hdt, __dadd_rn(C(es_dbx + k), -save[(SV_DBX + k) * ld + i])));
-  if (!do_sts) C(es_t) = __dadd_rn(C(es_t), __dmul_rn(hdt, __dadd_rn(C(es_ddt), -save[SV_DDT * ld + i])));
+  if (do_b)
+    for (int k = 0; k < 3; ++k)
+      C(es_bx + k) = __dadd_rn(C(es_bx + k), __dmul_rn(hdt, __dadd_rn(C(es_dbx + k), -save[(SV_DBX + k) * ld + i])));
+  if (do_t) C(es_t) = __dadd_rn(C(es_t), __dmul_rn(hdt, __dadd_rn(C(es_ddt), -save[SV_DDT * ld + i])));
 }
 
 // ---- timestep reductions (timestep.f90:40-166) -----------------------------------------------
@@ -1286,13 +1293,13 @@ void launch_pack_dev(int prec, int groups, int64_t ncap, const int32_t* ssrc, co
   note_launch();
 }
 void launch_predict(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
-                    double* save, const double* ctrl, int do_sts, cudaStream_t s) {
-  k_predict<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, do_sts);
+                    double* save, const double* ctrl, int mode, cudaStream_t s) {
+  k_predict<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, mode);
   note_launch();
 }
 void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows, int64_t n_int,
-                    const double* save, const double* ctrl, int do_sts, cudaStream_t s) {
-  k_correct<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, do_sts);
+                    const double* save, const double* ctrl, int mode, cudaStream_t s) {
+  k_correct<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, n_int, save, ctrl, mode);
   note_launch();
 }
 void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,

@@ -194,11 +194,14 @@ void launch_pack_dev(int prec, int groups, int64_t ncap, const int32_t* ssrc, co
 void launch_pack(int prec, int groups, int64_t n, const int32_t* ssrc, const double* sx,
                  const double* sy, const double* sz, const double* cols, int64_t ld,
                  PackGeom pg, PackBufs pb, cudaStream_t s);
+// leapfrog predictor / corrector; mode: LF_STS (the STS integrator moves T),
+// LF_NO_B (no equation changes B), LF_NO_T (none changes T)
+enum LeapfrogMode : int { LF_STS = 1, LF_NO_B = 2, LF_NO_T = 4 };
 void launch_predict(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
-                    int64_t n_int, double* save, const double* ctrl, int do_sts,
+                    int64_t n_int, double* save, const double* ctrl, int mode,
                     cudaStream_t s);
 void launch_correct(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
-                    int64_t n_int, const double* save, const double* ctrl, int do_sts,
+                    int64_t n_int, const double* save, const double* ctrl, int mode,
                     cudaStream_t s);
 void launch_timestep_reduce(const double* cols, int64_t ld, const int32_t* orig,
                             int64_t nrows, int64_t n_ts, Params P,
