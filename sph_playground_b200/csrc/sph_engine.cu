@@ -706,11 +706,12 @@ struct sph_handle {
     }
     {
       Phase pk(this, SPH_T_PACK);
+      const int groups = PACK_POS | ((eq_diff || eq_fld) ? PACK_TEMP : 0);
       if (dplan)
-        launch_pack_dev(prec, PACK_POS, nall_cap, ssrc.as<int32_t>(), sx.as<double>(),
+        launch_pack_dev(prec, groups, nall_cap, ssrc.as<int32_t>(), sx.as<double>(),
                         sy.as<double>(), sz.as<double>(), cols.as<double>(), nrows, dplan, pb, s);
       else
-        launch_pack(prec, PACK_POS, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
+        launch_pack(prec, groups, nall, ssrc.as<int32_t>(), sx.as<double>(), sy.as<double>(),
                     sz.as<double>(), cols.as<double>(), nrows, pgeom, pb, s);
     }
     Phase ph(this, SPH_T_CIRCUIT1);

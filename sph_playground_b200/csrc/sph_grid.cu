@@ -751,7 +751,7 @@ __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restric
     if (groups & PACK_POS) {
       pb.p[0][k] = make_double2(sx[k], sy[k]);
       pb.p[1][k] = make_double2(sz[k], m);
-      pb.p[6][k] = make_double2(C(es_vz), C(es_t));
+      if (groups & PACK_TEMP) pb.p[6][k] = make_double2(C(es_vz), C(es_t));
     }
     if (groups & PACK_HYDRO) {
       double h = C(es_h), rho = C(es_den), om = C(es_om), P = C(es_p);
@@ -778,7 +778,8 @@ __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restric
       float zl = __double2float_rn(zs - double(zh));
       pb.q[0][k] = make_float4(xh, yh, zh, float(m));
       pb.q[1][k] = make_float4(xl, yl, zl, float(1.0 / C(es_h)));
-      pb.q[4][k] = make_float4(float(C(es_t)), float(C(es_kappa)), float(C(es_dtdx)),
+      if (groups & PACK_TEMP)
+        pb.q[4][k] = make_float4(float(C(es_t)), float(C(es_kappa)), float(C(es_dtdx)),
                                float(C(es_dtdy)));
     }
     if (groups & PACK_HYDRO) {

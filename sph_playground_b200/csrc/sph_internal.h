@@ -183,7 +183,9 @@ size_t scan64_temp_bytes(int64_t n);
 void exclusive_scan64(void* tmp, size_t tmp_bytes, const int64_t* in, int64_t* out, int64_t n,
                       cudaStream_t s);
 // pack groups
-enum PackGroup : int { PACK_POS = 1, PACK_HYDRO = 2, PACK_EXTRA = 4 };
+// (PACK_TEMP: with PACK_POS, also the temperature stream the circuit1
+// sweeps of the diffusion paths read)
+enum PackGroup : int { PACK_POS = 1, PACK_HYDRO = 2, PACK_EXTRA = 4, PACK_TEMP = 8 };
 struct PackBufs {
   double2* p[11];
   float4* q[6];
