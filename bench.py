@@ -39,7 +39,8 @@ F1_C1 = 50.0
 F2_C2 = 150.0
 # DRAM bytes per in-support pair of the FP32-comp circuit2 launch:
 # dram__bytes_read.sum + dram__bytes_write.sum = 849.04 MB + 73.09 MB over
-# 157.49M pairs of the 96^3 capture in profiles/k_c2_fp32_sedov3d_96.md (the
+# 157.49M pairs of an ncu capture of k_c2 on the Sedov 96^3 step (FP32-comp, 4
+# lanes per centre, cell edge 0.4 krad h_min) (the
 # neighbour index, 4 B, plus the gathered pair data that misses L2); the
 # traffic scales with the pairs a launch processes
 C2_DRAM_BYTES_PER_PAIR = (849.04e6 + 73.09e6) / 157.49e6
@@ -414,7 +415,7 @@ def main():
     traffic = C2_DRAM_BYTES_PER_PAIR * cnt["c2_pairs"] / args.steps if dom == "circuit2" else None
     roofline = {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": peak32 / 1e12,
                 "unit": "TFLOP/s", "frac": ach / (peak32 / 1e12), "traffic": traffic,
-                "traffic_source": "ncu DRAM bytes of the 96^3 capture (profiles/k_c2_fp32_sedov3d_96.md) "
+                "traffic_source": "ncu DRAM bytes of the k_c2 capture on the Sedov 96^3 step "
                                   "per pair, times this launch's pairs",
                 "peak_source": "live FFMA-chain probe (libsph_peak.so) on this GPU; "
                                "MEASURED_PEAKS.json holds no non-tensor FP32 figure"}
