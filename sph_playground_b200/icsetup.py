@@ -126,20 +126,18 @@ def closepacked(state, box, dbsz, dx, padding=(0.0, 0.0, 0.0)):
 
     iy1, iy2, nymin, nymax = widen(ymin, ymax, sph * int(ymin / sph), sph * int(ymax / sph))
     iz1, iz2, nzmin, nzmax = widen(zmin, zmax, zmin, zmax)
-    pts = []
-    for i in range(ix1, ix2 - int(2 * pdg[0]) + 1):
-        for j in range(iy1, iy2 - int(2 * pdg[1]) * n2 + 1):
-            for k in range(iz1, iz2 - int(2 * pdg[2]) * n3 + 1):
-                jm = (j - iy1) % 2
-                if (k - iz1) % 2 == 0:
-                    if not (i == ix2 and jm != 0):
-                        pts.append((pdg[0] * spdx + spdx * i + jm * spdx2,
-                                    n2 * pdg[1] * sph + sph * j,
-                                    n3 * pdg[2] * sph + sph * k))
-                else:
-                    if not (i == ix1 and jm == 0):
-                        pts.append((spdx * i - spdx2 + jm * spdx2, sph * j + sph3, sph * k))
-    store = _store(np.array(pts, dtype=np.float64).reshape(-1, 3))
+    ii = np.arange(ix1, ix2 - int(2 * pdg[0]) + 1)
+    jj = np.arange(iy1, iy2 - int(2 * pdg[1]) * n2 + 1)
+    kk = np.arange(iz1, iz2 - int(2 * pdg[2]) * n3 + 1)
+    I, J, K = (a.ravel() for a in np.meshgrid(ii, jj, kk, indexing="ij"))  # k fastest
+    jm = (J - iy1) % 2
+    even = (K - iz1) % 2 == 0
+    keep = np.where(even, ~((I == ix2) & (jm != 0)), ~((I == ix1) & (jm == 0)))
+    x = np.where(even, pdg[0] * spdx + spdx * I + jm * spdx2, spdx * I - spdx2 + jm * spdx2)
+    y = np.where(even, n2 * pdg[1] * sph + sph * J, sph * J + sph3)
+    z = np.where(even, n3 * pdg[2] * sph + sph * K, sph * K)
+    pts = np.stack([x, y, z], axis=1)[keep]
+    store = _store(pts)
     set_state(state, "realpn", store.shape[0])
     set_state(state, "fixedpn", 0)
     _set_borders(state, (xmin, xmax, nymin, nymax, nzmin, nzmax), dbsz, pdg[1] * sph)
@@ -176,24 +174,27 @@ def create_fixed_borders(state, store, side):
     the z lists, so corners are mirrored again, as in the reference."""
     dim = int(get_state(state, "dim"))
     ib, lo, hi, bmin, bmax = _inside_border(state, store, dim)
-    rows = [store]
     k0 = store.shape[0]
-    new = []
+    blocks = []  # positions of the new rows, in creation order
+    nnew = 0
+    rx = col("rx")
 
     def mirror(pi_rows, axis, wall, later):
-        for pi in pi_rows:
-            src = store[pi] if pi < k0 else new[pi - k0]
-            row = np.zeros(consts.ES_TOTAL)
-            row[col("rx"):col("rz") + 1] = src[col("rx"):col("rz") + 1]
-            row[col("rx") + axis] = wall + (wall - row[col("rx") + axis])
-            row[col("type")] = ept["fixed"]
-            k = k0 + len(new)
-            new.append(row)
-            for a in later:
-                if row[col("rx") + a] < bmin[a]:
-                    ib["xyz"[a] + "1"].append(k)
-                elif row[col("rx") + a] > bmax[a]:
-                    ib["xyz"[a] + "2"].append(k)
+        # one side at a time, in list order: the images of the rows in this
+        # side's strip, and their indices appended to the later strips'
+        # lists in creation order
+        nonlocal nnew
+        if not len(pi_rows):
+            return
+        allpos = np.concatenate([store[:, rx:rx + 3]] + blocks) if blocks else store[:, rx:rx + 3]
+        p = allpos[np.asarray(pi_rows, dtype=np.int64)].copy()
+        p[:, axis] = wall + (wall - p[:, axis])
+        k = k0 + nnew + np.arange(p.shape[0])
+        for a in later:
+            ib["xyz"[a] + "1"].extend(k[p[:, a] < bmin[a]].tolist())
+            ib["xyz"[a] + "2"].extend(k[~(p[:, a] < bmin[a]) & (p[:, a] > bmax[a])].tolist())
+        blocks.append(p)
+        nnew += p.shape[0]
 
     if side in (ebc["all"], ebc["x"]):
         later = [a for a in (1, 2) if a < dim]
@@ -208,10 +209,13 @@ def create_fixed_borders(state, store, side):
         if dim == 3 and side in (ebc["all"], ebc["z"]):
             mirror(ib["z1"], 2, lo[2], [])
             mirror(ib["z2"], 2, hi[2], [])
-    if new:
-        rows.append(np.array(new))
-    out = np.concatenate(rows, axis=0)
-    set_state(state, "fixedpn", get_state(state, "fixedpn") + len(new))
+    out = store
+    if blocks:
+        new = np.zeros((nnew, consts.ES_TOTAL))
+        new[:, rx:rx + 3] = np.concatenate(blocks)
+        new[:, col("type")] = ept["fixed"]
+        out = np.concatenate([store, new], axis=0)
+    set_state(state, "fixedpn", get_state(state, "fixedpn") + nnew)
     return out
 
 
