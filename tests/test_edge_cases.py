@@ -62,3 +62,21 @@ def test_list_overflow_is_redone(oracle_lib, engine_lib, cuda_ok, prec):
     assert neighbour_sets_equal(nb_got, nb_ref)
     for f in ("den", "h", "om"):
         assert rel_particle(got[:, COL[f]], ref[:, COL[f]]) <= TOL[prec], f
+
+
+def test_fixedreal_copies_run_like_the_oracle(oracle_lib, engine_lib, cuda_ok, tmp_path):
+    """The runner/006.1 set-up (borderless 1D colliding flows with periodic
+    fixedreal copies of the border strips: integrated rows that are not
+    centres) run to t = 0.02 on both engines, FP64."""
+    from tests.test_driver import _runner_006_sequence
+    c = _runner_006_sequence(tmp_path)
+    out = []
+    for lib in (oracle_lib, engine_lib):
+        with abi.Engine(c.state, c.store, "m6", lib=lib) as e:
+            e.run_to(0.02)
+            out.append((e.get_store(), e.get_state()))
+    (s0, t0), (s1, t1) = out
+    assert t0[45] == t1[45]  # same time reached
+    for f in ("den", "u", "h"):
+        assert rel_particle(s1[:, COL[f]], s0[:, COL[f]]) <= 1e-9, f
+    np.testing.assert_allclose(s1[:, 0], s0[:, 0], rtol=0, atol=1e-11)
