@@ -376,8 +376,8 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
 // (almost always the whole group); for every row of cells that the segment's
 // spheres reach, the x-extent of the union of the spheres selects a run of
 // cells, which is one contiguous range of the sorted particles.  The group
-// stages up to 8G ranges in shared memory with a prefix of their lengths and
-// walks their concatenation G candidates at a time: every lane loads one
+// stages the ranges of RPL G rows at a time (a chunk) in shared memory with a
+// prefix of their lengths and walks their concatenation G candidates at a time: every lane loads one
 // candidate (coalesced) into shared memory, then every lane tests all G of
 // them against its own centre and appends the hits to its centre's list.  A
 // candidate is fetched once for the G centres, and no lane computes a range
@@ -393,7 +393,8 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
 // near the surface, so delta = 8 e / R + 4 (e / R)^2 + 1e-6 bounds it.  Only
 // the candidates with |sd32 - R^2| <= delta R^2 are tested in FP64; the FP64
 // test alone decides membership, so the sets equal the FP64 predicate's.
-constexpr int kNeibRowsPerLane = 6;
+constexpr int kNeibRowsPerLane = 2;  // RPL: rows of cells per lane and chunk (measured
+                                     // best of 1-8 on the 128^3 Sedov step)
 
 // minimum / maximum over the G lanes of a group (all lanes of the warp call)
 template <int G>
