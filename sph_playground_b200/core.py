@@ -136,7 +136,7 @@ class Context:
     def _out(self, name):
         return os.path.join(self.pwd, "output", name)
 
-    def SimpleRun(self):
+    def SimpleRun(self, lib=None):
         """./execute --key value ... with tfinish = 0: fillargs + place + dump."""
         s = self.setup.__dict__
         get = lambda k, d=None: s.get(k, d)
@@ -164,7 +164,7 @@ class Context:
         if int(ic.get_state(state, "ics")) == consts.ICS["none"]:
             store = icsetup.place(state, kernel)
         else:
-            store = icsetup.setup_v2(state, kernel, cv=1.0)
+            store = icsetup.setup_v2(state, kernel, cv=1.0, lib=lib)
         tf = ic.get_state(state, "tfinish")
         npics = max(int(ic.get_state(state, "npics")), 1)
         ic.set_state(state, "dtprint", tf / npics if tf > 0 else 1.0)
@@ -173,12 +173,14 @@ class Context:
         write_dump(self._out("dump_full.h5"), state, store)
         self.__tolog__("CMD [./execute " + " ".join(self.setup.toArgs()) + "] EXECUTED")
 
-    def CleanRun(self):
+    def CleanRun(self, lib=None):
+        """(lib: the engine library for the mti set-ups' density pass; the
+        CUDA engine when not given)"""
         out = os.path.join(self.pwd, "output")
         if os.path.isdir(out):
             shutil.rmtree(out)
         os.makedirs(out, exist_ok=True)
-        self.SimpleRun()
+        self.SimpleRun(lib)
 
     def CleanFinalDumps(self):
         for n in ("finaldump", "fulldump"):

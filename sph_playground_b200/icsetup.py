@@ -247,12 +247,12 @@ def place(state, kernel="m6", seed=None):
     return uniform_v4(state, box, dbsz, spacing, padding=0.5)
 
 
-def setup_v2(state, kernel="m6", cv=1.0, seed=None):
+def setup_v2(state, kernel="m6", cv=1.0, seed=None, lib=None):
     """setupV2 (IC/IC.f90:48-560) for the initial-condition type in the
-    state: lattice, fixed walls, fields.  Types whose set-up needs more
-    than placement and field formulas (mti, mtilowres: a stretch-mapped
-    density profile and a density pass) raise NotImplementedError; sin3
-    stops in the reference ("Not set yet") and raises ValueError here."""
+    state: lattice, fixed walls, fields.  The mti types end with a density
+    pass over every row (IC.f90:597-606), run by the engine library `lib`
+    (the CUDA engine by default).  sin3 stops in the reference ("Not set
+    yet") and raises ValueError here."""
     dim = int(get_state(state, "dim"))
     n2, n3 = _nulls(dim)
     hfac = get_state(state, "hfac")
@@ -276,8 +276,26 @@ def setup_v2(state, kernel="m6", cv=1.0, seed=None):
     fixed_side = None
     if ivt == ett["sin3"]:
         raise ValueError("sin3: Not set yet (IC.f90:103)")
-    elif ivt in (ett["mti"], ett["mtilowres"]):
-        raise NotImplementedError("mti / mtilowres set-up (stretch-mapped profile) is not built")
+    elif ivt == ett["mti"]:  # IC.f90:160-177
+        set_state(state, "dcondconst", 0.01)
+        rho1, gamma = 1.0, 5.0 / 3.0
+        b1, b2 = 0.0, 1.0 / 10.0
+        resol, pspc1 = res_from(b1, b2)
+        pspc2 = pspc1
+        box = (b1, b2, 0.0, n2 * 1.0 / 10.0, 0.0, n3 * 1.0 / 10.0)
+        bsz = nb * pspc2
+        store = uniform_v4(state, box, bsz, pspc1, padding=0.5)
+        store = create_fixed_borders(state, store, ebc["y"])
+        # the Hopkins (2017) profile rho(y) = 2 (3 - y)^(1 - g h), g = -1, h = 3
+        stretch_map(store, box[2] - bsz, box[3] + bsz, lambda y: 2.0 * (3.0 - y) ** 4, axis=1)
+    elif ivt == ett["mtilowres"]:  # IC.f90:178-205
+        set_state(state, "dcondconst", 0.1)
+        rho1, gamma = 1.0, 5.0 / 3.0
+        b1, b2 = -1.0, 1.0
+        resol, pspc1 = res_from(b1, b2)
+        pspc2 = pspc1
+        box = (b1, b2, -2.0, 2.0, 0.0, n3 * 1.0)
+        store = uniform_v4(state, box, nb * pspc2, pspc1, padding=0.5)
     elif ivt == ett["shock12"]:
         rho1, prs1, gamma = 1.0, 1.0, 5.0 / 3.0
         b1, b2 = -1.0, 1.0
@@ -464,5 +482,99 @@ def setup_v2(state, kernel="m6", cv=1.0, seed=None):
             -0.5 * (x * x + y * y + z * z) / (1.0 / 3.0) ** 2)
         s[:, C("u")] = prs1 / (gamma - 1.0) / rho1
         s[:, C("kappa")] = 0.1
+    elif ivt in (ett["mti"], ett["mtilowres"]):  # IC.f90:507-537
+        s[:, C("h")] = hfac * sp
+        s[:, C("m")] = sp ** dim * rho1
+        s[:, C("den")] = rho1
+        yy = y if ivt == ett["mti"] else np.abs(y)
+        s[:, C("u")] = (3.0 / 2.0) * (1.0 - yy / 3.0)
+        s[:, C("t")] = s[:, C("u")]
+        s[:, C("p")] = (gamma - 1.0) * s[:, C("den")] * s[:, C("u")]
+        s[:, C("vx")] = s[:, C("vy")] = s[:, C("vz")] = 0.0
+        s[:, C("bx")] = s[:, C("by")] = s[:, C("bz")] = 0.0
+        if ivt == ett["mti"]:
+            r2 = x * x + y * y + z * z
+            kick = (r2 > 0) & (s[:, C("type")] == ept["real"])
+            s[kick, C("vy")] = 1e-2 * np.sqrt(gamma * s[kick, C("p")] / s[kick, C("den")]) * \
+                np.sin(4.0 * pi * x[kick] / (box[1] - box[0]))
+        s[:, C("bx")] = 1e-11
+        s = _mti_density_pass(state, s, kernel, lib)
     del xmn, xmx
     return s
+
+
+def stretch_map(store, cmin, cmax, rhofunc, axis=1, ngrid=1024, tol=1e-9, maxits=100,
+                maxits_nr=30):
+    """Stretch mapping of a uniform arrangement onto the density profile
+    rhofunc along one axis (Price 2004, the cartesian form used by
+    set_density_profile, utils/stretchmap.f90): a particle at c moves to c'
+    with M(c') = rho0 (c - cmin), M(c) the mass of the profile between cmin
+    and c and rho0 = M(cmax) / (cmax - cmin).  M is the trapezoid rule on
+    ngrid steps with the first step's left end taken as 0, as the
+    reference integrates; the root is found by Newton steps held within
+    0.8-1.2 of the previous iterate, falling back to bisection, until
+    |M(c') - rho0 (c - cmin)| <= tol M(cmax).  Moves positions in place."""
+
+    def mass(x):  # x: array of end points
+        dx = (x - cmin) / ngrid
+        xi = cmin + dx[:, None] * np.arange(1, ngrid + 1)[None, :]
+        d = rhofunc(xi) * dx[:, None]
+        return d.sum(axis=1) - 0.5 * d[:, -1]
+
+    totmass = float(mass(np.array([cmax]))[0])
+    rhozero = totmass / (cmax - cmin)
+    c = store[:, col("rx") + axis]
+    for lo in range(0, c.shape[0], 4096):
+        idx = np.arange(lo, min(lo + 4096, c.shape[0]))
+        xold = c[idx]
+        act = xold > cmin
+        f0 = rhozero * (xold - cmin)
+        xi = xold.copy()
+        func = np.where(act, mass(np.where(act, xi, cmax)) - f0, 0.0)
+        blo, bhi = np.full_like(xi, cmin), np.full_like(xi, cmax)
+        bis = np.zeros(xi.shape, dtype=bool)
+        its = np.zeros(xi.shape, dtype=int)
+        run = act & (np.abs(func / totmass) > tol)
+        while run.any():
+            r = np.nonzero(run)[0]
+            xprev = xi[r]
+            its[r] += 1
+            fr = mass(xprev) - f0[r]
+            dfr = rhofunc(xprev)
+            nb_ = bis[r]
+            # bisection where it has taken over
+            bl, bh = blo[r], bhi[r]
+            bh = np.where(nb_ & (fr > 0), xprev, bh)
+            bl = np.where(nb_ & ~(fr > 0), xprev, bl)
+            xb = 0.5 * (bl + bh)
+            # Newton elsewhere, its step held within 0.8-1.2 of the previous
+            xn = xprev - fr / dfr
+            ax, ap = np.abs(xn), np.abs(xprev)
+            xn = np.where(ax < 0.8 * ap, 0.8 * xprev, np.where(ax > 1.2 * ap, 1.2 * xprev, xn))
+            fail = ~nb_ & ((xn > cmax) | (xn < cmin) | (its[r] > maxits_nr))
+            newbis = nb_ | fail
+            xnew = np.where(nb_, xb, np.where(fail, 0.5 * (bl + bh), xn))
+            xi[r], blo[r], bhi[r], bis[r] = xnew, bl, bh, newbis
+            func[r] = fr
+            run = act & (np.abs(func / totmass) > tol) & (its < maxits)
+        if np.any(act & (its >= maxits)):
+            raise ValueError("set_density_profile: Stretch mapping not converged")
+        c[idx] = np.where(act, xi, xold)
+    store[:, col("rx") + axis] = c
+
+
+def _mti_density_pass(state, store, kernel, lib):
+    """IC.f90:597-606: every row counted as real for one density pass with
+    periodic images along x (the mti types' boundary), then the numbers of
+    real and fixed rows restored."""
+    from . import abi
+    rpn, fpn = int(get_state(state, "realpn")), int(get_state(state, "fixedpn"))
+    st = state.copy()
+    set_state(st, "realpn", rpn + fpn)
+    set_state(st, "fixedpn", 0)
+    # the process whose boundary for these types is periodic along x alone
+    # (iterator.f90:99-110), as the set-up's createPeriodicBorder(ebc_x)
+    set_state(st, "process", consts.epc["backcompatibility"])
+    with abi.Engine(st, store, kernel, lib=lib if lib is not None else abi.load()) as e:
+        e.density()
+        return e.get_store()

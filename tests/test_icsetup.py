@@ -135,3 +135,43 @@ def test_gpu_hydroshock_with_fixed_walls_matches_oracle(engine_lib, oracle_lib, 
     np.testing.assert_allclose(s1[:, COL["den"]], s0[:, COL["den"]], rtol=1e-9)
     np.testing.assert_allclose(s1[:, :3], s0[:, :3], rtol=0, atol=1e-11)
     assert l1 == pytest.approx(l0, rel=1e-9)
+
+
+def test_mti_setups_on_the_oracle(oracle_lib):
+    """mti: the stretch map gives the lattice the Hopkins (2017) profile
+    rho ~ (3 - y)^4 (the density the closing pass finds follows its slope);
+    mtilowres: no walls, so the closing pass (periodic along x only) finds
+    the density falling off at the y edges.  Both end with the real / fixed
+    row counts of the lattice."""
+    st = ic.make_state(2, ics="mti", resolution=32, process="backcompatibility")
+    s = icsetup.setup_v2(st, "m6", lib=oracle_lib)
+    rpn, fpn = int(ic.get_state(st, "realpn")), int(ic.get_state(st, "fixedpn"))
+    assert fpn > 0 and s.shape[0] == rpn + fpn
+    r = s[:rpn]
+    y, d = r[:, 1], r[:, COL["den"]]
+    mid = (y > 0.02) & (y < 0.08)
+    prof = (3 - y[mid]) ** 4
+    slope = np.polyfit(y[mid], d[mid], 1)[0]
+    want = np.polyfit(y[mid], prof / prof.mean() * d[mid].mean(), 1)[0]
+    assert slope == pytest.approx(want, rel=0.05)
+    assert np.all(r[:, COL["bx"]] == 1e-11) and np.any(r[:, COL["vy"]] != 0)
+    st2 = ic.make_state(2, ics="mtilowres", resolution=32, process="backcompatibility")
+    s2 = icsetup.setup_v2(st2, "m6", lib=oracle_lib)
+    assert int(ic.get_state(st2, "fixedpn")) == 0
+    y2, d2 = s2[:, 1], s2[:, COL["den"]]
+    assert d2[np.abs(y2) > 1.9].mean() < 0.9 * d2[np.abs(y2) < 1.0].mean()
+
+
+def test_stretch_map_inverts_the_mass_function():
+    """A particle at c lands where the profile's mass from cmin equals
+    rho0 (c - cmin), the mass being the reference's trapezoid on 1024 steps
+    with the first left end taken as 0: M(x) = x + x^3 - rho(0) x / 2048
+    up to the O(dx^2) trapezoid error."""
+    store = np.zeros((50, consts.ES_TOTAL))
+    store[:, 1] = np.linspace(0.01, 0.99, 50)
+    rho = lambda y: 1.0 + 3.0 * y * y  # noqa: E731
+    icsetup.stretch_map(store, 0.0, 1.0, rho, axis=1)
+    y = store[:, 1]
+    m = lambda x: x + x ** 3 - x / 2048.0  # noqa: E731
+    np.testing.assert_allclose(m(y), m(1.0) * np.linspace(0.01, 0.99, 50), rtol=2e-6)
+
