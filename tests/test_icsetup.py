@@ -137,6 +137,21 @@ def test_gpu_hydroshock_with_fixed_walls_matches_oracle(engine_lib, oracle_lib, 
     assert l1 == pytest.approx(l0, rel=1e-9)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("ics", ["mti", "mtilowres"])
+def test_gpu_mti_setup_density_pass_matches_oracle(engine_lib, oracle_lib, cuda_ok, ics):
+    """The set-up's closing density pass on the CUDA engine (FP64) and on the
+    oracle: the same lattice, the same den / h / om."""
+    out = []
+    for lib in (oracle_lib, engine_lib):
+        st = ic.make_state(2, ics=ics, resolution=32, process="backcompatibility")
+        out.append(icsetup.setup_v2(st, "m6", lib=lib))
+    s0, s1 = out
+    np.testing.assert_array_equal(s1[:, :3], s0[:, :3])
+    for f in ("den", "h", "om"):
+        np.testing.assert_allclose(s1[:, COL[f]], s0[:, COL[f]], rtol=1e-9, err_msg=f)
+
+
 def test_mti_setups_on_the_oracle(oracle_lib):
     """mti: the stretch map gives the lattice the Hopkins (2017) profile
     rho ~ (3 - y)^4 (the density the closing pass finds follows its slope);
