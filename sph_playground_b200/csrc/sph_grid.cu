@@ -492,24 +492,24 @@ k_neighbours(NeibArgs a) {
     const int64_t room = a.nl_size - off;
     rcap = room <= 0 ? 0 : (room < int64_t(rcap0) ? int(room) : rcap0);
   }
-  int cnt = 0;   // hits written to the list
+  int cnt = 0;   // hits found so far (written to the list while they fit)
   int nheld = 0;  // hits waiting in held[threadIdx.x]
-  int32_t* const row = a.nl + off;
+  int32_t* dst = a.nl + off;  // the list slot of hit number cnt
   int32_t* const mine_held = held[threadIdx.x];
   int32_t* const warp_held = held[threadIdx.x & ~31];
   // writes the held hits of the lanes in `who` to their lists, all 32
-  // lanes of the warp carrying one lane's run at a time
+  // lanes of the warp carrying one lane's run at a time; a lane's run is
+  // cut at its row's capacity (the hits past it are only counted)
   auto flush = [&](unsigned who) {
+    const int nw = max(0, min(nheld, rcap - cnt));
     __syncwarp();
     while (who) {
       const int L = __ffs(who) - 1;
       who &= who - 1u;
-      const int nL = __shfl_sync(FULL, nheld, L);
-      const int baseL = __shfl_sync(FULL, cnt, L);
-      const int capL = __shfl_sync(FULL, rcap, L);
-      int32_t* const rowL = reinterpret_cast<int32_t*>(
-          __shfl_sync(FULL, reinterpret_cast<unsigned long long>(row), L));
-      if (wl < nL && baseL + wl < capL) rowL[baseL + wl] = warp_held[L * 33 + wl];
+      const int nL = __shfl_sync(FULL, nw, L);
+      int32_t* const dL = reinterpret_cast<int32_t*>(
+          __shfl_sync(FULL, reinterpret_cast<unsigned long long>(dst), L));
+      if (wl < nL) __stcg(dL + wl, warp_held[L * 33 + wl]);
     }
     __syncwarp();
   };
@@ -678,6 +678,7 @@ k_neighbours(NeibArgs a) {
           flush(full);
           if ((full >> wl) & 1u) {
             cnt += nheld;
+            dst += nheld;
             nheld = 0;
           }
         }
