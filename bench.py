@@ -21,6 +21,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -88,7 +89,8 @@ class Clocks:
     def __init__(self, uuid):
         self.uuid = uuid
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(os.environ.get("SPH_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
