@@ -177,6 +177,21 @@ def test_mti_setups_on_the_oracle(oracle_lib):
     assert d2[np.abs(y2) > 1.9].mean() < 0.9 * d2[np.abs(y2) < 1.0].mean()
 
 
+def test_context_cleanrun_mti_on_oracle(oracle_lib, tmp_path):
+    """Context.CleanRun with ics = mti writes the set-up, density pass
+    included, to output/dump_full.h5, which reads back unchanged."""
+    c = core.Context(pwd=str(tmp_path))
+    s = c.setup
+    s.kernel, s.dim, s.equations, s.hfac, s.tfinish = "m6", 2, "hydro", 1.2, 0.0
+    s.resolution, s.nsnapshots, s.ics, s.process = 32, 1, "mti", "backcompatibility"
+    c.CleanRun(lib=oracle_lib)
+    direct = icsetup.setup_v2(c.state.copy(), "m6", lib=oracle_lib)
+    c.ReadDumpHDF(os.path.join(str(tmp_path), "output", "dump_full.h5"))
+    assert c.store.shape == direct.shape
+    assert int(c.GetState("fixedpn")) > 0
+    np.testing.assert_array_equal(c.store[:, COL["den"]], direct[:, COL["den"]])
+
+
 def test_stretch_map_inverts_the_mass_function():
     """A particle at c lands where the profile's mass from cmin equals
     rho0 (c - cmin), the mass being the reference's trapezoid on 1024 steps
