@@ -45,6 +45,27 @@ F2_C2 = 150.0
 # neighbour index, 4 B, plus the gathered pair data that misses L2); the
 # traffic scales with the pairs a launch processes
 C2_DRAM_BYTES_PER_PAIR = (849.04e6 + 73.09e6) / 157.49e6
+# DRAM bytes per in-support pair of the neighbour search (k_neighbours),
+# same capture workload: 198.36 MB read + 684.48 MB written over 157.49M
+# pairs; the search's algorithmic bytes are the 4 B list entry per pair it
+# writes plus its per-centre reads and writes (FP32 image 16 B, h 8 B, row
+# offset / capacity 12 B, count 4 B)
+SEARCH_DRAM_BYTES_PER_PAIR = (198.36e6 + 684.48e6) / 157.49e6
+SEARCH_BYTES_PER_PAIR = 4.0
+SEARCH_BYTES_PER_CENTRE = 40.0
+# per-particle FLOP per step (Newton update, EOS, epilogue, leapfrog)
+F_PARTICLE = 100.0
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth of this pool's B200s when
+    the peaks file is present, else the stated fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s (no measured peaks file)"
 
 
 def parse():
@@ -66,7 +87,14 @@ def parse():
     ap.add_argument("--no-errors", action="store_true",
                     help="skip the FP32-vs-FP64 error check (profiling runs)")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-n", type=int, default=64, help="lattice per axis of the CPU sample")
+    ap.add_argument("--cpu-n", type=int, default=128,
+                    help="lattice per axis of the CPU baseline and the reference arm")
+    ap.add_argument("--no-oracle-errors", action="store_true",
+                    help="skip the errors against the CPU oracle at the bench size")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 21-instance diffusion batch (config 3)")
+    ap.add_argument("--no-160", action="store_true",
+                    help="skip the 160^3 Sedov throughput line (config 5b)")
     ap.add_argument("--param", action="append", default=[],
                     help="engine parameter NAME=VALUE (abi.P_* name or slot), for both arms")
     return ap.parse_args()
@@ -164,10 +192,98 @@ def cpu_baseline(n):
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": store.shape[0] / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"sedov3d {n}^3 ({store.shape[0]} particles), 1 leapfrog step after the "
-                      f"start-up iterate, CPU oracle (FP64, OpenMP {cores} threads)"}
+                      f"start-up iterate, CPU oracle (FP64, OpenMP {cores} threads)",
+            "same_config": True}
+
+
+def field_report(got, ref):
+    """rho, h per particle and a, du/dt, dh/dt relative to the field's
+    largest magnitude (max and 99.9th percentile)."""
+    C = {k: v - 1 for k, v in abi.consts.es.items()}
+    out = {}
+    for name in ("den", "h"):
+        rel = np.abs(got[:, C[name]] - ref[:, C[name]]) / np.abs(ref[:, C[name]])
+        out["rho" if name == "den" else name] = {"max": float(rel.max()),
+                                                 "p99.9": float(np.quantile(rel, 0.999))}
+    for name, cols in (("a", [C["ax"], C["ay"], C["az"]]), ("du", [C["du"]]),
+                       ("dh", [C["dh"]])):
+        d = np.linalg.norm(got[:, cols] - ref[:, cols], axis=1)
+        scale = np.linalg.norm(ref[:, cols], axis=1).max()
+        rel = d / scale if scale > 0 else d
+        out[name + "_rel_field_max"] = {"max": float(rel.max()),
+                                        "p99.9": float(np.quantile(rel, 0.999))}
+    return out
+
+
+def batch_block(lib, tfinish=0.01):
+    """Config 3: the anisotropic diffusion sweep, 7 lattices (32^2 .. 256^2)
+    x 3 second-derivative methods (fab, n2w, 2nw_ds) = 21 uneven instances,
+    fixed-stage STS to t = 0.01, stepped together as one batch; the batch's
+    host-clock time per precision and the L2 error of T against the analytic
+    exponential decay for every instance."""
+    from sph_playground_b200 import ic
+    sizes = (32, 48, 64, 96, 128, 192, 256)
+    methods = ("fab", "n2w", "2nw_ds")
+    sets = [(n, ddw, ic.diffusion2d(n, ddw=ddw, tfinish=tfinish)) for ddw in methods
+            for n in sizes]
+    C = {k: v - 1 for k, v in abi.consts.es.items()}
+    out = {"workload": "diffusion2d n^2 for n in 32..256 x ddw fab / n2w / 2nw_ds, "
+                       f"k_par b b^T diagonal form, STS 8 stages, to t = {tfinish}",
+           "instances": len(sets), "particles": int(sum(n * n for n, _, _ in sets))}
+    for prec, name in ((abi.PREC_FP64, "fp64"), (abi.PREC_FP32_COMP, "fp32_comp")):
+        # warm-up of the kernels and graphs on a short batch
+        eng = [abi.Engine(st, store, "m6", precision=prec, lib=lib) for _, _, (st, store) in sets]
+        with abi.Batch(eng) as b:
+            b.step(2)
+        for e in eng:
+            e.close()
+        eng = [abi.Engine(st, store, "m6", precision=prec, lib=lib) for _, _, (st, store) in sets]
+        t0 = time.perf_counter()
+        with abi.Batch(eng) as b:
+            b.run_to(tfinish)
+        el = time.perf_counter() - t0
+        l2, steps = {}, 0
+        for (n, ddw, _), e in zip(sets, eng):
+            s = e.get_store()
+            t = e.get_state()[abi.consts.ec["time"] - 1]
+            exact = ic.diffusion_exact(s[:, 0:3], t)
+            l2[f"{ddw}_{n}"] = float(np.sqrt(np.mean((s[:, C["t"]] - exact) ** 2)))
+            steps += e.counters()["steps"] * n * n
+            e.close()
+        out[name] = {"seconds": el, "particle_steps_per_s": steps / el, "l2_vs_analytic": l2}
+    out["timing"] = "host clock around the synchronous sph_batch_run_to call"
+    return out
+
+
+def size160_block(engine, st, store, steps, warmup):
+    """Config 5b: the Sedov step at 160^3 = 4,096,000 particles, FP32-comp
+    and FP64, device time of `steps` steps after `warmup` steps."""
+    out = {"workload": workload_name(160)}
+    N = store.shape[0]
+    for prec, name in ((abi.PREC_FP32_COMP, "fp32_comp"), (abi.PREC_FP64, "fp64")):
+        e = engine(prec, st, store)
+        e.set_param(abi.consts.ec["tfinish"], 1.0)
+        for _ in range(warmup):
+            e.step(1)
+        ms, cnt, tm = timed_steps(e, steps)
+        e.close()
+        out[name] = {"value": N * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                     "phases_ms_per_step": tm}
+    out["speedup_fp32_vs_fp64"] = out["fp32_comp"]["value"] / out["fp64"]["value"]
+    return out
+
+
+def workload_name(n):
+    return (f"sedov3d {n}^3 ({n ** 3} particles), M6 hfac 1.2, full leapfrog step "
+            "(timestep, predictor, images, neighbour lists, circuit1, circuit2, corrector)")
 
 
 def run_reference(args, ws, rank):
+    """The reference arm: the CPU oracle (the C++ FP64 OpenMP restatement of
+    the reference engine's path; the Fortran itself cannot be built without
+    gfortran and HDF5) on the same workload as the GPU arm, all host
+    threads, `warmup` untimed steps and `steps` timed steps after the
+    start-up iterate."""
     if rank != 0:
         return
     from sph_playground_b200 import ic
@@ -190,10 +306,11 @@ def run_reference(args, ws, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"sedov3d {n}^3 ({N} particles) sample of the 128^3 Sedov step, "
-                               "M6 hfac 1.2, full leapfrog step",
-                   "particles": N, "note": "reference Fortran not compiled (no gfortran/HDF5 "
-                   "in the image); the CPU oracle restatement of its path is timed instead"},
+        "config": {"workload": workload_name(n), "particles": N, "same_config": n == args.n,
+                   "note": "reference Fortran not compiled (no gfortran/HDF5 in the image); "
+                           "the CPU oracle restatement of its path is timed instead; its "
+                           "search is a uniform cell grid, not the reference's per-step "
+                           "kd-tree, so it is likely faster than the Fortran would be"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"sedov3d {n}^3, {args.steps} steps after {args.warmup} warm-up"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -240,16 +357,17 @@ def adjoint_block(lib, n=256, n_ref=64, nsteps=200, every=20, dt=5e-4):
             "timing": "host clock around synchronous C-ABI calls"}
 
 
-def density_block(lib, shapes, n=128, tol=1e-6, reps=5):
+def density_block(lib, shapes, n=128, tol=1e-6, reps=5, oracle=None):
     """The density-only workload: one density + Newton-h pass over a 3D
     periodic n^3 lattice perturbed by uniform(-0.1, 0.1) dx (seed 2), M6,
     hfac 1.2, Newton tolerance `tol`; FP32-comp against FP64: device time of
     the pass (CUDA events of the neighbour and circuit1 phases, averaged
-    over `reps` passes after one warm-up) and the per-particle relative
-    error of rho and h."""
+    over `reps` passes after one warm-up), its phases, and the per-particle
+    relative error of rho and h against the FP64 path and, when `oracle` is
+    given, against the CPU oracle (with the neighbour sets' digests)."""
     from sph_playground_b200 import ic
     st, store = ic.density3d(n=n, seed=2)
-    out, res = {}, {}
+    out, res, dig = {}, {}, {}
     for prec, name in ((abi.PREC_FP64, "fp64"), (abi.PREC_FP32_COMP, "fp32_comp")):
         e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
         for k, v in shapes.get(prec, {}).items():  # the launch shapes of the step arms
@@ -257,20 +375,41 @@ def density_block(lib, shapes, n=128, tol=1e-6, reps=5):
         e.set_param(abi.P_NEWTON_TOL, tol)
         e.density()
         res[name] = e.get_store()
+        dig[name] = e.get_neighbour_digest()
         e.reset_counters()
         e.set_param(abi.P_TIMING, 1)
         for _ in range(reps):
             e.set_store(store)
             e.density()
         t = e.timers()
+        c = e.counters()
         e.close()
-        ms = sum(t[k] for k in ("ghosts", "sort", "neighbours", "pack", "circuit1")) / reps
-        out[name] = {"ms_per_pass": ms, "particle_passes_per_s": store.shape[0] / (ms * 1e-3)}
+        ph = {k: t[k] / reps for k in ("ghosts", "sort", "neighbours", "pack", "circuit1")}
+        ms = sum(ph.values())
+        out[name] = {"ms_per_pass": ms, "particle_passes_per_s": store.shape[0] / (ms * 1e-3),
+                     "phases_ms": ph,
+                     "newton_sweeps_per_particle": c["c1_centre_sweeps"] / (reps * store.shape[0])}
     C = {k: v - 1 for k, v in abi.consts.es.items()}
     for f in ("den", "h"):
         rel = np.abs(res["fp32_comp"][:, C[f]] - res["fp64"][:, C[f]]) / np.abs(res["fp64"][:, C[f]])
         out[("rho" if f == "den" else f) + "_rel_err"] = {"max": float(rel.max()),
                                                         "p99.9": float(np.quantile(rel, 0.999))}
+    if oracle is not None:
+        with abi.Engine(st, store, "m6", lib=oracle) as o:
+            o.set_param(abi.P_NEWTON_TOL, tol)
+            o.density()
+            ref, dref = o.get_store(), o.get_neighbour_digest()
+        vs = {}
+        for name in ("fp64", "fp32_comp"):
+            r = {}
+            for f in ("den", "h", "om"):
+                rel = np.abs(res[name][:, C[f]] - ref[:, C[f]]) / np.abs(ref[:, C[f]])
+                r[{"den": "rho", "h": "h", "om": "omega"}[f]] = {
+                    "max": float(rel.max()), "p99.9": float(np.quantile(rel, 0.999))}
+            r["neighbour_sets_equal"] = bool(np.array_equal(dig[name][0], dref[0]) and
+                                             np.array_equal(dig[name][1], dref[1]))
+            vs[name] = r
+        out["errors_vs_oracle"] = vs
     out["fp32_over_fp64_speed"] = out["fp64"]["ms_per_pass"] / out["fp32_comp"]["ms_per_pass"]
     out["workload"] = (f"density3d {n}^3 ({store.shape[0]} particles), perturbed lattice, M6 hfac 1.2, "
                        f"Newton tolerance {tol}, one density pass (images, sort, search, circuit1)")
@@ -345,32 +484,35 @@ def main():
             e.set_param(int(k) if k.isdigit() else getattr(abi, k, k), float(v))
         return e
 
+    oracle = None
+    if rank == 0 and not args.no_oracle_errors:
+        oracle = abi.load(os.path.join(ROOT, "oracle", "liboracle.so"))
+
     def field_errors(st_, store_):
-        """FP32-comp vs FP64: one iterate on the same state; rho and h per
-        particle, a / du/dt / dh/dt per particle relative to the field's
-        largest magnitude (a lattice at rest has a ~ 0 almost everywhere)."""
-        e32, e64 = engine(abi.PREC_FP32_COMP, st_, store_), engine(abi.PREC_FP64, st_, store_)
-        e32.iterate()
-        e64.iterate()
-        r32, r64 = e32.get_store(), e64.get_store()
-        e32.close()
-        e64.close()
-        C = {k: v - 1 for k, v in abi.consts.es.items()}
-        out = {}
-        for name in ("den", "h"):
-            rel = np.abs(r32[:, C[name]] - r64[:, C[name]]) / np.abs(r64[:, C[name]])
-            out["rho" if name == "den" else name] = {"max": float(rel.max()),
-                                                     "p99.9": float(np.quantile(rel, 0.999))}
-        for name, cols in (("a", [C["ax"], C["ay"], C["az"]]), ("du", [C["du"]]),
-                           ("dh", [C["dh"]])):
-            d = np.linalg.norm(r32[:, cols] - r64[:, cols], axis=1)
-            ref = np.linalg.norm(r64[:, cols], axis=1).max()
-            rel = d / ref if ref > 0 else d
-            out[name + "_rel_field_max"] = {"max": float(rel.max()),
-                                            "p99.9": float(np.quantile(rel, 0.999))}
+        """One iterate on the same state: FP32-comp against FP64 on the GPU
+        and, with the oracle, both GPU paths against the CPU FP64 oracle
+        (rho and h per particle; a, du/dt, dh/dt relative to the field's
+        largest magnitude, since a lattice at rest has a ~ 0 almost
+        everywhere) with the neighbour sets' digests."""
+        res, dig = {}, {}
+        for prec, name in ((abi.PREC_FP32_COMP, "fp32_comp"), (abi.PREC_FP64, "fp64")):
+            e = engine(prec, st_, store_)
+            e.iterate()
+            res[name], dig[name] = e.get_store(), e.get_neighbour_digest()
+            e.close()
+        out = {"fp32_vs_fp64": field_report(res["fp32_comp"], res["fp64"])}
+        if oracle is not None:
+            with abi.Engine(st_, store_, "m6", lib=oracle) as o:
+                o.iterate()
+                ref, dref = o.get_store(), o.get_neighbour_digest()
+            for name in ("fp32_comp", "fp64"):
+                r = field_report(res[name], ref)
+                r["neighbour_sets_equal"] = bool(np.array_equal(dig[name][0], dref[0]) and
+                                                 np.array_equal(dig[name][1], dref[1]))
+                out[name + "_vs_oracle"] = r
         return out
 
-    # FP32 vs FP64 errors on the bench input and after the warm-up steps
+    # errors on the bench input and after the warm-up steps
     errs, rho_err = None, None
     if not args.no_errors:
         errs = {"t0": field_errors(st, store)}
@@ -380,7 +522,8 @@ def main():
         mid_store, mid_st = e64.get_store(), e64.get_state()
         e64.close()
         errs[f"after_{max(args.warmup, 1)}_steps"] = field_errors(mid_st, mid_store)
-        rho_err = max((v["rho"] for v in errs.values()), key=lambda x: x["max"])
+        key = "fp32_comp_vs_oracle" if oracle is not None else "fp32_vs_fp64"
+        rho_err = max((v[key]["rho"] for v in errs.values()), key=lambda x: x["max"])
 
     def run(prec):
         e = engine(prec)
@@ -406,21 +549,49 @@ def main():
     e, ms, cnt, tm, clocks = run(abi.PREC_FP32_COMP)
     value = replica_throughput(ws, N, args.steps, ms)
 
-    # roofline of the dominant pair kernel: algorithmic FLOPs / its event time
-    c1_flops = cnt["c1_pairs"] * F1_C1
-    c2_flops = cnt["c2_pairs"] * F2_C2
-    kern = {"circuit1": (c1_flops / args.steps, tm["circuit1"]),
-            "circuit2": (c2_flops / args.steps, tm["circuit2"])}
-    dom = max(kern, key=lambda k: kern[k][1])
-    # (no per-phase events inside a device-resident graph step)
-    ach = kern[dom][0] / (kern[dom][1] * 1e-3) / 1e12 if kern[dom][1] > 0 else 0.0
-    traffic = C2_DRAM_BYTES_PER_PAIR * cnt["c2_pairs"] / args.steps if dom == "circuit2" else None
-    roofline = {"bound": "fp32", "kernel": dom, "achieved": ach, "peak": peak32 / 1e12,
-                "unit": "TFLOP/s", "frac": ach / (peak32 / 1e12), "traffic": traffic,
-                "traffic_source": "ncu DRAM bytes of the k_c2 capture on the Sedov 96^3 step "
-                                  "per pair, times this launch's pairs",
-                "peak_source": "live FFMA-chain probe (libsph_peak.so) on this GPU; "
-                               "MEASURED_PEAKS.json holds no non-tensor FP32 figure"}
+    # per-kernel rooflines (algorithmic work per launch / its CUDA-event time)
+    # and the step-level figure; the roofline line is the kernel that takes
+    # the most time per step
+    K = args.steps
+    hbm, hbm_src = hbm_peak()
+    p32 = peak32 / 1e12
+    kernels = {
+        "neighbours": {"bound": "hbm", "unit": "GB/s", "peak": hbm,
+                       "work": (SEARCH_BYTES_PER_PAIR * cnt["neib_pairs"] +
+                                SEARCH_BYTES_PER_CENTRE * N * cnt["searches"]) / K,
+                       "traffic": SEARCH_DRAM_BYTES_PER_PAIR * cnt["neib_pairs"] / K,
+                       "ms": tm["neighbours"],
+                       "candidate_tests_per_s": cnt["candidates"] / K / (tm["neighbours"] * 1e-3)
+                       if tm["neighbours"] > 0 else None},
+        "circuit1": {"bound": "fp32", "unit": "TFLOP/s", "peak": p32,
+                     "work": cnt["c1_pairs"] * F1_C1 / K, "traffic": None, "ms": tm["circuit1"]},
+        "circuit2": {"bound": "fp32", "unit": "TFLOP/s", "peak": p32,
+                     "work": cnt["c2_pairs"] * F2_C2 / K,
+                     "traffic": C2_DRAM_BYTES_PER_PAIR * cnt["c2_pairs"] / K, "ms": tm["circuit2"]},
+    }
+    for name, kk in kernels.items():
+        scale = 1e9 if kk["unit"] == "GB/s" else 1e12
+        kk["achieved"] = kk["work"] / (kk["ms"] * 1e-3) / scale if kk["ms"] > 0 else 0.0
+        kk["frac"] = kk["achieved"] / kk["peak"]
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    step_flops = (cnt["c1_pairs"] * F1_C1 + cnt["c2_pairs"] * F2_C2) / K + N * F_PARTICLE
+    step_ach = step_flops / ((ms / K) * 1e-3) / 1e12
+    roofline = {"bound": kernels[dom]["bound"], "kernel": dom,
+                "achieved": kernels[dom]["achieved"], "peak": kernels[dom]["peak"],
+                "unit": kernels[dom]["unit"], "frac": kernels[dom]["frac"],
+                "traffic": kernels[dom]["traffic"],
+                "step_frac": step_ach / p32, "step_achieved_tflops": step_ach,
+                "kernels": kernels,
+                "traffic_source": "ncu DRAM bytes per pair of the kernel's capture on the "
+                                  "Sedov 96^3 step, times this launch's pairs",
+                "peak_source": {"fp32": "live FFMA-chain probe (libsph_peak.so) on this GPU; "
+                                        "MEASURED_PEAKS.json holds no non-tensor FP32 figure",
+                                "hbm": hbm_src},
+                "work_definition": "fp32 kernels: in-support pairs x per-pair FLOP (circuit1 "
+                                   f"{F1_C1:.0f} per sweep, circuit2 {F2_C2:.0f}); search: 4 B per "
+                                   f"pair written + {SEARCH_BYTES_PER_CENTRE:.0f} B per centre; "
+                                   "step: both pair passes + "
+                                   f"{F_PARTICLE:.0f} FLOP per particle"}
 
     # end to end through the C-ABI with pinned host buffers, per step:
     # H2D of the particle table, one step, D2H of the particle table
@@ -464,7 +635,15 @@ def main():
     dens = None
     if not args.no_density:
         extra = dict(kv.split("=") for kv in args.param if not kv.split("=")[0].isdigit())
-        dens = density_block(lib, {p: {**tuned[p], **extra} for p in tuned})
+        dens = density_block(lib, {p: {**tuned[p], **extra} for p in tuned}, oracle=oracle)
+    batch = None
+    if not args.no_batch:
+        batch = batch_block(lib)
+    big = None
+    if not args.no_160 and args.n == 128:
+        st160, store160 = ic.sedov3d(n=160)
+        big = size160_block(engine, st160, store160, args.steps, args.warmup)
+        del st160, store160
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -476,8 +655,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"sedov3d {args.n}^3 ({N} particles), M6 hfac 1.2, "
-                                   "FP32-comp pair sums, full leapfrog step",
+            "config": {"workload": workload_name(args.n) + ", FP32-comp pair sums",
                        "particles": N, "kernel": "m6", "precision": "fp32_comp",
                        "l2": "inputs larger than L2 (particle table "
                              f"{N * 32 * 8 / 1e6:.0f} MB + pair streams)",
@@ -491,8 +669,10 @@ def main():
             "e2e": e2e,
             "gpu_launches": cnt["launches"],
             "clocks": clocks,
-            "rho_rel_err_fp32_vs_fp64": rho_err,
-            "errors_fp32_vs_fp64": errs,
+            "rho_rel_err_fp32": rho_err,
+            "rho_rel_err_fp32_reference": "the CPU FP64 oracle" if oracle is not None
+                                          else "the FP64 GPU path",
+            "errors": errs,
             "phases_ms_per_step": tm,
             "work_per_step": {"neib_pairs": cnt["neib_pairs"] / args.steps,
                               "c1_pairs": cnt["c1_pairs"] / args.steps,
@@ -506,6 +686,8 @@ def main():
             "fp64": fp64,
             "adjoint": adj,
             "density_pass": dens,
+            "diffusion_batch": batch,
+            "sedov3d_160": big,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "peak_fp32_tflops": peak32 / 1e12,
         }

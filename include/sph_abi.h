@@ -180,6 +180,15 @@ int sph_get_state(sph_handle* h, double* out49);
 int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs,
                        int64_t cap);
 
+/* Digest of the same sets for comparisons at full size, where the pair
+ * arrays would take gigabytes of host memory (2.1M centres x 178 pairs):
+ * out[2 o] = number of neighbours of real row o, out[2 o + 1] = the sum
+ * (mod 2^64) of a 64-bit mix of every entry (rj << 5) | image of that row,
+ * which does not depend on the order of the row.  n >= n_real rows.
+ * Serves the same comparison as sph_get_neighbours (the reference's lists,
+ * neighboursearch.f90:74-180). */
+int sph_get_neighbour_digest(sph_handle* h, uint64_t* out, int64_t n);
+
 int sph_get_counters(sph_handle* h, int64_t* out, int n);
 int sph_reset_counters(sph_handle* h);
 int sph_get_timers(sph_handle* h, double* out_ms, int n);
@@ -235,7 +244,7 @@ int sph_errcalc(sph_handle* h, double* err_out, int64_t cap, double* l1_out);
 
 /* ---- batches of instances -----------------------------------------------
  * Many independent runs stepped together (the resolution x method sweeps
- * of the experiment runners, e.g. runner/anisotropic/
+ * of the experiment runners, e.g. runner/
  * 000_anisopaper_v1_gls_kxx.py, which run one Context after another through
  * CleanRun / ContinueRun, core.py:152-156).  Each instance keeps its own
  * handle, stream and time loop; a batch runs the instances' steps from one
@@ -268,7 +277,8 @@ void sph_batch_destroy(sph_batch* b);
  * n above SPH_NOALLOC_MAX_PARTICLES is rejected with SPH_ERR_ARG.  The first
  * call on a device looks the array up (make it before any stream capture).
  * Calls share the array: calls that overlap on the GPU race.  `stream` is a
- * cudaStream_t (NULL = default stream); the call synchronises it. */
+ * cudaStream_t of the current device (NULL = default stream; a stream of
+ * another device is rejected with SPH_ERR_ARG); the call synchronises it. */
 #define SPH_NOALLOC_MAX_PARTICLES 262144
 #define SPH_NOALLOC_SCRATCH_BYTES (32u << 20)
 int sph_density_noalloc(const double* x, const double* y, const double* z,

@@ -506,13 +506,21 @@ struct Oracle {
     if (!(hmin > 0)) hmin = 1e-300;
     double L = krad * hmin * std::max(1e-3, st[SPH_P_CELL_FACTOR]);
     int64_t nc[3];
+    const int64_t cell_cap = std::max<int64_t>(4 * sn, 1 << 16);
     for (;;) {
+      // cells per axis checked against the cap one axis at a time, so the
+      // product cannot overflow (a tiny h_min in a large box would need
+      // ~1e9 cells per axis)
       int64_t tot = 1;
-      for (int k = 0; k < 3; ++k) {
-        nc[k] = int64_t(std::floor((hi[k] - lo[k]) / L)) + 1;
-        tot *= nc[k];
+      bool ok = true;
+      for (int k = 0; k < 3 && ok; ++k) {
+        const double e = (hi[k] - lo[k]) / L;
+        if (!(e < 1e9)) { ok = false; break; }
+        nc[k] = int64_t(std::floor(e)) + 1;
+        if (tot > cell_cap / nc[k]) ok = false;
+        else tot *= nc[k];
       }
-      if (tot <= std::max<int64_t>(4 * sn, 1 << 16)) break;
+      if (ok) break;
       L *= 1.5;
     }
     auto cell_of = [&](int k, double x) {
@@ -1519,6 +1527,34 @@ int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs, int64_t 
     }
     std::sort(v.begin(), v.end());
     std::copy(v.begin(), v.end(), pairs + o.noff[i]);
+  }
+  return SPH_OK;
+}
+
+// Order-independent digest of each row's set (count, sum of a 64-bit mix of
+// the sph_get_neighbours encoding), as the CUDA engine computes it.
+static inline uint64_t mix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+int sph_get_neighbour_digest(sph_handle* h, uint64_t* out, int64_t n) {
+  if (!h || !out) return fail(SPH_ERR_ARG, "null argument");
+  Oracle& o = h->o;
+  if (o.noff.empty()) return fail(SPH_ERR_STATE, "no neighbour search yet");
+  if (n < o.realpn) return fail(SPH_ERR_ARG, "digest buffer shorter than the real rows");
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < o.realpn; ++i) {
+    uint64_t s = 0;
+    for (int64_t l = o.noff[i]; l < o.noff[i + 1]; ++l) {
+      const int64_t j = o.nidx[l];
+      const int64_t rj = j < o.nrows ? j : o.crossref[j - o.nrows];
+      const int64_t code = j < o.nrows ? 13 : o.gcode[j - o.nrows];
+      s += mix64(uint64_t((rj << 5) | code));
+    }
+    out[2 * i] = uint64_t(o.noff[i + 1] - o.noff[i]);
+    out[2 * i + 1] = s;
   }
   return SPH_OK;
 }

@@ -55,7 +55,7 @@ TIMERS = ["predict", "ghosts", "sort", "neighbours", "circuit1", "circuit2",
 ABI_SYMBOLS = [
     "sph_create", "sph_set_param", "sph_get_param", "sph_set_store",
     "sph_iterate", "sph_density", "sph_step", "sph_run_to", "sph_get_store",
-    "sph_get_state", "sph_get_neighbours", "sph_get_counters",
+    "sph_get_state", "sph_get_neighbours", "sph_get_neighbour_digest", "sph_get_counters",
     "sph_reset_counters", "sph_get_timers", "sph_last_error", "sph_destroy",
     "sph_batch_create", "sph_batch_step", "sph_batch_run_to", "sph_batch_status",
     "sph_batch_destroy", "sph_errcalc",
@@ -98,6 +98,7 @@ def load(path=None):
     lib.sph_get_store.argtypes = [vp, P(d), i64]
     lib.sph_get_state.argtypes = [vp, P(d)]
     lib.sph_get_neighbours.argtypes = [vp, P(i64), P(i64), i64]
+    lib.sph_get_neighbour_digest.argtypes = [vp, P(ctypes.c_uint64), i64]
     lib.sph_get_counters.argtypes = [vp, P(i64), c_int]
     lib.sph_reset_counters.argtypes = [vp]
     lib.sph_get_timers.argtypes = [vp, P(d), c_int]
@@ -275,6 +276,16 @@ class Engine:
         self._check(self.lib.sph_get_neighbours(self.h, _iptr(off), _iptr(pairs),
                                                 pairs.shape[0]))
         return off, pairs[: int(off[-1])]
+
+    def get_neighbour_digest(self):
+        """(count, digest) per real row in original order: the neighbour
+        count and the order-independent 64-bit sum of a mix of each entry of
+        get_neighbours' encoding; equal digests mean equal sets (up to a
+        2^-64 collision per row) without copying the pair arrays."""
+        out = np.zeros((self.n_real, 2), dtype=np.uint64)
+        self._check(self.lib.sph_get_neighbour_digest(
+            self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), self.n_real))
+        return out[:, 0].astype(np.int64), out[:, 1]
 
     def counters(self):
         out = np.zeros(len(COUNTERS), dtype=np.int64)

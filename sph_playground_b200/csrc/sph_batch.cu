@@ -4,7 +4,7 @@
 // instances overlap on the device.
 //
 // The reference runs such sweeps one Context after another (the experiment
-// runners, e.g. runner/anisotropic/000_anisopaper_v1_gls_kxx.py, through
+// runners, e.g. runner/000_anisopaper_v1_gls_kxx.py, through
 // CleanRun / ContinueRun, core.py:152-156); every instance here computes
 // exactly what sph_step / sph_run_to compute for it alone.
 #include <condition_variable>

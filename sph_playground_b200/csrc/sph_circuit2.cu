@@ -4,8 +4,9 @@
 // continuity term, anisotropic / isotropic / flux-limited diffusion with the
 // run-time second-derivative method, ideal-MHD stress and induction).
 //
-// One thread per centre walks its neighbour list; neighbour data come from the
-// packed sorted-order streams.  All nabla W terms are written as g * r_ab with
+// G lanes per centre walk its neighbour list (lane l takes entries l, l + G,
+// ...); neighbour data come from the packed sorted-order streams.  All
+// nabla W terms are written as g * r_ab with
 //   g_a = wCv f'(q_a) / (h_a^(d+1) r)      (nw_cart, kernel.f90:189-197)
 // and the reference's per-pair divisions by rho^2 Omega are the per-particle
 // factor Pi = 1/(rho^2 Omega) computed once when the streams are packed.

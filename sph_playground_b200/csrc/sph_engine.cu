@@ -560,15 +560,9 @@ struct sph_handle {
                                                 int64_t(1) << 31);
     int n3[3];
     for (int guard = 0;; ++guard) {
-      bool ok = true;
-      ncell = 1;
-      for (int k = 0; k < 3; ++k) {
-        double e = (hi[k] - lo[k]) / L;
-        if (!(e < 1e9)) { ok = false; break; }
-        n3[k] = int(std::floor(e)) + 1;
-        ncell *= n3[k];
-      }
-      if (ok && ncell <= ncell_cap) break;
+      double e[3];
+      for (int k = 0; k < 3; ++k) e[k] = (hi[k] - lo[k]) / L;
+      if (grid_dims(e, ncell_cap, n3, &ncell)) break;
       L *= 1.25;
       if (guard > 400) return fail(SPH_ERR_GRID, "cell grid would not fit");
     }
@@ -1854,6 +1848,23 @@ int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs, int64_t 
     }
     std::sort(pairs + base, pairs + base + cnt[c]);
   }
+  return SPH_OK;
+}
+
+int sph_get_neighbour_digest(sph_handle* h, uint64_t* out, int64_t n) {
+  if (!h || !out) return fail(SPH_ERR_ARG, "null argument");
+  if (!h->have_order) return fail(SPH_ERR_STATE, "no neighbour search since the last re-ordering");
+  if (n < h->nreal) return fail(SPH_ERR_ARG, "digest buffer shorter than the real rows");
+  const int64_t nc = h->nreal;
+  DevBuf d;
+  RC(d.ensure(sizeof(unsigned long long) * 2 * std::max<int64_t>(nc, 1)));
+  launch_neib_digest(nc, h->centre_p.as<int32_t>(), h->orig.as<int32_t>(),
+                     h->rowoff.as<int64_t>(), h->ncnt.as<int32_t>(), h->nl.as<int32_t>(),
+                     h->vals_alt.as<int32_t>(), h->ssrc.as<int32_t>(), h->gcode.as<int8_t>(),
+                     h->nrows, d.as<unsigned long long>(), h->s);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d.p, sizeof(uint64_t) * 2 * nc, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
   return SPH_OK;
 }
 

@@ -369,6 +369,45 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
   centre_p[c] = sidx[k];
 }
 
+// ---- neighbour-set digest ----------------------------------------------------------------
+// Per centre, in original row order: the neighbour count and the sum (mod
+// 2^64) of a 64-bit mix of each neighbour's (row << 5) | image code, the
+// encoding of sph_get_neighbours.  The sum does not depend on the order of a
+// row, so two engines with the same sets give the same digests; a differing
+// set changes the sum unless 64-bit mixes cancel.  One warp per centre.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+__global__ void k_neib_digest(int64_t nc, const int32_t* __restrict__ centre_p,
+                              const int32_t* __restrict__ orig, const int64_t* __restrict__ rowoff,
+                              const int32_t* __restrict__ ncnt, const int32_t* __restrict__ nl,
+                              const int32_t* __restrict__ sidx, const int32_t* __restrict__ ssrc,
+                              const int8_t* __restrict__ gcode, int64_t nrows,
+                              unsigned long long* __restrict__ out) {
+  const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= nc) return;
+  const int n = ncnt[c];
+  const int32_t* row = nl + rowoff[c];
+  unsigned long long s = 0;
+  for (int l = lane; l < n; l += 32) {
+    const int64_t q = row[l];
+    const int64_t u = sidx[q];
+    const long long rj = orig[ssrc[q]];
+    const long long code = u < nrows ? 13 : gcode[u - nrows];
+    s += mix64((unsigned long long)((rj << 5) | code));
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    const int64_t o = orig[centre_p[c]];
+    out[2 * o] = (unsigned long long)n;
+    out[2 * o + 1] = s;
+  }
+}
+
 // ---- neighbour search -------------------------------------------------------------------
 // One lane per centre; a group of G consecutive centres (in cell order, so
 // neighbours in space) shares one stream of candidates.  The centres of a
@@ -642,6 +681,10 @@ k_neighbours(NeibArgs a) {
           // closer than the FP32 images resolve) are decided in FP64 after
           // the batch, which recomputes sd32 bit for bit to find them (rare:
           // about once per centre)
+          // The candidate is written to the next free slot whether or not it
+          // is a hit and kept only by counting it (no branch per test): a
+          // lane starts a batch with at most FLUSH_AT - 1 = 32 - G held
+          // hits, so test t writes slot <= 32 - G + t <= 31 of its 33.
           bool anyband = false;
 #pragma unroll
           for (int t = 0; t < G; ++t) {
@@ -649,7 +692,7 @@ k_neighbours(NeibArgs a) {
             const float sd32 = dist2_f32(pj, pi);
             const bool in32 = sd32 < lo_thr && sd32 > 0.f;
             anyband |= !in32 && !(sd32 > hi_thr);
-            if (in32) mine_held[nheld] = __float_as_int(pj.w);
+            mine_held[nheld] = __float_as_int(pj.w);
             nheld += in32 ? 1 : 0;
           }
           if (anyband) {
@@ -977,15 +1020,9 @@ __global__ void k_plan(const unsigned long long* __restrict__ red,
   int64_t ncell = 1;
   bool fits = ok_in;
   for (int guard = 0; fits; ++guard) {
-    bool ok = true;
-    ncell = 1;
-    for (int k = 0; k < 3; ++k) {
-      const double e = __ddiv_rn(__dadd_rn(hi[k], -lo[k]), L);
-      if (!(e < 1e9)) { ok = false; break; }
-      n3[k] = int(floor(e)) + 1;
-      ncell *= n3[k];
-    }
-    if (ok && ncell <= ncap) break;
+    double e[3];
+    for (int k = 0; k < 3; ++k) e[k] = __ddiv_rn(__dadd_rn(hi[k], -lo[k]), L);
+    if (grid_dims(e, ncap, n3, &ncell)) break;
     L = __dmul_rn(L, 1.25);
     if (guard > 400) { fits = false; P.err = P.err ? P.err : SPH_ERR_GRID; }
   }
@@ -1243,6 +1280,15 @@ void launch_sorted_gather_dev(const int32_t* sidx, int64_t ncap, int64_t nrows, 
 void launch_centres(const int32_t* sidx, const int32_t* flag, const int32_t* pos, int64_t n,
                     int32_t* centre_k, int32_t* centre_p, cudaStream_t s) {
   k_centres<<<nblocks(n), TPB, 0, s>>>(sidx, flag, pos, n, centre_k, centre_p);
+  note_launch();
+}
+void launch_neib_digest(int64_t nc, const int32_t* centre_p, const int32_t* orig,
+                        const int64_t* rowoff, const int32_t* ncnt, const int32_t* nl,
+                        const int32_t* sidx, const int32_t* ssrc, const int8_t* gcode,
+                        int64_t nrows, unsigned long long* out, cudaStream_t s) {
+  if (nc <= 0) return;
+  k_neib_digest<<<nblocks(nc * 32), TPB, 0, s>>>(nc, centre_p, orig, rowoff, ncnt, nl, sidx,
+                                                  ssrc, gcode, nrows, out);
   note_launch();
 }
 template <int DIM, int G>

@@ -40,6 +40,25 @@ __host__ __device__ inline double dkey_inv(unsigned long long u) {
   return v;
 }
 
+// Cells per axis of a uniform grid, n3[k] = floor(e[k]) + 1 with e[k] the
+// extent of axis k in cell edges, and their product *ncell.  False when an
+// axis would need 1e9 cells or more, or when the product exceeds cap.  The
+// product is checked against cap one axis at a time (n > cap / n3 before
+// multiplying), so it never overflows: three axes just under 1e9 cells would
+// otherwise multiply past 2^63 and wrap to a value that may pass the test.
+__host__ __device__ inline bool grid_dims(const double e[3], int64_t cap, int n3[3],
+                                          int64_t* ncell) {
+  int64_t n = 1;
+  for (int k = 0; k < 3; ++k) {
+    if (!(e[k] < 1e9) || !(e[k] >= 0.0)) return false;
+    n3[k] = int(floor(e[k])) + 1;
+    if (n > cap / n3[k]) return false;
+    n *= n3[k];
+  }
+  *ncell = n;
+  return true;
+}
+
 // Reduction slots (unsigned long long, dkey-encoded min/max).
 enum RedSlot : int {
   RED_LO_X = 0, RED_LO_Y, RED_LO_Z, RED_HI_X, RED_HI_Y, RED_HI_Z, RED_HMIN,
@@ -175,6 +194,12 @@ struct NeibArgs {
   unsigned long long* dcnt;
 };
 void launch_neighbours(int dim, int G, const NeibArgs& a, cudaStream_t s);
+// per centre in original order: out[2 o] = count, out[2 o + 1] = sum of
+// mix64((row << 5) | image) over the neighbours (sph_get_neighbour_digest)
+void launch_neib_digest(int64_t nc, const int32_t* centre_p, const int32_t* orig,
+                        const int64_t* rowoff, const int32_t* ncnt, const int32_t* nl,
+                        const int32_t* sidx, const int32_t* ssrc, const int8_t* gcode,
+                        int64_t nrows, unsigned long long* out, cudaStream_t s);
 void launch_rowcap(int64_t nc, const int32_t* centre_p, const int32_t* orig,
                    const int32_t* count_prev, const float* h_prev, const double* hcol,
                    int dim, float slack, int64_t* rowcap64, int32_t* rowcap,

@@ -207,6 +207,19 @@ extern "C" int sph_density_noalloc(const double* x, const double* y, const doubl
   if (dim < 2) y = nullptr;
   if (dim < 3) z = nullptr;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The scratch address is the current device's; a stream of another device
+  // would run the kernels there with this device's address.
+  if (s) {
+    int cur = -1, sdev = -1;
+    cudaError_t ge = cudaGetDevice(&cur);
+    if (ge == cudaSuccess) ge = cudaStreamGetDevice(s, &sdev);
+    if (ge != cudaSuccess)
+      return sph_fail(SPH_ERR_CUDA, std::string("sph_density_noalloc: ") + cudaGetErrorString(ge));
+    if (sdev != cur)
+      return sph_fail(SPH_ERR_ARG, "sph_density_noalloc: the stream belongs to device " +
+                                       std::to_string(sdev) + ", the current device is " +
+                                       std::to_string(cur));
+  }
   void* base = nullptr;
   int rc = scratch_address(&base);
   if (rc) return rc;
@@ -252,15 +265,9 @@ extern "C" int sph_density_noalloc(const double* x, const double* y, const doubl
   int64_t ncell = 0;
   int n3[3] = {1, 1, 1};
   for (int guard = 0;; ++guard) {
-    bool ok = true;
-    ncell = 1;
-    for (int k = 0; k < 3; ++k) {
-      double ex = (hi[k] - lo[k]) / L;
-      if (!(ex < 1e9)) { ok = false; break; }
-      n3[k] = int(std::floor(ex)) + 1;
-      ncell *= n3[k];
-    }
-    if (ok && ncell <= max_cells) break;
+    double ex[3];
+    for (int k = 0; k < 3; ++k) ex[k] = (hi[k] - lo[k]) / L;
+    if (grid_dims(ex, max_cells, n3, &ncell)) break;
     L *= 1.25;
     if (guard > 400) return sph_fail(SPH_ERR_GRID, "cell grid would not fit");
   }
@@ -280,6 +287,9 @@ extern "C" int sph_density_noalloc(const double* x, const double* y, const doubl
     launch_density<KM4>(dim, x, y, z, m, h, n, g, krad, wcv, cstart, vals2, sorted, rho, status, s);
   else
     launch_density<KGAUSS>(dim, x, y, z, m, h, n, g, krad, wcv, cstart, vals2, sorted, rho, status, s);
+  // this library's own kernels (init, reduce, keys, starts, gather,
+  // density); the radix sort's kernels are CUB's and are not counted, as
+  // in the engine's launch counter
   note_launch(6);
   int hstatus = 0;
   e = cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, s);

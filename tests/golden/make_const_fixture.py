@@ -6,7 +6,7 @@ src/const.f90 into whitespace tokens and keeping `name = value,&` triples
 rule to the reference file and writes the dictionaries as JSON; the test
 suite compares sph_playground_b200.consts against the JSON.
 
-Usage: python tests/golden/make_const_fixture.py /root/reference/playground/src/const.f90
+Usage: python tests/golden/make_const_fixture.py <reference checkout>/playground/src/const.f90
 """
 import json
 import os

@@ -80,3 +80,32 @@ def test_fixedreal_copies_run_like_the_oracle(oracle_lib, engine_lib, cuda_ok, t
     for f in ("den", "u", "h"):
         assert rel_particle(s1[:, COL[f]], s0[:, COL[f]]) <= 1e-9, f
     np.testing.assert_allclose(s1[:, 0], s0[:, 0], rtol=0, atol=1e-11)
+
+
+@pytest.mark.parametrize("h_small", [1e-4, 1e-12])
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_tiny_smoothing_length_grid(oracle_lib, engine_lib, cuda_ok, prec, h_small):
+    """One particle with a tiny h in the unit box sets a cell edge that would
+    need up to ~1e9 cells per axis: the cell count is checked one axis at a
+    time (their product would overflow 64 bits) and the grid is widened to
+    fit, with the neighbour sets and densities of the oracle."""
+    rng = np.random.default_rng(32)
+    n = 3000
+    st = ic.make_state(3, equations="hydro", adden="no", process="borderless", hfac=1.2)
+    for k, v in (("realpn", n), ("fixedpn", 0), ("gamma", 5.0 / 3.0), ("dcondconst", 1.0),
+                 ("time", 0.0), ("dtprint", 1.0)):
+        ic.set_state(st, k, v)
+    store = np.zeros((n, 32))
+    store[:, 0:3] = rng.uniform(0.0, 1.0, (n, 3))
+    h = 1.2 * (1.0 / n) ** (1 / 3) * rng.uniform(0.9, 1.1, n)
+    h[7] = h_small
+    store[:, COL["h"]] = h
+    store[:, COL["m"]] = 1.0 / n
+    store[:, COL["den"]] = 1.0
+    store[:, COL["om"]] = 1.0
+    store[:, COL["u"]] = 1.0
+    store[:, COL["type"]] = 1.0
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "density")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "density")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    assert rel_particle(got[:, COL["den"]], ref[:, COL["den"]]) <= TOL[prec]

@@ -361,3 +361,65 @@ def test_radiation_exchange_conserves_energy(oracle_lib):
     assert np.all(s[:, C["u"]] > store[:, C["u"]])
     assert np.all(s[:, C["t"]] < store[:, C["t"]])
 
+
+
+@pytest.mark.parametrize("h_small", [1e-4, 1e-12])
+def test_tiny_smoothing_length_grid(oracle_lib, h_small):
+    """One particle with a tiny h in the unit box: its cell edge would need
+    up to ~1e9 cells per axis, whose product overflows 64 bits unless the
+    cell count is checked one axis at a time; the grid is widened instead,
+    and the density pass (direct summation) gives the brute-force sums."""
+    rng = np.random.default_rng(31)
+    n = 1500
+    st = ic.make_state(3, equations="hydro", adden="no", process="borderless", hfac=1.2)
+    for k, v in (("realpn", n), ("fixedpn", 0), ("gamma", 5.0 / 3.0), ("dcondconst", 1.0),
+                 ("time", 0.0), ("dtprint", 1.0)):
+        ic.set_state(st, k, v)
+    store = np.zeros((n, 32))
+    store[:, 0:3] = rng.uniform(0.0, 1.0, (n, 3))
+    h = 1.2 * (1.0 / n) ** (1 / 3) * rng.uniform(0.9, 1.1, n)
+    h[5] = h_small
+    store[:, COL["h"]] = h
+    store[:, COL["m"]] = 1.0 / n
+    store[:, COL["den"]] = 1.0
+    store[:, COL["om"]] = 1.0
+    store[:, COL["u"]] = 1.0
+    store[:, COL["type"]] = consts.ept["real"]
+    with abi.Engine(st, store, "m6", lib=oracle_lib) as e:
+        e.density()
+        rho = e.get_store()[:, COL["den"]]
+    pos = store[:, 0:3]
+    d = np.sqrt(((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+    q = d / h[:, None]
+    w = np.where(q < 3, _m6_shape(q), 0.0)
+    ref = (w * (1.0 / n)).sum(1) / (120 * math.pi) / h ** 3
+    assert np.all(np.isfinite(rho))
+    assert np.max(np.abs(rho / ref - 1)) < 1e-12
+
+
+def _m6_shape(q):
+    t = lambda c: np.maximum(c - q, 0.0) ** 5  # noqa: E731
+    return t(3) - 6 * t(2) + 15 * t(1)
+
+
+def _mix64(z):
+    z = (z + np.uint64(0x9E3779B97F4A7C15))
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def test_neighbour_digest_matches_sets(oracle_lib):
+    """sph_get_neighbour_digest: per row the count and the wrapped sum of
+    mix64 over the get_neighbours encoding of the row."""
+    st, store = ic.density3d(n=8, seed=2)
+    with abi.Engine(st, store, "m6", lib=oracle_lib) as e:
+        e.density()
+        off, pairs = e.get_neighbours()
+        cnt, dig = e.get_neighbour_digest()
+    assert np.array_equal(cnt, np.diff(off))
+    with np.errstate(over="ignore"):
+        mixed = _mix64(pairs.astype(np.uint64))
+        ref = np.add.reduceat(mixed, off[:-1]) if pairs.size else np.zeros_like(dig)
+    ref[np.diff(off) == 0] = 0
+    assert np.array_equal(ref, dig)
