@@ -1,13 +1,19 @@
 // Batches of independent instances (include/sph_abi.h, "batches of
-// instances"): one host worker per instance runs that instance's time loop
-// on its own stream, so that the kernels and host round trips of the
+// instances").  When every instance can take device-resident steps, the
+// batch steps as one device loop (sph::batch_graph_run: a CUDA graph whose
+// while node iterates one if node per instance, each holding that
+// instance's captured step, with per-instance clocks and error words on the
+// device); otherwise one host worker per instance runs that instance's time
+// loop on its own stream, so that the kernels and host round trips of the
 // instances overlap on the device.
 //
 // The reference runs such sweeps one Context after another (the experiment
 // runners, e.g. runner/000_anisopaper_v1_gls_kxx.py, through
 // CleanRun / ContinueRun, core.py:152-156); every instance here computes
 // exactly what sph_step / sph_run_to compute for it alone.
+#include <algorithm>
 #include <condition_variable>
+#include <limits>
 #include <functional>
 #include <mutex>
 #include <string>
@@ -30,6 +36,19 @@ struct sph_batch {
   long long generation = 0;             // bumped per call
   int pending = 0;
   bool quit = false;
+  sph::BatchGraph* bg = nullptr;  // the device loop, built on first use
+
+  // the device loop over all instances; *used = false when it does not apply
+  int device_loop(double tfinish, bool use_state, long long limit, bool* used) {
+    std::fill(status.begin(), status.end(), 0);
+    std::fill(msg.begin(), msg.end(), std::string());
+    int rc = sph::batch_graph_run(&bg, h.data(), int(h.size()), tfinish, use_state, limit, status,
+                                  msg, used);
+    if (rc || !*used) return rc;
+    for (size_t i = 0; i < h.size(); ++i)
+      if (status[i]) return sph::sph_fail(status[i], "instance " + std::to_string(i) + ": " + msg[i]);
+    return SPH_OK;
+  }
 
   void worker(int i) {
     cudaSetDevice(sph::handle_device(h[i]));
@@ -101,11 +120,17 @@ int sph_batch_create(int n_inst, sph_handle* const* handles, sph_batch** out) {
 
 int sph_batch_step(sph_batch* b, int nsteps) {
   if (!b || nsteps < 0) return sph::sph_fail(SPH_ERR_ARG, "bad argument");
+  bool used = false;
+  int rc = b->device_loop(0.0, true, nsteps, &used);
+  if (used || rc) return rc;
   return b->run([nsteps](sph_handle* h) { return sph_step(h, nsteps); });
 }
 
 int sph_batch_run_to(sph_batch* b, double tfinish) {
   if (!b) return sph::sph_fail(SPH_ERR_ARG, "null batch");
+  bool used = false;
+  int rc = b->device_loop(tfinish, false, std::numeric_limits<long long>::max(), &used);
+  if (used || rc) return rc;
   return b->run([tfinish](sph_handle* h) { return sph_run_to(h, tfinish); });
 }
 
@@ -124,6 +149,7 @@ void sph_batch_destroy(sph_batch* b) {
   }
   b->cv_go.notify_all();
   for (auto& t : b->workers) t.join();
+  sph::batch_graph_destroy(b->bg);
   delete b;
 }
 

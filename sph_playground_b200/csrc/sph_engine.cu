@@ -175,6 +175,11 @@ struct sph_handle {
   // when the step has to be redone on the host path), the capacities the
   // step is planned for, and the captured CUDA graph of one step
   DevBuf drs_plan, drs_clock, drs_err, drs_save;
+  // a batch's device loop: the clock saved at the start of the instance's
+  // step (restored when the step is redone on the host path), and a count
+  // of parameter changes (a captured loop holds the values it saw)
+  DevBuf bclk_save;
+  long long param_gen = 0;
   const DevPlan* dplan = nullptr;  // set while a device-resident step is built
   int64_t nghost_cap = 0, nall_cap = 0;
   int end_bit_cap = 0;
@@ -992,6 +997,7 @@ struct sph_handle {
     RC(drs_clock.ensure(sizeof(DevClock)));
     RC(drs_err.ensure(sizeof(int)));
     RC(drs_save.ensure(sizeof(double) * NCOL * size_t(nrows)));
+    RC(bclk_save.ensure(sizeof(DevClock)));
     if (eq_sts) RC(stsY.ensure(sizeof(double) * 6 * nrows));
     return SPH_OK;
   }
@@ -1131,6 +1137,49 @@ struct sph_handle {
     steps_since_reorder++;
     cnt_host[SPH_CNT_GRAPH_STEPS]++;
     return SPH_OK;
+  }
+
+  // ---- one instance of a batch's device loop -------------------------------------------------
+  // The body of the instance's if node: the reorder decision of one_step
+  // (every SPH_P_REORDER_EVERY steps, as the rows of the last search), the
+  // reorder itself in place, the table saved for a redo, the device-resident
+  // step of one_step_graph, and the check of its error words.  Captured with
+  // the capacities of drs_prepare.
+  int batch_step_body(BatchInst* b) {
+    launch_inst_begin(b, drs_clock.as<DevClock>(), bclk_save.as<DevClock>(), s);
+    launch_reorder_gated(b, cols.as<double>(), cols_alt.as<double>(), orig.as<int32_t>(),
+                         orig_alt.as<int32_t>(), centre_p.as<int32_t>(), nreal, nrows, s);
+    RC(copy_table(drs_save.p, cols.p));
+    RC(step_body_dev());
+    launch_inst_end(b, drs_err.as<int>(), overflow.as<int32_t>(), status.as<int>(), s);
+    return SPH_OK;
+  }
+  // host view of the clock before a device loop
+  void upload_clock(double tfinish) {
+    DevClock clk{};
+    clk.t = st[ec_time];
+    clk.ltout = ltout;
+    clk.dtout = dtout;
+    clk.tfinish = tfinish;
+    clk.stopped = stopped ? 1 : 0;
+    std::memcpy(h_ctrl + 1, &clk, sizeof(DevClock));
+  }
+  // host view after a device loop ran `steps` steps of this instance
+  void adopt_loop(const DevClock& clk, const DevPlan& plan, long long steps, int since) {
+    steps_since_reorder = since;
+    if (steps <= 0) return;
+    st[ec_time] = clk.t;
+    ltout = clk.ltout;
+    stopped = clk.stopped != 0;
+    have_order = true;
+    nghost = plan.nghost;
+    grid = plan.grid;
+    pgeom = plan.pg;
+    const long long per = eq_sts ? 1 + ival(ec_stsfixeds) : 1;
+    cnt_host[SPH_CNT_STEPS] += steps;
+    cnt_host[SPH_CNT_ITERATES] += steps * per;
+    cnt_host[SPH_CNT_SEARCHES] += steps * per;
+    cnt_host[SPH_CNT_GRAPH_STEPS] += steps;
   }
 
   // ---- closing error evaluation (main.f90:374-402) ---------------------------------------------
@@ -1612,6 +1661,288 @@ struct sph_handle {
   }
 };
 
+// ---- batches stepped by one device loop ----------------------------------------------------------
+// A batch of instances (config-3 sweeps: lattices x second-derivative
+// methods, run one Context after another by the reference's runners) steps
+// as one CUDA graph: a while node whose body is a gate kernel, one if node
+// per instance holding that instance's device-resident step, and a control
+// kernel.  The gate opens the if nodes of the instances whose time loop has
+// not ended (t < tfinish + eps and not stopped, main.f90:241); the if nodes
+// of one iteration are independent branches, so the instances' steps run
+// side by side on the device; the control kernel ends the loop when no
+// instance runs, when one set an error word, or after kLoopCap iterations
+// (a bound on every launch).  The host relaunches the loop until every
+// instance is done; an instance whose step set an error word (a capacity or
+// list row too small, Newton beyond its fixed sweeps) gets its table and
+// clock back and redoes that step on the host path, as one_step_graph does.
+namespace sph {
+
+constexpr int kLoopCap = 128;
+
+struct BatchGraph {
+  cudaStream_t s = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  std::vector<sph_handle*> members;
+  struct Mark { long long allocs, params; int64_t nall_cap; int end_bit; };
+  std::vector<Mark> marks;
+  DevBuf bi, ifh, iter;
+  std::vector<BatchInst> hbi;
+  void drop() {
+    if (x) cudaGraphExecDestroy(x);
+    if (g) cudaGraphDestroy(g);
+    x = nullptr;
+    g = nullptr;
+  }
+  ~BatchGraph() {
+    drop();
+    if (s) cudaStreamDestroy(s);
+  }
+  static Mark mark_of(const sph_handle* h) {
+    return {h->cnt_host[SPH_CNT_ALLOCS], h->param_gen, h->nall_cap, h->end_bit_cap};
+  }
+  bool stale(const std::vector<sph_handle*>& hs) const {
+    if (!x || hs != members) return true;
+    for (size_t i = 0; i < hs.size(); ++i) {
+      const Mark m = mark_of(hs[i]);
+      const Mark& o = marks[i];
+      if (m.allocs != o.allocs || m.params != o.params || m.nall_cap != o.nall_cap ||
+          m.end_bit != o.end_bit)
+        return true;
+    }
+    return false;
+  }
+  // the while node, its body (gate -> if nodes -> control) and each
+  // instance's step captured into its if node's body
+  int build(const std::vector<sph_handle*>& hs) {
+    drop();
+    const int n = int(hs.size());
+    if (!s) CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    RC(bi.ensure(sizeof(BatchInst) * n));
+    RC(ifh.ensure(sizeof(cudaGraphConditionalHandle) * n));
+    RC(iter.ensure(sizeof(int)));
+    BatchInst* dbi = bi.as<BatchInst>();
+    auto bad = [&](cudaError_t e, const char* what) {
+      cudaGetLastError();
+      drop();
+      return fail(SPH_ERR_CUDA, std::string("batch loop: ") + what + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return bad(e, "graph");
+    cudaGraphConditionalHandle wh;
+    e = cudaGraphConditionalHandleCreate(&wh, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return bad(e, "while handle");
+    cudaGraphNodeParams wp{};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = wh;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    e = cudaGraphAddNode(&wnode, g, nullptr, 0, &wp);
+    if (e != cudaSuccess) return bad(e, "while node");
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    // gate
+    cudaGraphNode_t gate_node = nullptr, last = nullptr;
+    {
+      e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return bad(e, "gate capture");
+      launch_batch_gate(dbi, n, ifh.as<cudaGraphConditionalHandle>(), s);
+      cudaGraph_t out;
+      e = cudaStreamEndCapture(s, &out);
+      if (e != cudaSuccess) return bad(e, "gate capture end");
+      size_t nn = 0;
+      e = cudaGraphGetNodes(body, nullptr, &nn);
+      if (e != cudaSuccess || nn != 1) return bad(e, "gate node");
+      e = cudaGraphGetNodes(body, &gate_node, &nn);
+      if (e != cudaSuccess) return bad(e, "gate node");
+    }
+    // one if node per instance, after the gate
+    std::vector<cudaGraphConditionalHandle> hh(n);
+    std::vector<cudaGraphNode_t> ifn(n);
+    for (int i = 0; i < n; ++i) {
+      sph_handle* h = hs[i];
+      e = cudaGraphConditionalHandleCreate(&hh[i], body, 0, 0);
+      if (e != cudaSuccess) return bad(e, "if handle");
+      cudaGraphNodeParams ip{};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hh[i];
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      e = cudaGraphAddNode(&ifn[i], body, &gate_node, 1, &ip);
+      if (e != cudaSuccess) return bad(e, "if node");
+      cudaGraph_t ib = ip.conditional.phGraph_out[0];
+      h->dplan = h->drs_plan.as<DevPlan>();
+      e = cudaStreamBeginCaptureToGraph(h->s, ib, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+      int rc = e == cudaSuccess ? h->batch_step_body(dbi + i) : SPH_ERR_CUDA;
+      cudaGraph_t out;
+      cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(h->s, &out) : e;
+      h->dplan = nullptr;
+      if (rc || e != cudaSuccess || e2 != cudaSuccess) {
+        cudaGetLastError();
+        drop();
+        return rc ? rc : fail(SPH_ERR_CUDA, std::string("batch loop: step capture: ") +
+                                                cudaGetErrorString(e != cudaSuccess ? e : e2));
+      }
+    }
+    // control, after every if node
+    {
+      e = cudaStreamBeginCaptureToGraph(s, body, ifn.data(), nullptr, ifn.size(),
+                                        cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return bad(e, "control capture");
+      launch_batch_ctl(dbi, n, wh, iter.as<int>(), kLoopCap, s);
+      cudaGraph_t out;
+      e = cudaStreamEndCapture(s, &out);
+      if (e != cudaSuccess) return bad(e, "control capture end");
+    }
+    (void)last;
+    CK(cudaMemcpyAsync(ifh.p, hh.data(), sizeof(cudaGraphConditionalHandle) * n,
+                       cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) return bad(e, "instantiate");
+    members = hs;
+    marks.clear();
+    for (auto* h : hs) marks.push_back(mark_of(h));
+    return SPH_OK;
+  }
+};
+
+void batch_graph_destroy(BatchGraph* bg) { delete bg; }
+
+// Step the instances of a batch to tfinish (use_state: each instance's own
+// tfinish) for at most `limit` steps each through the device loop.  *used =
+// false (and nothing done) when an instance cannot take device-resident
+// steps; the caller then runs the batch on host workers.
+int batch_graph_run(BatchGraph** pbg, sph_handle* const* hs_in, int n, double tfinish,
+                    bool use_state, long long limit, std::vector<int>& status,
+                    std::vector<std::string>& msg, bool* used) {
+  *used = false;
+  std::vector<sph_handle*> hs(hs_in, hs_in + n);
+  for (auto* h : hs)
+    if (handle_device(h) != handle_device(hs[0])) return SPH_OK;
+  CK(cudaSetDevice(handle_device(hs[0])));
+  std::vector<double> tf(n);
+  std::vector<long long> done_steps(n, 0);
+  // start every instance (the start-up iterate of main.f90 runs on the
+  // host path), then check that each can take device-resident steps
+  for (int i = 0; i < n; ++i) {
+    sph_handle* h = hs[i];
+    t_alloc_count = &h->cnt_host[SPH_CNT_ALLOCS];
+    if (!use_state) h->st[ec_tfinish] = tfinish;
+    tf[i] = h->st[ec_tfinish];
+    int rc = SPH_OK;
+    if (!h->started) rc = h->start_run();
+    if (!rc && h->ival(ec_eqs) != eeq_kd2) h->stopped = false;
+    t_alloc_count = nullptr;
+    if (rc) {
+      status[i] = rc;
+      msg[i] = g_err;
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    const char* why = nullptr;
+    if (!status[i] && !hs[i]->drs_eligible(&why)) {
+      // host workers instead (the instances keep their start)
+      std::fill(status.begin(), status.end(), 0);
+      return SPH_OK;
+    }
+  }
+  *used = true;
+  if (!*pbg) *pbg = new BatchGraph();
+  BatchGraph* bg = *pbg;
+  auto runs = [&](int i) {
+    const sph_handle* h = hs[i];
+    return status[i] == 0 && done_steps[i] < limit &&
+           h->st[ec_time] < tf[i] + std::numeric_limits<double>::epsilon() && !h->stopped;
+  };
+  for (int guard = 0;; ++guard) {
+    // the loop's members: every instance without an error (buffers of
+    // finished instances stay valid; their if nodes stay closed)
+    std::vector<int> live;
+    for (int i = 0; i < n; ++i) {
+      if (status[i]) continue;
+      t_alloc_count = &hs[i]->cnt_host[SPH_CNT_ALLOCS];
+      int rc = hs[i]->drs_prepare();
+      t_alloc_count = nullptr;
+      if (rc) {
+        status[i] = rc;
+        msg[i] = g_err;
+        continue;
+      }
+      live.push_back(i);
+    }
+    bool any = false;
+    for (int i : live) any |= runs(i);
+    if (!any) break;
+    std::vector<sph_handle*> lh;
+    for (int i : live) lh.push_back(hs[i]);
+    if (bg->stale(lh)) RC(bg->build(lh));
+    const int m = int(live.size());
+    BatchInst* dbi = bg->bi.as<BatchInst>();
+    bg->hbi.assign(m, BatchInst{});
+    for (int k = 0; k < m; ++k) {
+      const int i = live[k];
+      sph_handle* h = hs[i];
+      BatchInst& b = bg->hbi[k];
+      b.clk = h->drs_clock.as<DevClock>();
+      b.every = std::max(0, int(h->st[SPH_P_REORDER_EVERY]));
+      b.since = h->steps_since_reorder;
+      b.limit = runs(i) ? limit - done_steps[i] : 0;
+      h->upload_clock(tf[i]);
+      CK(cudaMemcpyAsync(h->drs_clock.p, h->h_ctrl + 1, sizeof(DevClock), cudaMemcpyHostToDevice,
+                         bg->s));
+    }
+    CK(cudaMemcpyAsync(dbi, bg->hbi.data(), sizeof(BatchInst) * m, cudaMemcpyHostToDevice, bg->s));
+    CK(cudaMemsetAsync(bg->iter.p, 0, sizeof(int), bg->s));
+    // the instances' own streams may still hold work (uploads, a host step)
+    for (auto* h : lh) CK(cudaStreamSynchronize(h->s));
+    CK(cudaGraphLaunch(bg->x, bg->s));
+    CK(cudaMemcpyAsync(bg->hbi.data(), dbi, sizeof(BatchInst) * m, cudaMemcpyDeviceToHost, bg->s));
+    CK(cudaStreamSynchronize(bg->s));
+    CK(cudaGetLastError());
+    for (int k = 0; k < m; ++k) {
+      const int i = live[k];
+      sph_handle* h = hs[i];
+      const BatchInst& b = bg->hbi[k];
+      if (b.steps <= 0 && !b.failed) continue;
+      DevClock clk{}, saved{};
+      CK(cudaMemcpy(&clk, h->drs_clock.p, sizeof(DevClock), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(&saved, h->bclk_save.p, sizeof(DevClock), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(h->h_plan, h->drs_plan.p, sizeof(DevPlan), cudaMemcpyDeviceToHost));
+      done_steps[i] += b.steps;
+      if (!b.failed) {
+        h->adopt_loop(clk, *h->h_plan, b.steps, b.since);
+        continue;
+      }
+      // the steps before the failed one stand; the failed one is redone on
+      // the host path from the table and the clock saved at its start
+      h->adopt_loop(saved, *h->h_plan, b.steps, b.since);
+      h->st[ec_time] = saved.t;
+      h->ltout = saved.ltout;
+      h->stopped = saved.stopped != 0;
+      t_alloc_count = &h->cnt_host[SPH_CNT_ALLOCS];
+      int rc = h->copy_table(h->cols.p, h->drs_save.p);
+      if (!rc && cudaMemsetAsync(h->status.p, 0, sizeof(int), h->s) != cudaSuccess)
+        rc = fail(SPH_ERR_CUDA, "status reset");
+      h->cnt_host[SPH_CNT_GRAPH_REDOS]++;
+      bool done = false;
+      if (!rc) rc = h->one_step(tf[i], done);
+      if (!rc && !done) done_steps[i] += 1;
+      t_alloc_count = nullptr;
+      if (rc) {
+        status[i] = rc;
+        msg[i] = g_err;
+      }
+    }
+    if (guard > 1000000) return fail(SPH_ERR_STATE, "batch loop did not finish");
+  }
+  for (auto* h : hs) h->collect_timers();
+  return SPH_OK;
+}
+
+}  // namespace sph
+
 extern "C" {
 
 // counts the device allocations of one C-ABI call on its handle
@@ -1704,7 +2035,10 @@ int sph_set_param(sph_handle* h, int index, double value) {
   if (!h || index < 1 || index > SPH_P_LAST) return fail(SPH_ERR_ARG, "bad param index");
   if ((index == ec_realpn || index == ec_fixedpn) && value != h->st[index])
     return fail(SPH_ERR_ARG, "particle counts are fixed by the store");
-  if (h->st[index] != value) h->graph_dirty = true;  // a captured step holds the old value
+  if (h->st[index] != value) {  // a captured step holds the old value
+    h->graph_dirty = true;
+    h->param_gen++;
+  }
   h->st[index] = value;
   if (index == SPH_P_NEIB_CAP && value > 0) h->est_count = 0;
   return SPH_OK;

@@ -1105,6 +1105,75 @@ __global__ void k_clock_advance(DevClock* __restrict__ clk) {
   if (blockIdx.x == 0 && threadIdx.x == 0) clk->t = __dadd_rn(clk->t, clk->dt);
 }
 
+// ---- the device loop of a batch ----------------------------------------------------
+// the time loop's condition of main.f90:241 as the host evaluates it
+// (t < tfinish + epsilon(1d0) and not stopped)
+__device__ __forceinline__ bool inst_runs(const BatchInst& b) {
+  const DevClock& c = *b.clk;
+  return !b.failed && b.steps < b.limit &&
+         c.t < __dadd_rn(c.tfinish, 2.220446049250313080847e-16) && !c.stopped;
+}
+__global__ void k_batch_gate(BatchInst* __restrict__ bi, int n,
+                             const cudaGraphConditionalHandle* __restrict__ ifh) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int r = inst_runs(bi[i]) ? 1 : 0;
+  bi[i].running = r;
+  cudaGraphSetConditional(ifh[i], r);
+}
+__global__ void k_batch_ctl(const BatchInst* __restrict__ bi, int n, cudaGraphConditionalHandle wh,
+                            int* __restrict__ iter, int cap) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  bool any = false, failed = false;
+  for (int i = 0; i < n; ++i) {
+    failed |= bi[i].failed != 0;
+    any |= inst_runs(bi[i]);
+  }
+  const int it = *iter + 1;
+  *iter = it;
+  // the cap bounds every launch of the loop, whatever the clocks say
+  cudaGraphSetConditional(wh, (any && !failed && it < cap) ? 1u : 0u);
+}
+__global__ void k_inst_begin(BatchInst* __restrict__ b, const DevClock* __restrict__ clk,
+                             DevClock* __restrict__ clk_save) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  *clk_save = *clk;
+  b->since_before = b->since;
+  b->reorder = (b->every > 0 && b->since >= b->every) ? 1 : 0;
+  if (b->reorder) b->since = 0;
+}
+__global__ void k_inst_end(BatchInst* __restrict__ b, const int* __restrict__ err,
+                           const int32_t* __restrict__ overflow, const int* __restrict__ status) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (*err || *overflow || *status) {
+    b->failed = 1;
+  } else {
+    b->steps += 1;
+    b->since += 1;
+  }
+}
+__global__ void k_reorder_gather_gated(const BatchInst* __restrict__ b,
+                                       const double* __restrict__ cin, double* __restrict__ cout,
+                                       const int32_t* __restrict__ oin, int32_t* __restrict__ oout,
+                                       const int32_t* __restrict__ centre_p, int64_t nreal,
+                                       int64_t n) {
+  if (!b->reorder) return;
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const int64_t src = i < nreal ? int64_t(centre_p[i]) : i;
+  for (int f = 0; f < NCOL; ++f) cout[f * n + i] = cin[f * n + src];
+  oout[i] = oin[src];
+}
+__global__ void k_reorder_back_gated(const BatchInst* __restrict__ b, const double* __restrict__ cin,
+                                     double* __restrict__ cout, const int32_t* __restrict__ oin,
+                                     int32_t* __restrict__ oout, int64_t n) {
+  if (!b->reorder) return;
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  for (int f = 0; f < NCOL; ++f) cout[f * n + i] = cin[f * n + i];
+  oout[i] = oin[i];
+}
+
 __global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i < n) p[i] = v;
@@ -1377,6 +1446,33 @@ void launch_dt(const unsigned long long* red, DtIn in, DevClock* clk, double* ct
 void launch_clock_advance(DevClock* clk, cudaStream_t s) {
   k_clock_advance<<<1, 32, 0, s>>>(clk);
   note_launch();
+}
+void launch_batch_gate(BatchInst* bi, int n, const cudaGraphConditionalHandle* ifh,
+                       cudaStream_t s) {
+  k_batch_gate<<<(n + 127) / 128, 128, 0, s>>>(bi, n, ifh);
+  note_launch();
+}
+void launch_batch_ctl(const BatchInst* bi, int n, cudaGraphConditionalHandle wh, int* iter,
+                      int cap, cudaStream_t s) {
+  k_batch_ctl<<<1, 32, 0, s>>>(bi, n, wh, iter, cap);
+  note_launch();
+}
+void launch_inst_begin(BatchInst* b, const DevClock* clk, DevClock* clk_save, cudaStream_t s) {
+  k_inst_begin<<<1, 32, 0, s>>>(b, clk, clk_save);
+  note_launch();
+}
+void launch_inst_end(BatchInst* b, const int* err, const int32_t* overflow, const int* status,
+                     cudaStream_t s) {
+  k_inst_end<<<1, 32, 0, s>>>(b, err, overflow, status);
+  note_launch();
+}
+void launch_reorder_gated(const BatchInst* b, double* cols, double* cols_alt, int32_t* orig,
+                          int32_t* orig_alt, const int32_t* centre_p, int64_t nreal,
+                          int64_t nrows, cudaStream_t s) {
+  k_reorder_gather_gated<<<nblocks(nrows), TPB, 0, s>>>(b, cols, cols_alt, orig, orig_alt,
+                                                        centre_p, nreal, nrows);
+  k_reorder_back_gated<<<nblocks(nrows), TPB, 0, s>>>(b, cols_alt, cols, orig_alt, orig, nrows);
+  note_launch(2);
 }
 void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s) {
   k_fill_i32<<<nblocks(n), TPB, 0, s>>>(p, n, v);

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "sph_device.cuh"
@@ -81,6 +82,17 @@ struct BoxGeom {
   int reflect[3];   // axes whose real particles are wrapped
 };
 
+// A batch's device loop (sph_engine.cu): step the instances to tfinish
+// (use_state: each instance's own tfinish), at most `limit` steps each, as
+// one CUDA graph per launch; per-instance codes and messages in status /
+// msg.  *used = false when some instance cannot take device-resident steps
+// (nothing stepped; the caller runs host workers instead).
+struct BatchGraph;
+int batch_graph_run(BatchGraph** bg, sph_handle* const* hs, int n, double tfinish,
+                    bool use_state, long long limit, std::vector<int>& status,
+                    std::vector<std::string>& msg, bool* used);
+void batch_graph_destroy(BatchGraph* bg);
+
 // Record an error message for sph_last_error and return `code`.
 int sph_fail(int code, const std::string& msg);
 // The device a handle was created on.
@@ -147,6 +159,38 @@ struct DtIn {
 };
 void launch_dt(const unsigned long long* red, DtIn in, DevClock* clk, double* ctrl, cudaStream_t s);
 void launch_clock_advance(DevClock* clk, cudaStream_t s);
+
+// ---- batches stepped by one device loop (a CUDA graph with a while node) ----
+// One record per instance of a batch, in device memory.  The loop's gate
+// kernel decides which instances step in an iteration (their if nodes);
+// each instance's step begins by deciding its row reorder and ends by
+// checking its error words.
+struct BatchInst {
+  const DevClock* clk;    // the instance's device clock
+  int running;            // this iteration steps the instance
+  int failed;             // a step set an error word: the host redoes it
+  int every, since;       // row-reorder period, steps since the last reorder
+  int reorder;            // the current step reorders the rows first
+  int since_before;       // `since` before the current step
+  long long steps, limit; // steps completed in the loop, the most it may take
+};
+// t < tfinish + eps and not stopped (the time loop's condition), for an
+// instance that has not failed and has steps left
+void launch_batch_gate(BatchInst* bi, int n, const cudaGraphConditionalHandle* ifh,
+                       cudaStream_t s);
+// after every instance of an iteration: continue while some instance runs,
+// none failed and fewer than cap iterations ran in this launch
+void launch_batch_ctl(const BatchInst* bi, int n, cudaGraphConditionalHandle wh, int* iter,
+                      int cap, cudaStream_t s);
+void launch_inst_begin(BatchInst* b, const DevClock* clk, DevClock* clk_save, cudaStream_t s);
+void launch_inst_end(BatchInst* b, const int* err, const int32_t* overflow, const int* status,
+                     cudaStream_t s);
+// the rows in the order of the last search (real rows by centre_p, then the
+// fixed rows as they are) when b->reorder is set: gathered into the spare
+// table, then copied back, so the table keeps its address
+void launch_reorder_gated(const BatchInst* b, double* cols, double* cols_alt, int32_t* orig,
+                          int32_t* orig_alt, const int32_t* centre_p, int64_t nreal,
+                          int64_t nrows, cudaStream_t s);
 void launch_keys_dev(const double* cols, int64_t nrows, const double* gx, const double* gy,
                      const double* gz, const DevPlan* plan, int64_t ncap, uint32_t* keys,
                      int32_t* vals, cudaStream_t s);

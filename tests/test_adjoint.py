@@ -287,3 +287,53 @@ def test_diffusion_torch_function(engine_lib, cuda_ok):
     e.close()
     assert np.allclose(T0.grad.numpy(), gT0, rtol=1e-12, atol=1e-14)
     assert dc.grad.item() == pytest.approx(gdc, rel=1e-12)
+
+
+def test_adjoint_workload_fd_spot_check(engine_lib, cuda_ok):
+    """The adjoint workload itself at its FP64 check size: shear flow on a
+    64^2 periodic lattice, M6, alpha = 1, beta = 2, 200 fixed-dt leapfrog
+    steps (dt 5e-4) with a checkpoint every 20 steps and recomputation in
+    between; the target is the final velocity field of the same run started
+    with shear amplitude 0.12 instead of 0.1.  Central differences
+    (eps = 1e-6) of the loss against the
+    adjoint for alpha and for single initial velocity components; the
+    tolerance, 1e-4 relative, allows for the few pairs whose v_ab . r_ab
+    crosses the viscosity's switch within eps over 200 steps."""
+    n, nsteps, every, dt, eps = 64, 200, 20, 5e-4, 1e-6
+    st, store = ic.shear2d(n=n)
+
+    def run(s, alpha=1.0):
+        e = abi.Engine(st, s, "m6", lib=engine_lib)
+        e.set_param(abi.P_AV_ALPHA, alpha)
+        e.set_param(abi.P_FIXED_DT, dt)
+        e.adjoint_forward(nsteps, every)
+        return e
+
+    e = run(ic.shear2d(n=n, amp=0.12)[1])
+    try:
+        target = e.get_store()[:, V]
+    finally:
+        e.close()
+    e = run(store)
+    try:
+        vT = e.get_store()[:, V]
+        g = e.adjoint_backward(dl_dv=2.0 * (vT - target))
+    finally:
+        e.close()
+
+    def loss(s, alpha=1.0):
+        e = run(s, alpha)
+        try:
+            return _loss(e.get_store()[:, V], target)
+        finally:
+            e.close()
+    fd = (loss(store, 1.0 + eps) - loss(store, 1.0 - eps)) / (2 * eps)
+    ad = float(g["g_par"][0])
+    assert abs(ad - fd) <= 1e-4 * abs(fd), ("alpha", ad, fd)
+    for i in (0, 1234, 3001):
+        sp, sm = store.copy(), store.copy()
+        sp[i, V[0]] += eps
+        sm[i, V[0]] -= eps
+        fd = (loss(sp) - loss(sm)) / (2 * eps)
+        ad = float(g["g_v0"][i, 0])
+        assert abs(ad - fd) <= 1e-4 * abs(fd) + 1e-9, (i, ad, fd)

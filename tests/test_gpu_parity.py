@@ -238,3 +238,41 @@ def test_nan_position_reports_status(engine_lib, cuda_ok):
         e.iterate()
     assert ex.value.code in (3, 4)
     e.close()
+
+
+def _gauss2d(n=32, seed=7):
+    """2D periodic hydro set-up with the Gauss kernel (base_gauss.f90,
+    support 10 h): an n^2 lattice perturbed by uniform(-0.1, 0.1) dx, a
+    pressure bump and a velocity shear, so that circuit2's pressure,
+    viscosity and conductivity terms all act."""
+    pos, dx = ic.periodic_lattice(n, 2, seed=seed, amp=0.1)
+    N = pos.shape[0]
+    st = ic._periodic_state(2, n, 1.2, "gauss", "hydro", tfinish=1.0)
+    for k, v in (("realpn", N), ("gamma", 5.0 / 3.0), ("dtprint", 1.0), ("time", 0.0),
+                 ("au", 1.0)):
+        ic.set_state(st, k, v)
+    store = np.zeros((N, 32))
+    store[:, 0:3] = pos
+    x, y = pos[:, 0], pos[:, 1]
+    P = 1.0 + 0.5 * np.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2) / 0.02)
+    store[:, COL["m"]] = 1.0 / N
+    store[:, COL["den"]] = 1.0
+    store[:, COL["h"]] = 1.2 * dx
+    store[:, COL["om"]] = 1.0
+    store[:, COL["u"]] = P / (2.0 / 3.0)
+    store[:, COL["p"]] = P
+    store[:, COL["c"]] = np.sqrt(5.0 / 3.0 * P)
+    store[:, COL["vx"]] = 0.1 * np.sin(2 * np.pi * y)
+    store[:, COL["type"]] = 1.0
+    return st, store
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_gauss_kernel_iterate(oracle_lib, engine_lib, cuda_ok, prec):
+    st, store = _gauss2d()
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "gauss", FP64, "iterate")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "gauss", prec, "iterate")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    bad = compare(ref, got, prec, part_fields=("den", "h", "om", "c"),
+                  field_fields=("ax", "ay", "du", "dh"))
+    assert not bad, bad
