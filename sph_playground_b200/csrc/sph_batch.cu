@@ -40,10 +40,24 @@ struct sph_batch {
 
   // the device loop over all instances; *used = false when it does not apply
   int device_loop(double tfinish, bool use_state, long long limit, bool* used) {
+    // start the instances that have not run yet on the host workers, side
+    // by side (the start-up iterate of main.f90 runs on the host path, with
+    // its round trips); an instance that fails there is reported below
+    constexpr int kStateTfinish = 11;  // the state slot of tfinish (const.f90 ec_tfinish)
+    if (!use_state)
+      for (auto* x : h) sph_set_param(x, kStateTfinish, tfinish);
+    run([](sph_handle* x) { return sph_step(x, 0); });
+    std::vector<int> st0 = status;
+    std::vector<std::string> msg0 = msg;
     std::fill(status.begin(), status.end(), 0);
     std::fill(msg.begin(), msg.end(), std::string());
     int rc = sph::batch_graph_run(&bg, h.data(), int(h.size()), tfinish, use_state, limit, status,
                                   msg, used);
+    for (size_t i = 0; i < h.size(); ++i)
+      if (st0[i] && !status[i]) {
+        status[i] = st0[i];
+        msg[i] = msg0[i];
+      }
     if (rc || !*used) return rc;
     for (size_t i = 0; i < h.size(); ++i)
       if (status[i]) return sph::sph_fail(status[i], "instance " + std::to_string(i) + ": " + msg[i]);

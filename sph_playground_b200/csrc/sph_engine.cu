@@ -1742,7 +1742,7 @@ struct BatchGraph {
     if (e != cudaSuccess) return bad(e, "while node");
     cudaGraph_t body = wp.conditional.phGraph_out[0];
     // gate
-    cudaGraphNode_t gate_node = nullptr, last = nullptr;
+    cudaGraphNode_t gate_node = nullptr;
     {
       e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) return bad(e, "gate capture");
@@ -1795,7 +1795,6 @@ struct BatchGraph {
       e = cudaStreamEndCapture(s, &out);
       if (e != cudaSuccess) return bad(e, "control capture end");
     }
-    (void)last;
     CK(cudaMemcpyAsync(ifh.p, hh.data(), sizeof(cudaGraphConditionalHandle) * n,
                        cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
