@@ -910,20 +910,28 @@ __global__ void __launch_bounds__(TPB)
 k_timestep_reduce(const double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ orig,
                   int64_t nrows, int64_t n_ts, Params P, unsigned long long* __restrict__ red) {
   // slots: hmin, cmax, denmin, cmin, kapmax, bmax, kapmin, lammax
+  // kappa (slots 4, 6) enters only the diffusion / FLD timesteps and B
+  // (slot 5) only the MHD one: their columns are read only when those
+  // equations are on (a slot left at its start value is not used)
   double v[8] = {1e308, -1e308, 1e308, 1e308, -1e308, -1e308, 1e308, -1e308};
   const bool is_max[8] = {false, true, false, false, true, true, false, true};
+  const bool need_ka = P.eq_diff || P.eq_fld, need_b = P.eq_magneto;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nrows;
        i += int64_t(gridDim.x) * blockDim.x) {
     if (orig[i] >= n_ts) continue;
     double h = cols[es_h * ld + i], c = cols[es_c * ld + i], d = cols[es_den * ld + i];
-    double ka = cols[es_kappa * ld + i];
     v[0] = fmin(v[0], h);
     v[1] = fmax(v[1], c);
     v[2] = fmin(v[2], d);
     v[3] = fmin(v[3], c);
-    v[4] = fmax(v[4], ka);
-    v[5] = fmax(v[5], fmax(fmax(cols[es_bx * ld + i], cols[es_by * ld + i]), cols[es_bz * ld + i]));
-    v[6] = fmin(v[6], ka);
+    double ka = 0.0;
+    if (need_ka) {
+      ka = cols[es_kappa * ld + i];
+      v[4] = fmax(v[4], ka);
+      v[6] = fmin(v[6], ka);
+    }
+    if (need_b)
+      v[5] = fmax(v[5], fmax(fmax(cols[es_bx * ld + i], cols[es_by * ld + i]), cols[es_bz * ld + i]));
     if (P.eq_fld) {
       double n0 = cols[es_dtdx * ld + i], n1 = cols[es_dtdy * ld + i], n2 = cols[es_dtdz * ld + i];
       double ta = cols[es_t * ld + i];
