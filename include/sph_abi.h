@@ -189,6 +189,29 @@ int sph_get_neighbours(sph_handle* h, int64_t* offsets, int64_t* pairs,
  * neighboursearch.f90:74-180). */
 int sph_get_neighbour_digest(sph_handle* h, uint64_t* out, int64_t n);
 
+/* ---- one leapfrog step in parts --------------------------------------------
+ * The step of sph_step (main.f90:241-373, leapfrog without STS or radiation
+ * exchange) split where a domain decomposition exchanges particle fields:
+ *   sph_timestep  -> dt = min over this handle's real rows of the equations'
+ *                    limits (timestep.f90:40-166; the caller takes the
+ *                    global minimum and clips it to tfinish / output times
+ *                    as main.f90:273-299 does);
+ *   sph_predict   (main.f90:323-342), sph_density (images, search,
+ *                    circuit1, EOS), [exchange of rho, h, Omega, P, c],
+ *   sph_forces    (circuit2 on the density pass's neighbour lists),
+ *                    [exchange of a, du/dt, dh/dt],
+ *   sph_correct   (main.f90:348-362; advances the handle's time by dt).
+ * Rows keep their physical order from sph_predict to sph_correct.
+ * sph_get_columns / sph_set_columns move whole columns of the table
+ * (1-based field indices of const.f90, nf of them) in caller row order:
+ * buf[k * n_rows + row]; buf may be host or device memory. */
+int sph_timestep(sph_handle* h, double* dt);
+int sph_predict(sph_handle* h, double dt);
+int sph_forces(sph_handle* h);
+int sph_correct(sph_handle* h, double dt);
+int sph_get_columns(sph_handle* h, const int* fields, int nf, double* buf);
+int sph_set_columns(sph_handle* h, const int* fields, int nf, const double* buf);
+
 int sph_get_counters(sph_handle* h, int64_t* out, int n);
 int sph_reset_counters(sph_handle* h);
 int sph_get_timers(sph_handle* h, double* out_ms, int n);

@@ -1180,6 +1180,65 @@ struct Oracle {
     return SPH_OK;
   }
 
+  // ---- one leapfrog step in parts (the split step of include/sph_abi.h):
+  // the predictor and corrector of one_step (main.f90:323-362) without STS
+  // or radiation exchange, and circuit2 alone on the lists of the last
+  // density pass
+  bool split_ok() {
+    eqset();
+    if (eq_sts || eq_radexch)
+      return fail(SPH_ERR_UNSUPPORTED, "split step: leapfrog without STS or radiation exchange only") == 0;
+    return true;
+  }
+  int split_predict(double dt) {
+    if (!split_ok()) return SPH_ERR_UNSUPPORTED;
+    const int64_t n = n_integrated();
+    tr.resize(3 * n); tv.resize(3 * n); ta.resize(3 * n); tdu.resize(n); tdh.resize(n);
+    tddt.resize(n); tdb.resize(3 * n);
+    for (int64_t i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) {
+        tr[3 * i + k] = S(i, es_rx + k); tv[3 * i + k] = S(i, es_vx + k);
+        ta[3 * i + k] = S(i, es_ax + k); tdb[3 * i + k] = S(i, es_dbx + k);
+      }
+      tdu[i] = S(i, es_du); tdh[i] = S(i, es_dh); tddt[i] = S(i, es_ddt);
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) {
+        S(i, es_rx + k) = S(i, es_rx + k) + dt * tv[3 * i + k] + 0.5 * dt * dt * ta[3 * i + k];
+        S(i, es_vx + k) = tv[3 * i + k] + dt * ta[3 * i + k];
+      }
+      S(i, es_u) = S(i, es_u) + dt * tdu[i];
+      S(i, es_h) = S(i, es_h) + dt * tdh[i];
+      S(i, es_t) = S(i, es_t) + dt * tddt[i];
+      for (int k = 0; k < 3; ++k) S(i, es_bx + k) = S(i, es_bx + k) + dt * tdb[3 * i + k];
+    }
+    return SPH_OK;
+  }
+  int split_forces() {
+    if (noff.empty()) return fail(SPH_ERR_STATE, "sph_forces needs the lists of a density pass");
+    int rc = c2();
+    if (rc) return rc;
+    cnt[SPH_CNT_ITERATES]++;
+    return SPH_OK;
+  }
+  int split_correct(double dt) {
+    if (!split_ok()) return SPH_ERR_UNSUPPORTED;
+    const int64_t n = n_integrated();
+    if (int64_t(tdu.size()) != n) return fail(SPH_ERR_STATE, "sph_correct without sph_predict");
+    for (int64_t i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k)
+        S(i, es_vx + k) = S(i, es_vx + k) + 0.5 * dt * (S(i, es_ax + k) - ta[3 * i + k]);
+      S(i, es_u) = S(i, es_u) + 0.5 * dt * (S(i, es_du) - tdu[i]);
+      S(i, es_h) = S(i, es_h) + 0.5 * dt * (S(i, es_dh) - tdh[i]);
+      for (int k = 0; k < 3; ++k)
+        S(i, es_bx + k) = S(i, es_bx + k) + 0.5 * dt * (S(i, es_dbx + k) - tdb[3 * i + k]);
+      S(i, es_t) = S(i, es_t) + 0.5 * dt * (S(i, es_ddt) - tddt[i]);
+    }
+    st[ec_time] = st[ec_time] + dt;
+    cnt[SPH_CNT_STEPS]++;
+    return SPH_OK;
+  }
+
   int one_step(double tfinish, bool& done) {
     double t = st[ec_time];
     if (!((t < tfinish + eps0) && !stopped)) { done = true; return SPH_OK; }
@@ -1456,6 +1515,59 @@ int sph_iterate(sph_handle* h) {
 int sph_density(sph_handle* h) {
   if (!h) return fail(SPH_ERR_ARG, "null handle");
   return h->o.density_pass();
+}
+
+int sph_timestep(sph_handle* h, double* dt) {
+  if (!h || !dt) return fail(SPH_ERR_ARG, "null argument");
+  Oracle& o = h->o;
+  o.eqset();
+  int rc = o.initkernel();
+  if (rc) return rc;
+  double dthydro, dtdiff, dtfld;
+  o.calctimestep(dthydro, dtdiff, dtfld, *dt);
+  return SPH_OK;
+}
+
+int sph_predict(sph_handle* h, double dt) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  return h->o.split_predict(dt);
+}
+
+int sph_forces(sph_handle* h) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  return h->o.split_forces();
+}
+
+int sph_correct(sph_handle* h, double dt) {
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  return h->o.split_correct(dt);
+}
+
+static int oracle_fields(const int* fields, int nf) {
+  if (!fields || nf < 1 || nf > ES) return fail(SPH_ERR_ARG, "1 to 32 fields");
+  for (int k = 0; k < nf; ++k)
+    if (fields[k] < 1 || fields[k] > ES) return fail(SPH_ERR_ARG, "bad field index");
+  return SPH_OK;
+}
+
+int sph_get_columns(sph_handle* h, const int* fields, int nf, double* buf) {
+  if (!h || !buf) return fail(SPH_ERR_ARG, "null argument");
+  int rc = oracle_fields(fields, nf);
+  if (rc) return rc;
+  Oracle& o = h->o;
+  for (int k = 0; k < nf; ++k)
+    for (int64_t i = 0; i < o.nrows; ++i) buf[k * o.nrows + i] = o.S(i, fields[k] - 1);
+  return SPH_OK;
+}
+
+int sph_set_columns(sph_handle* h, const int* fields, int nf, const double* buf) {
+  if (!h || !buf) return fail(SPH_ERR_ARG, "null argument");
+  int rc = oracle_fields(fields, nf);
+  if (rc) return rc;
+  Oracle& o = h->o;
+  for (int k = 0; k < nf; ++k)
+    for (int64_t i = 0; i < o.nrows; ++i) o.S(i, fields[k] - 1) = buf[k * o.nrows + i];
+  return SPH_OK;
 }
 
 int sph_step(sph_handle* h, int nsteps) {

@@ -58,7 +58,8 @@ ABI_SYMBOLS = [
     "sph_get_state", "sph_get_neighbours", "sph_get_neighbour_digest", "sph_get_counters",
     "sph_reset_counters", "sph_get_timers", "sph_last_error", "sph_destroy",
     "sph_batch_create", "sph_batch_step", "sph_batch_run_to", "sph_batch_status",
-    "sph_batch_destroy", "sph_errcalc",
+    "sph_batch_destroy", "sph_errcalc", "sph_timestep", "sph_predict", "sph_forces",
+    "sph_correct", "sph_get_columns", "sph_set_columns",
 ]
 
 
@@ -113,6 +114,12 @@ def load(path=None):
     lib.sph_batch_destroy.argtypes = [vp]
     lib.sph_batch_destroy.restype = None
     lib.sph_errcalc.argtypes = [vp, P(d), i64, P(d)]
+    lib.sph_timestep.argtypes = [vp, P(d)]
+    lib.sph_predict.argtypes = [vp, d]
+    lib.sph_forces.argtypes = [vp]
+    lib.sph_correct.argtypes = [vp, d]
+    lib.sph_get_columns.argtypes = [vp, P(c_int), c_int, vp]
+    lib.sph_set_columns.argtypes = [vp, P(c_int), c_int, vp]
     if hasattr(lib, "sph_adjoint_forward"):  # the CUDA engine only
         lib.sph_adjoint_forward.argtypes = [vp, c_int, c_int]
         lib.sph_adjoint_forward.restype = c_int
@@ -286,6 +293,49 @@ class Engine:
         self._check(self.lib.sph_get_neighbour_digest(
             self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), self.n_real))
         return out[:, 0].astype(np.int64), out[:, 1]
+
+    # ---- one leapfrog step in parts (sph_timestep .. sph_correct) ----------
+    def timestep(self):
+        """dt over this handle's real rows (before clipping to tfinish)."""
+        v = ctypes.c_double()
+        self._check(self.lib.sph_timestep(self.h, ctypes.byref(v)))
+        return v.value
+
+    def predict(self, dt):
+        self._check(self.lib.sph_predict(self.h, float(dt)))
+
+    def forces(self):
+        self._check(self.lib.sph_forces(self.h))
+
+    def correct(self, dt):
+        self._check(self.lib.sph_correct(self.h, float(dt)))
+
+    @staticmethod
+    def _fields(names):
+        idx = [consts.es[n] if isinstance(n, str) else int(n) for n in names]
+        return (ctypes.c_int * len(idx))(*idx), len(idx)
+
+    def get_columns(self, names, out=None):
+        """(len(names), n_rows) array of the named fields in caller row
+        order; `out` may be a numpy array or a device pointer (int)."""
+        f, nf = self._fields(names)
+        if out is None:
+            out = np.empty((nf, self.n_rows), dtype=np.float64)
+        ptr = out if isinstance(out, int) else out.ctypes.data
+        self._check(self.lib.sph_get_columns(self.h, f, nf, ctypes.c_void_p(ptr)))
+        return out
+
+    def set_columns(self, names, values):
+        """Write the named fields (len(names), n_rows) in caller row order;
+        `values` may be a numpy array or a device pointer (int)."""
+        f, nf = self._fields(names)
+        if isinstance(values, int):
+            ptr = values
+        else:
+            values = np.ascontiguousarray(values, dtype=np.float64)
+            assert values.shape == (nf, self.n_rows)
+            ptr = values.ctypes.data
+        self._check(self.lib.sph_set_columns(self.h, f, nf, ctypes.c_void_p(ptr)))
 
     def counters(self):
         out = np.zeros(len(COUNTERS), dtype=np.int64)

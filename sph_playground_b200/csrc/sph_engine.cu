@@ -180,6 +180,10 @@ struct sph_handle {
   // of parameter changes (a captured loop holds the values it saw)
   DevBuf bclk_save;
   long long param_gen = 0;
+  // between sph_predict and sph_correct of a split step: the rows keep their
+  // physical order (the predictor's saves are per physical row)
+  bool in_split_step = false;
+  DevBuf colbuf;  // staging of sph_get_columns / sph_set_columns
   const DevPlan* dplan = nullptr;  // set while a device-resident step is built
   int64_t nghost_cap = 0, nall_cap = 0;
   int end_bit_cap = 0;
@@ -485,7 +489,7 @@ struct sph_handle {
 
   // ---- physical re-ordering of the rows (locality of the pair loops) ---------------------
   int reorder_rows() {
-    if (!have_order) return SPH_OK;
+    if (!have_order || in_split_step) return SPH_OK;
     // perm = real rows in cell order, then the fixed rows as they are
     int32_t* perm = cpos.as<int32_t>();
     CK(cudaMemcpyAsync(perm, centre_p.p, sizeof(int32_t) * nreal, cudaMemcpyDeviceToDevice, s));
@@ -2198,6 +2202,109 @@ int sph_get_neighbour_digest(sph_handle* h, uint64_t* out, int64_t n) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, d.p, sizeof(uint64_t) * 2 * nc, cudaMemcpyDeviceToHost, h->s));
   CK(cudaStreamSynchronize(h->s));
+  return SPH_OK;
+}
+
+// ---- one leapfrog step in parts (a driver that exchanges fields between
+// the parts, one domain per GPU) ----
+int sph_timestep(sph_handle* h, double* dt) {
+  AllocScope alloc_scope(h);
+  if (!h || !dt) return fail(SPH_ERR_ARG, "null argument");
+  double dthydro = 0., dtdiff = 0., dtfld = 0., d = 0.;
+  RC(h->timestep(dthydro, dtdiff, dtfld, d));
+  *dt = d;
+  return SPH_OK;
+}
+
+static int split_step_supported(sph_handle* h) {
+  h->eqset();
+  if (h->eq_sts || h->eq_radexch)
+    return fail(SPH_ERR_UNSUPPORTED,
+                "split step: leapfrog without STS or radiation exchange only");
+  return SPH_OK;
+}
+
+int sph_predict(sph_handle* h, double dt) {
+  AllocScope alloc_scope(h);
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  RC(split_step_supported(h));
+  h->h_ctrl[0] = dt;
+  CK(cudaMemcpyAsync(h->ctrl.p, h->h_ctrl, sizeof(double), cudaMemcpyHostToDevice, h->s));
+  launch_predict(h->cols.as<double>(), h->nrows, h->orig.as<int32_t>(), h->nrows, h->n_int,
+                 h->save.as<double>(), h->ctrl.as<double>(), h->lf_mode(false), h->s);
+  CK(cudaGetLastError());
+  h->in_split_step = true;
+  return SPH_OK;
+}
+
+int sph_forces(sph_handle* h) {
+  AllocScope alloc_scope(h);
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  if (!h->have_order) return fail(SPH_ERR_STATE, "sph_forces needs the lists of a density pass");
+  Params P{};
+  RC(h->params(P));
+  Mode m;
+  RC(h->mode(m));
+  RC(h->circuit2(m, P));
+  RC(h->check_status());
+  h->cnt_host[SPH_CNT_ITERATES] += 1;
+  h->collect_timers();
+  return SPH_OK;
+}
+
+int sph_correct(sph_handle* h, double dt) {
+  AllocScope alloc_scope(h);
+  if (!h) return fail(SPH_ERR_ARG, "null handle");
+  RC(split_step_supported(h));
+  if (!h->in_split_step) return fail(SPH_ERR_STATE, "sph_correct without sph_predict");
+  h->h_ctrl[0] = dt;
+  CK(cudaMemcpyAsync(h->ctrl.p, h->h_ctrl, sizeof(double), cudaMemcpyHostToDevice, h->s));
+  launch_correct(h->cols.as<double>(), h->nrows, h->orig.as<int32_t>(), h->nrows, h->n_int,
+                 h->save.as<double>(), h->ctrl.as<double>(), h->lf_mode(false), h->s);
+  CK(cudaGetLastError());
+  h->in_split_step = false;
+  h->st[ec_time] += dt;
+  h->cnt_host[SPH_CNT_STEPS]++;
+  return SPH_OK;
+}
+
+static int column_set(const int* fields, int nf, ColumnSet* fs) {
+  if (!fields || nf < 1 || nf > SPH_ES_TOTAL) return fail(SPH_ERR_ARG, "1 to 32 fields");
+  fs->n = nf;
+  for (int k = 0; k < nf; ++k) {
+    if (fields[k] < 1 || fields[k] > SPH_ES_TOTAL) return fail(SPH_ERR_ARG, "bad field index");
+    fs->f[k] = fields[k] - 1;
+  }
+  return SPH_OK;
+}
+
+int sph_get_columns(sph_handle* h, const int* fields, int nf, double* out) {
+  AllocScope alloc_scope(h);
+  if (!h || !out) return fail(SPH_ERR_ARG, "null argument");
+  ColumnSet fs{};
+  RC(column_set(fields, nf, &fs));
+  const size_t bytes = sizeof(double) * size_t(nf) * size_t(h->nrows);
+  RC(h->colbuf.ensure(bytes));
+  launch_get_columns(h->cols.as<double>(), h->nrows, h->orig.as<int32_t>(), h->nrows, fs,
+                     h->colbuf.as<double>(), h->s);
+  CK(cudaMemcpyAsync(out, h->colbuf.p, bytes, cudaMemcpyDefault, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
+  return SPH_OK;
+}
+
+int sph_set_columns(sph_handle* h, const int* fields, int nf, const double* in) {
+  AllocScope alloc_scope(h);
+  if (!h || !in) return fail(SPH_ERR_ARG, "null argument");
+  ColumnSet fs{};
+  RC(column_set(fields, nf, &fs));
+  const size_t bytes = sizeof(double) * size_t(nf) * size_t(h->nrows);
+  RC(h->colbuf.ensure(bytes));
+  CK(cudaMemcpyAsync(h->colbuf.p, in, bytes, cudaMemcpyDefault, h->s));
+  launch_set_columns(h->cols.as<double>(), h->nrows, h->orig.as<int32_t>(), h->nrows, fs,
+                     h->colbuf.as<double>(), h->s);
+  CK(cudaStreamSynchronize(h->s));
+  CK(cudaGetLastError());
   return SPH_OK;
 }
 

@@ -1113,6 +1113,25 @@ __global__ void k_clock_advance(DevClock* __restrict__ clk) {
   if (blockIdx.x == 0 && threadIdx.x == 0) clk->t = __dadd_rn(clk->t, clk->dt);
 }
 
+// ---- selected columns in caller row order (the split step's exchanges) -------------
+// out[k * nrows + orig[p]] = column fs.f[k] of physical row p, and back
+__global__ void k_get_columns(const double* __restrict__ cols, int64_t ld,
+                              const int32_t* __restrict__ orig, int64_t nrows, ColumnSet fs,
+                              double* __restrict__ out) {
+  const int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p >= nrows) return;
+  const int64_t o = orig[p];
+  for (int k = 0; k < fs.n; ++k) out[k * nrows + o] = cols[fs.f[k] * ld + p];
+}
+__global__ void k_set_columns(double* __restrict__ cols, int64_t ld,
+                              const int32_t* __restrict__ orig, int64_t nrows, ColumnSet fs,
+                              const double* __restrict__ in) {
+  const int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (p >= nrows) return;
+  const int64_t o = orig[p];
+  for (int k = 0; k < fs.n; ++k) cols[fs.f[k] * ld + p] = in[k * nrows + o];
+}
+
 // ---- the device loop of a batch ----------------------------------------------------
 // the time loop's condition of main.f90:241 as the host evaluates it
 // (t < tfinish + epsilon(1d0) and not stopped)
@@ -1453,6 +1472,16 @@ void launch_dt(const unsigned long long* red, DtIn in, DevClock* clk, double* ct
 }
 void launch_clock_advance(DevClock* clk, cudaStream_t s) {
   k_clock_advance<<<1, 32, 0, s>>>(clk);
+  note_launch();
+}
+void launch_get_columns(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                        ColumnSet fs, double* out, cudaStream_t s) {
+  k_get_columns<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, fs, out);
+  note_launch();
+}
+void launch_set_columns(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                        ColumnSet fs, const double* in, cudaStream_t s) {
+  k_set_columns<<<nblocks(nrows), TPB, 0, s>>>(cols, ld, orig, nrows, fs, in);
   note_launch();
 }
 void launch_batch_gate(BatchInst* bi, int n, const cudaGraphConditionalHandle* ifh,

@@ -160,6 +160,16 @@ struct DtIn {
 void launch_dt(const unsigned long long* red, DtIn in, DevClock* clk, double* ctrl, cudaStream_t s);
 void launch_clock_advance(DevClock* clk, cudaStream_t s);
 
+// ---- selected columns of the table in caller row order ----
+struct ColumnSet {
+  int n;
+  int f[SPH_ES_TOTAL];  // 0-based store columns
+};
+void launch_get_columns(const double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                        ColumnSet fs, double* out, cudaStream_t s);
+void launch_set_columns(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
+                        ColumnSet fs, const double* in, cudaStream_t s);
+
 // ---- batches stepped by one device loop (a CUDA graph with a while node) ----
 // One record per instance of a batch, in device memory.  The loop's gate
 // kernel decides which instances step in an iteration (their if nodes);
