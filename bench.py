@@ -287,7 +287,12 @@ def size160_block(engine, st, store, steps, warmup):
         ms, cnt, tm = timed_steps(e, steps)
         e.close()
         out[name] = {"value": N * steps / (ms * 1e-3), "ms_per_step": ms / steps,
-                     "phases_ms_per_step": tm}
+                     "phases_ms_per_step": tm,
+                     "work_per_step": {"neib_pairs": cnt["neib_pairs"] / steps,
+                                       "c1_pairs": cnt["c1_pairs"] / steps,
+                                       "newton_sweeps_per_particle":
+                                           cnt["c1_centre_sweeps"] / (steps * N),
+                                       "c1_max_sweeps": cnt["c1_sweeps"]}}
     out["speedup_fp32_vs_fp64"] = out["fp32_comp"]["value"] / out["fp64"]["value"]
     return out
 
@@ -711,6 +716,8 @@ def main():
                               "c1_pairs": cnt["c1_pairs"] / args.steps,
                               "c2_pairs": cnt["c2_pairs"] / args.steps,
                               "c1_max_sweeps": cnt["c1_sweeps"],
+                              "newton_sweeps_per_particle":
+                                  cnt["c1_centre_sweeps"] / (args.steps * N),
                               "neib_max": cnt["neib_max"],
                               "searches": cnt["searches"] / args.steps,
                               "exact_tests": cnt["exact_tests"] / args.steps,
