@@ -95,6 +95,8 @@ def parse():
                     help="skip the 21-instance diffusion batch (config 3)")
     ap.add_argument("--no-160", action="store_true",
                     help="skip the 160^3 Sedov throughput line (config 5b)")
+    ap.add_argument("--no-decomposed", action="store_true",
+                    help="with N > 1: skip the one-problem-over-N-ranks block")
     ap.add_argument("--param", action="append", default=[],
                     help="engine parameter NAME=VALUE (abi.P_* name or slot), for both arms")
     return ap.parse_args()
@@ -272,6 +274,37 @@ def batch_block(lib, tfinish=0.01):
     out["timing"] = ("host clock around the synchronous sph_batch_step(1) (instance start-up, "
                      "loop build) and sph_batch_run_to (the device loop) calls")
     return out
+
+
+def decomposed_block(lib, st, store, steps, warmup, shapes, device):
+    """One problem over all ranks (sph_playground_b200.domain.DecomposedRun:
+    each rank computes the pairs of its Morton range of particles, two
+    all-gathers per step): the Sedov step of this workload, FP32-comp,
+    timed on the host between barriers after `warmup` steps (max over
+    ranks)."""
+    import torch
+    import torch.distributed as dist
+    from sph_playground_b200 import domain
+    run = domain.DecomposedRun(st, store, "m6", precision=abi.PREC_FP32_COMP, lib=lib,
+                               device=device)
+    for k, v in shapes.items():
+        run.e.set_param(getattr(abi, k), float(v))
+    run.start()
+    run.run_to(1.0, max_steps=warmup)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    run.run_to(1.0, max_steps=warmup + steps)
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0)
+    n_own = run.n_own
+    run.close()
+    N = store.shape[0]
+    return {"workload": workload_name(round(N ** (1 / 3))) + ", FP32-comp, one problem over "
+                        f"{dist.get_world_size()} ranks (particle decomposition)",
+            "value": N * steps / el, "unit": UNIT, "ms_per_step": 1e3 * el / steps,
+            "scaling": "strong", "owned_particles_rank0": n_own,
+            "timing": "host clock between barriers around synchronous steps, max over ranks"}
 
 
 def size160_block(engine, st, store, steps, warmup):
@@ -677,6 +710,10 @@ def main():
     batch = None
     if not args.no_batch:
         batch = batch_block(lib)
+    decomposed = None
+    if ws > 1 and not args.no_decomposed:
+        decomposed = decomposed_block(lib, st, store, args.steps, args.warmup,
+                                      tuned[abi.PREC_FP32_COMP], f"cuda:{local}")
     big = None
     if not args.no_160 and args.n == 128:
         st160, store160 = ic.sedov3d(n=160)
@@ -727,6 +764,7 @@ def main():
             "adjoint": adj,
             "density_pass": dens,
             "diffusion_batch": batch,
+            "decomposed": decomposed,
             "sedov3d_160": big,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "peak_fp32_tflops": peak32 / 1e12,

@@ -173,21 +173,38 @@ class DecomposedRun(SplitRun):
 
     def _exchange(self, fields):
         """All-gather the named fields of every rank's owned rows and write
-        them into this rank's non-owned rows."""
+        them into this rank's non-owned rows.  On a CUDA device the columns
+        go from the engine's table to a device buffer, through the
+        collective and back without touching the host."""
         import torch
         import torch.distributed as dist
-        vals = self.e.get_columns(fields)  # (nf, n) in local order
         nf = len(fields)
+        if str(self.device) == "cpu":
+            vals = self.e.get_columns(fields)  # (nf, n) in local order
+            mine = torch.zeros((nf, self.max_own), dtype=torch.float64)
+            mine[:, :self.n_own] = torch.from_numpy(vals[:, :self.n_own])
+            parts = [torch.empty_like(mine) for _ in range(self.size)]
+            dist.all_gather(parts, mine)
+            for r, part in enumerate(parts):
+                if r != self.rank:
+                    g = self.owned[r]
+                    vals[:, self.local_of[g]] = part[:, :g.shape[0]].numpy()
+            self.e.set_columns(fields, vals)
+            return
+        if getattr(self, "_dev_idx", None) is None:
+            self._dev_idx = [torch.as_tensor(self.local_of[g], device=self.device)
+                             for g in self.owned]
+        buf = torch.empty((nf, self.n), dtype=torch.float64, device=self.device)
+        self.e.get_columns(fields, out=buf.data_ptr())  # the engine syncs its stream
         mine = torch.zeros((nf, self.max_own), dtype=torch.float64, device=self.device)
-        mine[:, :self.n_own] = torch.from_numpy(vals[:, :self.n_own]).to(self.device)
+        mine[:, :self.n_own] = buf[:, :self.n_own]
         parts = [torch.empty_like(mine) for _ in range(self.size)]
         dist.all_gather(parts, mine)
         for r, part in enumerate(parts):
-            if r == self.rank:
-                continue
-            g = self.owned[r]
-            vals[:, self.local_of[g]] = part[:, :g.shape[0]].cpu().numpy()
-        self.e.set_columns(fields, vals)
+            if r != self.rank:
+                buf[:, self._dev_idx[r]] = part[:, :self.owned[r].shape[0]]
+        torch.cuda.current_stream(self.device).synchronize()
+        self.e.set_columns(fields, buf.data_ptr())
 
     def after_density(self):
         self._exchange(AFTER_DENSITY)

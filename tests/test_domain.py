@@ -139,3 +139,37 @@ def test_decomposed_engine_equals_single_domain(engine_lib, cuda_ok, prec):
     for got, nsteps, _ in res:
         assert nsteps == steps
         assert _rel(got, ref) <= tol
+
+
+@pytest.mark.gpu
+def test_decomposed_device_exchange_single_rank(engine_lib, cuda_ok):
+    """The exchange through device buffers (the NCCL path): one rank of an
+    NCCL group owns every particle, so the columns go from the engine's
+    table to a CUDA tensor, through the collective and back unchanged; the
+    run equals the split run on the same engine to rounding."""
+    import torch
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ["MASTER_PORT"] = str(29500 + (os.getpid() * 13) % 2000)
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        torch.cuda.set_device(0)
+        st, store = _sedov()
+        run = domain.DecomposedRun(st, store, "m6", precision=abi.PREC_FP64, lib=engine_lib,
+                                   device="cuda:0")
+        run.start()
+        run.run_to(T_END)
+        got = run.global_store()
+        nsteps = run.steps
+        run.close()
+    finally:
+        dist.destroy_process_group()
+    with abi.Engine(st, store, "m6", lib=engine_lib) as e:
+        ref_run = domain.SplitRun(e)
+        ref_run.start()
+        ref_run.run_to(T_END)
+        ref = e.get_store()
+    assert nsteps == ref_run.steps
+    # the rank's table holds the rows in Morton order, so the sums inside a
+    # neighbour list run in another order
+    assert _rel(got, ref) <= 1e-12
