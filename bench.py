@@ -712,8 +712,14 @@ def main():
         batch = batch_block(lib)
     decomposed = None
     if ws > 1 and not args.no_decomposed:
-        decomposed = decomposed_block(lib, st, store, args.steps, args.warmup,
-                                      tuned[abi.PREC_FP32_COMP], f"cuda:{local}")
+        # every rank runs the same steps, so an error is raised on all of them
+        # at the same point; it is recorded instead of ending the replicas'
+        # line
+        try:
+            decomposed = decomposed_block(lib, st, store, args.steps, args.warmup,
+                                          tuned[abi.PREC_FP32_COMP], f"cuda:{local}")
+        except Exception as exc:  # noqa: BLE001
+            decomposed = {"error": f"{type(exc).__name__}: {exc}"}
     big = None
     if not args.no_160 and args.n == 128:
         st160, store160 = ic.sedov3d(n=160)

@@ -72,7 +72,11 @@ extern "C" {
                                       replayed CUDA graph with no host round trip
                                       inside (a step that cannot be planned on
                                       the device is redone on the host path)   */
-#define SPH_P_LAST            63
+#define SPH_P_SEARCH_STAGED   64 /* 1: the neighbour search copies each chunk's
+                                      candidate runs into shared memory with
+                                      bulk (TMA) copies instead of fetching
+                                      them per batch (default 0)               */
+#define SPH_P_LAST            64
 
 /* ---- status codes --------------------------------------------------------- */
 #define SPH_OK                     0

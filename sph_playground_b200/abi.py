@@ -43,6 +43,7 @@ P_LANES_SEARCH = 60
 P_LANES_PAIR = 61
 P_FIXED_DT = 62
 P_GRAPH = 63
+P_SEARCH_STAGED = 64
 
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",

@@ -673,7 +673,7 @@ struct sph_handle {
       na.maxcnt = maxcnt.as<int32_t>();
       na.overflow = overflow.as<int32_t>();
       na.dcnt = dcnt.as<unsigned long long>();
-      launch_neighbours(d, lanes_search(), na, s);
+      launch_neighbours(d, lanes_search(), st[SPH_P_SEARCH_STAGED] != 0, na, s);
       CK(cudaMemcpyAsync(h_i32, maxcnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(h_i32 + 1, overflow.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
@@ -681,6 +681,9 @@ struct sph_handle {
       int mc = h_i32[0];
       cnt_host[SPH_CNT_NEIB_MAX] = mc;
       cnt_host[SPH_CNT_SEARCHES]++;
+      if (h_i32[1] & 2)
+        return fail(SPH_ERR_TIMEOUT, "neighbour search: a bulk copy into shared memory did not "
+                                     "complete within its wait limit");
       if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc + 1 > kb.maxneib[d - 1])
         return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
       if (!h_i32[1]) break;
@@ -947,7 +950,7 @@ struct sph_handle {
     na.maxcnt = maxcnt.as<int32_t>();
     na.overflow = overflow.as<int32_t>();
     na.dcnt = dcnt.as<unsigned long long>();
-    launch_neighbours(d, lanes_search(), na, s);
+    launch_neighbours(d, lanes_search(), st[SPH_P_SEARCH_STAGED] != 0, na, s);
     CK(cudaGetLastError());
     return SPH_OK;
   }

@@ -353,9 +353,11 @@ __global__ void k_sorted_gather(const int32_t* __restrict__ sidx, int64_t n, int
   }
   sx[k] = x; sy[k] = y; sz[k] = z;
   // FP32 image of the position, one binade for the whole extent (see PackGeom)
+  // (w carries the record's own sorted index, so that a copy of a run of
+  // records still knows where each came from)
   s32[k] = make_float4(__double2float_rn((x - pg.ox) + pg.shift),
                        __double2float_rn((y - pg.oy) + pg.shift),
-                       __double2float_rn((z - pg.oz) + pg.shift), 0.f);
+                       __double2float_rn((z - pg.oz) + pg.shift), __int_as_float(int32_t(k)));
 }
 
 __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __restrict__ flag,
@@ -367,6 +369,49 @@ __global__ void k_centres(const int32_t* __restrict__ sidx, const int32_t* __res
   int64_t c = pos[k];
   centre_k[c] = int32_t(k);
   centre_p[c] = sidx[k];
+}
+
+// ---- bulk copies into shared memory (the TMA engine's 1-D form) --------------------
+// cp.async.bulk moves a contiguous run of bytes from global to shared memory
+// and reports its bytes to an mbarrier; both addresses 16-byte aligned, the
+// size a multiple of 16.  No cluster multicast.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* m, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* m, uint32_t bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
+               ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* m, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok) : "r"(smem_u32(m)), "r"(parity) : "memory");
+  return ok != 0u;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         unsigned long long* m) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(m))
+      : "memory");
+}
+// waits for the phase with the given parity, at most `limit` polls; false
+// when it did not complete
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* m, uint32_t parity,
+                                                  int limit) {
+  for (int i = 0; i < limit; ++i)
+    if (mbar_test_wait(m, parity)) return true;
+  return false;
 }
 
 // ---- neighbour-set digest ----------------------------------------------------------------
@@ -456,10 +501,16 @@ __device__ __forceinline__ float dist2_f32(const float4& b, const float4& a) {
   return __fmaf_rn(fz, fz, __fmaf_rn(fy, fy, __fmul_rn(fx, fx)));
 }
 
-template <int DIM, int G>
-__global__ void __launch_bounds__(128, 7)
+// STAGED: each chunk's candidate runs (contiguous ranges of sorted records)
+// are copied into shared memory by bulk copies, one per run, and tested
+// from there, instead of being fetched a batch at a time by the lanes; a
+// chunk that does not fit the stage falls back to the fetch.
+constexpr int kStageRecords = 96;  // records staged per group and chunk
+template <int DIM, int G, bool STAGED>
+__global__ void __launch_bounds__(128, STAGED ? 4 : 7)
 k_neighbours(NeibArgs a) {
-  constexpr int RPL = kNeibRowsPerLane;
+  constexpr int RPL = STAGED ? 1 : kNeibRowsPerLane;
+  constexpr int STG = kStageRecords;
   constexpr int NG = 128 / G;
   constexpr unsigned FULL = 0xffffffffu;
   // Staged ranges per group, stored [entry of the lane][lane] so that the
@@ -477,12 +528,24 @@ k_neighbours(NeibArgs a) {
   // never overflows and a run never exceeds the warp's 32 lanes.
   constexpr int FLUSH_AT = 33 - G;
   __shared__ int32_t held[128][33];
+  // the staged runs of a chunk, then sentinels up to the warp's longest
+  // concatenation + G; one mbarrier per group counts the copies' bytes
+  __shared__ __align__(16) float4 stage[STAGED ? NG : 1][STAGED ? STG + G : 1];
+  __shared__ __align__(8) unsigned long long mbar[STAGED ? NG : 1];
   const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int lane = threadIdx.x & (G - 1);
   const int wl = threadIdx.x & 31;
   const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1u) << (wl & ~(G - 1)));
   int2* rs = ranges[threadIdx.x / G];
   float4* bt = batch[threadIdx.x / G];
+  float4* const sg = stage[STAGED ? threadIdx.x / G : 0];
+  unsigned long long* const mb = &mbar[STAGED ? threadIdx.x / G : 0];
+  uint32_t mphase = 0;  // parity of the group's mbarrier phase in use
+  if constexpr (STAGED) {
+    if (lane == 0) mbar_init(mb, 1);
+    mbar_init_fence();
+    __syncwarp();
+  }
   unsigned int ncand = 0, nexact = 0, nfound = 0;
   Grid g = a.g;
   double shift = a.shift;
@@ -577,6 +640,61 @@ k_neighbours(NeibArgs a) {
     const int ny_r = cy1 - cy0 + 1;
     const int nrows_r = seg ? ny_r * (cz1 - cz0 + 1) : 0;
     const float r2 = rmax * rmax;
+    // tests a batch of G candidates (cand[0 .. G-1], broadcast from shared
+    // memory) against each lane's centre, then flushes the lanes whose held
+    // hits reached FLUSH_AT
+    auto test_batch = [&](const float4* cand) {
+      if (mine) {
+        // FP32 decisions for the batch: 0 < sd32 < lo is inside for sure.
+        // The guard band and sd32 = 0 (the centre itself, or a particle
+        // closer than the FP32 images resolve) are decided in FP64 after
+        // the batch, which recomputes sd32 bit for bit to find them (rare:
+        // about once per centre)
+        // The candidate is written to the next free slot whether or not it
+        // is a hit and kept only by counting it (no branch per test): a
+        // lane starts a batch with at most FLUSH_AT - 1 = 32 - G held
+        // hits, so test t writes slot <= 32 - G + t <= 31 of its 33.
+        bool anyband = false;
+#pragma unroll
+        for (int t = 0; t < G; ++t) {
+          const float4 pj = cand[t];
+          const float sd32 = dist2_f32(pj, pi);
+          const bool in32 = sd32 < lo_thr && sd32 > 0.f;
+          anyband |= !in32 && !(sd32 > hi_thr);
+          mine_held[nheld] = __float_as_int(pj.w);
+          nheld += in32 ? 1 : 0;
+        }
+        if (anyband) {
+#pragma unroll 1
+        for (int t = 0; t < G; ++t) {
+          const float4 pj = cand[t];
+          const float sd32 = dist2_f32(pj, pi);
+          if ((sd32 < lo_thr && sd32 > 0.f) || sd32 > hi_thr) continue;
+          const int32_t q = __float_as_int(pj.w);
+          if (q == k) continue;
+          ++nexact;
+          double d0 = __dadd_rn(a.sx[q], -xi);
+          double d1 = __dadd_rn(a.sy[q], -yi);
+          double d2 = __dadd_rn(a.sz[q], -zi);
+          double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                __dmul_rn(d2, d2));
+          const bool take = !(sd > R2);
+          if (take) mine_held[nheld] = q;
+          nheld += take ? 1 : 0;
+        }
+        }
+      }
+      __syncwarp();  // the next batch overwrites this one
+      const unsigned full = __ballot_sync(FULL, nheld >= FLUSH_AT);
+      if (full) {
+        flush(full);
+        if ((full >> wl) & 1u) {
+          cnt += nheld;
+          dst += nheld;
+          nheld = 0;
+        }
+      }
+    };
     const int nch = __reduce_max_sync(FULL, (nrows_r + RPL * G - 1) / (RPL * G));
     for (int ch = 0; ch < nch; ++ch) {
       // The chunk's rows go round-robin over the lanes (row rbase + i G is
@@ -633,21 +751,53 @@ k_neighbours(NeibArgs a) {
       }
       const int total = __shfl_sync(FULL, incl, G - 1, G);
       int run = incl - mysum;
+      int soff[RPL], ssa[RPL], slen[RPL];  // each run: offset in the concatenation, start, length
 #pragma unroll
       for (int i = 0; i < RPL; ++i) {
         const int2 v = rs[i * G + lane];
+        soff[i] = run;
+        ssa[i] = v.x;
+        slen[i] = v.y;
         rs[i * G + lane] = make_int2(v.x - run, run + v.y);
         run += v.y;
       }
       __syncwarp();
       if (mine) ncand += unsigned(total);
       const int tmax = __reduce_max_sync(FULL, total);
+      const float4 far = make_float4(3.0e38f, 3.0e38f, 3.0e38f, __int_as_float(-1));
+      if constexpr (STAGED) {
+        if (__all_sync(FULL, total <= STG)) {
+          // earlier generic reads and writes of the stage before the async
+          // copies overwrite it
+          __syncwarp();
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (total > 0) {  // the same on all lanes of the group
+            if (lane == 0) mbar_arrive_expect_tx(mb, uint32_t(total) * 16u);
+#pragma unroll
+            for (int i = 0; i < RPL; ++i)
+              if (slen[i] > 0)
+                bulk_g2s(sg + soff[i], a.s32 + ssa[i], uint32_t(slen[i]) * 16u, mb);
+          }
+          for (int pos = total + lane; pos < tmax + G; pos += G) sg[pos] = far;
+          if (total > 0) {
+            if (!mbar_wait_bounded(mb, mphase, 1 << 20)) {
+              atomicOr(a.overflow, 2);  // reported as a timeout by the host
+              mbar_wait_bounded(mb, mphase, 1 << 20);
+            }
+            mphase ^= 1u;
+          }
+          __syncwarp();
+          for (int p0 = 0; p0 < tmax; p0 += G) test_batch(sg + p0);
+          __syncwarp();  // the next chunk overwrites the ranges and the stage
+          continue;
+        }
+      }
       // The walk: lane j of the group fetches candidate p0 + j of every
       // batch, one batch ahead of the tests (software pipelining), past the
       // end a far-away sentinel that no test accepts.
       int r = 0;
       int2 rw = rs[0];
-      const float4 far = make_float4(3.0e38f, 3.0e38f, 3.0e38f, 0.f);
       float4 nxt = far;
       int32_t nxt_q = -1;
       if (lane < total) {
@@ -675,56 +825,7 @@ k_neighbours(NeibArgs a) {
         }
         bt[lane] = cur;
         __syncwarp();
-        if (mine) {
-          // FP32 decisions for the batch: 0 < sd32 < lo is inside for sure.
-          // The guard band and sd32 = 0 (the centre itself, or a particle
-          // closer than the FP32 images resolve) are decided in FP64 after
-          // the batch, which recomputes sd32 bit for bit to find them (rare:
-          // about once per centre)
-          // The candidate is written to the next free slot whether or not it
-          // is a hit and kept only by counting it (no branch per test): a
-          // lane starts a batch with at most FLUSH_AT - 1 = 32 - G held
-          // hits, so test t writes slot <= 32 - G + t <= 31 of its 33.
-          bool anyband = false;
-#pragma unroll
-          for (int t = 0; t < G; ++t) {
-            const float4 pj = bt[t];
-            const float sd32 = dist2_f32(pj, pi);
-            const bool in32 = sd32 < lo_thr && sd32 > 0.f;
-            anyband |= !in32 && !(sd32 > hi_thr);
-            mine_held[nheld] = __float_as_int(pj.w);
-            nheld += in32 ? 1 : 0;
-          }
-          if (anyband) {
-#pragma unroll 1
-          for (int t = 0; t < G; ++t) {
-            const float4 pj = bt[t];
-            const float sd32 = dist2_f32(pj, pi);
-            if ((sd32 < lo_thr && sd32 > 0.f) || sd32 > hi_thr) continue;
-            const int32_t q = __float_as_int(pj.w);
-            if (q == k) continue;
-            ++nexact;
-            double d0 = __dadd_rn(a.sx[q], -xi);
-            double d1 = __dadd_rn(a.sy[q], -yi);
-            double d2 = __dadd_rn(a.sz[q], -zi);
-            double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
-                                  __dmul_rn(d2, d2));
-            const bool take = !(sd > R2);
-            if (take) mine_held[nheld] = q;
-            nheld += take ? 1 : 0;
-          }
-          }
-        }
-        __syncwarp();  // the next batch overwrites this one
-        const unsigned full = __ballot_sync(FULL, nheld >= FLUSH_AT);
-        if (full) {
-          flush(full);
-          if ((full >> wl) & 1u) {
-            cnt += nheld;
-            dst += nheld;
-            nheld = 0;
-          }
-        }
+        test_batch(bt);
       }
       __syncwarp();  // the next chunk overwrites the ranges
     }
@@ -1388,23 +1489,25 @@ void launch_neib_digest(int64_t nc, const int32_t* centre_p, const int32_t* orig
   note_launch();
 }
 template <int DIM, int G>
-static void neighbours_g(const NeibArgs& a, cudaStream_t s) {
+static void neighbours_g(bool staged, const NeibArgs& a, cudaStream_t s) {
   const int tpb = 128;
-  k_neighbours<DIM, G><<<nblocks(a.nc, tpb), tpb, 0, s>>>(a);
+  // (4-lane groups keep the fetch: 32 stages would not fit 48 KB)
+  if (staged && G >= 8) k_neighbours<DIM, G, (G >= 8)><<<nblocks(a.nc, tpb), tpb, 0, s>>>(a);
+  else k_neighbours<DIM, G, false><<<nblocks(a.nc, tpb), tpb, 0, s>>>(a);
 }
 template <int DIM>
-static void neighbours_dim(int G, const NeibArgs& a, cudaStream_t s) {
+static void neighbours_dim(int G, bool staged, const NeibArgs& a, cudaStream_t s) {
   switch (G) {
-    case 4: neighbours_g<DIM, 4>(a, s); break;
-    case 8: neighbours_g<DIM, 8>(a, s); break;
-    case 16: neighbours_g<DIM, 16>(a, s); break;
-    default: neighbours_g<DIM, 32>(a, s); break;
+    case 4: neighbours_g<DIM, 4>(staged, a, s); break;
+    case 8: neighbours_g<DIM, 8>(staged, a, s); break;
+    case 16: neighbours_g<DIM, 16>(staged, a, s); break;
+    default: neighbours_g<DIM, 32>(staged, a, s); break;
   }
 }
-void launch_neighbours(int dim, int G, const NeibArgs& a, cudaStream_t s) {
-  if (dim == 3) neighbours_dim<3>(G, a, s);
-  else if (dim == 2) neighbours_dim<2>(G, a, s);
-  else neighbours_dim<1>(G, a, s);
+void launch_neighbours(int dim, int G, bool staged, const NeibArgs& a, cudaStream_t s) {
+  if (dim == 3) neighbours_dim<3>(G, staged, a, s);
+  else if (dim == 2) neighbours_dim<2>(G, staged, a, s);
+  else neighbours_dim<1>(G, staged, a, s);
   note_launch();
 }
 void launch_rowcap(int64_t nc, const int32_t* centre_p, const int32_t* orig,

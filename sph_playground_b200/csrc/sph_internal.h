@@ -247,7 +247,9 @@ struct NeibArgs {
   int32_t* overflow;
   unsigned long long* dcnt;
 };
-void launch_neighbours(int dim, int G, const NeibArgs& a, cudaStream_t s);
+// staged: the candidate runs of a chunk copied into shared memory by bulk
+// copies (SPH_P_SEARCH_STAGED); overflow |= 2 if a copy's wait timed out
+void launch_neighbours(int dim, int G, bool staged, const NeibArgs& a, cudaStream_t s);
 // per centre in original order: out[2 o] = count, out[2 o + 1] = sum of
 // mix64((row << 5) | image) over the neighbours (sph_get_neighbour_digest)
 void launch_neib_digest(int64_t nc, const int32_t* centre_p, const int32_t* orig,
