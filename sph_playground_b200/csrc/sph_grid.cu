@@ -774,6 +774,7 @@ k_neighbours(NeibArgs a) {
           __syncwarp();
           if (total > 0) {  // the same on all lanes of the group
             if (lane == 0) mbar_arrive_expect_tx(mb, uint32_t(total) * 16u);
+            __syncwarp(gmask);  // the expected bytes are set before any copy lands
 #pragma unroll
             for (int i = 0; i < RPL; ++i)
               if (slen[i] > 0)
