@@ -109,3 +109,21 @@ def test_tiny_smoothing_length_grid(oracle_lib, engine_lib, cuda_ok, prec, h_sma
     got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "density")
     assert neighbour_sets_equal(nb_got, nb_ref)
     assert rel_particle(got[:, COL["den"]], ref[:, COL["den"]]) <= TOL[prec]
+
+
+@pytest.mark.parametrize("case", ["coincident", "tiny_box", "overflow"])
+def test_staged_search_edge_cases(oracle_lib, engine_lib, cuda_ok, case):
+    """The edge cases above with the bulk-copy staged search."""
+    if case == "coincident":
+        st, store = ic.density3d(n=10, seed=3)
+        store[1:4, COL["rx"]:COL["rz"] + 1] = store[0, COL["rx"]:COL["rz"] + 1]
+    elif case == "tiny_box":
+        st, store = ic.density3d(n=4, seed=5)
+    else:
+        st, store = ic.density3d(n=12, seed=4)
+        store[:, COL["rx"]:COL["rz"] + 1] *= 0.5
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "density")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", FP64, "density",
+                                 params={abi.P_SEARCH_STAGED: 1})
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    assert rel_particle(got[:, COL["den"]], ref[:, COL["den"]]) <= TOL[FP64]

@@ -153,3 +153,11 @@ def test_sod_to_t02(oracle_lib, engine_lib, cuda_ok):
         assert d_gpu <= d_ulp, (f, d_gpu, d_ulp)
     assert l1["gpu"] < 0.02
     assert abs(l1["gpu"] - l1["oracle"]) <= abs(l1["oracle_ulp"] - l1["oracle"])
+
+
+def test_staged_search_128(engine_lib, cuda_ok, density128):
+    """The bulk-copy staged search at 128^3: the same sets as the oracle."""
+    st, store, params, (ref, dref) = density128
+    got, dgot = _run(engine_lib, st, store, FP64, "density", {**params, abi.P_SEARCH_STAGED: 1})
+    assert np.array_equal(dgot[0], dref[0]) and np.array_equal(dgot[1], dref[1])
+    assert float(np.max(_part(got, ref, "den"))) <= PART[FP64]

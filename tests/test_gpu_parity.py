@@ -276,3 +276,19 @@ def test_gauss_kernel_iterate(oracle_lib, engine_lib, cuda_ok, prec):
     bad = compare(ref, got, prec, part_fields=("den", "h", "om", "c"),
                   field_fields=("ax", "ay", "du", "dh"))
     assert not bad, bad
+
+
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_staged_search_matches_oracle(oracle_lib, engine_lib, cuda_ok, prec, lanes):
+    """The search with its candidate runs copied into shared memory by bulk
+    copies (SPH_P_SEARCH_STAGED) finds the oracle's sets and gives the same
+    fields, for every group width that stages (8, 16, 32 lanes)."""
+    st, store = ic.density3d(n=16, seed=2)
+    params = {abi.P_SEARCH_STAGED: 1, abi.P_LANES_SEARCH: lanes}
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, nb_got, cnt, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate", params=params)
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    bad = compare(ref, got, prec, part_fields=("den", "h", "om"),
+                  field_fields=("ax", "ay", "az", "du"))
+    assert not bad, bad
