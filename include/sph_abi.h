@@ -76,7 +76,19 @@ extern "C" {
                                       candidate runs into shared memory with
                                       bulk (TMA) copies instead of fetching
                                       them per batch (default 0)               */
-#define SPH_P_LAST            64
+#define SPH_P_SKIN            65 /* s in (0, 1]: neighbour lists kept between
+                                      iterates as skin lists of radius
+                                      (1 + s) krad h; every iterate a centre
+                                      keeps its row (nothing near it moved),
+                                      refilters its skin list with the FP64
+                                      predicate, or (near a fast particle) is
+                                      searched afresh, so the sets equal a
+                                      fresh search's; the lists are rebuilt
+                                      when particles moved too far.  0 = a
+                                      fresh search every iterate.  Default 0.1.
+                                      (The device-resident steps of SPH_P_GRAPH
+                                      and the batch loop search afresh.)       */
+#define SPH_P_LAST            65
 
 /* ---- status codes --------------------------------------------------------- */
 #define SPH_OK                     0
@@ -122,7 +134,13 @@ extern "C" {
 #define SPH_CNT_ALLOCS        14 /* device allocations made by this handle    */
 #define SPH_CNT_GRAPH_STEPS   15 /* steps run as a device-resident graph      */
 #define SPH_CNT_GRAPH_REDOS   16 /* device-resident steps redone on the host  */
-#define SPH_CNT_TOTAL          17
+#define SPH_CNT_SKIN_BUILDS   17 /* searches that built skin lists          */
+#define SPH_CNT_SKIN_REUSES   18 /* iterates served from skin lists          */
+#define SPH_CNT_SKIN_DIRTY    19 /* centres searched afresh in those (sum)   */
+#define SPH_CNT_SKIN_KEPT     20 /* rows kept unchanged in those (sum)       */
+#define SPH_CNT_SKIN_RELAYOUTS 21 /* skin-list iterates that laid the whole
+                                     table out anew                          */
+#define SPH_CNT_TOTAL          22
 
 /* ---- per-kernel timers (sph_get_timers, milliseconds, cumulative) ------- */
 #define SPH_T_PREDICT    0

@@ -44,11 +44,14 @@ P_LANES_PAIR = 61
 P_FIXED_DT = 62
 P_GRAPH = 63
 P_SEARCH_STAGED = 64
+P_SKIN = 65
 
 COUNTERS = ["iterates", "steps", "neib_pairs", "c1_pairs", "c1_sweeps",
             "c2_pairs", "ghosts", "candidates", "centres",
             "c1_centre_sweeps", "launches", "neib_max", "searches",
-            "exact_tests", "allocs", "graph_steps", "graph_redos"]
+            "exact_tests", "allocs", "graph_steps", "graph_redos",
+            "skin_builds", "skin_reuses", "skin_dirty", "skin_kept",
+            "skin_relayouts"]
 TIMERS = ["predict", "ghosts", "sort", "neighbours", "circuit1", "circuit2",
           "correct", "timestep", "sts", "step", "pack"]
 

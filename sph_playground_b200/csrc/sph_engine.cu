@@ -140,6 +140,9 @@ long long launches_so_far() { return g_launches; }
 // Jacobi sweeps of circuit1 that a device-resident step runs before it asks
 // the host (a step whose particles need more is redone on the host path)
 constexpr int kDrsSweeps = 6;
+// iterates skin lists serve at most before the rows are re-sorted and the
+// lists rebuilt with them
+constexpr int kSkinMaxAge = 64;
 
 struct sph_handle {
   int dev = 0;  // the device current at sph_create
@@ -184,6 +187,29 @@ struct sph_handle {
   // physical order (the predictor's saves are per physical row)
   bool in_split_step = false;
   DevBuf colbuf;  // staging of sph_get_columns / sph_set_columns
+  // skin lists (SPH_P_SKIN): the lists of the last skin search (CSR like nl),
+  // the records' positions and the centres' h at that search, the rows'
+  // image signatures then; per record the largest displacement since and
+  // the marks of fast / moving records nearby; per centre the gap of its
+  // list at the search, the largest change of h since, its way (filter,
+  // search afresh, keep), the fresh-search flag, its scan and those centres
+  DevBuf skin_nl, skin_rowoff, skin_rowcap, skin_rowcap64, skin_cnt, skin_count_prev,
+      skin_h_prev, skin_bx, skin_by, skin_bz, skin_hb, skin_sig, skin_dsp, skin_near_f,
+      skin_near_m, skin_gap, skin_hdev, skin_mode, skin_dflag, skin_dpos, skin_dlist;
+  // the rows of the centres searched afresh, laid out anew every skin-list
+  // iterate after the end of the table's fixed part (skin_end[0]): their
+  // capacities and the scan of those
+  DevBuf skin_end, skin_dcap, skin_doff;
+  int64_t skin_nl_size = 0;
+  int skin_est = 0;
+  bool skin_valid = false;  // the skin lists describe the records of the current sort
+  bool skin_ending = false;  // the last reuse saw the lists near their end
+  double skin_s = 0.;        // their fraction s (radius (1 + s) krad h)
+  double skin_tau = 0.;      // displacement up to which a record is slow
+  double skin_eps = 0.;      // displacement up to which a record is still
+  double skin_hmin = 0.;     // h_min at their search
+  int skin_age = 0;          // iterates served since their search
+  int64_t kept_pairs = 0;    // neighbour pairs of the rows kept (counted as found)
   const DevPlan* dplan = nullptr;  // set while a device-resident step is built
   int64_t nghost_cap = 0, nall_cap = 0;
   int end_bit_cap = 0;
@@ -507,13 +533,457 @@ struct sph_handle {
     std::swap(orig.p, orig_alt.p);
     std::swap(orig.bytes, orig_alt.bytes);
     have_order = false;
+    skin_valid = false;
     steps_since_reorder = 0;
     CK(cudaGetLastError());
     return SPH_OK;
   }
 
+  // ---- neighbour tables ------------------------------------------------------------------------
+  // One CSR table: rows sized from each centre's count in the table's last
+  // pass, scaled for the change of h since (k_rowcap); a pass in which a row
+  // overflows is re-run with the counts it just measured.
+  struct Table {
+    DevBuf *nl, *rowoff, *rowcap, *rowcap64, *ncnt, *count_prev, *h_prev;
+    int64_t* nl_size;
+    int* est;
+  };
+  Table exact_table() {
+    return {&nl, &rowoff, &rowcap, &rowcap64, &ncnt, &count_prev, &h_prev, &nl_size, &est_count};
+  }
+  Table skin_table() {
+    return {&skin_nl, &skin_rowoff, &skin_rowcap, &skin_rowcap64, &skin_cnt, &skin_count_prev,
+            &skin_h_prev, &skin_nl_size, &skin_est};
+  }
+  NeibArgs neib_args(const Table& T, const Params& P) {
+    NeibArgs na{};
+    na.nc = nreal;
+    na.centre_k = centre_k.as<int32_t>();
+    na.centre_p = centre_p.as<int32_t>();
+    na.sx = sx.as<double>(); na.sy = sy.as<double>(); na.sz = sz.as<double>();
+    na.s32 = s32.as<float4>();
+    na.shift = pgeom.shift;
+    na.hcol = col(es_h);
+    na.krad = P.krad;
+    na.g = grid;
+    na.cstart = cstart.as<int32_t>();
+    na.rowoff = T.rowoff->as<int64_t>();
+    na.rowcap = T.rowcap->as<int32_t>();
+    na.nl_size = *T.nl_size;
+    na.nl = T.nl->as<int32_t>();
+    na.ncnt = T.ncnt->as<int32_t>();
+    na.orig = orig.as<int32_t>();
+    na.count_prev = T.count_prev->as<int32_t>();
+    na.h_prev = T.h_prev->as<float>();
+    na.maxcnt = maxcnt.as<int32_t>();
+    na.overflow = overflow.as<int32_t>();
+    na.dcnt = dcnt.as<unsigned long long>();
+    return na;
+  }
+  // runs `pass` (which fills the table's rows given its NeibArgs) until no
+  // row overflows; `exact`: the table the pair passes read (its longest row
+  // is reported and checked against the reference's maxneib cap)
+  // pass(na, attempt)
+  template <class Pass>
+  int fill_table(const Table& T, const Params& P, bool exact, Pass pass) {
+    const int d = P.dim;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+      Phase ph(this, SPH_T_NEIGHBOURS);
+      launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(),
+                    T.count_prev->as<int32_t>(), T.h_prev->as<float>(), col(es_h), d, 1.2f,
+                    T.rowcap64->as<int64_t>(), T.rowcap->as<int32_t>(), s);
+      exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, T.rowcap64->as<int64_t>(),
+                       T.rowoff->as<int64_t>(), nreal, s);
+      // (table sizes are multiples of 4 like the rows: a row that fits ends
+      // on a 16-byte boundary inside the table)
+      if (*T.nl_size <= 0) {
+        *T.nl_size = ((int64_t(*T.est) * 12 / 10 + 8) * nreal * 5 / 4 + 3) & ~int64_t(3);
+        RC(T.nl->ensure(sizeof(int32_t) * *T.nl_size));
+      }
+      if (attempt > 0) {
+        // a re-run: size the table for the rows computed from the new counts
+        CK(cudaMemcpyAsync(h_i32 + 2, T.rowcap->as<int32_t>() + (nreal - 1), sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(reinterpret_cast<int64_t*>(h_red + RED_TOTAL),
+                           T.rowoff->as<int64_t>() + (nreal - 1), sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        int64_t total = reinterpret_cast<int64_t*>(h_red + RED_TOTAL)[0] + h_i32[2];
+        if (total > *T.nl_size) {
+          *T.nl_size = (total + total / 4 + 3) & ~int64_t(3);
+          RC(T.nl->ensure(sizeof(int32_t) * *T.nl_size));
+        }
+      }
+      CK(cudaMemsetAsync(maxcnt.p, 0, sizeof(int32_t), s));
+      CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
+      NeibArgs na = neib_args(T, P);
+      pass(na, attempt);
+      CK(cudaMemcpyAsync(h_i32, maxcnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(h_i32 + 1, overflow.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      CK(cudaGetLastError());
+      int mc = h_i32[0];
+      if (h_i32[1] & 2)
+        return fail(SPH_ERR_TIMEOUT, "neighbour search: a bulk copy into shared memory did not "
+                                     "complete within its wait limit");
+      if (exact) {
+        cnt_host[SPH_CNT_NEIB_MAX] = mc;
+        if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc + 1 > kb.maxneib[d - 1])
+          return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
+      }
+      if (!h_i32[1]) break;
+      // count_prev now holds the exact counts, so the next attempt fits
+      if (attempt == 3) return fail(SPH_ERR_NEIB_OVERFLOW, "neighbour list capacity");
+    }
+    return SPH_OK;
+  }
+
+  // ---- skin lists (SPH_P_SKIN) -----------------------------------------------------------------
+  // The search runs with radius (1 + s) krad h and leaves its lists; the
+  // following iterates serve the pair passes from them (k_skin_* in
+  // sph_grid.cu: filter with the FP64 predicate, fresh search of the
+  // centres the filter cannot vouch for) until the records have moved too
+  // far, an image set changes or too many centres need the fresh search.
+  // rows may be re-sorted: no skin lists serve, or the ones that do are near
+  // their end (the re-sort ends them)
+  bool skin_lets_reorder() const {
+    return !skin_valid || skin_ending || skin_age >= kSkinMaxAge;
+  }
+  double skin_fraction() const {
+    const double v = st[SPH_P_SKIN];
+    return v > 0 ? std::min(v, 1.0) : 0.0;
+  }
+  int skin_alloc(int64_t nall) {
+    RC(skin_rowoff.ensure(sizeof(int64_t) * nreal));
+    RC(skin_rowcap.ensure(sizeof(int32_t) * nreal));
+    RC(skin_rowcap64.ensure(sizeof(int64_t) * nreal));
+    RC(skin_cnt.ensure(sizeof(int32_t) * nreal));
+    RC(skin_count_prev.ensure(sizeof(int32_t) * nrows));
+    RC(skin_h_prev.ensure(sizeof(float) * nrows));
+    RC(skin_hb.ensure(sizeof(double) * nreal));
+    RC(skin_dflag.ensure(sizeof(int32_t) * (nreal + 1)));
+    RC(skin_dpos.ensure(sizeof(int32_t) * (nreal + 1)));
+    RC(skin_dlist.ensure(sizeof(int32_t) * nreal));
+    RC(skin_sig.ensure(sizeof(uint8_t) * nrows));
+    RC(skin_bx.ensure(sizeof(double) * nall));
+    RC(skin_by.ensure(sizeof(double) * nall));
+    RC(skin_bz.ensure(sizeof(double) * nall));
+    RC(skin_dsp.ensure(sizeof(float) * nall));
+    RC(skin_near_f.ensure(sizeof(uint8_t) * nall));
+    RC(skin_near_m.ensure(sizeof(uint8_t) * nall));
+    RC(skin_gap.ensure(sizeof(float) * nreal));
+    RC(skin_hdev.ensure(sizeof(double) * nreal));
+    RC(skin_mode.ensure(sizeof(uint8_t) * nreal));
+    RC(skin_end.ensure(sizeof(int64_t)));
+    RC(skin_dcap.ensure(sizeof(int64_t) * (nreal + 1)));
+    RC(skin_doff.ensure(sizeof(int64_t) * (nreal + 1)));
+    RC(scan64_tmp.ensure(scan64_temp_bytes(nreal + 1)));
+    return SPH_OK;
+  }
+  SkinFilterArgs filter_args(const NeibArgs& na, bool keep, bool gaps) {
+    SkinFilterArgs f{};
+    f.nc = nreal;
+    f.mode = skin_mode.as<uint8_t>();
+    f.keep = keep ? 1 : 0;
+    f.gap = gaps ? skin_gap.as<float>() : nullptr;
+    // a distance between two FP32 images: per axis each image within one
+    // unit of the binade's last place (shift 2^-23) of its position
+    f.eimg = float(2.0 * std::sqrt(3.0) * pgeom.shift * 1.1920928955078125e-7);
+    f.centre_k = na.centre_k;
+    f.centre_p = na.centre_p;
+    f.skin_off = skin_rowoff.as<int64_t>();
+    f.skin_cnt = skin_cnt.as<int32_t>();
+    f.skin_nl = skin_nl.as<int32_t>();
+    f.sx = na.sx; f.sy = na.sy; f.sz = na.sz;
+    f.s32 = na.s32;
+    f.shift = na.shift;
+    f.hcol = na.hcol;
+    f.krad = na.krad;
+    f.rowoff = na.rowoff;
+    f.rowcap = na.rowcap;
+    f.nl_size = na.nl_size;
+    f.nl = na.nl;
+    f.ncnt = na.ncnt;
+    f.orig = na.orig;
+    f.count_prev = na.count_prev;
+    f.h_prev = na.h_prev;
+    f.maxcnt = na.maxcnt;
+    f.overflow = na.overflow;
+    f.dcnt = na.dcnt;
+    return f;
+  }
+  // after the sort: the skin search, what later iterates compare against,
+  // and the exact lists from the skin lists (every centre filters)
+  int skin_build(const Mode& m, const Params& P, double skin, double hmin) {
+    const int d = P.dim;
+    const int64_t nall = nrows + nghost;
+    RC(skin_alloc(nall));
+    const double kfac = 1.0 + skin;
+    if (skin_est <= 0) {
+      skin_est = int(est_count * std::pow(kfac, double(d))) + 8;
+      launch_fill_i32(skin_count_prev.as<int32_t>(), nrows, skin_est, s);
+      CK(cudaMemsetAsync(skin_h_prev.p, 0, sizeof(float) * nrows, s));
+    }
+    const bool staged = st[SPH_P_SEARCH_STAGED] != 0;
+    RC(fill_table(skin_table(), P, false, [&](NeibArgs& na, int) {
+      na.kfac = kfac;
+      na.skin_search = 1;
+      launch_neighbours(d, lanes_search(), staged, na, s);
+      cnt_host[SPH_CNT_SEARCHES]++;
+    }));
+    {
+      Phase ph(this, SPH_T_NEIGHBOURS);
+      CK(cudaMemcpyAsync(skin_bx.p, sx.p, sizeof(double) * nall, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(skin_by.p, sy.p, sizeof(double) * nall, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(skin_bz.p, sz.p, sizeof(double) * nall, cudaMemcpyDeviceToDevice, s));
+      SlotInit si{};
+      si.off[si.n] = RED_SKIN_HMAXB; si.val[si.n++] = dkey(0.0);
+      launch_init_slots(red.as<unsigned long long>(), si, s);
+      launch_gather_h(nreal, centre_p.as<int32_t>(), col(es_h), skin_hb.as<double>(),
+                      red.as<unsigned long long>(), RED_SKIN_HMAXB, s);
+      BoxGeom gg = box(m);
+      if (!m.ghosts) for (int k = 0; k < 3; ++k) gg.periodic[k] = 0;
+      launch_skin_sig(cols.as<double>(), nrows, gg, d, skin_sig.as<uint8_t>(), s);
+      CK(cudaMemsetAsync(skin_dsp.p, 0, sizeof(float) * nall, s));
+      CK(cudaMemsetAsync(skin_hdev.p, 0, sizeof(double) * nreal, s));
+      CK(cudaMemsetAsync(skin_mode.p, 0, sizeof(uint8_t) * nreal, s));
+      CK(cudaMemsetAsync(skin_dflag.p, 0, sizeof(int32_t) * (nreal + 1), s));
+    }
+    skin_tau = 0.25 * skin * P.krad * hmin;
+    skin_eps = 1e-4 * P.krad * hmin;
+    skin_hmin = hmin;
+    RC(fill_table(exact_table(), P, true, [&](NeibArgs& na, int) {
+      launch_skin_filter(filter_args(na, false, true), s);
+    }));
+    launch_table_end(rowoff.as<int64_t>(), rowcap.as<int32_t>(), nreal, skin_end.as<int64_t>(), s);
+    skin_valid = true;
+    skin_ending = false;
+    skin_s = skin;
+    skin_age = 0;
+    cnt_host[SPH_CNT_SKIN_BUILDS]++;
+    return SPH_OK;
+  }
+  FewArgs few_args(const NeibArgs& na, const int32_t* list, int64_t n, double reach) {
+    FewArgs f{};
+    f.n = n;
+    f.list = list;
+    f.centre_k = na.centre_k;
+    f.centre_p = na.centre_p;
+    f.sx = na.sx; f.sy = na.sy; f.sz = na.sz;
+    f.s32 = na.s32;
+    f.shift = na.shift;
+    f.hcol = na.hcol;
+    f.krad = na.krad;
+    f.g = na.g;
+    f.cstart = na.cstart;
+    f.reach = reach;
+    f.rowoff = na.rowoff;
+    f.rowcap = na.rowcap;
+    f.nl_size = na.nl_size;
+    f.nl = na.nl;
+    f.ncnt = na.ncnt;
+    f.orig = na.orig;
+    f.count_prev = na.count_prev;
+    f.h_prev = na.h_prev;
+    f.maxcnt = na.maxcnt;
+    f.overflow = na.overflow;
+    f.dcnt = na.dcnt;
+    return f;
+  }
+  // The exact table of a skin-list iterate.  The kept rows stay where they
+  // are; the filtered ones are written in place; the centres searched afresh
+  // (skin_dlist, ndirty of them) get rows laid out anew after the table's
+  // fixed part.  A filter row that overflows joins the centres searched
+  // afresh (for good: mode 1); when their rows find no room either, the
+  // whole table is laid out anew and every row written.
+  int skin_fill(const Params& P, int64_t ndirty, double reach) {
+    const int d = P.dim;
+    Table T = exact_table();
+    auto dyn = [&](int64_t nd) {
+      launch_dyn_rows(nd, skin_dlist.as<int32_t>(), centre_p.as<int32_t>(), orig.as<int32_t>(),
+                      count_prev.as<int32_t>(), h_prev.as<float>(), col(es_h), d,
+                      skin_dcap.as<int64_t>(), skin_doff.as<int64_t>(), scan64_tmp.p,
+                      scan64_tmp.bytes, skin_end.as<int64_t>(), rowoff.as<int64_t>(),
+                      rowcap.as<int32_t>(), s);
+    };
+    auto read_flags = [&](int& mc, int& ov) -> int {
+      CK(cudaMemcpyAsync(h_i32, maxcnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(h_i32 + 1, overflow.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      CK(cudaGetLastError());
+      mc = h_i32[0];
+      ov = h_i32[1];
+      if (ov & 2)
+        return fail(SPH_ERR_TIMEOUT, "neighbour search: a bulk copy into shared memory did not "
+                                     "complete within its wait limit");
+      return SPH_OK;
+    };
+    int mc = 0, ov = 0;
+    {
+      Phase ph(this, SPH_T_NEIGHBOURS);
+      CK(cudaMemsetAsync(maxcnt.p, 0, sizeof(int32_t), s));
+      CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
+      dyn(ndirty);
+      NeibArgs na = neib_args(T, P);
+      launch_skin_filter(filter_args(na, true, false), s);
+      launch_search_few(d, few_args(na, skin_dlist.as<int32_t>(), ndirty, reach), s);
+      RC(read_flags(mc, ov));
+    }
+    int mc_all = mc;
+    if (ov) {
+      // overflowed filter rows join the fresh searches; all of those anew
+      Phase ph(this, SPH_T_NEIGHBOURS);
+      launch_overflow_to_search(nreal, ncnt.as<int32_t>(), rowoff.as<int64_t>(),
+                                rowcap.as<int32_t>(), nl_size, skin_mode.as<uint8_t>(),
+                                skin_dflag.as<int32_t>(), s);
+      exclusive_scan(scan_tmp.p, scan_tmp.bytes, skin_dflag.as<int32_t>(),
+                     skin_dpos.as<int32_t>(), nreal + 1, s);
+      launch_skin_compact(nreal, skin_dflag.as<int32_t>(), skin_dpos.as<int32_t>(),
+                          skin_dlist.as<int32_t>(), s);
+      CK(cudaMemcpyAsync(h_i32 + 3, skin_dpos.as<int32_t>() + nreal, sizeof(int32_t),
+                         cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      ndirty = h_i32[3];
+      CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
+      dyn(ndirty);
+      NeibArgs na = neib_args(T, P);
+      launch_search_few(d, few_args(na, skin_dlist.as<int32_t>(), ndirty, reach), s);
+      RC(read_flags(mc, ov));
+      mc_all = std::max(mc_all, mc);
+    }
+    if (ov) {
+      // no room after the fixed part: lay the whole table out anew
+      RC(fill_table(T, P, true, [&](NeibArgs& na, int) {
+        launch_skin_filter(filter_args(na, false, false), s);
+        launch_search_few(d, few_args(na, skin_dlist.as<int32_t>(), ndirty, reach), s);
+      }));
+      launch_table_end(rowoff.as<int64_t>(), rowcap.as<int32_t>(), nreal,
+                       skin_end.as<int64_t>(), s);
+      cnt_host[SPH_CNT_SKIN_RELAYOUTS]++;
+      mc_all = int(cnt_host[SPH_CNT_NEIB_MAX]);
+    }
+    cnt_host[SPH_CNT_NEIB_MAX] = mc_all;
+    if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc_all + 1 > kb.maxneib[d - 1])
+      return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
+    cnt_host[SPH_CNT_SKIN_DIRTY] += ndirty;
+    return SPH_OK;
+  }
+  // an iterate served from the skin lists; served = false (nothing changed
+  // but the periodic wrap and the records' positions, which the fresh
+  // search redoes) when they no longer can serve it
+  int skin_reuse(const Mode& m, const Params& P, bool& served) {
+    served = false;
+    const int d = P.dim;
+    const int64_t nall = nrows + nghost;
+    BoxGeom g = box(m);
+    {
+      Phase ph(this, SPH_T_GHOSTS);
+      if (m.ghosts) launch_reflect(cols.as<double>(), nrows, nreal, g, s);
+    }
+    BoxGeom gg = g;
+    if (!m.ghosts) for (int k = 0; k < 3; ++k) gg.periodic[k] = 0;
+    const float tau = float(skin_tau), eps = float(skin_eps);
+    unsigned long long* rb = red.as<unsigned long long>();
+    {
+      Phase ph(this, SPH_T_NEIGHBOURS);
+      SlotInit si{};
+      for (int k = 0; k < 3; ++k) {
+        si.off[si.n] = RED_LO_X + k; si.val[si.n++] = dkey(1e308);
+        si.off[si.n] = RED_HI_X + k; si.val[si.n++] = dkey(-1e308);
+      }
+      si.off[si.n] = RED_SKIN_D; si.val[si.n++] = dkey(0.0);
+      si.off[si.n] = RED_SKIN_HMAX; si.val[si.n++] = dkey(0.0);
+      launch_init_slots(rb, si, s);
+      // (the signature flag and the four counts are plain integers)
+      CK(cudaMemsetAsync(rb + RED_SKIN_SIG, 0, 5 * sizeof(unsigned long long), s));
+      launch_skin_refresh(vals_alt.as<int32_t>(), nall, nrows, nreal, cols.as<double>(),
+                          gsrc.as<int32_t>(), gcode.as<int8_t>(), gg, d, skin_sig.as<uint8_t>(),
+                          skin_bx.as<double>(), skin_by.as<double>(), skin_bz.as<double>(),
+                          sx.as<double>(), sy.as<double>(), sz.as<double>(), s32.as<float4>(),
+                          pgeom, skin_dsp.as<float>(), tau, eps, rb, s);
+      CK(cudaMemcpyAsync(h_red, rb, sizeof(unsigned long long) * RED_TOTAL,
+                         cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      CK(cudaGetLastError());
+    }
+    const double D = dkey_inv(h_red[RED_SKIN_D]);
+    const double hmax = dkey_inv(h_red[RED_SKIN_HMAX]);
+    const double hmaxb = dkey_inv(h_red[RED_SKIN_HMAXB]);
+    const unsigned long long nfast = h_red[RED_SKIN_NFAST], nmove = h_red[RED_SKIN_NMOVE];
+    if (h_red[RED_SKIN_SIG]) return SPH_OK;  // some row's image set changed
+    const double dcap = P.krad * skin_hmin;
+    if (!(D <= dcap) || !(hmax > 0) || !std::isfinite(hmax) || !(hmaxb > 0)) return SPH_OK;
+    // every record inside the FP32 packing's binade: 0 <= x - origin < shift
+    const double o[3] = {pgeom.ox, pgeom.oy, pgeom.oz};
+    for (int k = 0; k < 3; ++k) {
+      const double lo = dkey_inv(h_red[RED_LO_X + k]), hi = dkey_inv(h_red[RED_HI_X + k]);
+      if (!(lo >= o[k]) || !(hi - o[k] < pgeom.shift * (1.0 - 1e-9))) return SPH_OK;
+    }
+    // the marking boxes, in cells: around fast records, every centre that
+    // may see them now; around moving ones, every skin list holding them
+    const double reach_f = (P.krad * hmax + skin_tau) * (1.0 + 1e-9);
+    const double reach_m = (1.0 + skin_s) * P.krad * hmaxb * (1.0 + 1e-9);
+    auto cells = [&](double reach) {
+      double c = 1.0;
+      for (int k = 0; k < d; ++k) c *= 2.0 * reach * grid.invL + 3.0;
+      return c;
+    };
+    const double budget = double(1 << 28);
+    if (double(nfast) > double(nall) / 8 || double(nfast) * cells(reach_f) > budget)
+      return SPH_OK;
+    // too many moving records to mark: no row is kept this time
+    const bool mark_m = double(nmove) * cells(reach_m) <= budget;
+    {
+      Phase ph(this, SPH_T_NEIGHBOURS);
+      CK(cudaMemsetAsync(skin_near_f.p, 0, sizeof(uint8_t) * nall, s));
+      if (mark_m) CK(cudaMemsetAsync(skin_near_m.p, 0, sizeof(uint8_t) * nall, s));
+      if (nfast || (mark_m && nmove))
+        launch_skin_mark(nall, skin_dsp.as<float>(), tau, eps, sx.as<double>(), sy.as<double>(),
+                         sz.as<double>(), skin_bx.as<double>(), skin_by.as<double>(),
+                         skin_bz.as<double>(), grid, cstart.as<int32_t>(), reach_f, reach_m,
+                         skin_near_f.as<uint8_t>(), mark_m ? skin_near_m.as<uint8_t>() : nullptr,
+                         s);
+      launch_skin_classify(nreal, centre_k.as<int32_t>(), centre_p.as<int32_t>(), col(es_h),
+                           skin_hb.as<double>(), skin_hdev.as<double>(), skin_gap.as<float>(),
+                           P.krad, 1.0 + skin_s, tau, eps, skin_dsp.as<float>(),
+                           skin_near_f.as<uint8_t>(),
+                           mark_m ? skin_near_m.as<uint8_t>() : nullptr,
+                           skin_mode.as<uint8_t>(), skin_dflag.as<int32_t>(),
+                           ncnt.as<int32_t>(), rb + RED_SKIN_NKEPT, s);
+      // (skin_dflag[nreal] stays 0: the scan's last entry is the count)
+      exclusive_scan(scan_tmp.p, scan_tmp.bytes, skin_dflag.as<int32_t>(),
+                     skin_dpos.as<int32_t>(), nreal + 1, s);
+      launch_skin_compact(nreal, skin_dflag.as<int32_t>(), skin_dpos.as<int32_t>(),
+                          skin_dlist.as<int32_t>(), s);
+      CK(cudaMemcpyAsync(h_i32, skin_dpos.as<int32_t>() + nreal, sizeof(int32_t),
+                         cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(h_red + RED_SKIN_NKEPT, rb + RED_SKIN_NKEPT,
+                         2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    const int64_t ndirty = h_i32[0];
+    const int64_t nkept = int64_t(h_red[RED_SKIN_NKEPT]);
+    if (ndirty > nreal / 4) return SPH_OK;
+    const double reach_d = D * (1.0 + 1e-9);
+    RC(skin_fill(P, ndirty, reach_d));
+    ++skin_age;
+    skin_ending = D > 0.5 * dcap || ndirty > nreal / 8;
+    cnt_host[SPH_CNT_SKIN_REUSES]++;
+    cnt_host[SPH_CNT_SKIN_KEPT] += nkept;
+    kept_pairs += int64_t(h_red[RED_SKIN_NKEPT_PAIRS]);
+    served = true;
+    return SPH_OK;
+  }
+
   // ---- neighbour phase: images, grid, sort, lists --------------------------------------------
   int neighbour_phase(const Mode& m, const Params& P) {
+    const double skin = skin_fraction();
+    if (skin > 0 && skin_valid && skin == skin_s) {
+      bool served = false;
+      RC(skin_reuse(m, P, served));
+      if (served) return SPH_OK;
+    }
+    skin_valid = false;
     const int d = P.dim;
     BoxGeom g = box(m);
     {
@@ -581,13 +1051,16 @@ struct sph_handle {
     int end_bit = 1;
     while ((int64_t(1) << end_bit) < ncell) ++end_bit;
     // FP32 position packing: one binade [2^E, 2^(E+1)) over the whole extent
-    double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    // (with skin lists, and room of one search radius on every side for the
+    // records to move before the next sort)
+    const double mg = skin > 0 ? P.krad * hmin : 0.0;
+    double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2])) + 2.0 * mg;
     double sh = 1.0;
     if (ext > 0) {
       while (sh < ext * 1.0001) sh *= 2.0;
       while (sh * 0.5 >= ext * 1.0001) sh *= 0.5;
     }
-    pgeom.ox = lo[0]; pgeom.oy = lo[1]; pgeom.oz = lo[2];
+    pgeom.ox = lo[0] - mg; pgeom.oy = lo[1] - mg; pgeom.oz = lo[2] - mg;
     pgeom.shift = sh;
     pgeom.mref = mref;
     {
@@ -624,71 +1097,14 @@ struct sph_handle {
       launch_fill_i32(count_prev.as<int32_t>(), nrows, est_count, s);
       CK(cudaMemsetAsync(h_prev.p, 0, sizeof(float) * nrows, s));
     }
-    for (int attempt = 0; attempt < 4; ++attempt) {
-      Phase ph(this, SPH_T_NEIGHBOURS);
-      launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(), count_prev.as<int32_t>(),
-                    h_prev.as<float>(), col(es_h), d, 1.2f, rowcap64.as<int64_t>(),
-                    rowcap.as<int32_t>(), s);
-      exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, rowcap64.as<int64_t>(), rowoff.as<int64_t>(),
-                       nreal, s);
-      if (nl_size <= 0) {
-        nl_size = (int64_t(est_count) * 12 / 10 + 8) * nreal * 5 / 4;
-        RC(nl.ensure(sizeof(int32_t) * nl_size));
-      }
-      if (attempt > 0) {
-        // a re-run: size the table for the rows computed from the new counts
-        CK(cudaMemcpyAsync(h_i32 + 2, rowcap.as<int32_t>() + (nreal - 1), sizeof(int32_t),
-                           cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(reinterpret_cast<int64_t*>(h_red + RED_TOTAL),
-                           rowoff.as<int64_t>() + (nreal - 1), sizeof(int64_t),
-                           cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        int64_t total = reinterpret_cast<int64_t*>(h_red + RED_TOTAL)[0] + h_i32[2];
-        if (total > nl_size) {
-          nl_size = total + total / 4;
-          RC(nl.ensure(sizeof(int32_t) * nl_size));
-        }
-      }
-      CK(cudaMemsetAsync(maxcnt.p, 0, sizeof(int32_t), s));
-      CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
-      NeibArgs na{};
-      na.nc = nreal;
-      na.centre_k = centre_k.as<int32_t>();
-      na.centre_p = centre_p.as<int32_t>();
-      na.sx = sx.as<double>(); na.sy = sy.as<double>(); na.sz = sz.as<double>();
-      na.s32 = s32.as<float4>();
-      na.shift = pgeom.shift;
-      na.hcol = col(es_h);
-      na.krad = P.krad;
-      na.g = grid;
-      na.cstart = cstart.as<int32_t>();
-      na.rowoff = rowoff.as<int64_t>();
-      na.rowcap = rowcap.as<int32_t>();
-      na.nl_size = nl_size;
-      na.nl = nl.as<int32_t>();
-      na.ncnt = ncnt.as<int32_t>();
-      na.orig = orig.as<int32_t>();
-      na.count_prev = count_prev.as<int32_t>();
-      na.h_prev = h_prev.as<float>();
-      na.maxcnt = maxcnt.as<int32_t>();
-      na.overflow = overflow.as<int32_t>();
-      na.dcnt = dcnt.as<unsigned long long>();
-      launch_neighbours(d, lanes_search(), st[SPH_P_SEARCH_STAGED] != 0, na, s);
-      CK(cudaMemcpyAsync(h_i32, maxcnt.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(h_i32 + 1, overflow.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      CK(cudaGetLastError());
-      int mc = h_i32[0];
-      cnt_host[SPH_CNT_NEIB_MAX] = mc;
-      cnt_host[SPH_CNT_SEARCHES]++;
-      if (h_i32[1] & 2)
-        return fail(SPH_ERR_TIMEOUT, "neighbour search: a bulk copy into shared memory did not "
-                                     "complete within its wait limit");
-      if (st[SPH_P_NEIB_CAP_CHECK] != 0 && mc + 1 > kb.maxneib[d - 1])
-        return fail(SPH_ERR_NEIB_OVERFLOW, "KDTree neibsearch result was truncated (neighboursearch.f90:131)");
-      if (!h_i32[1]) break;
-      // count_prev now holds the exact counts, so the next attempt fits
-      if (attempt == 3) return fail(SPH_ERR_NEIB_OVERFLOW, "neighbour list capacity");
+    if (skin > 0) {
+      RC(skin_build(m, P, skin, hmin));
+    } else {
+      const bool staged = st[SPH_P_SEARCH_STAGED] != 0;
+      RC(fill_table(exact_table(), P, true, [&](NeibArgs& na, int) {
+        launch_neighbours(d, lanes_search(), staged, na, s);
+        cnt_host[SPH_CNT_SEARCHES]++;
+      }));
     }
     have_order = true;
     cnt_host[SPH_CNT_GHOSTS] = nghost;
@@ -879,6 +1295,7 @@ struct sph_handle {
   // captured as a CUDA graph and replayed.
 
   int neighbour_phase_dev(const Mode& m, const Params& P) {
+    skin_valid = false;  // the device-resident step sorts afresh
     const int d = P.dim;
     BoxGeom g = box(m);
     if (m.ghosts) launch_reflect(cols.as<double>(), nrows, nreal, g, s);
@@ -982,6 +1399,7 @@ struct sph_handle {
 
   // capacities of the device-resident step, from the last host-planned one
   int drs_prepare() {
+    skin_valid = false;  // its capacities may move the sorted arrays
     const int64_t want_ghost = nghost + nghost / 4 + 1024;
     if (want_ghost > nghost_cap || nall_cap != nrows + nghost_cap) {
       nghost_cap = std::max(want_ghost, nghost_cap);
@@ -1398,6 +1816,7 @@ struct sph_handle {
   }
   size_t table_bytes() const { return sizeof(double) * NCOL * size_t(nrows); }
   int copy_table(void* dst, const void* src) {
+    if (dst == cols.p) skin_valid = false;  // the records' positions jump
     CK(cudaMemcpyAsync(dst, src, table_bytes(), cudaMemcpyDeviceToDevice, s));
     return SPH_OK;
   }
@@ -1448,6 +1867,8 @@ struct sph_handle {
     RC(adjoint_supported());
     if (nsteps < 1 || every < 1) return fail(SPH_ERR_ARG, "adjoint: nsteps and every must be >= 1");
     st[SPH_P_REORDER_EVERY] = 0;  // rows stay put: checkpoints are row images
+    st[SPH_P_SKIN] = 0;           // every iterate searches afresh (the replays' lists are
+                                  // then those of the recorded steps, in the same order)
     // The adjoint differentiates the converged density pass (h a function of
     // the positions alone).  The stored rho and Omega are those of the last
     // Newton iterate before its update of h, so with the parity tolerance
@@ -1597,7 +2018,10 @@ struct sph_handle {
     }
     done = false;
     int reorder_every = int(st[SPH_P_REORDER_EVERY]);
-    if (reorder_every > 0 && steps_since_reorder >= reorder_every) RC(reorder_rows());
+    // with skin lists the rows keep their order while the lists serve, and
+    // are re-sorted before the search that replaces lists near their end
+    if (reorder_every > 0 && steps_since_reorder >= reorder_every && skin_lets_reorder())
+      RC(reorder_rows());
     double dthydro, dtdiff, dtfld, dt;
     RC(timestep(dthydro, dtdiff, dtfld, dt));
     bool do_sts = false;
@@ -1984,6 +2408,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
   h->st[SPH_P_NEWTON_MAXITER] = 100;
   h->st[SPH_P_CELL_FACTOR] = 0.4;
   h->st[SPH_P_REORDER_EVERY] = 8;
+  h->st[SPH_P_SKIN] = 0.1;
   h->nreal = int64_t(h->st[ec_realpn]);
   h->nfixed = std::max<int64_t>(0, int64_t(h->st[ec_fixedpn]));
   if (h->nreal <= 0 || h->nreal + h->nfixed != n_rows) {
@@ -2044,6 +2469,15 @@ int sph_set_param(sph_handle* h, int index, double value) {
   if (h->st[index] != value) {  // a captured step holds the old value
     h->graph_dirty = true;
     h->param_gen++;
+    // parameters that cannot change a neighbour set leave skin lists valid
+    switch (index) {
+      case SPH_P_TIMING: case SPH_P_AV_ALPHA: case SPH_P_AV_BETA: case SPH_P_NEWTON_TOL:
+      case SPH_P_NEWTON_MAXITER: case SPH_P_LANES_PAIR: case SPH_P_FIXED_DT: case SPH_P_GRAPH:
+      case SPH_P_REORDER_EVERY: case ec_tfinish: case ec_dtprint: case ec_time:
+        break;
+      default:
+        h->skin_valid = false;
+    }
   }
   h->st[index] = value;
   if (index == SPH_P_NEIB_CAP && value > 0) h->est_count = 0;
@@ -2063,13 +2497,14 @@ int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
   CK(cudaStreamSynchronize(h->s));
   CK(cudaGetLastError());
   h->have_order = false;
+  h->skin_valid = false;  // rows back in caller order
   return SPH_OK;
 }
 
 int sph_iterate(sph_handle* h) {
   AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
-  RC(h->reorder_rows());
+  if (h->skin_lets_reorder()) RC(h->reorder_rows());
   int rc = h->iterate(true);
   h->collect_timers();
   return rc;
@@ -2078,7 +2513,7 @@ int sph_iterate(sph_handle* h) {
 int sph_density(sph_handle* h) {
   AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
-  RC(h->reorder_rows());
+  if (h->skin_lets_reorder()) RC(h->reorder_rows());
   int rc = h->iterate(false);
   h->collect_timers();
   return rc;
@@ -2306,6 +2741,10 @@ int sph_set_columns(sph_handle* h, const int* fields, int nf, const double* in) 
   CK(cudaMemcpyAsync(h->colbuf.p, in, bytes, cudaMemcpyDefault, h->s));
   launch_set_columns(h->cols.as<double>(), h->nrows, h->orig.as<int32_t>(), h->nrows, fs,
                      h->colbuf.as<double>(), h->s);
+  // skin lists follow moved positions and changed h by themselves (the next
+  // iterate measures both); a changed particle type may change the image set
+  for (int k = 0; k < fs.n; ++k)
+    if (fs.f[k] == es_type) h->skin_valid = false;
   CK(cudaStreamSynchronize(h->s));
   CK(cudaGetLastError());
   return SPH_OK;
@@ -2318,7 +2757,7 @@ int sph_get_counters(sph_handle* h, int64_t* out, int n) {
   CK(cudaStreamSynchronize(h->s));
   int64_t all[SPH_CNT_TOTAL];
   for (int k = 0; k < SPH_CNT_TOTAL; ++k) all[k] = h->cnt_host[k];
-  all[SPH_CNT_NEIB_PAIRS] = int64_t(d[DC_NEIB_PAIRS]);
+  all[SPH_CNT_NEIB_PAIRS] = int64_t(d[DC_NEIB_PAIRS]) + h->kept_pairs;
   all[SPH_CNT_C1_PAIRS] = int64_t(d[DC_C1_PAIRS]);
   all[SPH_CNT_C1_SWEEPS] = std::max<int64_t>(int64_t(d[DC_C1_MAXSWEEPS]), h->host_max_sweeps);
   all[SPH_CNT_C2_PAIRS] = int64_t(d[DC_C2_PAIRS]);
@@ -2336,6 +2775,7 @@ int sph_reset_counters(sph_handle* h) {
   CK(cudaStreamSynchronize(h->s));
   for (auto& c : h->cnt_host) c = 0;
   for (auto& t : h->timers) t = 0.;
+  h->kept_pairs = 0;
   h->host_max_sweeps = 0;
   h->launch_base = launches_so_far();
   return SPH_OK;

@@ -562,6 +562,7 @@ k_neighbours(NeibArgs a) {
   float lo_thr = -1.f, hi_thr = -1.f, ux = 0.f, uy = 0.f, uz = 0.f, rc = 0.f, mrg = 0.f;
   int rcap = 0, home = -1;
   int64_t off = 0;
+  int64_t cg = c;  // the centre's index in centre_k / centre_p / rowoff / rowcap / ncnt
   auto clampc = [](float v, int n) {
     float f = floorf(v);
     if (!(f >= 0.f)) return 0;
@@ -569,11 +570,13 @@ k_neighbours(NeibArgs a) {
     return int(f);
   };
   if (active) {
-    k = a.centre_k[c];
-    p = a.centre_p[c];
+    if (a.cmap) cg = a.cmap[c];
+    k = a.centre_k[cg];
+    p = a.centre_p[cg];
     xi = a.sx[k]; yi = a.sy[k]; zi = a.sz[k];
     pi = a.s32[k];
-    const double kh = __dmul_rn(a.krad, a.hcol[p]);
+    double kh = __dmul_rn(a.krad, a.hcol[p]);
+    if (a.kfac > 0.0 && a.kfac != 1.0) kh = __dmul_rn(kh, a.kfac);  // a skin search
     R2 = __dmul_rn(kh, kh);
     const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
     const double er = (shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
@@ -586,11 +589,11 @@ k_neighbours(NeibArgs a) {
     ux = float((xi - g.ox) * g.invL); uy = float((yi - g.oy) * g.invL);
     uz = float((zi - g.oz) * g.invL);
     mrg = 1e-3f + 1e-6f * (fabsf(ux) + fabsf(uy) + fabsf(uz));
-    rc = float(R * g.invL) * (1.f + 1e-5f) + mrg;
+    rc = float((R + a.reach) * g.invL) * (1.f + 1e-5f) + mrg;
     home = (DIM >= 2 ? clampc(uy, g.ny) : 0) + (DIM == 3 ? clampc(uz, g.nz) : 0) * g.ny;
-    off = a.rowoff[c];
+    off = a.rowoff[cg];
     // slots usable without leaving the table; a shorter row is an overflow
-    const int rcap0 = a.rowcap[c];
+    const int rcap0 = a.rowcap[cg];
     const int64_t room = a.nl_size - off;
     rcap = room <= 0 ? 0 : (room < int64_t(rcap0) ? int(room) : rcap0);
   }
@@ -838,20 +841,601 @@ k_neighbours(NeibArgs a) {
     nheld = 0;
   }
   if (active) {
-    a.ncnt[c] = cnt;
+    a.ncnt[cg] = cnt;
     a.count_prev[a.orig[p]] = cnt;
     a.h_prev[a.orig[p]] = float(a.hcol[p]);
-    atomicMax(a.maxcnt, cnt);
-    if (cnt > rcap) atomicOr(a.overflow, 1);
     nfound = unsigned(cnt);
+  }
+  // the longest row and any overflow leave the warp as one atomic each (one
+  // per centre on a single address would serialise in its L2 slice)
+  {
+    const int wmax = __reduce_max_sync(FULL, active ? cnt : 0);
+    const bool wovf = __any_sync(FULL, active && cnt > rcap);
+    if (wl == 0) {
+      if (wmax) atomicMax(a.maxcnt, wmax);
+      if (wovf) atomicOr(a.overflow, 1);
+    }
   }
   unsigned int wc = __reduce_add_sync(FULL, ncand);
   unsigned int wf = __reduce_add_sync(FULL, nfound);
   unsigned int we = __reduce_add_sync(FULL, nexact);
   if (wl == 0) {
     atomicAdd(&a.dcnt[DC_CANDIDATES], (unsigned long long)wc);
-    atomicAdd(&a.dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
+    if (!a.skin_search) atomicAdd(&a.dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
     atomicAdd(&a.dcnt[DC_EXACT_TESTS], (unsigned long long)we);
+  }
+}
+
+// ---- skin lists (SPH_P_SKIN) -------------------------------------------------------------
+// A search of radius kfac krad h (kfac = 1 + s) at step b leaves each centre
+// its skin list: every record within that radius at b.  At a later step t
+// every record has moved by at most d (the running maximum of its FP64
+// distance from its position at b), so a record j outside centre i's skin
+// list lies at least kfac krad h_b - d_i - d_j from it (triangle
+// inequality): it cannot pass i's predicate at t while
+// krad h_t + d_i + d_j < kfac krad h_b.  Each centre takes one of three
+// ways at t:
+//  * fresh search (the search over the cells of step b, its cell range
+//    widened by the largest displacement D): a record that moved more than
+//    tau ("fast") is within reach, the centre moved more than tau itself, or
+//    its h grew too far for the inequality above;
+//  * keep: no record of its skin list moved more than eps, nor did the
+//    centre, and 2 eps + krad |h_t - h_b| (running maximum) stays below the
+//    gap of step b (the smallest distance of a skin-list record from the
+//    sphere krad h_b): no record crossed the sphere, so the row written at
+//    b is the set at t (the row is not touched; the ways are monotone, so a
+//    kept row was never rewritten since b);
+//  * filter: its skin list through the FP64 predicate.
+// Either way each centre's set is the FP64 predicate's over all records,
+// i.e. that of a fresh search.  The image records of step b are reused when
+// no row's image signature changed (the image set is then the one the image
+// builder would make at t) and are placed by the same arithmetic
+// (image_coord).
+
+// which periodic sides hold the row: per axis the unpadded side (-1, 0, +1)
+// and whether the padded test agrees, 6 states per axis
+__device__ __forceinline__ uint8_t image_sig(const double* r, const BoxGeom& g, int dim) {
+  const AxisSigns sg = axis_signs(r, g, dim);
+  int v = 0, m = 1;
+  for (int k = 0; k < 3; ++k) {
+    v += m * ((sg.npad[k] + 1) + 3 * (sg.pad[k] != 0 ? 1 : 0));
+    m *= 6;
+  }
+  return uint8_t(v);
+}
+
+__global__ void k_skin_sig(const double* __restrict__ cols, int64_t ld, int64_t nrows,
+                           BoxGeom g, int dim, uint8_t* __restrict__ sig) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nrows) return;
+  const double r[3] = {cols[es_rx * ld + i], cols[es_ry * ld + i], cols[es_rz * ld + i]};
+  sig[i] = ghost_source(cols[es_type * ld + i]) ? image_sig(r, g, dim) : uint8_t(0);
+}
+
+__global__ void __launch_bounds__(TPB)
+k_skin_refresh(const int32_t* __restrict__ sidx, int64_t n, int64_t nrows, int64_t nreal,
+               const double* __restrict__ cols, int64_t ld, const int32_t* __restrict__ gsrc,
+               const int8_t* __restrict__ gcode, BoxGeom g, int dim,
+               const uint8_t* __restrict__ sig_b, const double* __restrict__ bx,
+               const double* __restrict__ by, const double* __restrict__ bz,
+               double* __restrict__ sx, double* __restrict__ sy, double* __restrict__ sz,
+               float4* __restrict__ s32, PackGeom pg, float* __restrict__ dsp, float tau,
+               float eps, unsigned long long* __restrict__ red) {
+  // slots: lo x, y, z (min), hi x, y, z (max), D (max), h of the real rows (max)
+  double v[8] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 0.0, 0.0};
+  const bool is_max[8] = {false, false, false, true, true, true, true, true};
+  unsigned nfast = 0, nmove = 0;
+  bool sigchg = false;
+  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n;
+       k += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t u = sidx[k];
+    double x, y, z;
+    if (u < nrows) {
+      x = cols[es_rx * ld + u]; y = cols[es_ry * ld + u]; z = cols[es_rz * ld + u];
+      if (u < nreal) v[7] = fmax(v[7], cols[es_h * ld + u]);
+      if (ghost_source(cols[es_type * ld + u])) {
+        const double r[3] = {x, y, z};
+        sigchg |= image_sig(r, g, dim) != sig_b[u];
+      }
+    } else {
+      const int64_t q = u - nrows;
+      const int64_t src = gsrc[q];
+      const int code = gcode[q];
+      x = image_coord(cols[es_rx * ld + src], code % 3 - 1, g.emin[0], g.emax[0]);
+      y = image_coord(cols[es_ry * ld + src], (code / 3) % 3 - 1, g.emin[1], g.emax[1]);
+      z = image_coord(cols[es_rz * ld + src], code / 9 - 1, g.emin[2], g.emax[2]);
+    }
+    sx[k] = x; sy[k] = y; sz[k] = z;
+    s32[k] = make_float4(__double2float_rn((x - pg.ox) + pg.shift),
+                         __double2float_rn((y - pg.oy) + pg.shift),
+                         __double2float_rn((z - pg.oz) + pg.shift), __int_as_float(int32_t(k)));
+    const double ex = x - bx[k], ey = y - by[k], ez = z - bz[k];
+    // a few ulp of rounding in the differences, squares, sum and root: the
+    // factor and the floor make the stored value an upper bound
+    const double d = sqrt(ex * ex + ey * ey + ez * ez) * (1.0 + 1e-12) + 1e-300;
+    const float df = fmaxf(dsp[k], __double2float_ru(d));  // running maximum since b
+    dsp[k] = df;
+    nfast += df > tau ? 1u : 0u;
+    nmove += df > eps ? 1u : 0u;
+    v[6] = fmax(v[6], double(df));
+    v[0] = fmin(v[0], x); v[1] = fmin(v[1], y); v[2] = fmin(v[2], z);
+    v[3] = fmax(v[3], x); v[4] = fmax(v[4], y); v[5] = fmax(v[5], z);
+  }
+  const unsigned wf = __reduce_add_sync(0xffffffffu, nfast);
+  const unsigned wm = __reduce_add_sync(0xffffffffu, nmove);
+  const unsigned ws = __ballot_sync(0xffffffffu, sigchg);
+  if ((threadIdx.x & 31) == 0) {
+    if (wf) atomicAdd(&red[RED_SKIN_NFAST], (unsigned long long)wf);
+    if (wm) atomicAdd(&red[RED_SKIN_NMOVE], (unsigned long long)wm);
+    if (ws) atomicMax(&red[RED_SKIN_SIG], 1ull);
+  }
+  block_minmax<8>(v, is_max);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 3; ++k) {
+      if (v[k] < 1e300) red_min(&red[RED_LO_X + k], v[k]);
+      if (v[3 + k] > -1e300) red_max(&red[RED_HI_X + k], v[3 + k]);
+    }
+    red_max(&red[RED_SKIN_D], v[6]);
+    red_max(&red[RED_SKIN_HMAX], v[7]);
+  }
+}
+
+// clamped cell coordinate of an FP64 cell-unit value (NaN -> 0)
+__device__ __forceinline__ int clamp_cell(double f, int n) {
+  f = floor(f);
+  if (!(f >= 0.0)) return 0;
+  if (f >= double(n - 1)) return n - 1;
+  return int(f);
+}
+
+// sets flag[q] = 1 for every record q of the cells within `reach` (plus one
+// cell) of (x, y, z), walking the rows of cells of that box
+__device__ void mark_box(double x, double y, double z, double reach, const Grid& g,
+                         const int32_t* __restrict__ cstart, uint8_t* __restrict__ flag) {
+  const int x0 = clamp_cell((x - reach - g.ox) * g.invL - 1.0, g.nx);
+  const int x1 = clamp_cell((x + reach - g.ox) * g.invL + 1.0, g.nx);
+  const int y0 = clamp_cell((y - reach - g.oy) * g.invL - 1.0, g.ny);
+  const int y1 = clamp_cell((y + reach - g.oy) * g.invL + 1.0, g.ny);
+  const int z0 = clamp_cell((z - reach - g.oz) * g.invL - 1.0, g.nz);
+  const int z1 = clamp_cell((z + reach - g.oz) * g.invL + 1.0, g.nz);
+  for (int cz = z0; cz <= z1; ++cz)
+    for (int cy = y0; cy <= y1; ++cy) {
+      const int64_t row = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+      const int32_t a = cstart[row + x0], b = cstart[row + x1 + 1];
+      for (int32_t q = a; q < b; ++q) flag[q] = 1;
+    }
+}
+
+// one thread per record: a record that moved more than eps marks the
+// records whose cells lie within reach_m of its position at b (every centre
+// whose skin list holds it: near_m); one that moved more than tau marks
+// those within reach_f of its position now (near_f)
+__global__ void k_skin_mark(int64_t n, const float* __restrict__ dsp, float tau, float eps,
+                            const double* __restrict__ sx, const double* __restrict__ sy,
+                            const double* __restrict__ sz, const double* __restrict__ bx,
+                            const double* __restrict__ by, const double* __restrict__ bz,
+                            Grid g, const int32_t* __restrict__ cstart, double reach_f,
+                            double reach_m, uint8_t* __restrict__ near_f,
+                            uint8_t* __restrict__ near_m) {
+  const int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (k >= n) return;
+  const float d = dsp[k];
+  if (near_m && d > eps) mark_box(bx[k], by[k], bz[k], reach_m, g, cstart, near_m);
+  if (d > tau) mark_box(sx[k], sy[k], sz[k], reach_f, g, cstart, near_f);
+}
+
+// The way of each centre (mode: 0 filter, 1 fresh search, 2 keep; dflag =
+// 1 for the fresh search).  The margins of 1e-12 (relative) lie far above
+// the FP64 rounding of the predicate and of the displacements, so that no
+// record outside a list can pass the FP64 predicate at t; near_m == NULL
+// (too many moving records to mark) means no centre keeps its row.
+__global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k,
+                                const int32_t* __restrict__ centre_p,
+                                const double* __restrict__ hcol, const double* __restrict__ hb,
+                                double* __restrict__ hdev, const float* __restrict__ gap,
+                                double krad, double kfac, float tau, float eps,
+                                const float* __restrict__ dsp,
+                                const uint8_t* __restrict__ near_f,
+                                const uint8_t* __restrict__ near_m,
+                                uint8_t* __restrict__ mode, int32_t* __restrict__ dflag,
+                                const int32_t* __restrict__ ncnt,
+                                unsigned long long* __restrict__ nkept) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  uint8_t w = 1;
+  if (c < nc) {
+    const bool was_searched = mode[c] == 1;  // (a centre once searched afresh stays so)
+    const int32_t k = centre_k[c];
+    const double h = hcol[centre_p[c]], h0 = hb[c];
+    const double hd = fmax(hdev[c], fabs(h - h0));
+    hdev[c] = hd;
+    const double di = double(dsp[k]);
+    const double lhs = krad * h * (1.0 + 1e-12) + di + double(tau);
+    const double rhs = krad * h0 * kfac * (1.0 - 1e-12);
+    const bool clean = !was_searched && !near_f[k] && dsp[k] <= tau && lhs < rhs;
+    if (clean) {
+      const bool keep = near_m && !near_m[k] && dsp[k] <= eps &&
+                        2.0 * double(eps) + krad * hd * (1.0 + 1e-12) + 1e-12 * krad * h0 <
+                            double(gap[c]);
+      w = keep ? 2 : 0;
+    }
+    mode[c] = w;
+    dflag[c] = w == 1 ? 1 : 0;
+  }
+  // rows kept and their neighbours: nkept[0], nkept[1]
+  const bool kp = c < nc && w == 2;
+  const unsigned kept = __ballot_sync(0xffffffffu, kp);
+  const unsigned pairs = __reduce_add_sync(0xffffffffu, kp ? unsigned(ncnt[c]) : 0u);
+  if ((threadIdx.x & 31) == 0 && kept) {
+    atomicAdd(nkept, (unsigned long long)__popc(kept));
+    atomicAdd(nkept + 1, (unsigned long long)pairs);
+  }
+}
+
+__global__ void k_skin_compact(int64_t nc, const int32_t* __restrict__ dflag,
+                               const int32_t* __restrict__ dpos, int32_t* __restrict__ dlist) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c < nc && dflag[c]) dlist[dpos[c]] = int32_t(c);
+}
+
+// hb[c] = h of centre c, and the largest of them into red[slot] (dkey max)
+__global__ void __launch_bounds__(TPB)
+k_gather_h(int64_t nc, const int32_t* __restrict__ centre_p, const double* __restrict__ hcol,
+           double* __restrict__ hb, unsigned long long* __restrict__ red, int slot) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  double v[1] = {0.0};
+  const bool is_max[1] = {true};
+  if (c < nc) {
+    v[0] = hcol[centre_p[c]];
+    hb[c] = v[0];
+  }
+  block_minmax<1>(v, is_max);
+  if (threadIdx.x == 0) red_max(&red[slot], v[0]);
+}
+
+// G lanes per centre walk its skin list 4 G records at a time: every lane
+// loads 4 consecutive entries at once (rows start on 16-byte boundaries:
+// row capacities are multiples of 4) and gathers their 4 FP32 images
+// together; FP32 test with the search's guard band, FP64 predicate in the
+// band (the same arithmetic as the search, so the same decisions); the
+// round's hits go to the row in list order (prefix of the lanes' counts).
+// With gap != NULL each centre also records the smallest distance of a
+// list record from its sphere, less the FP32 images' error bound.
+// Counters and the longest row are summed over the block's whole share of
+// centres (a grid of a few blocks per SM strides over them) and leave it as
+// one atomic each: one atomic per centre on a single address would
+// serialise in its L2 slice.
+template <int G>
+__global__ void __launch_bounds__(128) k_skin_filter(SkinFilterArgs a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int V = 4;
+  constexpr int PER = G * V;
+  constexpr int CPB = 128 / G;  // centres per block and pass
+  const int lane = threadIdx.x & (G - 1);
+  unsigned long long ncand = 0, nfound = 0, nexact = 0;
+  int maxc = 0;
+  bool ovf = false;
+  for (int64_t cb = blockIdx.x; cb * CPB < a.nc; cb += gridDim.x) {
+    const int64_t c = cb * CPB + threadIdx.x / G;
+    bool active = c < a.nc;
+    if (active) {
+      const uint8_t w = a.mode[c];
+      active = w == 0 || (w == 2 && !a.keep);
+    }
+    int32_t k = -1, n = 0, rcap = 0;
+    int64_t off = 0;
+    const int4* src = reinterpret_cast<const int4*>(a.skin_nl);
+    double xi = 0.0, yi = 0.0, zi = 0.0, R2 = 0.0, hi_ = 0.0, Rx = 0.0;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    float lo_thr = -1.f, hi_thr = -1.f, Rf = 0.f;
+    if (active) {
+      k = a.centre_k[c];
+      const int32_t p = a.centre_p[c];
+      xi = a.sx[k]; yi = a.sy[k]; zi = a.sz[k];
+      pi = a.s32[k];
+      hi_ = a.hcol[p];
+      const double kh = __dmul_rn(a.krad, hi_);
+      R2 = __dmul_rn(kh, kh);
+      Rx = sqrt(R2);
+      Rf = float(Rx);
+      const double R = Rx * (1.0 + 1e-9) + 1e-300;
+      const double er = (a.shift * 1.1920928955078125e-7) / R;
+      const double delta = 8.0 * er + 4.0 * er * er + 1e-6;
+      lo_thr = float(R2 * (1.0 - delta));
+      hi_thr = float(R2 * (1.0 + delta));
+      n = a.skin_cnt[c];
+      src = reinterpret_cast<const int4*>(a.skin_nl + a.skin_off[c]);
+      off = a.rowoff[c];
+      const int rcap0 = a.rowcap[c];
+      const int64_t room = a.nl_size - off;
+      rcap = room <= 0 ? 0 : (room < int64_t(rcap0) ? int(room) : rcap0);
+    }
+    const int rounds = __reduce_max_sync(FULL, active ? (n + PER - 1) / PER : 0);
+    int cnt = 0;
+    float gmin = 3.0e38f;
+    int32_t* const dst = a.nl + off;
+    for (int r = 0; r < rounds; ++r) {
+      const int base = r * PER + lane * V;
+      int32_t q[V] = {-1, -1, -1, -1};
+      unsigned m = 0;
+      if (active && base < n) {
+        // the int4 holding entry base lies inside the row's capacity
+        const int4 v = __ldcs(src + (r * G + lane));
+        q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = v.w;
+        float4 pj[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j)
+          if (base + j < n) pj[j] = __ldg(a.s32 + q[j]);
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          if (base + j >= n) continue;
+          const float sd32 = dist2_f32(pj[j], pi);
+          if ((sd32 < lo_thr && sd32 > 0.f) || sd32 > hi_thr) {
+            if (sd32 <= hi_thr) m |= 1u << j;
+            if (a.gap) {
+              // |r - R| from the images: their error (eimg) and the FP32
+              // rounding of the distance, the root and the difference
+              const float r32 = sqrtf(sd32);
+              gmin = fminf(gmin, fabsf(r32 - Rf) - (a.eimg + 4e-7f * (Rf + r32)));
+            }
+          } else if (q[j] != k) {
+            ++nexact;
+            const double d0 = __dadd_rn(a.sx[q[j]], -xi);
+            const double d1 = __dadd_rn(a.sy[q[j]], -yi);
+            const double d2 = __dadd_rn(a.sz[q[j]], -zi);
+            const double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                        __dmul_rn(d2, d2));
+            if (!(sd > R2)) m |= 1u << j;
+            if (a.gap) gmin = fminf(gmin, __double2float_rd(fabs(sqrt(sd) - Rx) - 1e-9 * Rx));
+          }
+        }
+      }
+      // exclusive prefix of the hit counts over the group's lanes
+      const int nh = __popc(m);
+      int incl = nh;
+#pragma unroll
+      for (int d = 1; d < G; d <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, d, G);
+        if (lane >= d) incl += t;
+      }
+      const int total = __shfl_sync(FULL, incl, G - 1, G);
+      int pos = cnt + incl - nh;
+#pragma unroll
+      for (int j = 0; j < V; ++j)
+        if ((m >> j) & 1u) {
+          if (pos < rcap) __stcg(dst + pos, q[j]);
+          ++pos;
+        }
+      cnt += total;
+    }
+    if (a.gap) {
+#pragma unroll
+      for (int d = 1; d < G; d <<= 1) gmin = fminf(gmin, __shfl_xor_sync(FULL, gmin, d, G));
+    }
+    if (active && lane == 0) {
+      const int32_t p = a.centre_p[c];
+      a.ncnt[c] = cnt;
+      a.count_prev[a.orig[p]] = cnt;
+      a.h_prev[a.orig[p]] = float(hi_);
+      if (a.gap) a.gap[c] = gmin;
+      maxc = max(maxc, cnt);
+      ovf |= cnt > rcap;
+      nfound += unsigned(cnt);
+      ncand += unsigned(n);
+    }
+  }
+  // block totals: warp reductions, then the 4 warps through shared memory
+  __shared__ unsigned long long part[4][3];
+  __shared__ int pmax[4], povf[4];
+  const int w = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  for (int o = 16; o > 0; o >>= 1) {
+    ncand += __shfl_xor_sync(FULL, ncand, o);
+    nfound += __shfl_xor_sync(FULL, nfound, o);
+    nexact += __shfl_xor_sync(FULL, nexact, o);
+  }
+  const int wmax = __reduce_max_sync(FULL, maxc);
+  const bool wovf = __any_sync(FULL, ovf);
+  if (wl == 0) {
+    part[w][0] = ncand; part[w][1] = nfound; part[w][2] = nexact;
+    pmax[w] = wmax;
+    povf[w] = wovf ? 1 : 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t[3] = {0, 0, 0};
+    int mx = 0, ov = 0;
+    for (int i = 0; i < int(blockDim.x >> 5); ++i) {
+      for (int j = 0; j < 3; ++j) t[j] += part[i][j];
+      mx = max(mx, pmax[i]);
+      ov |= povf[i];
+    }
+    if (t[0]) atomicAdd(&a.dcnt[DC_CANDIDATES], t[0]);
+    if (t[1]) atomicAdd(&a.dcnt[DC_NEIB_PAIRS], t[1]);
+    if (t[2]) atomicAdd(&a.dcnt[DC_EXACT_TESTS], t[2]);
+    if (mx) atomicMax(a.maxcnt, mx);
+    if (ov) atomicOr(a.overflow, 1);
+  }
+}
+
+// ---- rows of the centres searched afresh (skin-list iterates) -----------------------------
+// They are laid out anew every iterate after the table's fixed part (whose
+// rows the other centres keep): cap[i] for centre list[i] from its last
+// count as k_rowcap sizes rows, then (after the scan) rowoff / rowcap.
+__global__ void k_dyn_caps(int64_t nd, const int32_t* __restrict__ list,
+                           const int32_t* __restrict__ centre_p, const int32_t* __restrict__ orig,
+                           const int32_t* __restrict__ count_prev,
+                           const float* __restrict__ h_prev, const double* __restrict__ hcol,
+                           int dim, float slack, int64_t* __restrict__ cap) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i > nd) return;
+  if (i == nd) { cap[i] = 0; return; }
+  const int32_t p = centre_p[list[i]];
+  const int32_t o = orig[p];
+  float est = float(count_prev[o]);
+  const float hp = h_prev[o];
+  if (hp > 0.f) {
+    float g = float(hcol[p]) / hp;
+    g = fminf(fmaxf(g, 0.5f), 4.f);
+    est *= dim == 3 ? g * g * g : (dim == 2 ? g * g : g);
+  }
+  cap[i] = (int64_t(fminf(est * slack, 1.0e9f)) + 8 + 3) & ~int64_t(3);
+}
+__global__ void k_dyn_assign(int64_t nd, const int32_t* __restrict__ list,
+                             const int64_t* __restrict__ off, const int64_t* __restrict__ cap,
+                             const int64_t* __restrict__ base, int64_t* __restrict__ rowoff,
+                             int32_t* __restrict__ rowcap) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= nd) return;
+  const int32_t c = list[i];
+  rowoff[c] = *base + off[i];
+  rowcap[c] = int32_t(cap[i]);
+}
+// end[0] = rowoff[n - 1] + rowcap[n - 1] (the end of a freshly laid-out table)
+__global__ void k_table_end(const int64_t* __restrict__ rowoff, const int32_t* __restrict__ rowcap,
+                            int64_t n, int64_t* __restrict__ end) {
+  end[0] = n > 0 ? rowoff[n - 1] + rowcap[n - 1] : 0;
+}
+// filter rows that overflowed their place join the centres searched afresh:
+// mode[c] = 1, and dflag[c] = 1 for every centre of mode 1
+__global__ void k_overflow_to_search(int64_t nc, const int32_t* __restrict__ ncnt,
+                                     const int64_t* __restrict__ rowoff,
+                                     const int32_t* __restrict__ rowcap, int64_t nl_size,
+                                     uint8_t* __restrict__ mode, int32_t* __restrict__ dflag) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= nc) return;
+  uint8_t w = mode[c];
+  if (w == 0) {
+    const int64_t room = nl_size - rowoff[c];
+    const int64_t rc = room < int64_t(rowcap[c]) ? (room > 0 ? room : 0) : int64_t(rowcap[c]);
+    if (int64_t(ncnt[c]) > rc) w = 1;
+  }
+  mode[c] = w;
+  dflag[c] = w == 1 ? 1 : 0;
+}
+
+// Search of a few centres (a list): G lanes per centre walk the rows of
+// cells its sphere reaches (radius krad h + reach, the records having moved
+// up to `reach` from the positions they were sorted by), each row's x-run of
+// cells one contiguous run of records, G records at a time: the search's FP32
+// test with its guard band, the FP64 predicate in the band, the hits in walk
+// order (ballot + prefix within the group).  Row by row in increasing cell
+// index, so each row of the list is in increasing record order.
+template <int DIM, int G>
+__global__ void __launch_bounds__(128) k_search_few(FewArgs a) {
+  constexpr int CPB = 128 / G;
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gmask = (G == 32) ? 0xffffffffu
+                                   : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+  const unsigned below = (1u << lane) - 1u;
+  unsigned long long ncand = 0, nfound = 0, nexact = 0;
+  int maxc = 0;
+  bool ovf = false;
+  for (int64_t cb = blockIdx.x; cb * CPB < a.n; cb += gridDim.x) {
+    const int64_t i = cb * CPB + threadIdx.x / G;
+    if (i >= a.n) continue;  // (the whole group)
+    const int32_t c = a.list[i];
+    const int32_t k = a.centre_k[c], p = a.centre_p[c];
+    const double xi = a.sx[k], yi = a.sy[k], zi = a.sz[k];
+    const float4 pi = a.s32[k];
+    const double hi_ = a.hcol[p];
+    const double kh = __dmul_rn(a.krad, hi_);
+    const double R2 = __dmul_rn(kh, kh);
+    const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
+    const double er = (a.shift * 1.1920928955078125e-7) / R;
+    const double delta = 8.0 * er + 4.0 * er * er + 1e-6;
+    const float lo_thr = float(R2 * (1.0 - delta)), hi_thr = float(R2 * (1.0 + delta));
+    const Grid& g = a.g;
+    const double ux = (xi - g.ox) * g.invL, uy = (yi - g.oy) * g.invL, uz = (zi - g.oz) * g.invL;
+    // radius in cells, widened far above its rounding
+    const double rr = (R + a.reach) * g.invL * (1.0 + 1e-9) +
+                      1e-9 * (fabs(ux) + fabs(uy) + fabs(uz)) + 1e-6;
+    const int cy0 = DIM >= 2 ? clamp_cell(uy - rr, g.ny) : 0;
+    const int cy1 = DIM >= 2 ? clamp_cell(uy + rr, g.ny) : 0;
+    const int cz0 = DIM == 3 ? clamp_cell(uz - rr, g.nz) : 0;
+    const int cz1 = DIM == 3 ? clamp_cell(uz + rr, g.nz) : 0;
+    const int64_t off = a.rowoff[c];
+    const int rcap0 = a.rowcap[c];
+    const int64_t room = a.nl_size - off;
+    const int rcap = room <= 0 ? 0 : (room < int64_t(rcap0) ? int(room) : rcap0);
+    int32_t* const dst = a.nl + off;
+    int cnt = 0;
+    for (int cz = cz0; cz <= cz1; ++cz) {
+      const double dzc = DIM == 3 ? fmax(0.0, fmax(double(cz) - uz, uz - double(cz + 1))) : 0.0;
+      for (int cy = cy0; cy <= cy1; ++cy) {
+        const double dyc = DIM >= 2 ? fmax(0.0, fmax(double(cy) - uy, uy - double(cy + 1))) : 0.0;
+        const double rem = rr * rr - dyc * dyc - dzc * dzc;
+        if (rem < 0.0) continue;
+        const double w = sqrt(rem);
+        const int cx0 = clamp_cell(ux - w, g.nx), cx1 = clamp_cell(ux + w, g.nx);
+        const int64_t rowc = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+        const int32_t q0 = __ldg(a.cstart + rowc + cx0), q1 = __ldg(a.cstart + rowc + cx1 + 1);
+        ncand += (lane == 0) ? unsigned(q1 - q0) : 0u;
+        for (int32_t b = q0; b < q1; b += G) {
+          const int32_t q = b + lane;
+          bool hit = false;
+          if (q < q1) {
+            const float sd32 = dist2_f32(__ldg(a.s32 + q), pi);
+            if (sd32 < lo_thr && sd32 > 0.f) {
+              hit = true;
+            } else if (!(sd32 > hi_thr) && q != k) {
+              ++nexact;
+              const double d0 = __dadd_rn(a.sx[q], -xi);
+              const double d1 = __dadd_rn(a.sy[q], -yi);
+              const double d2 = __dadd_rn(a.sz[q], -zi);
+              const double sd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)),
+                                          __dmul_rn(d2, d2));
+              hit = !(sd > R2);
+            }
+          }
+          const unsigned hb = __ballot_sync(gmask, hit) >> ((threadIdx.x & 31) & ~(G - 1));
+          if (hit) {
+            const int pos = cnt + __popc(hb & below);
+            if (pos < rcap) __stcg(dst + pos, q);
+          }
+          cnt += __popc(hb);
+        }
+      }
+    }
+    if (lane == 0) {
+      a.ncnt[c] = cnt;
+      a.count_prev[a.orig[p]] = cnt;
+      a.h_prev[a.orig[p]] = float(hi_);
+      maxc = max(maxc, cnt);
+      ovf |= cnt > rcap;
+      nfound += unsigned(cnt);
+    }
+  }
+  // block totals (as k_skin_filter)
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ unsigned long long part[4][3];
+  __shared__ int pmax[4], povf[4];
+  const int w = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  __syncwarp();
+  for (int o = 16; o > 0; o >>= 1) {
+    ncand += __shfl_xor_sync(FULL, ncand, o);
+    nfound += __shfl_xor_sync(FULL, nfound, o);
+    nexact += __shfl_xor_sync(FULL, nexact, o);
+  }
+  const int wmax = __reduce_max_sync(FULL, maxc);
+  const bool wovf = __any_sync(FULL, ovf);
+  if (wl == 0) {
+    part[w][0] = ncand; part[w][1] = nfound; part[w][2] = nexact;
+    pmax[w] = wmax;
+    povf[w] = wovf ? 1 : 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t[3] = {0, 0, 0};
+    int mx = 0, ov = 0;
+    for (int j = 0; j < int(blockDim.x >> 5); ++j) {
+      for (int q = 0; q < 3; ++q) t[q] += part[j][q];
+      mx = max(mx, pmax[j]);
+      ov |= povf[j];
+    }
+    if (t[0]) atomicAdd(&a.dcnt[DC_CANDIDATES], t[0]);
+    if (t[1]) atomicAdd(&a.dcnt[DC_NEIB_PAIRS], t[1]);
+    if (t[2]) atomicAdd(&a.dcnt[DC_EXACT_TESTS], t[2]);
+    if (mx) atomicMax(a.maxcnt, mx);
+    if (ov) atomicOr(a.overflow, 1);
   }
 }
 
@@ -875,7 +1459,8 @@ __global__ void k_rowcap(int64_t nc, const int32_t* __restrict__ centre_p,
     g = fminf(fmaxf(g, 0.5f), 4.f);
     est *= dim == 3 ? g * g * g : (dim == 2 ? g * g : g);
   }
-  const int cap = int(fminf(est * slack, 1.0e9f)) + 8;
+  // a multiple of 4, so that every row starts on a 16-byte boundary
+  const int cap = (int(fminf(est * slack, 1.0e9f)) + 8 + 3) & ~3;
   rowcap[c] = cap;
   rowcap64[c] = cap;
 }
@@ -1517,6 +2102,104 @@ void launch_rowcap(int64_t nc, const int32_t* centre_p, const int32_t* orig,
                    cudaStream_t s) {
   k_rowcap<<<nblocks(nc), TPB, 0, s>>>(nc, centre_p, orig, count_prev, h_prev, hcol, dim, slack,
                                        rowcap64, rowcap);
+  note_launch();
+}
+void launch_skin_sig(const double* cols, int64_t nrows, BoxGeom g, int dim, uint8_t* sig,
+                     cudaStream_t s) {
+  if (nrows <= 0) return;
+  k_skin_sig<<<nblocks(nrows), TPB, 0, s>>>(cols, nrows, nrows, g, dim, sig);
+  note_launch();
+}
+void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
+                         const double* cols, const int32_t* gsrc, const int8_t* gcode,
+                         BoxGeom g, int dim, const uint8_t* sig_b, const double* bx,
+                         const double* by, const double* bz, double* sx, double* sy, double* sz,
+                         float4* s32, PackGeom pg, float* dsp, float tau, float eps,
+                         unsigned long long* red, cudaStream_t s) {
+  if (n <= 0) return;
+  k_skin_refresh<<<reduce_blocks(n), TPB, 0, s>>>(sidx, n, nrows, nreal, cols, nrows, gsrc, gcode,
+                                                  g, dim, sig_b, bx, by, bz, sx, sy, sz, s32, pg,
+                                                  dsp, tau, eps, red);
+  note_launch();
+}
+void launch_skin_mark(int64_t n, const float* dsp, float tau, float eps, const double* sx,
+                      const double* sy, const double* sz, const double* bx, const double* by,
+                      const double* bz, Grid g, const int32_t* cstart, double reach_f,
+                      double reach_m, uint8_t* near_f, uint8_t* near_m, cudaStream_t s) {
+  if (n <= 0) return;
+  k_skin_mark<<<nblocks(n), TPB, 0, s>>>(n, dsp, tau, eps, sx, sy, sz, bx, by, bz, g, cstart,
+                                         reach_f, reach_m, near_f, near_m);
+  note_launch();
+}
+void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
+                          const double* hcol, const double* hb, double* hdev, const float* gap,
+                          double krad, double kfac, float tau, float eps, const float* dsp,
+                          const uint8_t* near_f, const uint8_t* near_m, uint8_t* mode,
+                          int32_t* dflag, const int32_t* ncnt, unsigned long long* nkept,
+                          cudaStream_t s) {
+  if (nc <= 0) return;
+  k_skin_classify<<<nblocks(nc), TPB, 0, s>>>(nc, centre_k, centre_p, hcol, hb, hdev, gap, krad,
+                                              kfac, tau, eps, dsp, near_f, near_m, mode, dflag,
+                                              ncnt, nkept);
+  note_launch();
+}
+void launch_dyn_rows(int64_t nd, const int32_t* list, const int32_t* centre_p,
+                     const int32_t* orig, const int32_t* count_prev, const float* h_prev,
+                     const double* hcol, int dim, int64_t* cap, int64_t* off, void* scan_tmp,
+                     size_t scan_bytes, const int64_t* base, int64_t* rowoff, int32_t* rowcap,
+                     cudaStream_t s) {
+  if (nd <= 0) return;
+  k_dyn_caps<<<nblocks(nd + 1), TPB, 0, s>>>(nd, list, centre_p, orig, count_prev, h_prev, hcol,
+                                             dim, 1.2f, cap);
+  exclusive_scan64(scan_tmp, scan_bytes, cap, off, nd + 1, s);
+  k_dyn_assign<<<nblocks(nd), TPB, 0, s>>>(nd, list, off, cap, base, rowoff, rowcap);
+  note_launch(2);
+}
+void launch_table_end(const int64_t* rowoff, const int32_t* rowcap, int64_t n, int64_t* end,
+                      cudaStream_t s) {
+  k_table_end<<<1, 1, 0, s>>>(rowoff, rowcap, n, end);
+  note_launch();
+}
+void launch_overflow_to_search(int64_t nc, const int32_t* ncnt, const int64_t* rowoff,
+                               const int32_t* rowcap, int64_t nl_size, uint8_t* mode,
+                               int32_t* dflag, cudaStream_t s) {
+  if (nc <= 0) return;
+  k_overflow_to_search<<<nblocks(nc), TPB, 0, s>>>(nc, ncnt, rowoff, rowcap, nl_size, mode, dflag);
+  note_launch();
+}
+template <int DIM>
+static void search_few_dim(const FewArgs& a, cudaStream_t s) {
+  constexpr int G = 8;
+  const int64_t need = (a.n * G + 127) / 128;
+  const int grid = int(need < 148 * 8 ? need : 148 * 8);
+  k_search_few<DIM, G><<<grid, 128, 0, s>>>(a);
+}
+void launch_search_few(int dim, const FewArgs& a, cudaStream_t s) {
+  if (a.n <= 0) return;
+  if (dim == 3) search_few_dim<3>(a, s);
+  else if (dim == 2) search_few_dim<2>(a, s);
+  else search_few_dim<1>(a, s);
+  note_launch();
+}
+void launch_skin_compact(int64_t nc, const int32_t* dflag, const int32_t* dpos, int32_t* dlist,
+                         cudaStream_t s) {
+  if (nc <= 0) return;
+  k_skin_compact<<<nblocks(nc), TPB, 0, s>>>(nc, dflag, dpos, dlist);
+  note_launch();
+}
+void launch_gather_h(int64_t nc, const int32_t* centre_p, const double* hcol, double* hb,
+                     unsigned long long* red, int slot, cudaStream_t s) {
+  if (nc <= 0) return;
+  k_gather_h<<<nblocks(nc), TPB, 0, s>>>(nc, centre_p, hcol, hb, red, slot);
+  note_launch();
+}
+void launch_skin_filter(const SkinFilterArgs& a, cudaStream_t s) {
+  constexpr int G = 8;
+  if (a.nc <= 0) return;
+  // 6 blocks of 128 threads fit an SM (76 registers a thread)
+  const int64_t need = (a.nc * G + 127) / 128;
+  const int grid = int(need < 148 * 6 ? need : 148 * 6);
+  k_skin_filter<G><<<grid, 128, 0, s>>>(a);
   note_launch();
 }
 size_t scan64_temp_bytes(int64_t n) {

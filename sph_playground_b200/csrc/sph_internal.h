@@ -64,7 +64,14 @@ __host__ __device__ inline bool grid_dims(const double e[3], int64_t cap, int n3
 enum RedSlot : int {
   RED_LO_X = 0, RED_LO_Y, RED_LO_Z, RED_HI_X, RED_HI_Y, RED_HI_Z, RED_HMIN,
   RED_TS_HMIN, RED_TS_CMAX, RED_TS_DENMIN, RED_TS_CMIN, RED_TS_KAPMAX,
-  RED_TS_BMAX, RED_TS_KAPMIN, RED_TS_LAMMAX, RED_C1_ACTIVE, RED_C1_ACTIVE2, RED_TOTAL
+  RED_TS_BMAX, RED_TS_KAPMIN, RED_TS_LAMMAX, RED_C1_ACTIVE, RED_C1_ACTIVE2,
+  // skin lists: largest displacement and h (dkey max), image signature
+  // changed (0/1), records that moved more than tau and eps (plain counts)
+  RED_SKIN_D, RED_SKIN_HMAX, RED_SKIN_SIG, RED_SKIN_NFAST, RED_SKIN_NMOVE,
+  RED_SKIN_NKEPT,   // rows a skin-list iterate keeps (plain count)
+  RED_SKIN_NKEPT_PAIRS,  // their neighbours (plain count)
+  RED_SKIN_HMAXB,   // largest h of the centres at the skin search (dkey max)
+  RED_TOTAL
 };
 
 // Device counters (unsigned long long, cumulative).
@@ -246,7 +253,133 @@ struct NeibArgs {
   int32_t* maxcnt;
   int32_t* overflow;
   unsigned long long* dcnt;
+  // optional: the centres to search are cmap[0 .. nc-1] (indices into
+  // centre_k / centre_p / rowoff / rowcap / ncnt) instead of 0 .. nc-1
+  const int32_t* cmap;
+  // the predicate's radius is kfac * krad * h (0 or 1: krad * h), and the
+  // cells searched reach `reach` further (records that moved since they
+  // were sorted into their cells)
+  double kfac;
+  double reach;
+  int skin_search;  // a skin search: its pairs are not the neighbour pairs counted
 };
+// ---- skin lists (SPH_P_SKIN; sph_grid.cu) ----
+// per row: the row's image signature (the periodic sides that hold it; its
+// image set is a function of it), 0 for rows that get no images
+void launch_skin_sig(const double* cols, int64_t nrows, BoxGeom g, int dim, uint8_t* sig,
+                     cudaStream_t s);
+// per record (sorted order) from the rows' current positions: sx/sy/sz and
+// the FP32 images, the displacement since the skin search (FP64, rounded
+// up, kept in dsp as the running maximum, FP32 rounded up) and the slots
+// RED_LO_* / RED_HI_* (bounding box), RED_SKIN_D, RED_SKIN_HMAX (real
+// rows), RED_SKIN_SIG (a row whose image signature differs from sig_b),
+// RED_SKIN_NFAST (displacement > tau) and RED_SKIN_NMOVE (> eps)
+void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
+                         const double* cols, const int32_t* gsrc, const int8_t* gcode,
+                         BoxGeom g, int dim, const uint8_t* sig_b, const double* bx,
+                         const double* by, const double* bz, double* sx, double* sy, double* sz,
+                         float4* s32, PackGeom pg, float* dsp, float tau, float eps,
+                         unsigned long long* red, cudaStream_t s);
+// near_f[q] = 1 for the records in the cells within reach_f of a record that
+// moved more than tau; near_m[q] = 1 (near_m may be NULL) for those within
+// reach_m of the position at the skin search of one that moved more than eps
+void launch_skin_mark(int64_t n, const float* dsp, float tau, float eps, const double* sx,
+                      const double* sy, const double* sz, const double* bx, const double* by,
+                      const double* bz, Grid g, const int32_t* cstart, double reach_f,
+                      double reach_m, uint8_t* near_f, uint8_t* near_m, cudaStream_t s);
+// mode[c] = 0 (filter the skin list), 1 (search afresh; dflag[c] = 1) or 2
+// (keep the row) for every centre (see sph_grid.cu); hdev[c] = running
+// maximum of |h - hb[c]|
+void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
+                          const double* hcol, const double* hb, double* hdev, const float* gap,
+                          double krad, double kfac, float tau, float eps, const float* dsp,
+                          const uint8_t* near_f, const uint8_t* near_m, uint8_t* mode,
+                          int32_t* dflag, const int32_t* ncnt, unsigned long long* nkept,
+                          cudaStream_t s);
+// rows of the centres list[0 .. nd-1] laid out after *base: capacities
+// from their last counts (as k_rowcap), their scan, rowoff / rowcap
+void launch_dyn_rows(int64_t nd, const int32_t* list, const int32_t* centre_p,
+                     const int32_t* orig, const int32_t* count_prev, const float* h_prev,
+                     const double* hcol, int dim, int64_t* cap, int64_t* off, void* scan_tmp,
+                     size_t scan_bytes, const int64_t* base, int64_t* rowoff, int32_t* rowcap,
+                     cudaStream_t s);
+// end[0] = rowoff[n - 1] + rowcap[n - 1]
+void launch_table_end(const int64_t* rowoff, const int32_t* rowcap, int64_t n, int64_t* end,
+                      cudaStream_t s);
+// filter rows (mode 0) whose count exceeds their row become mode 1; dflag[c]
+// = 1 for every centre of mode 1
+void launch_overflow_to_search(int64_t nc, const int32_t* ncnt, const int64_t* rowoff,
+                               const int32_t* rowcap, int64_t nl_size, uint8_t* mode,
+                               int32_t* dflag, cudaStream_t s);
+// search of the centres list[0 .. n-1], G lanes each (see sph_grid.cu)
+struct FewArgs {
+  int64_t n;
+  const int32_t* list;
+  const int32_t* centre_k;
+  const int32_t* centre_p;
+  const double* sx;
+  const double* sy;
+  const double* sz;
+  const float4* s32;
+  double shift;
+  const double* hcol;
+  double krad;
+  Grid g;
+  const int32_t* cstart;
+  double reach;
+  const int64_t* rowoff;
+  const int32_t* rowcap;
+  int64_t nl_size;
+  int32_t* nl;
+  int32_t* ncnt;
+  const int32_t* orig;
+  int32_t* count_prev;
+  float* h_prev;
+  int32_t* maxcnt;
+  int32_t* overflow;
+  unsigned long long* dcnt;
+};
+void launch_search_few(int dim, const FewArgs& a, cudaStream_t s);
+// dlist[dpos[c]] = c for every c with dflag[c] != 0
+void launch_skin_compact(int64_t nc, const int32_t* dflag, const int32_t* dpos, int32_t* dlist,
+                         cudaStream_t s);
+// hb[c] = hcol[centre_p[c]], and their maximum into red[slot] (dkey max)
+void launch_gather_h(int64_t nc, const int32_t* centre_p, const double* hcol, double* hb,
+                     unsigned long long* red, int slot, cudaStream_t s);
+struct SkinFilterArgs {
+  int64_t nc;
+  const uint8_t* mode;  // 0: filter; 1: left to the search; 2: kept when keep != 0
+  int keep;
+  float* gap;           // optional: per centre, the smallest |r - krad h| of its list
+  float eimg;           // error bound of a distance between two FP32 images
+  const int32_t* centre_k;
+  const int32_t* centre_p;
+  const int64_t* skin_off;
+  const int32_t* skin_cnt;
+  const int32_t* skin_nl;
+  const double* sx;
+  const double* sy;
+  const double* sz;
+  const float4* s32;
+  double shift;
+  const double* hcol;
+  double krad;
+  const int64_t* rowoff;
+  const int32_t* rowcap;
+  int64_t nl_size;
+  int32_t* nl;
+  int32_t* ncnt;
+  const int32_t* orig;
+  int32_t* count_prev;
+  float* h_prev;
+  int32_t* maxcnt;
+  int32_t* overflow;
+  unsigned long long* dcnt;
+};
+// each centre's neighbour row = its skin list's records that pass the FP64
+// predicate ((dx*dx + dy*dy) + dz*dz) <= (krad*h)^2, in skin-list order
+void launch_skin_filter(const SkinFilterArgs& a, cudaStream_t s);
+
 // staged: the candidate runs of a chunk copied into shared memory by bulk
 // copies (SPH_P_SEARCH_STAGED); overflow |= 2 if a copy's wait timed out
 void launch_neighbours(int dim, int G, bool staged, const NeibArgs& a, cudaStream_t s);

@@ -42,9 +42,12 @@ def apply(engine, params):
 
 
 def time_steps(state, store, kernel, precision, params, steps=3, warmup=2, lib=None):
-    """Device ms per step of `steps` leapfrog steps after `warmup` ones."""
+    """Device ms per step of `steps` leapfrog steps after `warmup` ones, each
+    with a fresh neighbour search (no skin lists: the search's shapes are
+    what is tuned, and skin-list iterates rarely search)."""
     e = abi.Engine(state, store, kernel, precision=precision, lib=lib)
     try:
+        e.set_param(abi.P_SKIN, 0.0)
         apply(e, params)
         e.set_param("tfinish", 1e30)
         e.step(warmup)

@@ -19,9 +19,12 @@ def _instances():
 
 
 def _alone(lib, prec=abi.PREC_FP64):
+    # a fresh search every iterate, as the batch's device loop takes (skin
+    # lists give the same sets in another order, so not the same bits)
     out = []
     for st, store in _instances():
         with abi.Engine(st, store, "m6", precision=prec, lib=lib) as e:
+            e.set_param(abi.P_SKIN, 0.0)
             e.run_to(T_END)
             out.append((e.get_store(), e.get_state()))
     return out
@@ -29,6 +32,8 @@ def _alone(lib, prec=abi.PREC_FP64):
 
 def _batched(lib, prec=abi.PREC_FP64, steps=None):
     engines = [abi.Engine(st, store, "m6", precision=prec, lib=lib) for st, store in _instances()]
+    for e in engines:
+        e.set_param(abi.P_SKIN, 0.0)
     try:
         with abi.Batch(engines) as b:
             if steps is None:
@@ -107,9 +112,12 @@ SWEEP_FULL = [(n, ddw) for ddw in ("fab", "n2w", "2nw_ds")
 
 
 def _engines(lib, sets, prec, params=None):
+    # a fresh search every iterate, as the device loop's steps take (skin
+    # lists give the same sets in another order, so not the same bits)
     out = []
     for st, store in sets:
         e = abi.Engine(st, store, "m6", precision=prec, lib=lib)
+        e.set_param(abi.P_SKIN, 0.0)
         for k, v in (params or {}).items():
             e.set_param(k, v)
         out.append(e)

@@ -1,8 +1,10 @@
 """Device-resident steps replayed as CUDA graphs (SPH_P_GRAPH): the same
 kernels as the host-driven step with every size and decision taken on the
-device, so the results must equal the host-driven step's bit for bit; a step
-that cannot be planned on the device (here: Newton sweeps beyond the
-device-resident limit) is redone on the host path, with the same result."""
+device, so the results must equal the host-driven step's bit for bit (the
+host step with a fresh search every iterate, SPH_P_SKIN = 0, as the graph
+takes: skin lists give the same sets in another order); a step that cannot
+be planned on the device (here: Newton sweeps beyond the device-resident
+limit) is redone on the host path, with the same result."""
 import numpy as np
 import pytest
 
@@ -15,6 +17,7 @@ FP64, FP32 = abi.PREC_FP64, abi.PREC_FP32_COMP
 
 def _run(lib, st, store, prec, steps, graph, kernel="m6", params=None):
     with abi.Engine(st, store, kernel, precision=prec, lib=lib) as e:
+        e.set_param(abi.P_SKIN, 0.0)
         for k, v in (params or {}).items():
             e.set_param(k, v)
         e.set_param(abi.P_GRAPH, 1.0 if graph else 0.0)
@@ -84,6 +87,7 @@ def test_graph_parameter_change_mid_run(engine_lib, cuda_ok):
     out = []
     for graph in (False, True):
         with abi.Engine(st, store, "m6", precision=FP64, lib=engine_lib) as e:
+            e.set_param(abi.P_SKIN, 0.0)  # (as the graph's steps: a fresh search)
             e.set_param(abi.P_GRAPH, 1.0 if graph else 0.0)
             e.step(4)
             e.set_param(abi.P_NEWTON_TOL, 1e-6)

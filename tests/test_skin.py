@@ -1,0 +1,171 @@
+"""Skin lists (SPH_P_SKIN): neighbour lists kept between iterates with a
+radius of (1 + s) krad h; every iterate each centre keeps its row (nothing
+near it moved), refilters its skin list with the FP64 predicate, or (near
+a fast particle) is searched afresh.  The sets must be those of a fresh
+search on the same state, step after step, through iterates served from
+the lists and through rebuilds.
+
+The check runs each step in parts (timestep, predict, density, forces,
+correct): after the predictor the table goes to a fresh oracle handle,
+whose density pass searches the same positions and h; its neighbour-set
+digests must equal the engine's.  The fields of whole runs must match the
+runs without skin lists to the summation-order level (FP64) or within the
+FP32 path's tolerances of the FP64 oracle."""
+import numpy as np
+import pytest
+
+from sph_playground_b200 import abi, consts, ic
+from parity import COL, rel_field, rel_particle
+
+FP64, FP32 = abi.PREC_FP64, abi.PREC_FP32_COMP
+
+
+def _split_run(engine_lib, oracle_lib, st, store, prec, nsteps, skin=0.1, kernel="m6",
+               params=None, between=None):
+    """nsteps leapfrog steps in parts; after every predictor the engine's
+    neighbour sets are compared with a fresh oracle search on the same
+    table.  Returns the engine's counters and final store."""
+    e = abi.Engine(st, store, kernel, precision=prec, lib=engine_lib)
+    try:
+        e.set_param(abi.P_SKIN, skin)
+        for k, v in (params or {}).items():
+            e.set_param(k, v)
+        e.density()
+        e.forces()
+        for step in range(nsteps):
+            if between is not None:
+                between(e, step)
+            dt = e.timestep()
+            e.predict(dt)
+            mid, mst = e.get_store(), e.get_state()
+            e.density()
+            got = e.get_neighbour_digest()
+            with abi.Engine(mst, mid, kernel, precision=FP64, lib=oracle_lib) as o:
+                o.density()
+                ref = o.get_neighbour_digest()
+            assert np.array_equal(got[0], ref[0]), f"step {step}: neighbour counts differ"
+            assert np.array_equal(got[1], ref[1]), f"step {step}: neighbour sets differ"
+            e.forces()
+            e.correct(dt)
+        return e.counters(), e.get_store()
+    finally:
+        e.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_skin_sedov_sets_match_oracle(engine_lib, oracle_lib, cuda_ok, prec):
+    """Sedov blast: the blast particles move (fast records, dirty centres
+    searched afresh with a widened cell range), the rest are at rest (at
+    48^3 the blast is a small part of the box, as in the 128^3 workload)."""
+    st, store = ic.sedov3d(n=48)
+    cnt, _ = _split_run(engine_lib, oracle_lib, st, store, prec, nsteps=24)
+    info = {k: cnt[k] for k in ("skin_builds", "skin_reuses", "skin_dirty", "skin_kept",
+                                "searches")}
+    assert cnt["skin_builds"] >= 1, info
+    assert cnt["skin_reuses"] >= 12, info
+    assert cnt["skin_dirty"] > 0, info  # some centres were searched afresh,
+    assert cnt["skin_kept"] > 0, info  # some rows kept,
+    n = st[abi.consts.ec["realpn"] - 1]  # and some filtered
+    assert cnt["skin_kept"] + cnt["skin_dirty"] < cnt["skin_reuses"] * n, info
+
+
+@pytest.mark.gpu
+def test_skin_sedov_rebuilds(engine_lib, oracle_lib, cuda_ok):
+    """A thin skin (s = 0.02) runs out within a few steps: lists rebuilt
+    mid-run, sets still the fresh search's."""
+    st, store = ic.sedov3d(n=16)
+    cnt, _ = _split_run(engine_lib, oracle_lib, st, store, FP64, nsteps=16, skin=0.02)
+    info = {k: cnt[k] for k in ("skin_builds", "skin_reuses", "skin_dirty")}
+    assert cnt["skin_builds"] >= 2, info
+    assert cnt["skin_reuses"] >= 1, info
+
+
+@pytest.mark.gpu
+def test_skin_shear_flow_across_boundaries(engine_lib, oracle_lib, cuda_ok):
+    """2D shear flow in a periodic box: particles cross the image strips and
+    the box faces (image sets change, rows wrap)."""
+    st, store = ic.shear2d(n=24, amp=0.3)
+    cnt, _ = _split_run(engine_lib, oracle_lib, st, store, FP64, nsteps=12)
+    assert cnt["skin_builds"] >= 1
+
+
+@pytest.mark.gpu
+def test_skin_sod_tube(engine_lib, oracle_lib, cuda_ok):
+    """Sod tube (y periodic, hfac 1: lattice pairs at exactly the radius)."""
+    st, store = ic.sod2d()
+    cnt, _ = _split_run(engine_lib, oracle_lib, st, store, FP64, nsteps=8)
+    assert cnt["skin_reuses"] + cnt["skin_builds"] >= 8
+
+
+@pytest.mark.gpu
+def test_skin_moved_by_the_caller(engine_lib, oracle_lib, cuda_ok):
+    """Positions and h written by the caller between steps (sph_set_columns)
+    are measured like the integrator's moves."""
+    st, store = ic.sedov3d(n=12)
+    dx = 1.0 / 12
+    rng = np.random.default_rng(3)
+
+    def nudge(e, step):
+        if step % 3 == 1:
+            x = e.get_columns(["rx", "ry", "rz", "h"])
+            x[:3] += rng.uniform(-0.05 * dx, 0.05 * dx, size=x[:3].shape)
+            x[3] *= 1.0 + rng.uniform(0.0, 0.02, size=x[3].shape)
+            e.set_columns(["rx", "ry", "rz", "h"], x)
+
+    cnt, _ = _split_run(engine_lib, oracle_lib, st, store, FP64, nsteps=9, between=nudge)
+    assert cnt["skin_reuses"] >= 1, {k: cnt[k] for k in ("skin_builds", "skin_reuses")}
+
+
+@pytest.mark.gpu
+def test_skin_fields_match_fresh_search(engine_lib, oracle_lib, cuda_ok):
+    """Whole runs through sph_step: FP64 with skin lists equals FP64 without
+    them up to summation order; FP32-comp with skin lists stays within the
+    FP32 tolerances of the FP64 oracle."""
+    st, store = ic.sedov3d(n=48, npics=1)  # (no output-time clipping: see test_domain)
+    out = {}
+    for name, lib, prec, skin in (("ref", oracle_lib, FP64, 0.0), ("fresh", engine_lib, FP64, 0.0),
+                                  ("skin64", engine_lib, FP64, 0.1),
+                                  ("skin32", engine_lib, FP32, 0.1)):
+        with abi.Engine(st, store, "m6", precision=prec, lib=lib) as e:
+            e.set_param(abi.P_SKIN, skin)
+            e.step(15)
+            out[name] = (e.get_store(), e.get_state(), e.counters())
+    assert out["skin64"][2]["skin_reuses"] >= 8, out["skin64"][2]
+    s_f, s_s = out["fresh"][0], out["skin64"][0]
+    t_f, t_s = (out[k][1][consts.ec["time"] - 1] for k in ("fresh", "skin64"))
+    assert abs(t_s - t_f) <= 1e-12 * t_f  # (dt from fields summed in another order)
+    for f in ("den", "h", "om"):
+        assert rel_particle(s_s[:, COL[f]], s_f[:, COL[f]]) < 1e-12, f
+    for f in ("rx", "ry", "rz", "vx", "vy", "vz", "u"):
+        assert rel_field(s_s[:, COL[f]], s_f[:, COL[f]]) < 1e-12, f
+    ref, s32 = out["ref"][0], out["skin32"][0]
+    assert rel_particle(s32[:, COL["den"]], ref[:, COL["den"]]) < 1e-6
+    for f in ("vx", "vy", "vz", "u"):
+        assert rel_field(s32[:, COL[f]], ref[:, COL[f]]) < 1e-5, f
+
+
+@pytest.mark.gpu
+def test_skin_parameter_change_rebuilds(engine_lib, oracle_lib, cuda_ok):
+    """Density passes over a table that does not move are served from the
+    lists; a parameter that can change the sets (the cell factor) ends them,
+    one that cannot (the timing switch) keeps them."""
+    st, store = ic.density3d(n=16, seed=2)
+    with abi.Engine(st, store, "m6", precision=FP64, lib=engine_lib) as e:
+        e.set_param(abi.P_SKIN, 0.1)
+        for _ in range(3):
+            e.density()
+        c = e.counters()
+        assert (c["skin_builds"], c["skin_reuses"]) == (1, 2)
+        e.set_param(abi.P_TIMING, 1)
+        e.density()
+        assert e.counters()["skin_builds"] == 1
+        e.set_param(abi.P_CELL_FACTOR, 0.45)
+        mid, mst = e.get_store(), e.get_state()  # (each pass moves h)
+        e.density()
+        assert e.counters()["skin_builds"] == 2
+        got = e.get_neighbour_digest()
+    with abi.Engine(mst, mid, "m6", precision=FP64, lib=oracle_lib) as o:
+        o.density()
+        ref = o.get_neighbour_digest()
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
