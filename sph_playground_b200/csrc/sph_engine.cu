@@ -140,9 +140,12 @@ long long launches_so_far() { return g_launches; }
 // Jacobi sweeps of circuit1 that a device-resident step runs before it asks
 // the host (a step whose particles need more is redone on the host path)
 constexpr int kDrsSweeps = 6;
-// iterates skin lists serve at most before the rows are re-sorted and the
-// lists rebuilt with them
-constexpr int kSkinMaxAge = 64;
+constexpr int kSkinShort = 4, kSkinPause0 = 8, kSkinPauseMax = 128;
+// centres searched afresh above which the search's own kernel takes them
+constexpr int64_t kFewCentres = 65536;
+// fresh searches of a served iterate (centres x widening) as a share of all
+// centres, above which the iterate searches plainly instead
+constexpr double kSkinDirtyShare = 0.15;
 
 struct sph_handle {
   int dev = 0;  // the device current at sph_create
@@ -189,26 +192,32 @@ struct sph_handle {
   DevBuf colbuf;  // staging of sph_get_columns / sph_set_columns
   // skin lists (SPH_P_SKIN): the lists of the last skin search (CSR like nl),
   // the records' positions and the centres' h at that search, the rows'
-  // image signatures then; per record the largest displacement since and
-  // the marks of fast / moving records nearby; per centre the gap of its
+  // image signatures then; per record the largest displacement since; per
+  // cell the dilated marks of fast / moving records; per centre the gap of its
   // list at the search, the largest change of h since, its way (filter,
   // search afresh, keep), the fresh-search flag, its scan and those centres
   DevBuf skin_nl, skin_rowoff, skin_rowcap, skin_rowcap64, skin_cnt, skin_count_prev,
-      skin_h_prev, skin_bx, skin_by, skin_bz, skin_hb, skin_sig, skin_dsp, skin_near_f,
-      skin_near_m, skin_gap, skin_hdev, skin_mode, skin_dflag, skin_dpos, skin_dlist;
+      skin_h_prev, skin_bx, skin_by, skin_bz, skin_hb, skin_sig, skin_dsp, skin_fcell,
+      skin_mcell, skin_ctmp, skin_gap, skin_hdev, skin_mode, skin_dflag, skin_dpos, skin_dlist;
   // the rows of the centres searched afresh, laid out anew every skin-list
   // iterate after the end of the table's fixed part (skin_end[0]): their
   // capacities and the scan of those
   DevBuf skin_end, skin_dcap, skin_doff;
+  DevBuf skin_sig_alt, skin_inv;  // a row re-sort's spare signatures, inverse permutation
   int64_t skin_nl_size = 0;
   int skin_est = 0;
   bool skin_valid = false;  // the skin lists describe the records of the current sort
-  bool skin_ending = false;  // the last reuse saw the lists near their end
   double skin_s = 0.;        // their fraction s (radius (1 + s) krad h)
   double skin_tau = 0.;      // displacement up to which a record is slow
   double skin_eps = 0.;      // displacement up to which a record is still
   double skin_hmin = 0.;     // h_min at their search
   int skin_age = 0;          // iterates served since their search
+  // lists that serve fewer than kSkinShort iterates cost more than they save
+  // (their search is dearer than a plain one): after such lists the next
+  // skin_pause iterates search plainly, a pause that doubles while lists
+  // keep ending early (up to kSkinPauseMax) and resets when they last
+  int skin_pause = 0, skin_pause_len = 0;
+  bool skin_trace = std::getenv("SPH_SKIN_TRACE") != nullptr;
   int64_t kept_pairs = 0;    // neighbour pairs of the rows kept (counted as found)
   const DevPlan* dplan = nullptr;  // set while a device-resident step is built
   int64_t nghost_cap = 0, nall_cap = 0;
@@ -241,6 +250,7 @@ struct sph_handle {
   PackGeom pgeom{};
   double mref = 1.0;
   bool have_order = false;
+  bool rows_in_order = false;  // the rows are in the order of the current sort
   int steps_since_reorder = 0;
 
   // time loop state (main.f90)
@@ -515,7 +525,7 @@ struct sph_handle {
 
   // ---- physical re-ordering of the rows (locality of the pair loops) ---------------------
   int reorder_rows() {
-    if (!have_order || in_split_step) return SPH_OK;
+    if (!have_order || in_split_step || rows_in_order) return SPH_OK;
     // perm = real rows in cell order, then the fixed rows as they are
     int32_t* perm = cpos.as<int32_t>();
     CK(cudaMemcpyAsync(perm, centre_p.p, sizeof(int32_t) * nreal, cudaMemcpyDeviceToDevice, s));
@@ -532,8 +542,20 @@ struct sph_handle {
     std::swap(cols.bytes, cols_alt.bytes);
     std::swap(orig.p, orig_alt.p);
     std::swap(orig.bytes, orig_alt.bytes);
-    have_order = false;
-    skin_valid = false;
+    if (skin_valid) {
+      // the skin lists name records, which stay; what names rows follows
+      RC(skin_sig_alt.ensure(sizeof(uint8_t) * nrows));
+      RC(skin_inv.ensure(sizeof(int32_t) * nrows));
+      launch_rows_renamed(perm, skin_inv.as<int32_t>(), nrows + nghost, nrows, nghost, nreal,
+                          vals_alt.as<int32_t>(), ssrc.as<int32_t>(), gsrc.as<int32_t>(),
+                          centre_p.as<int32_t>(), skin_sig.as<uint8_t>(),
+                          skin_sig_alt.as<uint8_t>(), s);
+      std::swap(skin_sig.p, skin_sig_alt.p);
+      std::swap(skin_sig.bytes, skin_sig_alt.bytes);
+      rows_in_order = true;  // (until a sort puts them in another order)
+    } else {
+      have_order = false;
+    }
     steps_since_reorder = 0;
     CK(cudaGetLastError());
     return SPH_OK;
@@ -644,11 +666,6 @@ struct sph_handle {
   // sph_grid.cu: filter with the FP64 predicate, fresh search of the
   // centres the filter cannot vouch for) until the records have moved too
   // far, an image set changes or too many centres need the fresh search.
-  // rows may be re-sorted: no skin lists serve, or the ones that do are near
-  // their end (the re-sort ends them)
-  bool skin_lets_reorder() const {
-    return !skin_valid || skin_ending || skin_age >= kSkinMaxAge;
-  }
   double skin_fraction() const {
     const double v = st[SPH_P_SKIN];
     return v > 0 ? std::min(v, 1.0) : 0.0;
@@ -669,8 +686,6 @@ struct sph_handle {
     RC(skin_by.ensure(sizeof(double) * nall));
     RC(skin_bz.ensure(sizeof(double) * nall));
     RC(skin_dsp.ensure(sizeof(float) * nall));
-    RC(skin_near_f.ensure(sizeof(uint8_t) * nall));
-    RC(skin_near_m.ensure(sizeof(uint8_t) * nall));
     RC(skin_gap.ensure(sizeof(float) * nreal));
     RC(skin_hdev.ensure(sizeof(double) * nreal));
     RC(skin_mode.ensure(sizeof(uint8_t) * nreal));
@@ -757,7 +772,6 @@ struct sph_handle {
     }));
     launch_table_end(rowoff.as<int64_t>(), rowcap.as<int32_t>(), nreal, skin_end.as<int64_t>(), s);
     skin_valid = true;
-    skin_ending = false;
     skin_s = skin;
     skin_age = 0;
     cnt_host[SPH_CNT_SKIN_BUILDS]++;
@@ -799,6 +813,22 @@ struct sph_handle {
   int skin_fill(const Params& P, int64_t ndirty, double reach) {
     const int d = P.dim;
     Table T = exact_table();
+    // the centres searched afresh (skin_dlist): a lane group each when they
+    // are few (the search's shared streams would leave most SMs idle), the
+    // search's own groups of consecutive centres when they are many
+    auto search_dirty = [&](const NeibArgs& na, int64_t nd, double rch) {
+      if (nd <= 0) return;
+      if (nd < kFewCentres) {
+        launch_search_few(d, few_args(na, skin_dlist.as<int32_t>(), nd, rch), s);
+      } else {
+        NeibArgs nb = na;
+        nb.cmap = skin_dlist.as<int32_t>();
+        nb.nc = nd;
+        nb.reach = rch;
+        launch_neighbours(d, lanes_search(), st[SPH_P_SEARCH_STAGED] != 0, nb, s);
+        cnt_host[SPH_CNT_SEARCHES]++;
+      }
+    };
     auto dyn = [&](int64_t nd) {
       launch_dyn_rows(nd, skin_dlist.as<int32_t>(), centre_p.as<int32_t>(), orig.as<int32_t>(),
                       count_prev.as<int32_t>(), h_prev.as<float>(), col(es_h), d,
@@ -826,7 +856,7 @@ struct sph_handle {
       dyn(ndirty);
       NeibArgs na = neib_args(T, P);
       launch_skin_filter(filter_args(na, true, false), s);
-      launch_search_few(d, few_args(na, skin_dlist.as<int32_t>(), ndirty, reach), s);
+      search_dirty(na, ndirty, reach);
       RC(read_flags(mc, ov));
     }
     int mc_all = mc;
@@ -847,7 +877,7 @@ struct sph_handle {
       CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
       dyn(ndirty);
       NeibArgs na = neib_args(T, P);
-      launch_search_few(d, few_args(na, skin_dlist.as<int32_t>(), ndirty, reach), s);
+      search_dirty(na, ndirty, reach);
       RC(read_flags(mc, ov));
       mc_all = std::max(mc_all, mc);
     }
@@ -855,7 +885,7 @@ struct sph_handle {
       // no room after the fixed part: lay the whole table out anew
       RC(fill_table(T, P, true, [&](NeibArgs& na, int) {
         launch_skin_filter(filter_args(na, false, false), s);
-        launch_search_few(d, few_args(na, skin_dlist.as<int32_t>(), ndirty, reach), s);
+        search_dirty(na, ndirty, reach);
       }));
       launch_table_end(rowoff.as<int64_t>(), rowcap.as<int32_t>(), nreal,
                        skin_end.as<int64_t>(), s);
@@ -910,46 +940,54 @@ struct sph_handle {
     const double hmax = dkey_inv(h_red[RED_SKIN_HMAX]);
     const double hmaxb = dkey_inv(h_red[RED_SKIN_HMAXB]);
     const unsigned long long nfast = h_red[RED_SKIN_NFAST], nmove = h_red[RED_SKIN_NMOVE];
-    if (h_red[RED_SKIN_SIG]) return SPH_OK;  // some row's image set changed
+    // (SPH_SKIN_TRACE in the environment: why lists end, on stderr)
+    auto end_lists = [&](const char* why) {
+      if (skin_trace)
+        std::fprintf(stderr, "skin lists end after %d iterates: %s (D %.3g, fast %llu, moving %llu)\n",
+                     skin_age, why, D, nfast, nmove);
+      if (skin_age < kSkinShort) {
+        skin_pause_len = skin_pause_len ? std::min(2 * skin_pause_len, kSkinPauseMax) : kSkinPause0;
+        skin_pause = skin_pause_len;
+      } else {
+        skin_pause_len = 0;
+      }
+      return SPH_OK;
+    };
+    if (h_red[RED_SKIN_SIG]) return end_lists("an image set changed");
     const double dcap = P.krad * skin_hmin;
-    if (!(D <= dcap) || !(hmax > 0) || !std::isfinite(hmax) || !(hmaxb > 0)) return SPH_OK;
+    if (!(D <= dcap)) return end_lists("records moved a search radius");
+    if (!(hmax > 0) || !std::isfinite(hmax) || !(hmaxb > 0)) return end_lists("h");
     // every record inside the FP32 packing's binade: 0 <= x - origin < shift
     const double o[3] = {pgeom.ox, pgeom.oy, pgeom.oz};
     for (int k = 0; k < 3; ++k) {
       const double lo = dkey_inv(h_red[RED_LO_X + k]), hi = dkey_inv(h_red[RED_HI_X + k]);
-      if (!(lo >= o[k]) || !(hi - o[k] < pgeom.shift * (1.0 - 1e-9))) return SPH_OK;
+      if (!(lo >= o[k]) || !(hi - o[k] < pgeom.shift * (1.0 - 1e-9)))
+        return end_lists("a record left the FP32 binade");
     }
-    // the marking boxes, in cells: around fast records, every centre that
-    // may see them now; around moving ones, every skin list holding them
+    // the marks, in cells: around fast records every centre that may see
+    // them now (reach_f), around moving ones every skin list holding them
+    // (reach_m)
     const double reach_f = (P.krad * hmax + skin_tau) * (1.0 + 1e-9);
     const double reach_m = (1.0 + skin_s) * P.krad * hmaxb * (1.0 + 1e-9);
-    auto cells = [&](double reach) {
-      double c = 1.0;
-      for (int k = 0; k < d; ++k) c *= 2.0 * reach * grid.invL + 3.0;
-      return c;
-    };
-    const double budget = double(1 << 28);
-    if (double(nfast) > double(nall) / 8 || double(nfast) * cells(reach_f) > budget)
-      return SPH_OK;
-    // too many moving records to mark: no row is kept this time
-    const bool mark_m = double(nmove) * cells(reach_m) <= budget;
+    const int wf = int(std::ceil(reach_f * grid.invL)) + 1;
+    const int wm = int(std::ceil(reach_m * grid.invL)) + 1;
+    if (wf > 256 || wm > 256) return end_lists("a search radius spans too many cells");
+    const int64_t ncell = int64_t(grid.nx) * grid.ny * grid.nz;
+    RC(skin_fcell.ensure(size_t(ncell)));
+    RC(skin_mcell.ensure(size_t(ncell)));
+    RC(skin_ctmp.ensure(size_t(ncell)));
     {
       Phase ph(this, SPH_T_NEIGHBOURS);
-      CK(cudaMemsetAsync(skin_near_f.p, 0, sizeof(uint8_t) * nall, s));
-      if (mark_m) CK(cudaMemsetAsync(skin_near_m.p, 0, sizeof(uint8_t) * nall, s));
-      if (nfast || (mark_m && nmove))
-        launch_skin_mark(nall, skin_dsp.as<float>(), tau, eps, sx.as<double>(), sy.as<double>(),
-                         sz.as<double>(), skin_bx.as<double>(), skin_by.as<double>(),
-                         skin_bz.as<double>(), grid, cstart.as<int32_t>(), reach_f, reach_m,
-                         skin_near_f.as<uint8_t>(), mark_m ? skin_near_m.as<uint8_t>() : nullptr,
-                         s);
+      launch_skin_marks(nall, skin_dsp.as<float>(), tau, eps, keys_alt.as<uint32_t>(),
+                        sx.as<double>(), sy.as<double>(), sz.as<double>(), grid, d, wf, wm,
+                        skin_fcell.as<uint8_t>(), skin_mcell.as<uint8_t>(),
+                        skin_ctmp.as<uint8_t>(), s);
       launch_skin_classify(nreal, centre_k.as<int32_t>(), centre_p.as<int32_t>(), col(es_h),
                            skin_hb.as<double>(), skin_hdev.as<double>(), skin_gap.as<float>(),
                            P.krad, 1.0 + skin_s, tau, eps, skin_dsp.as<float>(),
-                           skin_near_f.as<uint8_t>(),
-                           mark_m ? skin_near_m.as<uint8_t>() : nullptr,
-                           skin_mode.as<uint8_t>(), skin_dflag.as<int32_t>(),
-                           ncnt.as<int32_t>(), rb + RED_SKIN_NKEPT, s);
+                           keys_alt.as<uint32_t>(), skin_fcell.as<uint8_t>(),
+                           skin_mcell.as<uint8_t>(), skin_mode.as<uint8_t>(),
+                           skin_dflag.as<int32_t>(), ncnt.as<int32_t>(), rb + RED_SKIN_NKEPT, s);
       // (skin_dflag[nreal] stays 0: the scan's last entry is the count)
       exclusive_scan(scan_tmp.p, scan_tmp.bytes, skin_dflag.as<int32_t>(),
                      skin_dpos.as<int32_t>(), nreal + 1, s);
@@ -963,11 +1001,18 @@ struct sph_handle {
     }
     const int64_t ndirty = h_i32[0];
     const int64_t nkept = int64_t(h_red[RED_SKIN_NKEPT]);
-    if (ndirty > nreal / 4) return SPH_OK;
+    // Their search over cells of step b, its range widened by D, costs
+    // several times a search's share per centre (measured on the 128^3
+    // Sedov blast: about 20 ns a centre against 1 ns); the iterate is
+    // served only while that stays well below a plain search (images, sort
+    // and search) with the widening of the smallest radius
+    const double rmin = P.krad * skin_hmin;
+    const double widen = std::pow((rmin + D) / rmin, double(d));
+    if (double(ndirty) * widen > kSkinDirtyShare * double(nreal))
+      return end_lists("too many centres to search afresh");
     const double reach_d = D * (1.0 + 1e-9);
     RC(skin_fill(P, ndirty, reach_d));
     ++skin_age;
-    skin_ending = D > 0.5 * dcap || ndirty > nreal / 8;
     cnt_host[SPH_CNT_SKIN_REUSES]++;
     cnt_host[SPH_CNT_SKIN_KEPT] += nkept;
     kept_pairs += int64_t(h_red[RED_SKIN_NKEPT_PAIRS]);
@@ -977,13 +1022,17 @@ struct sph_handle {
 
   // ---- neighbour phase: images, grid, sort, lists --------------------------------------------
   int neighbour_phase(const Mode& m, const Params& P) {
-    const double skin = skin_fraction();
+    double skin = skin_fraction();
     if (skin > 0 && skin_valid && skin == skin_s) {
       bool served = false;
       RC(skin_reuse(m, P, served));
       if (served) return SPH_OK;
     }
     skin_valid = false;
+    if (skin > 0 && skin_pause > 0) {  // lists ended early: plain searches for now
+      --skin_pause;
+      skin = 0.0;
+    }
     const int d = P.dim;
     BoxGeom g = box(m);
     {
@@ -1107,6 +1156,7 @@ struct sph_handle {
       }));
     }
     have_order = true;
+    rows_in_order = false;
     cnt_host[SPH_CNT_GHOSTS] = nghost;
     return SPH_OK;
   }
@@ -1553,6 +1603,7 @@ struct sph_handle {
     ltout = clk.ltout;
     stopped = clk.stopped != 0;
     have_order = true;
+    rows_in_order = false;
     nghost = h_plan->nghost;  // the host view of the last search, as after a host step
     grid = h_plan->grid;
     pgeom = h_plan->pg;
@@ -1597,6 +1648,7 @@ struct sph_handle {
     ltout = clk.ltout;
     stopped = clk.stopped != 0;
     have_order = true;
+    rows_in_order = false;
     nghost = plan.nghost;
     grid = plan.grid;
     pgeom = plan.pg;
@@ -2020,8 +2072,7 @@ struct sph_handle {
     int reorder_every = int(st[SPH_P_REORDER_EVERY]);
     // with skin lists the rows keep their order while the lists serve, and
     // are re-sorted before the search that replaces lists near their end
-    if (reorder_every > 0 && steps_since_reorder >= reorder_every && skin_lets_reorder())
-      RC(reorder_rows());
+    if (reorder_every > 0 && steps_since_reorder >= reorder_every) RC(reorder_rows());
     double dthydro, dtdiff, dtfld, dt;
     RC(timestep(dthydro, dtdiff, dtfld, dt));
     bool do_sts = false;
@@ -2504,7 +2555,7 @@ int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
 int sph_iterate(sph_handle* h) {
   AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
-  if (h->skin_lets_reorder()) RC(h->reorder_rows());
+  RC(h->reorder_rows());
   int rc = h->iterate(true);
   h->collect_timers();
   return rc;
@@ -2513,7 +2564,7 @@ int sph_iterate(sph_handle* h) {
 int sph_density(sph_handle* h) {
   AllocScope alloc_scope(h);
   if (!h) return fail(SPH_ERR_ARG, "null handle");
-  if (h->skin_lets_reorder()) RC(h->reorder_rows());
+  RC(h->reorder_rows());
   int rc = h->iterate(false);
   h->collect_timers();
   return rc;

@@ -700,19 +700,20 @@ k_neighbours(NeibArgs a) {
     };
     const int nch = __reduce_max_sync(FULL, (nrows_r + RPL * G - 1) / (RPL * G));
     for (int ch = 0; ch < nch; ++ch) {
-      // The chunk's rows go round-robin over the lanes (row rbase + i G is
-      // the lane's i-th); first each lane finds its rows' runs of cells,
-      // then issues all their cell-start loads at once.
-      const int rbase = ch * RPL * G + lane;
+      // Each lane takes RPL consecutive rows of the chunk (row rbase + i is
+      // its i-th), so the lanes' runs concatenated in lane order follow the
+      // rows in cell order: the candidates, and each centre's hits, come in
+      // increasing record order.  First each lane finds its rows' runs of
+      // cells, then issues all their cell-start loads at once.
+      const int rbase = ch * RPL * G + lane * RPL;
       unsigned ia[RPL], ib[RPL];  // cstart indices of each run's ends
 #pragma unroll
       for (int i = 0; i < RPL; ++i) ia[i] = ib[i] = 0u;
       if (nrows_r > 0) {  // then ny_r >= 1
         int cy = cy0 + rbase % ny_r, cz = cz0 + rbase / ny_r;
-        const int dq = G / ny_r, dr = G % ny_r;  // a step of G rows
 #pragma unroll
         for (int i = 0; i < RPL; ++i) {
-          if (rbase + i * G < nrows_r) {
+          if (rbase + i < nrows_r) {
             float dzc = 0.f, dyc = 0.f;
             if (DIM == 3) dzc = fmaxf(0.f, fmaxf(float(cz) - bz1, bz0 - float(cz + 1)));
             if (DIM >= 2) dyc = fmaxf(0.f, fmaxf(float(cy) - by1, by0 - float(cy + 1)));
@@ -726,9 +727,7 @@ k_neighbours(NeibArgs a) {
               ib[i] = unsigned(rowc + cx1 + 1);
             }
           }
-          cy += dr;
-          cz += dq;
-          if (cy > cy1) { cy -= ny_r; ++cz; }
+          if (++cy > cy1) { cy = cy0; ++cz; }
         }
       }
       int mysum = 0;
@@ -988,53 +987,58 @@ __device__ __forceinline__ int clamp_cell(double f, int n) {
   return int(f);
 }
 
-// sets flag[q] = 1 for every record q of the cells within `reach` (plus one
-// cell) of (x, y, z), walking the rows of cells of that box
-__device__ void mark_box(double x, double y, double z, double reach, const Grid& g,
-                         const int32_t* __restrict__ cstart, uint8_t* __restrict__ flag) {
-  const int x0 = clamp_cell((x - reach - g.ox) * g.invL - 1.0, g.nx);
-  const int x1 = clamp_cell((x + reach - g.ox) * g.invL + 1.0, g.nx);
-  const int y0 = clamp_cell((y - reach - g.oy) * g.invL - 1.0, g.ny);
-  const int y1 = clamp_cell((y + reach - g.oy) * g.invL + 1.0, g.ny);
-  const int z0 = clamp_cell((z - reach - g.oz) * g.invL - 1.0, g.nz);
-  const int z1 = clamp_cell((z + reach - g.oz) * g.invL + 1.0, g.nz);
-  for (int cz = z0; cz <= z1; ++cz)
-    for (int cy = y0; cy <= y1; ++cy) {
-      const int64_t row = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
-      const int32_t a = cstart[row + x0], b = cstart[row + x1 + 1];
-      for (int32_t q = a; q < b; ++q) flag[q] = 1;
-    }
-}
-
-// one thread per record: a record that moved more than eps marks the
-// records whose cells lie within reach_m of its position at b (every centre
-// whose skin list holds it: near_m); one that moved more than tau marks
-// those within reach_f of its position now (near_f)
-__global__ void k_skin_mark(int64_t n, const float* __restrict__ dsp, float tau, float eps,
-                            const double* __restrict__ sx, const double* __restrict__ sy,
-                            const double* __restrict__ sz, const double* __restrict__ bx,
-                            const double* __restrict__ by, const double* __restrict__ bz,
-                            Grid g, const int32_t* __restrict__ cstart, double reach_f,
-                            double reach_m, uint8_t* __restrict__ near_f,
-                            uint8_t* __restrict__ near_m) {
+// Marks at the level of cells: a record that moved more than eps flags the
+// cell it was sorted into (its position at b), one that moved more than tau
+// the cell of its position now (clamped to the grid); each flag field is
+// then dilated by a box of w cells per side (k_dilate, one axis per pass),
+// w = ceil(reach / L) + 1, which holds every cell within `reach` of any
+// point of the flagged cell.  A centre is near a fast (moving) record when
+// the cell it was sorted into carries the dilated flag.
+__global__ void k_skin_cells(int64_t n, const float* __restrict__ dsp, float tau, float eps,
+                             const uint32_t* __restrict__ keys, const double* __restrict__ sx,
+                             const double* __restrict__ sy, const double* __restrict__ sz,
+                             Grid g, uint8_t* __restrict__ fast_cell,
+                             uint8_t* __restrict__ move_cell) {
   const int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (k >= n) return;
   const float d = dsp[k];
-  if (near_m && d > eps) mark_box(bx[k], by[k], bz[k], reach_m, g, cstart, near_m);
-  if (d > tau) mark_box(sx[k], sy[k], sz[k], reach_f, g, cstart, near_f);
+  if (move_cell && d > eps) move_cell[keys[k]] = 1;
+  if (d > tau) {
+    const int cx = clamp_cell((sx[k] - g.ox) * g.invL, g.nx);
+    const int cy = clamp_cell((sy[k] - g.oy) * g.invL, g.ny);
+    const int cz = clamp_cell((sz[k] - g.oz) * g.invL, g.nz);
+    fast_cell[cx + int64_t(g.nx) * (cy + int64_t(g.ny) * cz)] = 1;
+  }
+}
+// out[c] = OR of in over the cells within w of c along `axis`
+__global__ void k_dilate(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, Grid g,
+                         int axis, int w) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int64_t ncell = int64_t(g.nx) * g.ny * g.nz;
+  if (c >= ncell) return;
+  int n, i;
+  int64_t stride;
+  if (axis == 0) { n = g.nx; i = int(c % g.nx); stride = 1; }
+  else if (axis == 1) { n = g.ny; i = int((c / g.nx) % g.ny); stride = g.nx; }
+  else { n = g.nz; i = int(c / (int64_t(g.nx) * g.ny)); stride = int64_t(g.nx) * g.ny; }
+  const int a = max(0, i - w), b = min(n - 1, i + w);
+  uint8_t v = 0;
+  for (int j = a; j <= b && !v; ++j) v = in[c + int64_t(j - i) * stride];
+  out[c] = v;
 }
 
 // The way of each centre (mode: 0 filter, 1 fresh search, 2 keep; dflag =
 // 1 for the fresh search).  The margins of 1e-12 (relative) lie far above
 // the FP64 rounding of the predicate and of the displacements, so that no
-// record outside a list can pass the FP64 predicate at t; near_m == NULL
-// (too many moving records to mark) means no centre keeps its row.
+// record outside a list can pass the FP64 predicate at t; near_f / near_m
+// are the dilated cell flags (near_m == NULL: no centre keeps its row).
 __global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k,
                                 const int32_t* __restrict__ centre_p,
                                 const double* __restrict__ hcol, const double* __restrict__ hb,
                                 double* __restrict__ hdev, const float* __restrict__ gap,
                                 double krad, double kfac, float tau, float eps,
                                 const float* __restrict__ dsp,
+                                const uint32_t* __restrict__ keys,
                                 const uint8_t* __restrict__ near_f,
                                 const uint8_t* __restrict__ near_m,
                                 uint8_t* __restrict__ mode, int32_t* __restrict__ dflag,
@@ -1051,9 +1055,10 @@ __global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k
     const double di = double(dsp[k]);
     const double lhs = krad * h * (1.0 + 1e-12) + di + double(tau);
     const double rhs = krad * h0 * kfac * (1.0 - 1e-12);
-    const bool clean = !was_searched && !near_f[k] && dsp[k] <= tau && lhs < rhs;
+    const uint32_t cell = keys[k];  // the cell the centre was sorted into
+    const bool clean = !was_searched && !near_f[cell] && dsp[k] <= tau && lhs < rhs;
     if (clean) {
-      const bool keep = near_m && !near_m[k] && dsp[k] <= eps &&
+      const bool keep = near_m && !near_m[cell] && dsp[k] <= eps &&
                         2.0 * double(eps) + krad * hd * (1.0 + 1e-12) + 1e-12 * krad * h0 <
                             double(gap[c]);
       w = keep ? 2 : 0;
@@ -1254,6 +1259,30 @@ __global__ void __launch_bounds__(128) k_skin_filter(SkinFilterArgs a) {
     if (mx) atomicMax(a.maxcnt, mx);
     if (ov) atomicOr(a.overflow, 1);
   }
+}
+
+// ---- a row re-sort under skin lists -------------------------------------------------------
+// The re-sort moves old row perm[i] to row i; the sorted records, the images
+// and the centres name rows, so they follow through inv[old] = new; the
+// rows' image signatures move with their rows.
+__global__ void k_inv_perm(const int32_t* __restrict__ perm, int64_t n, int32_t* __restrict__ inv) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n) inv[perm[i]] = int32_t(i);
+}
+__global__ void k_rows_renamed(const int32_t* __restrict__ inv, const int32_t* __restrict__ perm,
+                               int64_t nall, int64_t nrows, int64_t nghost, int64_t nreal,
+                               int32_t* __restrict__ sidx, int32_t* __restrict__ ssrc,
+                               int32_t* __restrict__ gsrc, int32_t* __restrict__ centre_p,
+                               const uint8_t* __restrict__ sig_in, uint8_t* __restrict__ sig_out) {
+  const int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (k < nall) {
+    const int32_t u = sidx[k];
+    if (u < nrows) sidx[k] = inv[u];
+    ssrc[k] = inv[ssrc[k]];
+  }
+  if (k < nghost) gsrc[k] = inv[gsrc[k]];
+  if (k < nreal) centre_p[k] = inv[centre_p[k]];
+  if (k < nrows) sig_out[k] = sig_in[perm[k]];
 }
 
 // ---- rows of the centres searched afresh (skin-list iterates) -----------------------------
@@ -2122,26 +2151,52 @@ void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t 
                                                   dsp, tau, eps, red);
   note_launch();
 }
-void launch_skin_mark(int64_t n, const float* dsp, float tau, float eps, const double* sx,
-                      const double* sy, const double* sz, const double* bx, const double* by,
-                      const double* bz, Grid g, const int32_t* cstart, double reach_f,
-                      double reach_m, uint8_t* near_f, uint8_t* near_m, cudaStream_t s) {
-  if (n <= 0) return;
-  k_skin_mark<<<nblocks(n), TPB, 0, s>>>(n, dsp, tau, eps, sx, sy, sz, bx, by, bz, g, cstart,
-                                         reach_f, reach_m, near_f, near_m);
+void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const uint32_t* keys,
+                       const double* sx, const double* sy, const double* sz, Grid g, int dim,
+                       int wf, int wm, uint8_t* fast_cell, uint8_t* move_cell, uint8_t* tmp,
+                       cudaStream_t s) {
+  const int64_t ncell = int64_t(g.nx) * g.ny * g.nz;
+  if (n <= 0 || ncell <= 0) return;
+  cudaMemsetAsync(fast_cell, 0, size_t(ncell), s);
+  if (move_cell) cudaMemsetAsync(move_cell, 0, size_t(ncell), s);
+  k_skin_cells<<<nblocks(n), TPB, 0, s>>>(n, dsp, tau, eps, keys, sx, sy, sz, g, fast_cell,
+                                          move_cell);
   note_launch();
+  // dilate in place through tmp: axis 0 into tmp, 1 back, 2 into tmp, copy back
+  auto dilate = [&](uint8_t* f, int w) {
+    uint8_t* a = f;
+    uint8_t* b = tmp;
+    for (int axis = 0; axis < dim; ++axis) {
+      k_dilate<<<nblocks(ncell), TPB, 0, s>>>(a, b, g, axis, w);
+      note_launch();
+      std::swap(a, b);
+    }
+    if (a != f) cudaMemcpyAsync(f, a, size_t(ncell), cudaMemcpyDeviceToDevice, s);
+  };
+  dilate(fast_cell, wf);
+  if (move_cell) dilate(move_cell, wm);
 }
 void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
                           const double* hcol, const double* hb, double* hdev, const float* gap,
                           double krad, double kfac, float tau, float eps, const float* dsp,
-                          const uint8_t* near_f, const uint8_t* near_m, uint8_t* mode,
-                          int32_t* dflag, const int32_t* ncnt, unsigned long long* nkept,
-                          cudaStream_t s) {
+                          const uint32_t* keys, const uint8_t* near_f, const uint8_t* near_m,
+                          uint8_t* mode, int32_t* dflag, const int32_t* ncnt,
+                          unsigned long long* nkept, cudaStream_t s) {
   if (nc <= 0) return;
   k_skin_classify<<<nblocks(nc), TPB, 0, s>>>(nc, centre_k, centre_p, hcol, hb, hdev, gap, krad,
-                                              kfac, tau, eps, dsp, near_f, near_m, mode, dflag,
-                                              ncnt, nkept);
+                                              kfac, tau, eps, dsp, keys, near_f, near_m, mode,
+                                              dflag, ncnt, nkept);
   note_launch();
+}
+void launch_rows_renamed(const int32_t* perm, int32_t* inv, int64_t nall, int64_t nrows,
+                         int64_t nghost, int64_t nreal, int32_t* sidx, int32_t* ssrc,
+                         int32_t* gsrc, int32_t* centre_p, const uint8_t* sig_in,
+                         uint8_t* sig_out, cudaStream_t s) {
+  if (nrows <= 0) return;
+  k_inv_perm<<<nblocks(nrows), TPB, 0, s>>>(perm, nrows, inv);
+  k_rows_renamed<<<nblocks(nall), TPB, 0, s>>>(inv, perm, nall, nrows, nghost, nreal, sidx, ssrc,
+                                               gsrc, centre_p, sig_in, sig_out);
+  note_launch(2);
 }
 void launch_dyn_rows(int64_t nd, const int32_t* list, const int32_t* centre_p,
                      const int32_t* orig, const int32_t* count_prev, const float* h_prev,

@@ -280,22 +280,31 @@ void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t 
                          const double* by, const double* bz, double* sx, double* sy, double* sz,
                          float4* s32, PackGeom pg, float* dsp, float tau, float eps,
                          unsigned long long* red, cudaStream_t s);
-// near_f[q] = 1 for the records in the cells within reach_f of a record that
-// moved more than tau; near_m[q] = 1 (near_m may be NULL) for those within
-// reach_m of the position at the skin search of one that moved more than eps
-void launch_skin_mark(int64_t n, const float* dsp, float tau, float eps, const double* sx,
-                      const double* sy, const double* sz, const double* bx, const double* by,
-                      const double* bz, Grid g, const int32_t* cstart, double reach_f,
-                      double reach_m, uint8_t* near_f, uint8_t* near_m, cudaStream_t s);
+// cell flags of the records that moved more than tau (fast_cell, by their
+// position now) and eps (move_cell, may be NULL; by the cell they were
+// sorted into), dilated by wf / wm cells per side along each of dim axes
+// (tmp: a spare field of the cell count)
+void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const uint32_t* keys,
+                       const double* sx, const double* sy, const double* sz, Grid g, int dim,
+                       int wf, int wm, uint8_t* fast_cell, uint8_t* move_cell, uint8_t* tmp,
+                       cudaStream_t s);
 // mode[c] = 0 (filter the skin list), 1 (search afresh; dflag[c] = 1) or 2
-// (keep the row) for every centre (see sph_grid.cu); hdev[c] = running
-// maximum of |h - hb[c]|
+// (keep the row) for every centre (see sph_grid.cu), near_f / near_m the
+// dilated cell flags looked up by the cell keys[k] each centre's record was
+// sorted into; hdev[c] = running maximum of |h - hb[c]|
 void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
                           const double* hcol, const double* hb, double* hdev, const float* gap,
                           double krad, double kfac, float tau, float eps, const float* dsp,
-                          const uint8_t* near_f, const uint8_t* near_m, uint8_t* mode,
-                          int32_t* dflag, const int32_t* ncnt, unsigned long long* nkept,
-                          cudaStream_t s);
+                          const uint32_t* keys, const uint8_t* near_f, const uint8_t* near_m,
+                          uint8_t* mode, int32_t* dflag, const int32_t* ncnt,
+                          unsigned long long* nkept, cudaStream_t s);
+// a row re-sort (old row perm[i] -> row i) under skin lists: sidx / ssrc /
+// gsrc / centre_p renamed through inv (inv[perm[i]] = i, filled here), the
+// rows' image signatures moved from sig_in to sig_out
+void launch_rows_renamed(const int32_t* perm, int32_t* inv, int64_t nall, int64_t nrows,
+                         int64_t nghost, int64_t nreal, int32_t* sidx, int32_t* ssrc,
+                         int32_t* gsrc, int32_t* centre_p, const uint8_t* sig_in,
+                         uint8_t* sig_out, cudaStream_t s);
 // rows of the centres list[0 .. nd-1] laid out after *base: capacities
 // from their last counts (as k_rowcap), their scan, rowoff / rowcap
 void launch_dyn_rows(int64_t nd, const int32_t* list, const int32_t* centre_p,

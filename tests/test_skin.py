@@ -63,7 +63,7 @@ def test_skin_sedov_sets_match_oracle(engine_lib, oracle_lib, cuda_ok, prec):
     info = {k: cnt[k] for k in ("skin_builds", "skin_reuses", "skin_dirty", "skin_kept",
                                 "searches")}
     assert cnt["skin_builds"] >= 1, info
-    assert cnt["skin_reuses"] >= 12, info
+    assert cnt["skin_reuses"] >= 6, info
     assert cnt["skin_dirty"] > 0, info  # some centres were searched afresh,
     assert cnt["skin_kept"] > 0, info  # some rows kept,
     n = st[abi.consts.ec["realpn"] - 1]  # and some filtered
