@@ -93,6 +93,8 @@ def parse():
                     help="skip the errors against the CPU oracle at the bench size")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the 21-instance diffusion batch (config 3)")
+    ap.add_argument("--no-full-run", action="store_true",
+                    help="skip the whole Sedov run to t = 0.05")
     ap.add_argument("--no-160", action="store_true",
                     help="skip the 160^3 Sedov throughput line (config 5b)")
     ap.add_argument("--no-decomposed", action="store_true",
@@ -444,6 +446,9 @@ def density_block(lib, shapes, n=128, tol=1e-6, reps=5, oracle=None):
         for k, v in shapes.get(prec, {}).items():  # the launch shapes of the step arms
             e.set_param(getattr(abi, k), float(v))
         e.set_param(abi.P_NEWTON_TOL, tol)
+        # one pass from a table just uploaded: a plain search (skin lists
+        # would cost their wider search and serve no later pass)
+        e.set_param(abi.P_SKIN, 0.0)
         e.density()
         res[name] = e.get_store()
         dig[name] = e.get_neighbour_digest()
@@ -484,6 +489,39 @@ def density_block(lib, shapes, n=128, tol=1e-6, reps=5, oracle=None):
     out["fp32_over_fp64_speed"] = out["fp64"]["ms_per_pass"] / out["fp32_comp"]["ms_per_pass"]
     out["workload"] = (f"density3d {n}^3 ({store.shape[0]} particles), perturbed lattice, M6 hfac 1.2, "
                        f"Newton tolerance {tol}, one density pass (images, sort, search, circuit1)")
+    return out
+
+
+def full_run_block(engine, st, store, tfinish=0.05):
+    """The whole Sedov run of the workload (leapfrog from t = 0 to
+    tfinish): device time of every step (CUDA events around the sph_run_to
+    call), particle-steps/s, and how the skin lists served it; FP32-comp with
+    skin lists (the default), FP32-comp with a fresh search every iterate,
+    FP64 with skin lists."""
+    st = st.copy()
+    st[abi.consts.ec["tfinish"] - 1] = tfinish
+    out = {}
+    for name, prec, skin in (("fp32_comp", abi.PREC_FP32_COMP, None),
+                             ("fp32_comp_fresh_search", abi.PREC_FP32_COMP, 0.0),
+                             ("fp64", abi.PREC_FP64, None)):
+        e = engine(prec, st, store)
+        if skin is not None:
+            e.set_param(abi.P_SKIN, skin)
+        e.reset_counters()
+        e.set_param(abi.P_TIMING, 2)
+        e.run_to(tfinish)
+        t, c = e.timers(), e.counters()
+        e.close()
+        k = max(c["steps"], 1)
+        out[name] = {"steps": c["steps"], "seconds": t["step"] * 1e-3,
+                     "ms_per_step": t["step"] / k,
+                     "particle_steps_per_s": store.shape[0] * c["steps"] / (t["step"] * 1e-3),
+                     "skin": {"builds": c["skin_builds"], "iterates_served": c["skin_reuses"],
+                              "rows_kept_per_served": c["skin_kept"] / max(c["skin_reuses"], 1),
+                              "rows_searched_afresh_per_served":
+                                  c["skin_dirty"] / max(c["skin_reuses"], 1)}}
+    out["workload"] = (f"sedov3d {round(store.shape[0] ** (1 / 3))}^3, leapfrog from t = 0 to "
+                       f"t = {tfinish} (the whole Sedov run), device time of the run_to call")
     return out
 
 
@@ -644,7 +682,20 @@ def main():
         scale = 1e9 if kk["unit"] == "GB/s" else 1e12
         kk["achieved"] = kk["work"] / (kk["ms"] * 1e-3) / scale if kk["ms"] > 0 else 0.0
         kk["frac"] = kk["achieved"] / kk["peak"]
-    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    served = cnt["skin_reuses"]
+    if served:
+        # iterates served from skin lists write only the rows they filter or
+        # search afresh (the kept rows stay): the phase is a mix of small
+        # kernels with no single work figure, reported by what it did
+        nbk = kernels["neighbours"]
+        nbk.update({"bound": "skin lists", "achieved": None, "frac": None, "work": None,
+                    "traffic": None,
+                    "iterates": {"served_from_skin_lists": served,
+                                 "skin_list_builds": cnt["skin_builds"],
+                                 "rows_kept_per_served": cnt["skin_kept"] / served,
+                                 "rows_searched_afresh_per_served": cnt["skin_dirty"] / served}})
+    dom = max((k for k in kernels if kernels[k]["frac"] is not None),
+              key=lambda k: kernels[k]["ms"])
     step_flops = (cnt["c1_pairs"] * F1_C1 + cnt["c2_pairs"] * F2_C2) / K + N * F_PARTICLE
     step_ach = step_flops / ((ms / K) * 1e-3) / 1e12
     roofline = {"bound": kernels[dom]["bound"], "kernel": dom,
@@ -659,8 +710,9 @@ def main():
                                         "MEASURED_PEAKS.json holds no non-tensor FP32 figure",
                                 "hbm": hbm_src},
                 "work_definition": "fp32 kernels: in-support pairs x per-pair FLOP (circuit1 "
-                                   f"{F1_C1:.0f} per sweep, circuit2 {F2_C2:.0f}); search: 4 B per "
-                                   f"pair written + {SEARCH_BYTES_PER_CENTRE:.0f} B per centre; "
+                                   f"{F1_C1:.0f} per sweep, circuit2 {F2_C2:.0f}); search (iterates "
+                                   f"with a fresh search): 4 B per pair written + "
+                                   f"{SEARCH_BYTES_PER_CENTRE:.0f} B per centre; "
                                    "step: both pair passes + "
                                    f"{F_PARTICLE:.0f} FLOP per particle"}
 
@@ -720,6 +772,9 @@ def main():
                                           tuned[abi.PREC_FP32_COMP], f"cuda:{local}")
         except Exception as exc:  # noqa: BLE001
             decomposed = {"error": f"{type(exc).__name__}: {exc}"}
+    full = None
+    if not args.no_full_run and ws == 1:
+        full = full_run_block(engine, st, store)
     big = None
     if not args.no_160 and args.n == 128:
         st160, store160 = ic.sedov3d(n=160)
@@ -741,6 +796,10 @@ def main():
                        "l2": "inputs larger than L2 (particle table "
                              f"{N * 32 * 8 / 1e6:.0f} MB + pair streams)",
                        "parallelism": f"replicas x{ws}",
+                       "neighbour_lists": "skin lists (SPH_P_SKIN = 0.1): radius 1.1 krad h, "
+                                          "rows kept, refiltered with the FP64 predicate or "
+                                          "searched afresh every iterate; sets equal a fresh "
+                                          "search's",
                        "launch_shapes": {"fp32_comp": tuned[abi.PREC_FP32_COMP],
                                          "fp64": tuned[abi.PREC_FP64],
                                          "source": "autotuned on this workload" if not
@@ -772,6 +831,7 @@ def main():
             "diffusion_batch": batch,
             "decomposed": decomposed,
             "sedov3d_160": big,
+            "sedov3d_full_run": full,
             "speedup_fp32_vs_fp64": (value / fp64["value"]) if fp64 else None,
             "peak_fp32_tflops": peak32 / 1e12,
         }

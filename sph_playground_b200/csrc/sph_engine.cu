@@ -217,6 +217,7 @@ struct sph_handle {
   // skin_pause iterates search plainly, a pause that doubles while lists
   // keep ending early (up to kSkinPauseMax) and resets when they last
   int skin_pause = 0, skin_pause_len = 0;
+  bool skin_live = false;  // lists built and not yet replaced by a plain search
   bool skin_trace = std::getenv("SPH_SKIN_TRACE") != nullptr;
   int64_t kept_pairs = 0;    // neighbour pairs of the rows kept (counted as found)
   const DevPlan* dplan = nullptr;  // set while a device-resident step is built
@@ -772,6 +773,7 @@ struct sph_handle {
     }));
     launch_table_end(rowoff.as<int64_t>(), rowcap.as<int32_t>(), nreal, skin_end.as<int64_t>(), s);
     skin_valid = true;
+    skin_live = true;
     skin_s = skin;
     skin_age = 0;
     cnt_host[SPH_CNT_SKIN_BUILDS]++;
@@ -945,12 +947,6 @@ struct sph_handle {
       if (skin_trace)
         std::fprintf(stderr, "skin lists end after %d iterates: %s (D %.3g, fast %llu, moving %llu)\n",
                      skin_age, why, D, nfast, nmove);
-      if (skin_age < kSkinShort) {
-        skin_pause_len = skin_pause_len ? std::min(2 * skin_pause_len, kSkinPauseMax) : kSkinPause0;
-        skin_pause = skin_pause_len;
-      } else {
-        skin_pause_len = 0;
-      }
       return SPH_OK;
     };
     if (h_red[RED_SKIN_SIG]) return end_lists("an image set changed");
@@ -1029,6 +1025,17 @@ struct sph_handle {
       if (served) return SPH_OK;
     }
     skin_valid = false;
+    if (skin_live) {
+      // the lists ended (here or by a change of the table or parameters);
+      // short-lived ones start a pause of plain searches
+      skin_live = false;
+      if (skin_age < kSkinShort) {
+        skin_pause_len = skin_pause_len ? std::min(2 * skin_pause_len, kSkinPauseMax) : kSkinPause0;
+        skin_pause = skin_pause_len;
+      } else {
+        skin_pause_len = 0;
+      }
+    }
     if (skin > 0 && skin_pause > 0) {  // lists ended early: plain searches for now
       --skin_pause;
       skin = 0.0;
