@@ -203,7 +203,8 @@ struct sph_handle {
   // iterate after the end of the table's fixed part (skin_end[0]): their
   // capacities and the scan of those
   DevBuf skin_end, skin_dcap, skin_doff;
-  DevBuf skin_sig_alt, skin_inv;  // a row re-sort's spare signatures, inverse permutation
+  // rows renamed: spare signatures, the two permutations, the old types, a flag
+  DevBuf skin_sig_alt, skin_inv, skin_perm, skin_type, skin_flag;
   int64_t skin_nl_size = 0;
   int skin_est = 0;
   bool skin_valid = false;  // the skin lists describe the records of the current sort
@@ -524,6 +525,18 @@ struct sph_handle {
     return SPH_OK;
   }
 
+  // what names rows under skin lists, after old row perm[i] became row i
+  // (inv[perm[i]] = i)
+  int rename_rows(const int32_t* perm, const int32_t* inv) {
+    RC(skin_sig_alt.ensure(sizeof(uint8_t) * nrows));
+    launch_rows_renamed(perm, inv, nrows + nghost, nrows, nghost, nreal, vals_alt.as<int32_t>(),
+                        ssrc.as<int32_t>(), gsrc.as<int32_t>(), centre_p.as<int32_t>(),
+                        skin_sig.as<uint8_t>(), skin_sig_alt.as<uint8_t>(), s);
+    std::swap(skin_sig.p, skin_sig_alt.p);
+    std::swap(skin_sig.bytes, skin_sig_alt.bytes);
+    return SPH_OK;
+  }
+
   // ---- physical re-ordering of the rows (locality of the pair loops) ---------------------
   int reorder_rows() {
     if (!have_order || in_split_step || rows_in_order) return SPH_OK;
@@ -545,14 +558,9 @@ struct sph_handle {
     std::swap(orig.bytes, orig_alt.bytes);
     if (skin_valid) {
       // the skin lists name records, which stay; what names rows follows
-      RC(skin_sig_alt.ensure(sizeof(uint8_t) * nrows));
       RC(skin_inv.ensure(sizeof(int32_t) * nrows));
-      launch_rows_renamed(perm, skin_inv.as<int32_t>(), nrows + nghost, nrows, nghost, nreal,
-                          vals_alt.as<int32_t>(), ssrc.as<int32_t>(), gsrc.as<int32_t>(),
-                          centre_p.as<int32_t>(), skin_sig.as<uint8_t>(),
-                          skin_sig_alt.as<uint8_t>(), s);
-      std::swap(skin_sig.p, skin_sig_alt.p);
-      std::swap(skin_sig.bytes, skin_sig_alt.bytes);
+      launch_inverse(perm, nrows, skin_inv.as<int32_t>(), s);
+      RC(rename_rows(perm, skin_inv.as<int32_t>()));
       rows_in_order = true;  // (until a sort puts them in another order)
     } else {
       have_order = false;
@@ -691,6 +699,12 @@ struct sph_handle {
     RC(skin_hdev.ensure(sizeof(double) * nreal));
     RC(skin_mode.ensure(sizeof(uint8_t) * nreal));
     RC(skin_end.ensure(sizeof(int64_t)));
+    // (renaming rows: re-sorts and uploads allocate nothing while lists serve)
+    RC(skin_sig_alt.ensure(sizeof(uint8_t) * nrows));
+    RC(skin_inv.ensure(sizeof(int32_t) * nrows));
+    RC(skin_perm.ensure(sizeof(int32_t) * nrows));
+    RC(skin_type.ensure(sizeof(double) * nrows));
+    RC(skin_flag.ensure(sizeof(int32_t)));
     RC(skin_dcap.ensure(sizeof(int64_t) * (nreal + 1)));
     RC(skin_doff.ensure(sizeof(int64_t) * (nreal + 1)));
     RC(scan64_tmp.ensure(scan64_temp_bytes(nreal + 1)));
@@ -2549,13 +2563,41 @@ int sph_get_param(sph_handle* h, int index, double* value) {
 }
 
 int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
+  AllocScope alloc_scope(h);
   if (!h || !store || n_rows != h->nrows) return fail(SPH_ERR_ARG, "row count mismatch");
+  // Skin lists outlive the upload: it puts the rows back in caller order
+  // (old row p becomes row orig[p]), so what names rows is renamed; the new
+  // positions and h are measured by the next iterate like any move; a
+  // changed particle type (the image set) ends the lists.
+  const bool keep = h->skin_valid;
+  if (keep) {
+    RC(h->skin_inv.ensure(sizeof(int32_t) * n_rows));
+    RC(h->skin_perm.ensure(sizeof(int32_t) * n_rows));
+    RC(h->skin_type.ensure(sizeof(double) * n_rows));
+    RC(h->skin_flag.ensure(sizeof(int32_t)));
+    CK(cudaMemcpyAsync(h->skin_inv.p, h->orig.p, sizeof(int32_t) * n_rows,
+                       cudaMemcpyDeviceToDevice, h->s));
+    CK(cudaMemcpyAsync(h->skin_type.p, h->col(es_type), sizeof(double) * n_rows,
+                       cudaMemcpyDeviceToDevice, h->s));
+    CK(cudaMemsetAsync(h->skin_flag.p, 0, sizeof(int32_t), h->s));
+  }
   CK(cudaMemcpyAsync(h->staging.p, store, sizeof(double) * NCOL * n_rows, cudaMemcpyHostToDevice, h->s));
   launch_upload_store(h->staging.as<double>(), h->cols.as<double>(), h->orig.as<int32_t>(), n_rows, h->s);
+  if (keep) {
+    launch_inverse(h->skin_inv.as<int32_t>(), n_rows, h->skin_perm.as<int32_t>(), h->s);
+    launch_type_changed(h->cols.as<double>(), n_rows, h->skin_type.as<double>(),
+                        h->skin_perm.as<int32_t>(), h->skin_flag.as<int32_t>(), h->s);
+    RC(h->rename_rows(h->skin_perm.as<int32_t>(), h->skin_inv.as<int32_t>()));
+    CK(cudaMemcpyAsync(h->h_i32 + 4, h->skin_flag.p, sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
+  }
   CK(cudaStreamSynchronize(h->s));
   CK(cudaGetLastError());
-  h->have_order = false;
-  h->skin_valid = false;  // rows back in caller order
+  if (keep && h->h_i32[4] == 0) {
+    h->rows_in_order = false;  // (caller order: the next re-sort restores cell order)
+  } else {
+    h->have_order = false;
+    h->skin_valid = false;
+  }
   return SPH_OK;
 }
 

@@ -1261,13 +1261,21 @@ __global__ void __launch_bounds__(128) k_skin_filter(SkinFilterArgs a) {
   }
 }
 
-// ---- a row re-sort under skin lists -------------------------------------------------------
-// The re-sort moves old row perm[i] to row i; the sorted records, the images
-// and the centres name rows, so they follow through inv[old] = new; the
-// rows' image signatures move with their rows.
+// ---- rows renamed under skin lists (a re-sort, a table upload) -----------------------------
+// Old row perm[i] becomes row i; the sorted records, the images and the
+// centres name rows, so they follow through inv[old] = new; the rows' image
+// signatures move with their rows.
 __global__ void k_inv_perm(const int32_t* __restrict__ perm, int64_t n, int32_t* __restrict__ inv) {
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i < n) inv[perm[i]] = int32_t(i);
+}
+// *changed = 1 if a row's particle type differs from the one its row had
+// (old types by old row, perm[new] = old)
+__global__ void k_type_changed(const double* __restrict__ cols, int64_t ld, int64_t n,
+                               const double* __restrict__ old_type,
+                               const int32_t* __restrict__ perm, int32_t* __restrict__ changed) {
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i < n && !(cols[es_type * ld + i] == old_type[perm[i]])) *changed = 1;
 }
 __global__ void k_rows_renamed(const int32_t* __restrict__ inv, const int32_t* __restrict__ perm,
                                int64_t nall, int64_t nrows, int64_t nghost, int64_t nreal,
@@ -2188,15 +2196,25 @@ void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* ce
                                               dflag, ncnt, nkept);
   note_launch();
 }
-void launch_rows_renamed(const int32_t* perm, int32_t* inv, int64_t nall, int64_t nrows,
+void launch_inverse(const int32_t* p, int64_t n, int32_t* q, cudaStream_t s) {
+  if (n <= 0) return;
+  k_inv_perm<<<nblocks(n), TPB, 0, s>>>(p, n, q);
+  note_launch();
+}
+void launch_type_changed(const double* cols, int64_t n, const double* old_type,
+                         const int32_t* perm, int32_t* changed, cudaStream_t s) {
+  if (n <= 0) return;
+  k_type_changed<<<nblocks(n), TPB, 0, s>>>(cols, n, n, old_type, perm, changed);
+  note_launch();
+}
+void launch_rows_renamed(const int32_t* perm, const int32_t* inv, int64_t nall, int64_t nrows,
                          int64_t nghost, int64_t nreal, int32_t* sidx, int32_t* ssrc,
                          int32_t* gsrc, int32_t* centre_p, const uint8_t* sig_in,
                          uint8_t* sig_out, cudaStream_t s) {
   if (nrows <= 0) return;
-  k_inv_perm<<<nblocks(nrows), TPB, 0, s>>>(perm, nrows, inv);
   k_rows_renamed<<<nblocks(nall), TPB, 0, s>>>(inv, perm, nall, nrows, nghost, nreal, sidx, ssrc,
                                                gsrc, centre_p, sig_in, sig_out);
-  note_launch(2);
+  note_launch();
 }
 void launch_dyn_rows(int64_t nd, const int32_t* list, const int32_t* centre_p,
                      const int32_t* orig, const int32_t* count_prev, const float* h_prev,

@@ -298,13 +298,18 @@ void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* ce
                           const uint32_t* keys, const uint8_t* near_f, const uint8_t* near_m,
                           uint8_t* mode, int32_t* dflag, const int32_t* ncnt,
                           unsigned long long* nkept, cudaStream_t s);
-// a row re-sort (old row perm[i] -> row i) under skin lists: sidx / ssrc /
-// gsrc / centre_p renamed through inv (inv[perm[i]] = i, filled here), the
-// rows' image signatures moved from sig_in to sig_out
-void launch_rows_renamed(const int32_t* perm, int32_t* inv, int64_t nall, int64_t nrows,
+// rows renamed under skin lists (old row perm[i] -> row i, inv[perm[i]] =
+// i): sidx / ssrc / gsrc / centre_p renamed through inv, the rows' image
+// signatures moved from sig_in to sig_out
+void launch_rows_renamed(const int32_t* perm, const int32_t* inv, int64_t nall, int64_t nrows,
                          int64_t nghost, int64_t nreal, int32_t* sidx, int32_t* ssrc,
                          int32_t* gsrc, int32_t* centre_p, const uint8_t* sig_in,
                          uint8_t* sig_out, cudaStream_t s);
+// q[p[i]] = i
+void launch_inverse(const int32_t* p, int64_t n, int32_t* q, cudaStream_t s);
+// *changed = 1 if some row's particle type differs from old_type[perm[row]]
+void launch_type_changed(const double* cols, int64_t n, const double* old_type,
+                         const int32_t* perm, int32_t* changed, cudaStream_t s);
 // rows of the centres list[0 .. nd-1] laid out after *base: capacities
 // from their last counts (as k_rowcap), their scan, rowoff / rowcap
 void launch_dyn_rows(int64_t nd, const int32_t* list, const int32_t* centre_p,

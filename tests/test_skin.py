@@ -169,3 +169,36 @@ def test_skin_parameter_change_rebuilds(engine_lib, oracle_lib, cuda_ok):
         o.density()
         ref = o.get_neighbour_digest()
     assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+
+
+@pytest.mark.gpu
+def test_skin_lists_survive_a_table_upload(engine_lib, oracle_lib, cuda_ok):
+    """sph_set_store puts the rows back in caller order: the lists are
+    renamed and serve the next pass, whose sets equal a fresh search's on the
+    uploaded table (moved positions and h measured like any move); a changed
+    particle type ends them."""
+    st, store = ic.density3d(n=16, seed=2)
+    dx = 1.0 / 16
+    rng = np.random.default_rng(5)
+    with abi.Engine(st, store, "m6", precision=FP64, lib=engine_lib) as e:
+        e.set_param(abi.P_SKIN, 0.1)
+        for _ in range(5):
+            e.density()
+        b0 = e.counters()["skin_builds"]
+        table = e.get_store()
+        table[:, 0:3] += rng.uniform(-0.02 * dx, 0.02 * dx, size=(table.shape[0], 3))
+        table[:, COL["h"]] *= 1.0 + rng.uniform(0.0, 0.01, size=table.shape[0])
+        e.set_store(table)
+        mst = e.get_state()
+        e.density()
+        assert e.counters()["skin_builds"] == b0  # served from the renamed lists
+        got = e.get_neighbour_digest()
+        with abi.Engine(mst, table, "m6", precision=FP64, lib=oracle_lib) as o:
+            o.density()
+            ref = o.get_neighbour_digest()
+        assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+        table = e.get_store()
+        table[3, COL["type"]] = consts.ept["fixed"]
+        e.set_store(table)
+        e.density()
+        assert e.counters()["skin_builds"] == b0 + 1  # a changed type ends them
