@@ -39,12 +39,12 @@ UNIT = "particle-steps/s"
 F1_C1 = 50.0
 F2_C2 = 150.0
 # DRAM bytes per in-support pair of the FP32-comp circuit2 launch:
-# dram__bytes_read.sum + dram__bytes_write.sum = 849.04 MB + 73.09 MB over
+# dram__bytes_read.sum + dram__bytes_write.sum = 841.77 MB + 67.19 MB over
 # 157.49M pairs of an ncu capture of k_c2 on the Sedov 96^3 step (FP32-comp, 4
-# lanes per centre, cell edge 0.4 krad h_min) (the
-# neighbour index, 4 B, plus the gathered pair data that misses L2); the
-# traffic scales with the pairs a launch processes
-C2_DRAM_BYTES_PER_PAIR = (849.04e6 + 73.09e6) / 157.49e6
+# lanes per centre, cell edge 0.4 krad h_min, an iterate served from skin
+# lists) (the neighbour index, 4 B, plus the gathered pair data that misses
+# L2); the traffic scales with the pairs a launch processes
+C2_DRAM_BYTES_PER_PAIR = (841.77e6 + 67.19e6) / 157.49e6
 # DRAM bytes per in-support pair of the neighbour search (k_neighbours),
 # same capture workload: 198.36 MB read + 684.48 MB written over 157.49M
 # pairs; the search's algorithmic bytes are the 4 B list entry per pair it
