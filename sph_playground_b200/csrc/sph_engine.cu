@@ -198,7 +198,8 @@ struct sph_handle {
   // search afresh, keep), the fresh-search flag, its scan and those centres
   DevBuf skin_nl, skin_rowoff, skin_rowcap, skin_rowcap64, skin_cnt, skin_count_prev,
       skin_h_prev, skin_bx, skin_by, skin_bz, skin_hb, skin_sig, skin_dsp, skin_fcell,
-      skin_mcell, skin_ctmp, skin_gap, skin_hdev, skin_mode, skin_dflag, skin_dpos, skin_dlist;
+      skin_mcell, skin_ctmp, skin_gap, skin_hdev, skin_mode, skin_dflag, skin_dpos, skin_dlist,
+      skin_hrec, skin_ways, skin_wpos, skin_flist;
   // the rows of the centres searched afresh, laid out anew every skin-list
   // iterate after the end of the table's fixed part (skin_end[0]): their
   // capacities and the scan of those
@@ -698,6 +699,10 @@ struct sph_handle {
     RC(skin_gap.ensure(sizeof(float) * nreal));
     RC(skin_hdev.ensure(sizeof(double) * nreal));
     RC(skin_mode.ensure(sizeof(uint8_t) * nreal));
+    RC(skin_hrec.ensure(sizeof(double) * nall));
+    RC(skin_ways.ensure(sizeof(int64_t) * (nreal + 1)));
+    RC(skin_wpos.ensure(sizeof(int64_t) * (nreal + 1)));
+    RC(skin_flist.ensure(sizeof(int32_t) * nreal));
     RC(skin_end.ensure(sizeof(int64_t)));
     // (renaming rows: re-sorts and uploads allocate nothing while lists serve)
     RC(skin_sig_alt.ensure(sizeof(uint8_t) * nrows));
@@ -826,7 +831,7 @@ struct sph_handle {
   // fixed part.  A filter row that overflows joins the centres searched
   // afresh (for good: mode 1); when their rows find no room either, the
   // whole table is laid out anew and every row written.
-  int skin_fill(const Params& P, int64_t ndirty, double reach) {
+  int skin_fill(const Params& P, int64_t ndirty, int64_t nfilter, double reach) {
     const int d = P.dim;
     Table T = exact_table();
     // the centres searched afresh (skin_dlist): a lane group each when they
@@ -871,7 +876,10 @@ struct sph_handle {
       CK(cudaMemsetAsync(overflow.p, 0, sizeof(int32_t), s));
       dyn(ndirty);
       NeibArgs na = neib_args(T, P);
-      launch_skin_filter(filter_args(na, true, false), s);
+      SkinFilterArgs fa = filter_args(na, true, false);
+      fa.list = skin_flist.as<int32_t>();  // (the centres that filter)
+      fa.nc = nfilter;
+      launch_skin_filter(fa, s);
       search_dirty(na, ndirty, reach);
       RC(read_flags(mc, ov));
     }
@@ -946,7 +954,7 @@ struct sph_handle {
                           gsrc.as<int32_t>(), gcode.as<int8_t>(), gg, d, skin_sig.as<uint8_t>(),
                           skin_bx.as<double>(), skin_by.as<double>(), skin_bz.as<double>(),
                           sx.as<double>(), sy.as<double>(), sz.as<double>(), s32.as<float4>(),
-                          pgeom, skin_dsp.as<float>(), tau, eps, rb, s);
+                          pgeom, skin_dsp.as<float>(), tau, eps, skin_hrec.as<double>(), rb, s);
       CK(cudaMemcpyAsync(h_red, rb, sizeof(unsigned long long) * RED_TOTAL,
                          cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
@@ -992,24 +1000,22 @@ struct sph_handle {
                         sx.as<double>(), sy.as<double>(), sz.as<double>(), grid, d, wf, wm,
                         skin_fcell.as<uint8_t>(), skin_mcell.as<uint8_t>(),
                         skin_ctmp.as<uint8_t>(), s);
-      launch_skin_classify(nreal, centre_k.as<int32_t>(), centre_p.as<int32_t>(), col(es_h),
+      launch_skin_classify(nreal, centre_k.as<int32_t>(), skin_hrec.as<double>(),
                            skin_hb.as<double>(), skin_hdev.as<double>(), skin_gap.as<float>(),
                            P.krad, 1.0 + skin_s, tau, eps, skin_dsp.as<float>(),
                            keys_alt.as<uint32_t>(), skin_fcell.as<uint8_t>(),
                            skin_mcell.as<uint8_t>(), skin_mode.as<uint8_t>(),
-                           skin_dflag.as<int32_t>(), ncnt.as<int32_t>(), rb + RED_SKIN_NKEPT, s);
-      // (skin_dflag[nreal] stays 0: the scan's last entry is the count)
-      exclusive_scan(scan_tmp.p, scan_tmp.bytes, skin_dflag.as<int32_t>(),
-                     skin_dpos.as<int32_t>(), nreal + 1, s);
-      launch_skin_compact(nreal, skin_dflag.as<int32_t>(), skin_dpos.as<int32_t>(),
-                          skin_dlist.as<int32_t>(), s);
-      CK(cudaMemcpyAsync(h_i32, skin_dpos.as<int32_t>() + nreal, sizeof(int32_t),
+                           skin_ways.as<int64_t>(), skin_wpos.as<int64_t>(),
+                           skin_dlist.as<int32_t>(), skin_flist.as<int32_t>(), scan64_tmp.p,
+                           scan64_tmp.bytes, ncnt.as<int32_t>(), rb + RED_SKIN_NKEPT, s);
+      CK(cudaMemcpyAsync(h_red + RED_TOTAL, skin_wpos.as<int64_t>() + nreal, sizeof(int64_t),
                          cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(h_red + RED_SKIN_NKEPT, rb + RED_SKIN_NKEPT,
                          2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
     }
-    const int64_t ndirty = h_i32[0];
+    const int64_t counts = reinterpret_cast<const int64_t*>(h_red + RED_TOTAL)[0];
+    const int64_t ndirty = counts & 0xffffffffll, nfilter = counts >> 32;
     const int64_t nkept = int64_t(h_red[RED_SKIN_NKEPT]);
     // Their search over cells of step b, its range widened by D, costs
     // several times a search's share per centre (measured on the 128^3
@@ -1021,7 +1027,7 @@ struct sph_handle {
     if (double(ndirty) * widen > kSkinDirtyShare * double(nreal))
       return end_lists("too many centres to search afresh");
     const double reach_d = D * (1.0 + 1e-9);
-    RC(skin_fill(P, ndirty, reach_d));
+    RC(skin_fill(P, ndirty, nfilter, reach_d));
     ++skin_age;
     cnt_host[SPH_CNT_SKIN_REUSES]++;
     cnt_host[SPH_CNT_SKIN_KEPT] += nkept;

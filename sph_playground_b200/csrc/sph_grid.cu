@@ -919,7 +919,7 @@ k_skin_refresh(const int32_t* __restrict__ sidx, int64_t n, int64_t nrows, int64
                const double* __restrict__ by, const double* __restrict__ bz,
                double* __restrict__ sx, double* __restrict__ sy, double* __restrict__ sz,
                float4* __restrict__ s32, PackGeom pg, float* __restrict__ dsp, float tau,
-               float eps, unsigned long long* __restrict__ red) {
+               float eps, double* __restrict__ hrec, unsigned long long* __restrict__ red) {
   // slots: lo x, y, z (min), hi x, y, z (max), D (max), h of the real rows (max)
   double v[8] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 0.0, 0.0};
   const bool is_max[8] = {false, false, false, true, true, true, true, true};
@@ -931,7 +931,9 @@ k_skin_refresh(const int32_t* __restrict__ sidx, int64_t n, int64_t nrows, int64
     double x, y, z;
     if (u < nrows) {
       x = cols[es_rx * ld + u]; y = cols[es_ry * ld + u]; z = cols[es_rz * ld + u];
-      if (u < nreal) v[7] = fmax(v[7], cols[es_h * ld + u]);
+      const double h = cols[es_h * ld + u];
+      hrec[k] = h;  // (for the centres' ways, read in record order)
+      if (u < nreal) v[7] = fmax(v[7], h);
       if (ghost_source(cols[es_type * ld + u])) {
         const double r[3] = {x, y, z};
         sigchg |= image_sig(r, g, dim) != sig_b[u];
@@ -1033,15 +1035,14 @@ __global__ void k_dilate(const uint8_t* __restrict__ in, uint8_t* __restrict__ o
 // record outside a list can pass the FP64 predicate at t; near_f / near_m
 // are the dilated cell flags (near_m == NULL: no centre keeps its row).
 __global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k,
-                                const int32_t* __restrict__ centre_p,
-                                const double* __restrict__ hcol, const double* __restrict__ hb,
+                                const double* __restrict__ hrec, const double* __restrict__ hb,
                                 double* __restrict__ hdev, const float* __restrict__ gap,
                                 double krad, double kfac, float tau, float eps,
                                 const float* __restrict__ dsp,
                                 const uint32_t* __restrict__ keys,
                                 const uint8_t* __restrict__ near_f,
                                 const uint8_t* __restrict__ near_m,
-                                uint8_t* __restrict__ mode, int32_t* __restrict__ dflag,
+                                uint8_t* __restrict__ mode, int64_t* __restrict__ ways,
                                 const int32_t* __restrict__ ncnt,
                                 unsigned long long* __restrict__ nkept) {
   const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -1049,7 +1050,7 @@ __global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k
   if (c < nc) {
     const bool was_searched = mode[c] == 1;  // (a centre once searched afresh stays so)
     const int32_t k = centre_k[c];
-    const double h = hcol[centre_p[c]], h0 = hb[c];
+    const double h = hrec[k], h0 = hb[c];
     const double hd = fmax(hdev[c], fabs(h - h0));
     hdev[c] = hd;
     const double di = double(dsp[k]);
@@ -1064,7 +1065,9 @@ __global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k
       w = keep ? 2 : 0;
     }
     mode[c] = w;
-    dflag[c] = w == 1 ? 1 : 0;
+    // one scan counts both lists: fresh searches in the low word, filters
+    // in the high one
+    ways[c] = (w == 1 ? 1ll : 0ll) | (w == 0 ? (1ll << 32) : 0ll);
   }
   // rows kept and their neighbours: nkept[0], nkept[1]
   const bool kp = c < nc && w == 2;
@@ -1074,6 +1077,18 @@ __global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k
     atomicAdd(nkept, (unsigned long long)__popc(kept));
     atomicAdd(nkept + 1, (unsigned long long)pairs);
   }
+}
+
+// the lists of the centres searched afresh and of those that filter, in
+// centre order, from the scan of k_skin_classify's ways
+__global__ void k_skin_lists(int64_t nc, const int64_t* __restrict__ ways,
+                             const int64_t* __restrict__ pos, int32_t* __restrict__ dlist,
+                             int32_t* __restrict__ flist) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= nc) return;
+  const int64_t w = ways[c], p = pos[c];
+  if (w & 1) dlist[p & 0xffffffffll] = int32_t(c);
+  if (w >> 32) flist[p >> 32] = int32_t(c);
 }
 
 __global__ void k_skin_compact(int64_t nc, const int32_t* __restrict__ dflag,
@@ -1120,9 +1135,12 @@ __global__ void __launch_bounds__(128) k_skin_filter(SkinFilterArgs a) {
   int maxc = 0;
   bool ovf = false;
   for (int64_t cb = blockIdx.x; cb * CPB < a.nc; cb += gridDim.x) {
-    const int64_t c = cb * CPB + threadIdx.x / G;
-    bool active = c < a.nc;
-    if (active) {
+    const int64_t i = cb * CPB + threadIdx.x / G;
+    int64_t c = i;
+    bool active = i < a.nc;
+    if (a.list) {
+      c = active ? a.list[i] : 0;  // (the list holds the centres that filter)
+    } else if (active) {
       const uint8_t w = a.mode[c];
       active = w == 0 || (w == 2 && !a.keep);
     }
@@ -2152,11 +2170,11 @@ void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t 
                          BoxGeom g, int dim, const uint8_t* sig_b, const double* bx,
                          const double* by, const double* bz, double* sx, double* sy, double* sz,
                          float4* s32, PackGeom pg, float* dsp, float tau, float eps,
-                         unsigned long long* red, cudaStream_t s) {
+                         double* hrec, unsigned long long* red, cudaStream_t s) {
   if (n <= 0) return;
   k_skin_refresh<<<reduce_blocks(n), TPB, 0, s>>>(sidx, n, nrows, nreal, cols, nrows, gsrc, gcode,
                                                   g, dim, sig_b, bx, by, bz, sx, sy, sz, s32, pg,
-                                                  dsp, tau, eps, red);
+                                                  dsp, tau, eps, hrec, red);
   note_launch();
 }
 void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const uint32_t* keys,
@@ -2184,17 +2202,21 @@ void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const 
   dilate(fast_cell, wf);
   if (move_cell) dilate(move_cell, wm);
 }
-void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
-                          const double* hcol, const double* hb, double* hdev, const float* gap,
-                          double krad, double kfac, float tau, float eps, const float* dsp,
+void launch_skin_classify(int64_t nc, const int32_t* centre_k, const double* hrec,
+                          const double* hb, double* hdev, const float* gap, double krad,
+                          double kfac, float tau, float eps, const float* dsp,
                           const uint32_t* keys, const uint8_t* near_f, const uint8_t* near_m,
-                          uint8_t* mode, int32_t* dflag, const int32_t* ncnt,
-                          unsigned long long* nkept, cudaStream_t s) {
+                          uint8_t* mode, int64_t* ways, int64_t* pos, int32_t* dlist,
+                          int32_t* flist, void* scan_tmp, size_t scan_bytes,
+                          const int32_t* ncnt, unsigned long long* nkept, cudaStream_t s) {
   if (nc <= 0) return;
-  k_skin_classify<<<nblocks(nc), TPB, 0, s>>>(nc, centre_k, centre_p, hcol, hb, hdev, gap, krad,
-                                              kfac, tau, eps, dsp, keys, near_f, near_m, mode,
-                                              dflag, ncnt, nkept);
-  note_launch();
+  k_skin_classify<<<nblocks(nc), TPB, 0, s>>>(nc, centre_k, hrec, hb, hdev, gap, krad, kfac, tau,
+                                              eps, dsp, keys, near_f, near_m, mode, ways, ncnt,
+                                              nkept);
+  cudaMemsetAsync(ways + nc, 0, sizeof(int64_t), s);
+  exclusive_scan64(scan_tmp, scan_bytes, ways, pos, nc + 1, s);
+  k_skin_lists<<<nblocks(nc), TPB, 0, s>>>(nc, ways, pos, dlist, flist);
+  note_launch(2);
 }
 void launch_inverse(const int32_t* p, int64_t n, int32_t* q, cudaStream_t s) {
   if (n <= 0) return;

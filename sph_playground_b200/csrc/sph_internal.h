@@ -279,7 +279,7 @@ void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t 
                          BoxGeom g, int dim, const uint8_t* sig_b, const double* bx,
                          const double* by, const double* bz, double* sx, double* sy, double* sz,
                          float4* s32, PackGeom pg, float* dsp, float tau, float eps,
-                         unsigned long long* red, cudaStream_t s);
+                         double* hrec, unsigned long long* red, cudaStream_t s);
 // cell flags of the records that moved more than tau (fast_cell, by their
 // position now) and eps (move_cell, may be NULL; by the cell they were
 // sorted into), dilated by wf / wm cells per side along each of dim axes
@@ -288,16 +288,20 @@ void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const 
                        const double* sx, const double* sy, const double* sz, Grid g, int dim,
                        int wf, int wm, uint8_t* fast_cell, uint8_t* move_cell, uint8_t* tmp,
                        cudaStream_t s);
-// mode[c] = 0 (filter the skin list), 1 (search afresh; dflag[c] = 1) or 2
-// (keep the row) for every centre (see sph_grid.cu), near_f / near_m the
-// dilated cell flags looked up by the cell keys[k] each centre's record was
-// sorted into; hdev[c] = running maximum of |h - hb[c]|
-void launch_skin_classify(int64_t nc, const int32_t* centre_k, const int32_t* centre_p,
-                          const double* hcol, const double* hb, double* hdev, const float* gap,
-                          double krad, double kfac, float tau, float eps, const float* dsp,
+// mode[c] = 0 (filter the skin list), 1 (search afresh) or 2 (keep the row)
+// for every centre (see sph_grid.cu), near_f / near_m the dilated cell
+// flags looked up by the cell keys[k] each centre's record was sorted into,
+// h of the centres from hrec (per record); hdev[c] = running maximum of
+// |h - hb[c]|.  The centres searched afresh go to dlist, those that filter
+// to flist (in centre order); pos[nc] = their counts (low / high 32 bits);
+// ways and pos hold nc + 1 entries.  nkept[0..1] += rows kept, their pairs.
+void launch_skin_classify(int64_t nc, const int32_t* centre_k, const double* hrec,
+                          const double* hb, double* hdev, const float* gap, double krad,
+                          double kfac, float tau, float eps, const float* dsp,
                           const uint32_t* keys, const uint8_t* near_f, const uint8_t* near_m,
-                          uint8_t* mode, int32_t* dflag, const int32_t* ncnt,
-                          unsigned long long* nkept, cudaStream_t s);
+                          uint8_t* mode, int64_t* ways, int64_t* pos, int32_t* dlist,
+                          int32_t* flist, void* scan_tmp, size_t scan_bytes,
+                          const int32_t* ncnt, unsigned long long* nkept, cudaStream_t s);
 // rows renamed under skin lists (old row perm[i] -> row i, inv[perm[i]] =
 // i): sidx / ssrc / gsrc / centre_p renamed through inv, the rows' image
 // signatures moved from sig_in to sig_out
@@ -361,7 +365,8 @@ void launch_skin_compact(int64_t nc, const int32_t* dflag, const int32_t* dpos, 
 void launch_gather_h(int64_t nc, const int32_t* centre_p, const double* hcol, double* hb,
                      unsigned long long* red, int slot, cudaStream_t s);
 struct SkinFilterArgs {
-  int64_t nc;
+  int64_t nc;           // centres (list == NULL) or list entries
+  const int32_t* list;  // optional: the centres to filter
   const uint8_t* mode;  // 0: filter; 1: left to the search; 2: kept when keep != 0
   int keep;
   float* gap;           // optional: per centre, the smallest |r - krad h| of its list

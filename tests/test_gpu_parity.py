@@ -292,3 +292,29 @@ def test_staged_search_matches_oracle(oracle_lib, engine_lib, cuda_ok, prec, lan
     bad = compare(ref, got, prec, part_fields=("den", "h", "om"),
                   field_fields=("ax", "ay", "az", "du"))
     assert not bad, bad
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32])
+@pytest.mark.parametrize("case", ["sedov3d_hfac1.5", "sod2d_hfac3.5"])
+def test_large_neighbour_counts(oracle_lib, engine_lib, cuda_ok, prec, case):
+    """circuit2's FP32 per-lane sums (plain sums, added over the lanes in
+    FP64) at neighbour counts well above the 3D hfac 1.2 workload's 178:
+    388 per particle in 3D (hfac 1.5), 344 on average (up to 840) in 2D
+    (hfac 3.5, the Sod lattices), through an iterate and three steps."""
+    if case.startswith("sedov3d"):
+        st, store = ic.sedov3d(n=14, hfac=1.5)
+        fields = ("ax", "ay", "az", "du", "dh")
+    else:
+        st, store = ic.sod2d(hfac=3.5)
+        fields = ("ax", "ay", "du", "dh")
+    ref, nb_ref, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "iterate")
+    got, nb_got, _, _ = run_pass(engine_lib, st, store, "m6", prec, "iterate")
+    assert neighbour_sets_equal(nb_got, nb_ref)
+    counts = np.diff(nb_ref[0])
+    assert counts.mean() > 300, counts.mean()
+    bad = compare(ref, got, prec, part_fields=("den", "h", "om"), field_fields=fields)
+    assert not bad, bad
+    ref, _, _, _ = run_pass(oracle_lib, st, store, "m6", FP64, "steps", steps=3)
+    got, _, _, _ = run_pass(engine_lib, st, store, "m6", prec, "steps", steps=3)
+    bad = compare(ref, got, prec, part_fields=("den", "h"), field_fields=("vx", "u"))
+    assert not bad, bad
