@@ -96,8 +96,11 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
 // G lanes per centre: lane l takes neighbours l, l+G, ... of the centre's
 // list row; per-lane partial sums are added over the group in FP64 and
 // lane 0 stores the result.
+// (FP32: 9 blocks of 128 threads per SM, 56 registers with a 4-byte spill,
+// measured 2.01 -> 1.95 ms on the 128^3 Sedov step against 8 blocks at 64
+// registers; 10 blocks spill 44 bytes and take 2.5 ms)
 template <int K, int DIM, class R, bool GENERAL, int G>
-__global__ void __launch_bounds__(TPB, sizeof(R) == 8 ? 5 : 8)
+__global__ void __launch_bounds__(TPB, sizeof(R) == 8 ? 5 : 9)
 k_c2(C2Args a, PackBufs pb, Params P) {
   const int64_t c = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) / G;
   const int lane = threadIdx.x & (G - 1);
