@@ -165,6 +165,7 @@ struct sph_handle {
   int64_t nghost = 0;
   // sort + cells
   DevBuf keys, keys_alt, vals, vals_alt, sort_tmp, cstart;
+  DevBuf cell_count, cell_ctr;  // the counting sort's counts and counters
   // sorted arrays
   DevBuf sx, sy, sz, s32, ssrc, cflag, cpos, centre_k, centre_p;
   DevBuf hk_s, dk_s, ok_s;
@@ -1143,15 +1144,27 @@ struct sph_handle {
       Phase ph(this, SPH_T_SORT);
       launch_keys(cols.as<double>(), nrows, gx.as<double>(), gy.as<double>(), gz.as<double>(),
                   nghost, grid, keys.as<uint32_t>(), vals.as<int32_t>(), s);
-      sort_pairs(sort_tmp.p, sort_tmp.bytes, keys.as<uint32_t>(), keys_alt.as<uint32_t>(),
-                 vals.as<int32_t>(), vals_alt.as<int32_t>(), nall, end_bit, s);
       // the cell count follows 1 / h_min^d, which drifts from step to step:
       // room for four times the current count (at most the cap) keeps the
       // reallocation out of the steady state
+      const size_t cells = size_t(std::min<int64_t>(4 * (ncell + 1), ncell_cap + 1));
       if (sizeof(int32_t) * size_t(ncell + 1) > cstart.bytes)
-        RC(cstart.ensure(sizeof(int32_t) *
-                         size_t(std::min<int64_t>(4 * (ncell + 1), ncell_cap + 1))));
-      launch_cell_starts(keys_alt.as<uint32_t>(), nall, ncell, cstart.as<int32_t>(), s);
+        RC(cstart.ensure(sizeof(int32_t) * cells));
+      if (sizeof(int32_t) * size_t(ncell + 1) > cell_count.bytes)
+        RC(cell_count.ensure(sizeof(int32_t) * cells));
+      const size_t sb = scan_temp_bytes(ncell + 1);
+      if (sb > scan_tmp.bytes) RC(scan_tmp.ensure(sb));
+      RC(cell_ctr.ensure(2 * sizeof(int32_t)));
+      // counting sort by cell (vals serves as its list of crowded cells);
+      // a cell of more than 4096 records takes the library's radix sort
+      if (!cell_sort(keys.as<uint32_t>(), nall, ncell, cell_count.as<int32_t>(),
+                     cstart.as<int32_t>(), vals_alt.as<int32_t>(), keys_alt.as<uint32_t>(),
+                     vals.as<int32_t>(), cell_ctr.as<int32_t>(), scan_tmp.p, scan_tmp.bytes,
+                     h_i32 + 5, s)) {
+        sort_pairs(sort_tmp.p, sort_tmp.bytes, keys.as<uint32_t>(), keys_alt.as<uint32_t>(),
+                   vals.as<int32_t>(), vals_alt.as<int32_t>(), nall, end_bit, s);
+        launch_cell_starts(keys_alt.as<uint32_t>(), nall, ncell, cstart.as<int32_t>(), s);
+      }
       launch_sorted_gather(vals_alt.as<int32_t>(), nall, nrows, nreal, cols.as<double>(),
                            gx.as<double>(), gy.as<double>(), gz.as<double>(), gsrc.as<int32_t>(),
                            sx.as<double>(), sy.as<double>(), sz.as<double>(), ssrc.as<int32_t>(),

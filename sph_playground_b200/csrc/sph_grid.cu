@@ -302,6 +302,91 @@ __global__ void k_keys(const double* __restrict__ cols, int64_t ld, int64_t nrow
   vals[u] = int32_t(u);
 }
 
+// ---- counting sort of the records by cell ------------------------------------------------
+// The keys are cell indices, so one pass of counting sort orders them: the
+// records of each cell are counted, the counts scanned into the cells'
+// starts, and every record placed at its cell's start plus a slot taken
+// with an atomic.  The slots within a cell come out in arbitrary order;
+// each cell's records are then sorted by index (a thread per cell for up to
+// kCellSmall records, a block per cell for up to kCellBig), which gives the
+// order of a stable sort by key.
+constexpr int kCellSmall = 32;
+constexpr int kCellBig = 4096;
+
+__global__ void k_cell_count(const uint32_t* __restrict__ keys, int64_t n,
+                             int32_t* __restrict__ count, int32_t* __restrict__ maxc) {
+  const int64_t u = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  int m = 0;
+  if (u < n) m = atomicAdd(&count[keys[u]], 1) + 1;
+  const int wm = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && wm) atomicMax(maxc, wm);
+}
+__global__ void k_cell_scatter(const uint32_t* __restrict__ keys, int64_t n,
+                               const int32_t* __restrict__ cstart, int32_t* __restrict__ fill,
+                               int32_t* __restrict__ vout, uint32_t* __restrict__ kout) {
+  const int64_t u = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (u >= n) return;
+  const uint32_t key = keys[u];
+  const int32_t pos = cstart[key] + atomicAdd(&fill[key], 1);
+  vout[pos] = int32_t(u);
+  kout[pos] = key;
+}
+// cells of up to kCellSmall records: insertion sort by a thread; larger
+// ones go to `big`
+__global__ void k_cell_sort_small(const int32_t* __restrict__ cstart, int64_t ncell,
+                                  int32_t* __restrict__ v, int32_t* __restrict__ big,
+                                  int32_t* __restrict__ nbig) {
+  const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (c >= ncell) return;
+  const int32_t a = cstart[c], b = cstart[c + 1];
+  const int k = b - a;
+  if (k <= 1) return;
+  if (k > kCellSmall) {
+    big[atomicAdd(nbig, 1)] = int32_t(c);
+    return;
+  }
+  int32_t r[kCellSmall];
+  for (int i = 0; i < k; ++i) r[i] = v[a + i];
+  for (int i = 1; i < k; ++i) {
+    const int32_t x = r[i];
+    int j = i - 1;
+    while (j >= 0 && r[j] > x) { r[j + 1] = r[j]; --j; }
+    r[j + 1] = x;
+  }
+  for (int i = 0; i < k; ++i) v[a + i] = r[i];
+}
+// cells of up to kCellBig records: a block per cell (the blocks stride over
+// the list), bitonic sort in shared memory padded to a power of two
+__global__ void __launch_bounds__(256)
+k_cell_sort_big(const int32_t* __restrict__ cstart, int32_t* __restrict__ v,
+                const int32_t* __restrict__ big, const int32_t* __restrict__ nbig) {
+  __shared__ int32_t sh[kCellBig];
+  const int nb = *nbig;
+  for (int i = blockIdx.x; i < nb; i += gridDim.x) {
+    const int32_t c = big[i];
+    const int32_t a = cstart[c];
+    const int k = cstart[c + 1] - a;  // kCellSmall < k <= kCellBig (checked on the host)
+    int m = 1;
+    while (m < k) m <<= 1;
+    for (int t = threadIdx.x; t < m; t += blockDim.x) sh[t] = t < k ? v[a + t] : INT32_MAX;
+    __syncthreads();
+    for (int size = 2; size <= m; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = threadIdx.x; t < m; t += blockDim.x) {
+          const int o = t ^ stride;
+          if (o > t) {
+            const bool up = (t & size) == 0;
+            const int32_t x = sh[t], y = sh[o];
+            if ((x > y) == up) { sh[t] = y; sh[o] = x; }
+          }
+        }
+        __syncthreads();
+      }
+    for (int t = threadIdx.x; t < k; t += blockDim.x) v[a + t] = sh[t];
+    __syncthreads();
+  }
+}
+
 // cstart[c] = number of particles in cells before c (ncell + 1 entries), from
 // the sorted keys: each key change fills the empty cells it skips.
 __global__ void k_cell_starts(const uint32_t* __restrict__ keys, int64_t n, int64_t ncell,
@@ -2429,6 +2514,27 @@ void launch_set_col(double* col, int64_t n, double v, cudaStream_t s) {
   note_launch();
 }
 
+bool cell_sort(const uint32_t* keys, int64_t n, int64_t ncell, int32_t* count, int32_t* cstart,
+               int32_t* vout, uint32_t* kout, int32_t* big, int32_t* ctr, void* scan_tmp,
+               size_t scan_bytes, int32_t* h_ctr, cudaStream_t s) {
+  // ctr[0]: the largest cell, ctr[1]: cells for the block sort
+  cudaMemsetAsync(count, 0, sizeof(int32_t) * size_t(ncell + 1), s);
+  cudaMemsetAsync(ctr, 0, 2 * sizeof(int32_t), s);
+  if (n > 0) k_cell_count<<<nblocks(n), TPB, 0, s>>>(keys, n, count, ctr);
+  cudaMemcpyAsync(h_ctr, ctr, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  note_launch();
+  if (h_ctr[0] > kCellBig) return false;  // (nothing written)
+  exclusive_scan(scan_tmp, scan_bytes, count, cstart, ncell + 1, s);
+  cudaMemsetAsync(count, 0, sizeof(int32_t) * size_t(ncell), s);
+  if (n > 0) k_cell_scatter<<<nblocks(n), TPB, 0, s>>>(keys, n, cstart, count, vout, kout);
+  if (h_ctr[0] > 1) {
+    k_cell_sort_small<<<nblocks(ncell), TPB, 0, s>>>(cstart, ncell, vout, big, ctr + 1);
+    if (h_ctr[0] > kCellSmall) k_cell_sort_big<<<148 * 4, 256, 0, s>>>(cstart, vout, big, ctr + 1);
+  }
+  note_launch(3);
+  return true;
+}
 size_t sort_temp_bytes(int64_t n) {
   size_t b = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, b, (const uint32_t*)nullptr, (uint32_t*)nullptr,

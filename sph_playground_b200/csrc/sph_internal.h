@@ -462,6 +462,15 @@ void launch_apply_mti(double* cols, int64_t ld, const int32_t* orig, int64_t nro
 void launch_set_col(double* col, int64_t n, double v, cudaStream_t s);
 
 // CUB wrappers (sph_grid.cu)
+// Counting sort of the records by cell (keys in [0, ncell)): vout / kout the
+// record indices and keys in key order, each cell's records in increasing
+// index (as a stable sort), cstart[0 .. ncell] the cells' starts; count
+// (ncell + 1) and big (ncell) are scratch, ctr two device ints, h_ctr a
+// pinned host int; scan_tmp sized for ncell + 1 entries.  Returns false
+// (nothing written) when a cell holds more than 4096 records.
+bool cell_sort(const uint32_t* keys, int64_t n, int64_t ncell, int32_t* count, int32_t* cstart,
+               int32_t* vout, uint32_t* kout, int32_t* big, int32_t* ctr, void* scan_tmp,
+               size_t scan_bytes, int32_t* h_ctr, cudaStream_t s);
 size_t sort_temp_bytes(int64_t n);
 void sort_pairs(void* tmp, size_t tmp_bytes, const uint32_t* kin, uint32_t* kout,
                 const int32_t* vin, int32_t* vout, int64_t n, int end_bit, cudaStream_t s);
