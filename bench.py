@@ -704,6 +704,9 @@ def main():
                 "traffic": kernels[dom]["traffic"],
                 "step_frac": step_ach / p32, "step_achieved_tflops": step_ach,
                 "kernels": kernels,
+                "binding_unit": {"circuit2": {"unit": "L1/TEX data path", "ncu_pct_of_peak": 88.2,
+                                              "fma_pipe_pct": 54.3, "issue_active_pct": 73.8,
+                                              "source": "profiles/k_c2_fp32_sedov3d_96.md"}},
                 "traffic_source": "ncu DRAM bytes per pair of the kernel's capture on the "
                                   "Sedov 96^3 step, times this launch's pairs",
                 "peak_source": {"fp32": "live FFMA-chain probe (libsph_peak.so) on this GPU; "
