@@ -46,7 +46,7 @@ struct sph_batch {
     constexpr int kStateTfinish = 11;  // the state slot of tfinish (const.f90 ec_tfinish)
     if (!use_state)
       for (auto* x : h) sph_set_param(x, kStateTfinish, tfinish);
-    run([](sph_handle* x) { return sph_step(x, 0); });
+    run([](sph_handle* x) { return sph::start_for_device_loop(x); });
     std::vector<int> st0 = status;
     std::vector<std::string> msg0 = msg;
     std::fill(status.begin(), status.end(), 0);

@@ -190,6 +190,9 @@ struct sph_handle {
   // between sph_predict and sph_correct of a split step: the rows keep their
   // physical order (the predictor's saves are per physical row)
   bool in_split_step = false;
+  // the start-up iterate of an instance joining the batch device loop, which
+  // searches afresh every iterate: lists built then would serve none
+  bool skin_suspended = false;
   DevBuf colbuf;  // staging of sph_get_columns / sph_set_columns
   // skin lists (SPH_P_SKIN): the lists of the last skin search (CSR like nl),
   // the records' positions and the centres' h at that search, the rows'
@@ -678,6 +681,7 @@ struct sph_handle {
   // centres the filter cannot vouch for) until the records have moved too
   // far, an image set changes or too many centres need the fresh search.
   double skin_fraction() const {
+    if (skin_suspended) return 0.0;
     const double v = st[SPH_P_SKIN];
     return v > 0 ? std::min(v, 1.0) : 0.0;
   }
@@ -2954,4 +2958,13 @@ void sph_destroy(sph_handle* h) {
 
 namespace sph {
 int handle_device(const sph_handle* h) { return h->dev; }
+
+int start_for_device_loop(sph_handle* h) {
+  if (!h) return sph_fail(SPH_ERR_ARG, "null handle");
+  if (h->started) return sph_step(h, 0);
+  h->skin_suspended = true;
+  const int rc = sph_step(h, 0);
+  h->skin_suspended = false;
+  return rc;
+}
 }  // namespace sph

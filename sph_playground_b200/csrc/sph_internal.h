@@ -104,6 +104,10 @@ void batch_graph_destroy(BatchGraph* bg);
 int sph_fail(int code, const std::string& msg);
 // The device a handle was created on.
 int handle_device(const sph_handle* h);
+// sph_step(h, 0) for an instance about to join the batch device loop: its
+// start-up iterate (if it has not run) builds no skin lists, which the
+// loop's fresh searches would drop unused.
+int start_for_device_loop(sph_handle* h);
 
 // Count of this library's kernel launches (process-wide).
 void note_launch(int n = 1);
