@@ -351,10 +351,12 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
           double eps = newton_update<DIM>(ha, ha0, ma, P.hfac, wsum, osum, rho, om, hn);
           if (hn <= 0.) raise_status(a.status, SPH_ERR_H_NEG);
           if constexpr (sizeof(R) == 4) {
-            // FP32 noise floor, as in k_c1_newton: a stagnating eps below 1e-7
-            // counts as converged
+            // FP32 noise floor, as in k_c1_newton: an eps below 1e-7 on the
+            // first sweep, or a stagnating one later, counts as converged
+            // (a table at rest otherwise takes 2-3 sweeps per iterate that
+            // move h only within the FP32 sums' noise)
             const double eps_prev = a.eps[p];
-            if (eps > P.tol && eps < 1e-7 && eps >= 0.5 * eps_prev) eps = 0.0;
+            if (eps > P.tol && eps < 1e-7 && (a.first || eps >= 0.5 * eps_prev)) eps = 0.0;
           }
           a.eps[p] = eps;
           a.dkp1[p] = rho;

@@ -1286,6 +1286,7 @@ struct sph_handle {
             iter == 1 ? nullptr : rb + ((iter - 1) % 2 ? RED_C1_ACTIVE : RED_C1_ACTIVE2);
         a.active_slot = iter % 2 ? RED_C1_ACTIVE : RED_C1_ACTIVE2;
         a.gate = gate;
+        a.first = iter == 1;
         launch_c1_snapshot(nall_cap, ssrc.as<int32_t>(), hkp1.as<double>(), dkp1.as<double>(),
                            okp1.as<double>(), hk_s.as<double>(), dk_s.as<double>(),
                            ok_s.as<double>(), s, dplan, gate);
@@ -1300,6 +1301,7 @@ struct sph_handle {
     } else
     for (;;) {
       ++iter;
+      a.first = iter == 1;
       launch_c1_snapshot(nall, ssrc.as<int32_t>(), hkp1.as<double>(), dkp1.as<double>(),
                          okp1.as<double>(), hk_s.as<double>(), dk_s.as<double>(),
                          ok_s.as<double>(), s);

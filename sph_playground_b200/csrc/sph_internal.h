@@ -508,6 +508,7 @@ struct C1Args {
   unsigned long long* red;
   int active_slot;                  // red slot the sweep marks when a particle stays active
   const unsigned long long* gate;   // if set and zero, the sweep has nothing to do
+  int first;                        // the iterate's first sweep
 };
 void launch_c1_newton(int prec, int kernel, int dim, const C1Args& a, PackBufs pb, Params P,
                       cudaStream_t s);
