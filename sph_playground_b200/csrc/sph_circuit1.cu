@@ -356,7 +356,8 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
             // (a table at rest otherwise takes 2-3 sweeps per iterate that
             // move h only within the FP32 sums' noise)
             const double eps_prev = a.eps[p];
-            if (eps > P.tol && eps < 1e-7 && (a.first || eps >= 0.5 * eps_prev)) eps = 0.0;
+            const bool first = a.iter_dev ? *a.iter_dev == 0 : a.first != 0;
+            if (eps > P.tol && eps < 1e-7 && (first || eps >= 0.5 * eps_prev)) eps = 0.0;
           }
           a.eps[p] = eps;
           a.dkp1[p] = rho;

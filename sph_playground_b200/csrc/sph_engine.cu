@@ -21,6 +21,8 @@
 
 #include "sph_internal.h"
 
+#include <chrono>
+
 using namespace sph;
 
 namespace {
@@ -227,6 +229,14 @@ struct sph_handle {
   bool skin_trace = std::getenv("SPH_SKIN_TRACE") != nullptr;
   int64_t kept_pairs = 0;    // neighbour pairs of the rows kept (counted as found)
   const DevPlan* dplan = nullptr;  // set while a device-resident step is built
+  // skin lists of the device-resident step (DevSkin, device memory): they
+  // share the host lists' buffers; dlists_ok = nothing on the host has
+  // touched the records, rows or lists since the last device-resident run
+  // (else the next one starts without lists)
+  DevBuf dskin;
+  bool dlists_ok = false;
+  DevBuf c1_iter;  // the sweep count of the device-resident Newton loop
+  cudaStream_t cap_s = nullptr;  // captures the bodies of conditional nodes
   int64_t nghost_cap = 0, nall_cap = 0;
   int end_bit_cap = 0;
   // captured steps, one per table pointer pair: a row reorder swaps the
@@ -545,6 +555,7 @@ struct sph_handle {
   // ---- physical re-ordering of the rows (locality of the pair loops) ---------------------
   int reorder_rows() {
     if (!have_order || in_split_step || rows_in_order) return SPH_OK;
+    dlists_ok = false;  // (the device-resident lists are not renamed)
     // perm = real rows in cell order, then the fixed rows as they are
     int32_t* perm = cpos.as<int32_t>();
     CK(cudaMemcpyAsync(perm, centre_p.p, sizeof(int32_t) * nreal, cudaMemcpyDeviceToDevice, s));
@@ -685,7 +696,8 @@ struct sph_handle {
     const double v = st[SPH_P_SKIN];
     return v > 0 ? std::min(v, 1.0) : 0.0;
   }
-  int skin_alloc(int64_t nall) {
+  // the buffers of both paths' lists (the device-resident step needs no more)
+  int skin_alloc_common(int64_t nall) {
     RC(skin_rowoff.ensure(sizeof(int64_t) * nreal));
     RC(skin_rowcap.ensure(sizeof(int32_t) * nreal));
     RC(skin_rowcap64.ensure(sizeof(int64_t) * nreal));
@@ -693,18 +705,22 @@ struct sph_handle {
     RC(skin_count_prev.ensure(sizeof(int32_t) * nrows));
     RC(skin_h_prev.ensure(sizeof(float) * nrows));
     RC(skin_hb.ensure(sizeof(double) * nreal));
-    RC(skin_dflag.ensure(sizeof(int32_t) * (nreal + 1)));
-    RC(skin_dpos.ensure(sizeof(int32_t) * (nreal + 1)));
-    RC(skin_dlist.ensure(sizeof(int32_t) * nreal));
     RC(skin_sig.ensure(sizeof(uint8_t) * nrows));
     RC(skin_bx.ensure(sizeof(double) * nall));
     RC(skin_by.ensure(sizeof(double) * nall));
     RC(skin_bz.ensure(sizeof(double) * nall));
     RC(skin_dsp.ensure(sizeof(float) * nall));
+    RC(skin_hrec.ensure(sizeof(double) * nall));
+    return SPH_OK;
+  }
+  int skin_alloc(int64_t nall) {
+    RC(skin_alloc_common(nall));
+    RC(skin_dflag.ensure(sizeof(int32_t) * (nreal + 1)));
+    RC(skin_dpos.ensure(sizeof(int32_t) * (nreal + 1)));
+    RC(skin_dlist.ensure(sizeof(int32_t) * nreal));
     RC(skin_gap.ensure(sizeof(float) * nreal));
     RC(skin_hdev.ensure(sizeof(double) * nreal));
     RC(skin_mode.ensure(sizeof(uint8_t) * nreal));
-    RC(skin_hrec.ensure(sizeof(double) * nall));
     RC(skin_ways.ensure(sizeof(int64_t) * (nreal + 1)));
     RC(skin_wpos.ensure(sizeof(int64_t) * (nreal + 1)));
     RC(skin_flist.ensure(sizeof(int32_t) * nreal));
@@ -1050,6 +1066,7 @@ struct sph_handle {
       if (served) return SPH_OK;
     }
     skin_valid = false;
+    dlists_ok = false;
     if (skin_live) {
       // the lists ended (here or by a change of the table or parameters);
       // short-lived ones start a pause of plain searches
@@ -1273,31 +1290,40 @@ struct sph_handle {
     launch_set_col(epsb.as<double>(), nrows, 1.0, s);
     int iter = 0;
     if (dplan) {
-      // device-resident step: a fixed number of sweeps without looking at
-      // the host; a particle that converged skips the later sweeps, so the
-      // result equals the host loop's as long as all converge within them
-      // (otherwise the error word sends the step back to the host path)
-      // (sweep k marks slot k % 2; sweep k + 1 and its snapshot do nothing
-      // once that slot stays zero)
-      const int sweeps = a.simple ? 1 : std::max(1, std::min(P.maxiter, kDrsSweeps));
+      // device-resident step: the sweeps as a while node, as many as the
+      // particles need (up to kDrsSweeps) without looking at the host; a
+      // particle still active after the last of fewer than maxiter sweeps
+      // sets the error word, which sends the step back to the host path
       unsigned long long* rb = red.as<unsigned long long>();
-      for (iter = 1; iter <= sweeps; ++iter) {
-        const unsigned long long* gate =
-            iter == 1 ? nullptr : rb + ((iter - 1) % 2 ? RED_C1_ACTIVE : RED_C1_ACTIVE2);
-        a.active_slot = iter % 2 ? RED_C1_ACTIVE : RED_C1_ACTIVE2;
-        a.gate = gate;
-        a.first = iter == 1;
-        launch_c1_snapshot(nall_cap, ssrc.as<int32_t>(), hkp1.as<double>(), dkp1.as<double>(),
-                           okp1.as<double>(), hk_s.as<double>(), dk_s.as<double>(),
-                           ok_s.as<double>(), s, dplan, gate);
-        launch_fill_u64(rb + a.active_slot, 1, 0ull, s);
-        launch_c1_sweep(prec, kernel_id, P.dim, a, pb, P, s);
-      }
-      --iter;
-      if (!a.simple && sweeps < P.maxiter)
-        launch_flag_if_nonzero(rb + a.active_slot, drs_err.as<int>(), SPH_ERR_STATE, s);
       a.active_slot = RED_C1_ACTIVE;
       a.gate = nullptr;
+      auto sweep = [&]() {
+        launch_c1_snapshot(nall_cap, ssrc.as<int32_t>(), hkp1.as<double>(), dkp1.as<double>(),
+                           okp1.as<double>(), hk_s.as<double>(), dk_s.as<double>(),
+                           ok_s.as<double>(), s, dplan, nullptr);
+        launch_fill_u64(rb + RED_C1_ACTIVE, 1, 0ull, s);
+        launch_c1_sweep(prec, kernel_id, P.dim, a, pb, P, s);
+      };
+      if (a.simple) {
+        a.first = 1;
+        sweep();
+        iter = 1;
+      } else {
+        const int sweeps = std::max(1, std::min(P.maxiter, kDrsSweeps));
+        int* itd = c1_iter.as<int>();
+        a.iter_dev = itd;
+        RC(capture_cond(
+            cudaGraphCondTypeWhile,
+            [&](cudaGraphConditionalHandle hw) { launch_sweeps_init(itd, hw, s); },
+            [&](cudaGraphConditionalHandle hw) {
+              sweep();
+              launch_sweeps_ctl(itd, rb + RED_C1_ACTIVE, sweeps, P.maxiter, drs_err.as<int>(), hw,
+                                s);
+              return SPH_OK;
+            }));
+        a.iter_dev = nullptr;
+        iter = sweeps;
+      }
     } else
     for (;;) {
       ++iter;
@@ -1390,11 +1416,130 @@ struct sph_handle {
   // table saved at its start.  With no host round trip inside, one step is
   // captured as a CUDA graph and replayed.
 
+  // Adds an if node after the work captured so far on s: `pre(handle)`
+  // captures the kernel that sets the handle, then `body` is captured into
+  // the node's body graph (its launches go to s while it runs).
+  template <class Pre, class Body>
+  int capture_if(Pre&& pre, Body&& body) {
+    return capture_cond(cudaGraphCondTypeIf, pre, body);
+  }
+  // the same with a while node: the body runs again while the handle is
+  // non-zero after it (a kernel in the body sets it)
+  template <class Pre, class Body>
+  int capture_cond(cudaGraphConditionalNodeType type, Pre&& pre, Body&& body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(SPH_ERR_STATE, "if node outside a capture");
+    cudaGraphConditionalHandle hnd;
+    CK(cudaGraphConditionalHandleCreate(&hnd, g, 0, 0));
+    pre(hnd);
+    CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hnd;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    if (!cap_s) CK(cudaStreamCreateWithFlags(&cap_s, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCaptureToGraph(cap_s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    std::swap(s, cap_s);
+    const int rc = body(hnd);
+    std::swap(s, cap_s);
+    cudaGraph_t out;
+    const cudaError_t e = cudaStreamEndCapture(cap_s, &out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(SPH_ERR_CUDA, std::string("if node body: ") + cudaGetErrorString(e));
+    return SPH_OK;
+  }
+
+  // The device-resident step's neighbour phase.  Without skin lists: images,
+  // sort, centres and the search, every iterate (search_dev).  With them
+  // (SPH_P_SKIN > 0): the records' positions refreshed in the lists' sorted
+  // order, every centre checked against its list, and the search only when
+  // the device decides so (an if node: a skin search, or a plain one in a
+  // pause after short-lived lists); every centre's row is then its list's
+  // records that pass the FP64 predicate.  No host decision either way.
   int neighbour_phase_dev(const Mode& m, const Params& P) {
-    skin_valid = false;  // the device-resident step sorts afresh
+    skin_valid = false;  // (the host path's lists)
+    const double skin = skin_fraction();
+    if (!(skin > 0)) return search_dev(m, P, false);
     const int d = P.dim;
     BoxGeom g = box(m);
     if (m.ghosts) launch_reflect(cols.as<double>(), nrows, nreal, g, s);
+    BoxGeom gg = g;
+    if (!m.ghosts) for (int k = 0; k < 3; ++k) gg.periodic[k] = 0;
+    unsigned long long* rb = red.as<unsigned long long>();
+    DevSkin* ds = dskin.as<DevSkin>();
+    DevPlan* plan = drs_plan.as<DevPlan>();
+    SlotInit si{};
+    for (int k = 0; k < 3; ++k) {
+      si.off[si.n] = RED_LO_X + k; si.val[si.n++] = dkey(1e308);
+      si.off[si.n] = RED_HI_X + k; si.val[si.n++] = dkey(-1e308);
+    }
+    si.off[si.n] = RED_SKIN_D; si.val[si.n++] = dkey(0.0);
+    si.off[si.n] = RED_SKIN_HMAX; si.val[si.n++] = dkey(0.0);
+    si.off[si.n] = RED_DSKIN_FAIL; si.val[si.n++] = 0ull;
+    si.off[si.n] = RED_SKIN_SIG; si.val[si.n++] = 0ull;
+    launch_init_slots(rb, si, s);
+    launch_skin_refresh(vals_alt.as<int32_t>(), nall_cap, nrows, nreal, cols.as<double>(),
+                        gsrc.as<int32_t>(), gcode.as<int8_t>(), gg, d, skin_sig.as<uint8_t>(),
+                        skin_bx.as<double>(), skin_by.as<double>(), skin_bz.as<double>(),
+                        sx.as<double>(), sy.as<double>(), sz.as<double>(), s32.as<float4>(),
+                        PackGeom{}, skin_dsp.as<float>(), 0.f, 0.f, skin_hrec.as<double>(), rb, s,
+                        plan, ds);
+    launch_dskin_check(nreal, centre_p.as<int32_t>(), col(es_h), skin_hb.as<double>(), P.krad, ds,
+                       rb, s);
+    RC(capture_if(
+        [&](cudaGraphConditionalHandle hs) {
+          launch_dskin_decide(ds, rb, plan, P.krad, skin, kSkinShort, kSkinPause0, kSkinPauseMax,
+                              hs, dcnt.as<unsigned long long>(), s);
+        },
+        [&](cudaGraphConditionalHandle) { return search_dev(m, P, true); }));
+    // every centre's row from its skin list
+    SkinFilterArgs f{};
+    f.nc = nreal;
+    f.centre_k = centre_k.as<int32_t>();
+    f.centre_p = centre_p.as<int32_t>();
+    f.skin_off = skin_rowoff.as<int64_t>();
+    f.skin_cnt = skin_cnt.as<int32_t>();
+    f.skin_nl = skin_nl.as<int32_t>();
+    f.sx = sx.as<double>(); f.sy = sy.as<double>(); f.sz = sz.as<double>();
+    f.s32 = s32.as<float4>();
+    f.hcol = col(es_h);
+    f.krad = P.krad;
+    f.rowoff = rowoff.as<int64_t>();
+    f.rowcap = rowcap.as<int32_t>();
+    f.nl_size = nl_size;
+    f.nl = nl.as<int32_t>();
+    f.ncnt = ncnt.as<int32_t>();
+    f.orig = orig.as<int32_t>();
+    f.count_prev = count_prev.as<int32_t>();
+    f.h_prev = h_prev.as<float>();
+    f.maxcnt = maxcnt.as<int32_t>();
+    f.overflow = overflow.as<int32_t>();
+    f.dcnt = dcnt.as<unsigned long long>();
+    f.plan = plan;
+    f.skin_cap = skin_rowcap.as<int32_t>();
+    f.skin_size = skin_nl_size;
+    launch_skin_filter(f, s);
+    CK(cudaGetLastError());
+    return SPH_OK;
+  }
+
+  // images, keys, sort, centres and the search of the device-resident step;
+  // skin: the search of skin lists (radius factor from the device, into the
+  // skin table), what later iterates compare against, and the layout of the
+  // rows filtered from them (the positions are already wrapped)
+  int search_dev(const Mode& m, const Params& P, bool skin) {
+    const int d = P.dim;
+    BoxGeom g = box(m);
+    if (m.ghosts && !skin) launch_reflect(cols.as<double>(), nrows, nreal, g, s);
     SlotInit si{};
     for (int k = 0; k < 3; ++k) {
       si.off[si.n] = RED_LO_X + k; si.val[si.n++] = dkey(1e308);
@@ -1437,10 +1582,18 @@ struct sph_handle {
                    nall_cap + 1, s);
     launch_centres(vals_alt.as<int32_t>(), cflag.as<int32_t>(), cpos.as<int32_t>(), nall_cap,
                    centre_k.as<int32_t>(), centre_p.as<int32_t>(), s);
-    launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(), count_prev.as<int32_t>(),
-                  h_prev.as<float>(), col(es_h), d, 1.2f, rowcap64.as<int64_t>(),
-                  rowcap.as<int32_t>(), s);
-    exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, rowcap64.as<int64_t>(), rowoff.as<int64_t>(),
+    // (the skin table's rows: their last counts, plain or skin, with room
+    // for a skin search after a plain one)
+    const float slack = skin ? float(1.2 * std::pow(1.0 + skin_fraction(), double(d))) : 1.2f;
+    DevBuf& t_cap = skin ? skin_rowcap : rowcap;
+    DevBuf& t_cap64 = skin ? skin_rowcap64 : rowcap64;
+    DevBuf& t_off = skin ? skin_rowoff : rowoff;
+    DevBuf& t_cp = skin ? skin_count_prev : count_prev;
+    DevBuf& t_hp = skin ? skin_h_prev : h_prev;
+    launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(), t_cp.as<int32_t>(),
+                  t_hp.as<float>(), col(es_h), d, slack, t_cap64.as<int64_t>(),
+                  t_cap.as<int32_t>(), s);
+    exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, t_cap64.as<int64_t>(), t_off.as<int64_t>(),
                      nreal, s);
     NeibArgs na{};
     na.plan = plan;
@@ -1452,18 +1605,42 @@ struct sph_handle {
     na.hcol = col(es_h);
     na.krad = P.krad;
     na.cstart = cstart.as<int32_t>();
-    na.rowoff = rowoff.as<int64_t>();
-    na.rowcap = rowcap.as<int32_t>();
-    na.nl_size = nl_size;
-    na.nl = nl.as<int32_t>();
-    na.ncnt = ncnt.as<int32_t>();
+    na.rowoff = t_off.as<int64_t>();
+    na.rowcap = t_cap.as<int32_t>();
+    na.nl_size = skin ? skin_nl_size : nl_size;
+    na.nl = skin ? skin_nl.as<int32_t>() : nl.as<int32_t>();
+    na.ncnt = skin ? skin_cnt.as<int32_t>() : ncnt.as<int32_t>();
     na.orig = orig.as<int32_t>();
-    na.count_prev = count_prev.as<int32_t>();
-    na.h_prev = h_prev.as<float>();
+    na.count_prev = t_cp.as<int32_t>();
+    na.h_prev = t_hp.as<float>();
     na.maxcnt = maxcnt.as<int32_t>();
     na.overflow = overflow.as<int32_t>();
     na.dcnt = dcnt.as<unsigned long long>();
+    if (skin) {
+      DevSkin* ds = dskin.as<DevSkin>();
+      na.kfac_dev = &ds->kfac;
+      na.skin_search = 1;
+    }
     launch_neighbours(d, lanes_search(), st[SPH_P_SEARCH_STAGED] != 0, na, s);
+    if (skin) {
+      // what the next iterates compare against: positions, centres' h and
+      // the rows' image signatures of this search; no displacement yet
+      unsigned long long* rb = red.as<unsigned long long>();
+      CK(cudaMemcpyAsync(skin_bx.p, sx.p, sizeof(double) * nall_cap, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(skin_by.p, sy.p, sizeof(double) * nall_cap, cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(skin_bz.p, sz.p, sizeof(double) * nall_cap, cudaMemcpyDeviceToDevice, s));
+      launch_gather_h(nreal, centre_p.as<int32_t>(), col(es_h), skin_hb.as<double>(), rb,
+                      RED_SKIN_HMAXB, s);
+      launch_skin_sig(cols.as<double>(), nrows, gg, d, skin_sig.as<uint8_t>(), s);
+      CK(cudaMemsetAsync(skin_dsp.p, 0, sizeof(float) * nall_cap, s));
+      launch_dskin_built(dskin.as<DevSkin>(), rb, s);
+      // the rows filtered from the lists: their last counts
+      launch_rowcap(nreal, centre_p.as<int32_t>(), orig.as<int32_t>(), count_prev.as<int32_t>(),
+                    h_prev.as<float>(), col(es_h), d, 1.2f, rowcap64.as<int64_t>(),
+                    rowcap.as<int32_t>(), s);
+      exclusive_scan64(scan64_tmp.p, scan64_tmp.bytes, rowcap64.as<int64_t>(),
+                       rowoff.as<int64_t>(), nreal, s);
+    }
     CK(cudaGetLastError());
     return SPH_OK;
   }
@@ -1517,9 +1694,37 @@ struct sph_handle {
     RC(drs_plan.ensure(sizeof(DevPlan)));
     RC(drs_clock.ensure(sizeof(DevClock)));
     RC(drs_err.ensure(sizeof(int)));
+    RC(c1_iter.ensure(sizeof(int)));
     RC(drs_save.ensure(sizeof(double) * NCOL * size_t(nrows)));
     RC(bclk_save.ensure(sizeof(DevClock)));
     if (eq_sts) RC(stsY.ensure(sizeof(double) * 6 * nrows));
+    const double skin = skin_fraction();
+    if (skin > 0) {
+      // the device-resident lists: the host lists' buffers at the device
+      // step's capacities, the skin table sized for the rows search_dev lays
+      // out (last counts x 1.2 (1 + s)^d, counts up to (1 + s)^d those of
+      // the exact rows)
+      RC(skin_alloc_common(nall_cap));
+      RC(dskin.ensure(sizeof(DevSkin)));
+      const double kf = std::pow(1.0 + skin, double(dim()));
+      const int64_t need = int64_t(double(nl_size) * kf * kf * 1.05) + 16 * nreal;
+      if (need > skin_nl_size) {
+        RC(skin_nl.ensure(sizeof(int32_t) * size_t(need)));
+        skin_nl_size = need;
+      }
+      if (skin_est <= 0) {
+        skin_est = int(est_count * kf) + 8;
+        launch_fill_i32(skin_count_prev.as<int32_t>(), nrows, skin_est, s);
+        CK(cudaMemsetAsync(skin_h_prev.p, 0, sizeof(float) * nrows, s));
+      }
+    }
+    return SPH_OK;
+  }
+  // before a device-resident run: it starts without lists when the host has
+  // touched the records, rows or lists since the last one
+  int dlists_reset(cudaStream_t st_) {
+    if (skin_fraction() > 0 && !dlists_ok)
+      CK(cudaMemsetAsync(dskin.p, 0, sizeof(DevSkin), st_));
     return SPH_OK;
   }
 
@@ -1628,6 +1833,7 @@ struct sph_handle {
       gs->k_cols = cols.p;
       gs->k_orig = orig.p;
     }
+    RC(dlists_reset(s));
     CK(cudaGraphLaunch(gs->x, s));
     // one read-back per step: the clock, the error words
     CK(cudaMemcpyAsync(h_ctrl + 1, drs_clock.p, sizeof(DevClock), cudaMemcpyDeviceToHost, s));
@@ -1655,7 +1861,9 @@ struct sph_handle {
     pgeom = h_plan->pg;
     cnt_host[SPH_CNT_STEPS]++;
     cnt_host[SPH_CNT_ITERATES] += eq_sts ? 1 + ival(ec_stsfixeds) : 1;
-    cnt_host[SPH_CNT_SEARCHES] += eq_sts ? 1 + ival(ec_stsfixeds) : 1;
+    // (with skin lists the device counts its searches)
+    if (!(skin_fraction() > 0)) cnt_host[SPH_CNT_SEARCHES] += eq_sts ? 1 + ival(ec_stsfixeds) : 1;
+    dlists_ok = true;
     steps_since_reorder++;
     cnt_host[SPH_CNT_GRAPH_STEPS]++;
     return SPH_OK;
@@ -1670,7 +1878,8 @@ struct sph_handle {
   int batch_step_body(BatchInst* b) {
     launch_inst_begin(b, drs_clock.as<DevClock>(), bclk_save.as<DevClock>(), s);
     launch_reorder_gated(b, cols.as<double>(), cols_alt.as<double>(), orig.as<int32_t>(),
-                         orig_alt.as<int32_t>(), centre_p.as<int32_t>(), nreal, nrows, s);
+                         orig_alt.as<int32_t>(), centre_p.as<int32_t>(), nreal, nrows,
+                         skin_fraction() > 0 ? dskin.as<DevSkin>() : nullptr, s);
     RC(copy_table(drs_save.p, cols.p));
     RC(step_body_dev());
     launch_inst_end(b, drs_err.as<int>(), overflow.as<int32_t>(), status.as<int>(), s);
@@ -1701,7 +1910,7 @@ struct sph_handle {
     const long long per = eq_sts ? 1 + ival(ec_stsfixeds) : 1;
     cnt_host[SPH_CNT_STEPS] += steps;
     cnt_host[SPH_CNT_ITERATES] += steps * per;
-    cnt_host[SPH_CNT_SEARCHES] += steps * per;
+    if (!(skin_fraction() > 0)) cnt_host[SPH_CNT_SEARCHES] += steps * per;
     cnt_host[SPH_CNT_GRAPH_STEPS] += steps;
   }
 
@@ -1914,7 +2123,7 @@ struct sph_handle {
   }
   size_t table_bytes() const { return sizeof(double) * NCOL * size_t(nrows); }
   int copy_table(void* dst, const void* src) {
-    if (dst == cols.p) skin_valid = false;  // the records' positions jump
+    if (dst == cols.p) skin_valid = dlists_ok = false;  // the records' positions jump
     CK(cudaMemcpyAsync(dst, src, table_bytes(), cudaMemcpyDeviceToDevice, s));
     return SPH_OK;
   }
@@ -2185,6 +2394,7 @@ struct sph_handle {
     if (h_red) cudaFreeHost(h_red);
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (h_i32) cudaFreeHost(h_i32);
+    if (cap_s) cudaStreamDestroy(cap_s);
     if (s) cudaStreamDestroy(s);
   }
 };
@@ -2326,8 +2536,14 @@ struct BatchGraph {
     CK(cudaMemcpyAsync(ifh.p, hh.data(), sizeof(cudaGraphConditionalHandle) * n,
                        cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
+    const auto ti = std::chrono::steady_clock::now();
     e = cudaGraphInstantiate(&x, g, 0);
     if (e != cudaSuccess) return bad(e, "instantiate");
+    static const bool trace = std::getenv("SPH_BATCH_TRACE") != nullptr;
+    if (trace)
+      std::fprintf(stderr, "batch loop instantiated in %.1f ms\n",
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ti)
+                       .count());
     members = hs;
     marks.clear();
     for (auto* h : hs) marks.push_back(mark_of(h));
@@ -2404,7 +2620,16 @@ int batch_graph_run(BatchGraph** pbg, sph_handle* const* hs_in, int n, double tf
     if (!any) break;
     std::vector<sph_handle*> lh;
     for (int i : live) lh.push_back(hs[i]);
-    if (bg->stale(lh)) RC(bg->build(lh));
+    // (SPH_BATCH_TRACE in the environment: the loop's build times, on stderr)
+    static const bool trace = std::getenv("SPH_BATCH_TRACE") != nullptr;
+    if (bg->stale(lh)) {
+      const auto t0 = std::chrono::steady_clock::now();
+      RC(bg->build(lh));
+      if (trace)
+        std::fprintf(stderr, "batch loop built for %zu instances in %.1f ms\n", lh.size(),
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                         .count());
+    }
     const int m = int(live.size());
     BatchInst* dbi = bg->bi.as<BatchInst>();
     bg->hbi.assign(m, BatchInst{});
@@ -2419,6 +2644,7 @@ int batch_graph_run(BatchGraph** pbg, sph_handle* const* hs_in, int n, double tf
       h->upload_clock(tf[i]);
       CK(cudaMemcpyAsync(h->drs_clock.p, h->h_ctrl + 1, sizeof(DevClock), cudaMemcpyHostToDevice,
                          bg->s));
+      RC(h->dlists_reset(bg->s));
     }
     CK(cudaMemcpyAsync(dbi, bg->hbi.data(), sizeof(BatchInst) * m, cudaMemcpyHostToDevice, bg->s));
     CK(cudaMemsetAsync(bg->iter.p, 0, sizeof(int), bg->s));
@@ -2440,6 +2666,7 @@ int batch_graph_run(BatchGraph** pbg, sph_handle* const* hs_in, int n, double tf
       done_steps[i] += b.steps;
       if (!b.failed) {
         h->adopt_loop(clk, *h->h_plan, b.steps, b.since);
+        h->dlists_ok = true;
         continue;
       }
       // the steps before the failed one stand; the failed one is redone on
@@ -2573,7 +2800,7 @@ int sph_set_param(sph_handle* h, int index, double value) {
       case SPH_P_REORDER_EVERY: case ec_tfinish: case ec_dtprint: case ec_time:
         break;
       default:
-        h->skin_valid = false;
+        h->skin_valid = h->dlists_ok = false;
     }
   }
   h->st[index] = value;
@@ -2607,6 +2834,7 @@ int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
     CK(cudaMemsetAsync(h->skin_flag.p, 0, sizeof(int32_t), h->s));
   }
   CK(cudaMemcpyAsync(h->staging.p, store, sizeof(double) * NCOL * n_rows, cudaMemcpyHostToDevice, h->s));
+  h->dlists_ok = false;
   launch_upload_store(h->staging.as<double>(), h->cols.as<double>(), h->orig.as<int32_t>(), n_rows, h->s);
   if (keep) {
     launch_inverse(h->skin_inv.as<int32_t>(), n_rows, h->skin_perm.as<int32_t>(), h->s);
@@ -2869,7 +3097,7 @@ int sph_set_columns(sph_handle* h, const int* fields, int nf, const double* in) 
   // skin lists follow moved positions and changed h by themselves (the next
   // iterate measures both); a changed particle type may change the image set
   for (int k = 0; k < fs.n; ++k)
-    if (fs.f[k] == es_type) h->skin_valid = false;
+    if (fs.f[k] == es_type) h->skin_valid = h->dlists_ok = false;
   CK(cudaStreamSynchronize(h->s));
   CK(cudaGetLastError());
   return SPH_OK;
@@ -2890,6 +3118,9 @@ int sph_get_counters(sph_handle* h, int64_t* out, int n) {
   all[SPH_CNT_C1_CENTRE_SWEEPS] = int64_t(d[DC_C1_CENTRE_SWEEPS]);
   all[SPH_CNT_LAUNCHES] = int64_t(launches_so_far() - h->launch_base);
   all[SPH_CNT_EXACT_TESTS] = int64_t(d[DC_EXACT_TESTS]);
+  all[SPH_CNT_SEARCHES] += int64_t(d[DC_SEARCHES]);
+  all[SPH_CNT_SKIN_BUILDS] += int64_t(d[DC_SKIN_BUILDS]);
+  all[SPH_CNT_SKIN_REUSES] += int64_t(d[DC_SKIN_REUSES]);
   for (int k = 0; k < n && k < SPH_CNT_TOTAL; ++k) out[k] = all[k];
   return SPH_OK;
 }

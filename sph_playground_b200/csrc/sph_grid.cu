@@ -661,7 +661,8 @@ k_neighbours(NeibArgs a) {
     xi = a.sx[k]; yi = a.sy[k]; zi = a.sz[k];
     pi = a.s32[k];
     double kh = __dmul_rn(a.krad, a.hcol[p]);
-    if (a.kfac > 0.0 && a.kfac != 1.0) kh = __dmul_rn(kh, a.kfac);  // a skin search
+    const double kf = a.kfac_dev ? *a.kfac_dev : a.kfac;
+    if (kf > 0.0 && kf != 1.0) kh = __dmul_rn(kh, kf);  // a skin search
     R2 = __dmul_rn(kh, kh);
     const double R = sqrt(R2) * (1.0 + 1e-9) + 1e-300;
     const double er = (shift * 1.1920928955078125e-7) / R;  // per-axis image error / R
@@ -1004,7 +1005,13 @@ k_skin_refresh(const int32_t* __restrict__ sidx, int64_t n, int64_t nrows, int64
                const double* __restrict__ by, const double* __restrict__ bz,
                double* __restrict__ sx, double* __restrict__ sy, double* __restrict__ sz,
                float4* __restrict__ s32, PackGeom pg, float* __restrict__ dsp, float tau,
-               float eps, double* __restrict__ hrec, unsigned long long* __restrict__ red) {
+               float eps, double* __restrict__ hrec, unsigned long long* __restrict__ red,
+               const DevPlan* __restrict__ plan, const DevSkin* __restrict__ gate) {
+  if (gate && !gate->live) return;
+  if (plan) {
+    n = plan->nall;
+    pg = plan->pg;
+  }
   // slots: lo x, y, z (min), hi x, y, z (max), D (max), h of the real rows (max)
   double v[8] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 0.0, 0.0};
   const bool is_max[8] = {false, false, false, true, true, true, true, true};
@@ -1212,6 +1219,7 @@ k_gather_h(int64_t nc, const int32_t* __restrict__ centre_p, const double* __res
 template <int G>
 __global__ void __launch_bounds__(128) k_skin_filter(SkinFilterArgs a) {
   constexpr unsigned FULL = 0xffffffffu;
+  if (a.plan) a.shift = a.plan->pg.shift;
   constexpr int V = 4;
   constexpr int PER = G * V;
   constexpr int CPB = 128 / G;  // centres per block and pass
@@ -1225,7 +1233,7 @@ __global__ void __launch_bounds__(128) k_skin_filter(SkinFilterArgs a) {
     bool active = i < a.nc;
     if (a.list) {
       c = active ? a.list[i] : 0;  // (the list holds the centres that filter)
-    } else if (active) {
+    } else if (active && a.mode) {
       const uint8_t w = a.mode[c];
       active = w == 0 || (w == 2 && !a.keep);
     }
@@ -1251,6 +1259,11 @@ __global__ void __launch_bounds__(128) k_skin_filter(SkinFilterArgs a) {
       lo_thr = float(R2 * (1.0 - delta));
       hi_thr = float(R2 * (1.0 + delta));
       n = a.skin_cnt[c];
+      if (a.skin_cap) {
+        const int64_t sroom = a.skin_size - a.skin_off[c];
+        const int scap = sroom <= 0 ? 0 : int(min(int64_t(a.skin_cap[c]), sroom));
+        n = min(n, scap);
+      }
       src = reinterpret_cast<const int4*>(a.skin_nl + a.skin_off[c]);
       off = a.rowoff[c];
       const int rcap0 = a.rowcap[c];
@@ -2020,9 +2033,10 @@ __global__ void k_reorder_gather_gated(const BatchInst* __restrict__ b,
 }
 __global__ void k_reorder_back_gated(const BatchInst* __restrict__ b, const double* __restrict__ cin,
                                      double* __restrict__ cout, const int32_t* __restrict__ oin,
-                                     int32_t* __restrict__ oout, int64_t n) {
+                                     int32_t* __restrict__ oout, int64_t n, DevSkin* ds) {
   if (!b->reorder) return;
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (ds && i == 0) ds->live = 0;  // the lists name records by the old rows
   if (i >= n) return;
   for (int f = 0; f < NCOL; ++f) cout[f * n + i] = cin[f * n + i];
   oout[i] = oin[i];
@@ -2255,11 +2269,101 @@ void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t 
                          BoxGeom g, int dim, const uint8_t* sig_b, const double* bx,
                          const double* by, const double* bz, double* sx, double* sy, double* sz,
                          float4* s32, PackGeom pg, float* dsp, float tau, float eps,
-                         double* hrec, unsigned long long* red, cudaStream_t s) {
+                         double* hrec, unsigned long long* red, cudaStream_t s,
+                         const DevPlan* plan, const DevSkin* gate) {
   if (n <= 0) return;
   k_skin_refresh<<<reduce_blocks(n), TPB, 0, s>>>(sidx, n, nrows, nreal, cols, nrows, gsrc, gcode,
                                                   g, dim, sig_b, bx, by, bz, sx, sy, sz, s32, pg,
-                                                  dsp, tau, eps, hrec, red);
+                                                  dsp, tau, eps, hrec, red, plan, gate);
+  note_launch();
+}
+
+// ---- skin lists of the device-resident step ---------------------------------------------
+__global__ void k_dskin_check(int64_t nc, const int32_t* __restrict__ centre_p,
+                              const double* __restrict__ hcol, const double* __restrict__ hb,
+                              double krad, const DevSkin* __restrict__ ds,
+                              unsigned long long* __restrict__ red) {
+  if (!ds->live) return;
+  const double D = dkey_inv(red[RED_SKIN_D]);
+  const double kfb = ds->kfac_b;
+  bool bad = false;
+  for (int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; c < nc;
+       c += int64_t(gridDim.x) * blockDim.x) {
+    // relative margins far above the rounding of both sides and of the
+    // search's own radius kfac (krad h)
+    const double need = (krad * hcol[centre_p[c]] + 2.0 * D) * (1.0 + 1e-12);
+    const double have = kfb * (krad * hb[c]) * (1.0 - 1e-12);
+    bad |= !(need <= have);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicMax(&red[RED_DSKIN_FAIL], 1ull);
+}
+__global__ void k_dskin_decide(DevSkin* __restrict__ ds, const unsigned long long* __restrict__ red,
+                               const DevPlan* __restrict__ plan, double krad, double skin,
+                               int short_age, int pause0, int pause_max,
+                               cudaGraphConditionalHandle hsearch,
+                               unsigned long long* __restrict__ dcnt) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  DevSkin d = *ds;
+  bool ok = d.live != 0;
+  if (ok) {
+    const double D = dkey_inv(red[RED_SKIN_D]), hmax = dkey_inv(red[RED_SKIN_HMAX]);
+    ok = red[RED_SKIN_SIG] == 0ull && red[RED_DSKIN_FAIL] == 0ull && D <= krad * d.hmin_b &&
+         hmax > 0.0 && isfinite(hmax);
+    // every record inside the FP32 packing's binade: 0 <= x - origin < shift
+    const double o[3] = {plan->pg.ox, plan->pg.oy, plan->pg.oz};
+    for (int k = 0; k < 3; ++k) {
+      const double lo = dkey_inv(red[RED_LO_X + k]), hi = dkey_inv(red[RED_HI_X + k]);
+      ok = ok && lo >= o[k] && hi - o[k] < plan->pg.shift * (1.0 - 1e-9);
+    }
+  }
+  if (ok) {
+    ++d.age;
+    ++dcnt[DC_SKIN_REUSES];
+  } else {
+    if (d.live) {  // the lists ended: short-lived ones start a pause of plain searches
+      if (d.age < short_age) {
+        d.pause_len = d.pause_len ? min(2 * d.pause_len, pause_max) : pause0;
+        d.pause = d.pause_len;
+      } else {
+        d.pause_len = 0;
+      }
+    }
+    if (d.pause > 0) {
+      --d.pause;
+      d.kfac = 1.0;
+    } else {
+      d.kfac = 1.0 + skin;
+      ++dcnt[DC_SKIN_BUILDS];
+    }
+    d.live = 0;
+    ++dcnt[DC_SEARCHES];
+  }
+  *ds = d;
+  cudaGraphSetConditional(hsearch, ok ? 0u : 1u);
+}
+__global__ void k_dskin_built(DevSkin* __restrict__ ds, const unsigned long long* __restrict__ red) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  ds->live = ds->kfac > 1.0 ? 1 : 0;
+  ds->age = 0;
+  ds->kfac_b = ds->kfac;
+  ds->hmin_b = dkey_inv(red[RED_HMIN]);
+}
+void launch_dskin_check(int64_t nc, const int32_t* centre_p, const double* hcol, const double* hb,
+                        double krad, const DevSkin* ds, unsigned long long* red, cudaStream_t s) {
+  if (nc <= 0) return;
+  k_dskin_check<<<reduce_blocks(nc), TPB, 0, s>>>(nc, centre_p, hcol, hb, krad, ds, red);
+  note_launch();
+}
+void launch_dskin_decide(DevSkin* ds, const unsigned long long* red, const DevPlan* plan,
+                         double krad, double skin, int short_age, int pause0, int pause_max,
+                         cudaGraphConditionalHandle hsearch, unsigned long long* dcnt,
+                         cudaStream_t s) {
+  k_dskin_decide<<<1, 32, 0, s>>>(ds, red, plan, krad, skin, short_age, pause0, pause_max, hsearch,
+                                  dcnt);
+  note_launch();
+}
+void launch_dskin_built(DevSkin* ds, const unsigned long long* red, cudaStream_t s) {
+  k_dskin_built<<<1, 32, 0, s>>>(ds, red);
   note_launch();
 }
 void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const uint32_t* keys,
@@ -2429,6 +2533,30 @@ void launch_plan(const unsigned long long* red, const int32_t* nghost_dev, PlanI
   k_plan<<<1, 32, 0, s>>>(red, nghost_dev, in, plan, err_out);
   note_launch();
 }
+__global__ void k_sweeps_init(int* __restrict__ iter, cudaGraphConditionalHandle h) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  *iter = 0;
+  cudaGraphSetConditional(h, 1u);
+}
+__global__ void k_sweeps_ctl(int* __restrict__ iter, const unsigned long long* __restrict__ active,
+                             int sweeps, int maxiter, int* __restrict__ err,
+                             cudaGraphConditionalHandle h) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const int it = *iter + 1;
+  *iter = it;
+  const bool act = *active != 0ull;
+  if (act && it >= sweeps && sweeps < maxiter) atomicCAS(err, 0, SPH_ERR_STATE);
+  cudaGraphSetConditional(h, (act && it < sweeps) ? 1u : 0u);
+}
+void launch_sweeps_init(int* iter, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_sweeps_init<<<1, 32, 0, s>>>(iter, h);
+  note_launch();
+}
+void launch_sweeps_ctl(int* iter, const unsigned long long* active, int sweeps, int maxiter,
+                       int* err, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_sweeps_ctl<<<1, 32, 0, s>>>(iter, active, sweeps, maxiter, err, h);
+  note_launch();
+}
 void launch_flag_if_nonzero(const unsigned long long* v, int* err, int code, cudaStream_t s) {
   k_flag_if_nonzero<<<1, 32, 0, s>>>(v, err, code);
   note_launch();
@@ -2472,10 +2600,10 @@ void launch_inst_end(BatchInst* b, const int* err, const int32_t* overflow, cons
 }
 void launch_reorder_gated(const BatchInst* b, double* cols, double* cols_alt, int32_t* orig,
                           int32_t* orig_alt, const int32_t* centre_p, int64_t nreal,
-                          int64_t nrows, cudaStream_t s) {
+                          int64_t nrows, DevSkin* ds, cudaStream_t s) {
   k_reorder_gather_gated<<<nblocks(nrows), TPB, 0, s>>>(b, cols, cols_alt, orig, orig_alt,
                                                         centre_p, nreal, nrows);
-  k_reorder_back_gated<<<nblocks(nrows), TPB, 0, s>>>(b, cols_alt, cols, orig_alt, orig, nrows);
+  k_reorder_back_gated<<<nblocks(nrows), TPB, 0, s>>>(b, cols_alt, cols, orig_alt, orig, nrows, ds);
   note_launch(2);
 }
 void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s) {

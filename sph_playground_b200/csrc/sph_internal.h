@@ -71,13 +71,16 @@ enum RedSlot : int {
   RED_SKIN_NKEPT,   // rows a skin-list iterate keeps (plain count)
   RED_SKIN_NKEPT_PAIRS,  // their neighbours (plain count)
   RED_SKIN_HMAXB,   // largest h of the centres at the skin search (dkey max)
+  RED_DSKIN_FAIL,   // device-resident lists: a centre whose row cannot be filtered (0/1)
   RED_TOTAL
 };
 
 // Device counters (unsigned long long, cumulative).
 enum DevCnt : int {
   DC_NEIB_PAIRS = 0, DC_C1_PAIRS, DC_C2_PAIRS, DC_CANDIDATES,
-  DC_C1_CENTRE_SWEEPS, DC_C1_MAXSWEEPS, DC_EXACT_TESTS, DC_TOTAL
+  DC_C1_CENTRE_SWEEPS, DC_C1_MAXSWEEPS, DC_EXACT_TESTS,
+  // the device-resident step's searches, skin-list builds and iterates served
+  DC_SEARCHES, DC_SKIN_BUILDS, DC_SKIN_REUSES, DC_TOTAL
 };
 
 // Periodic geometry for the image builder (BC.f90:46-68, 196-475).
@@ -150,6 +153,17 @@ struct DevPlan {
   uint32_t pad_key;
   int err;
 };
+// Skin lists of the device-resident step (device memory, one per handle).
+// Every iterate either serves every centre's row from its skin list (the
+// FP64 predicate over the list) or searches afresh; no host decision.
+struct DevSkin {
+  int live;             // the lists describe the records of the current sort
+  int age;              // iterates served since their search
+  int pause, pause_len; // plain searches left, length of the last pause
+  double kfac;          // radius factor of this iterate's search (1 + s, or 1 in a pause)
+  double kfac_b;        // that of the lists' search
+  double hmin_b;        // smallest h at that search
+};
 // the time-loop state of main.f90:241-373 on the device
 struct DevClock {
   double t, ltout, dtout, tfinish, dt;
@@ -164,6 +178,14 @@ void launch_plan(const unsigned long long* red, const int32_t* nghost_dev, PlanI
                  DevPlan* plan, int* err_out, cudaStream_t s);
 // err := code (first error wins) if *v != 0
 void launch_flag_if_nonzero(const unsigned long long* v, int* err, int code, cudaStream_t s);
+// the device-resident Newton sweeps as a while node: *iter = 0 and the
+// handle set before it; after each sweep ++*iter, and the loop goes on while
+// a particle stays active and *iter < sweeps (err := SPH_ERR_STATE when one
+// is still active after the last of fewer than maxiter sweeps: the host
+// loop would sweep on)
+void launch_sweeps_init(int* iter, cudaGraphConditionalHandle h, cudaStream_t s);
+void launch_sweeps_ctl(int* iter, const unsigned long long* active, int sweeps, int maxiter,
+                       int* err, cudaGraphConditionalHandle h, cudaStream_t s);
 struct DtIn {
   int eq_hydro, eq_magneto, eq_diff, eq_fld, sts_fixed, sts_s;
   double cn_hydro, cnd2;
@@ -211,7 +233,7 @@ void launch_inst_end(BatchInst* b, const int* err, const int32_t* overflow, cons
 // table, then copied back, so the table keeps its address
 void launch_reorder_gated(const BatchInst* b, double* cols, double* cols_alt, int32_t* orig,
                           int32_t* orig_alt, const int32_t* centre_p, int64_t nreal,
-                          int64_t nrows, cudaStream_t s);
+                          int64_t nrows, DevSkin* ds, cudaStream_t s);
 void launch_keys_dev(const double* cols, int64_t nrows, const double* gx, const double* gy,
                      const double* gz, const DevPlan* plan, int64_t ncap, uint32_t* keys,
                      int32_t* vals, cudaStream_t s);
@@ -266,6 +288,7 @@ struct NeibArgs {
   double kfac;
   double reach;
   int skin_search;  // a skin search: its pairs are not the neighbour pairs counted
+  const double* kfac_dev;  // if set: kfac read from the device (device-resident step)
 };
 // ---- skin lists (SPH_P_SKIN; sph_grid.cu) ----
 // per row: the row's image signature (the periodic sides that hold it; its
@@ -278,12 +301,30 @@ void launch_skin_sig(const double* cols, int64_t nrows, BoxGeom g, int dim, uint
 // RED_LO_* / RED_HI_* (bounding box), RED_SKIN_D, RED_SKIN_HMAX (real
 // rows), RED_SKIN_SIG (a row whose image signature differs from sig_b),
 // RED_SKIN_NFAST (displacement > tau) and RED_SKIN_NMOVE (> eps)
+// (device-resident step: with plan set, n and pg come from the plan (n the
+// launch bound); with gate set, nothing is done unless gate->live)
 void launch_skin_refresh(const int32_t* sidx, int64_t n, int64_t nrows, int64_t nreal,
                          const double* cols, const int32_t* gsrc, const int8_t* gcode,
                          BoxGeom g, int dim, const uint8_t* sig_b, const double* bx,
                          const double* by, const double* bz, double* sx, double* sy, double* sz,
                          float4* s32, PackGeom pg, float* dsp, float tau, float eps,
-                         double* hrec, unsigned long long* red, cudaStream_t s);
+                         double* hrec, unsigned long long* red, cudaStream_t s,
+                         const DevPlan* plan = nullptr, const DevSkin* gate = nullptr);
+// with the lists live, per centre: can its row come from its skin list?
+// Every record now within krad h of the centre was within krad h + 2 D at
+// the lists' search (both moved at most D since), and the list holds all
+// within kfac_b krad h_b; red[RED_DSKIN_FAIL] = 1 where that fails
+void launch_dskin_check(int64_t nc, const int32_t* centre_p, const double* hcol, const double* hb,
+                        double krad, const DevSkin* ds, unsigned long long* red, cudaStream_t s);
+// the iterate's way: rows from the lists (hsearch = 0) or a search
+// (hsearch = 1, radius factor ds->kfac: 1 + skin, or 1 for the plain
+// searches of a pause after lists that served fewer than short_age iterates)
+void launch_dskin_decide(DevSkin* ds, const unsigned long long* red, const DevPlan* plan,
+                         double krad, double skin, int short_age, int pause0, int pause_max,
+                         cudaGraphConditionalHandle hsearch, unsigned long long* dcnt,
+                         cudaStream_t s);
+// after the search: its lists are live when it was a skin search
+void launch_dskin_built(DevSkin* ds, const unsigned long long* red, cudaStream_t s);
 // cell flags of the records that moved more than tau (fast_cell, by their
 // position now) and eps (move_cell, may be NULL; by the cell they were
 // sorted into), dilated by wf / wm cells per side along each of dim axes
@@ -372,6 +413,7 @@ struct SkinFilterArgs {
   int64_t nc;           // centres (list == NULL) or list entries
   const int32_t* list;  // optional: the centres to filter
   const uint8_t* mode;  // 0: filter; 1: left to the search; 2: kept when keep != 0
+                        // (NULL with list NULL: every centre filters)
   int keep;
   float* gap;           // optional: per centre, the smallest |r - krad h| of its list
   float eimg;           // error bound of a distance between two FP32 images
@@ -398,6 +440,12 @@ struct SkinFilterArgs {
   int32_t* maxcnt;
   int32_t* overflow;
   unsigned long long* dcnt;
+  const DevPlan* plan;  // if set: shift from the device plan
+  // if set: each skin row's slots (and skin_size the table's), to which the
+  // entries read are clamped (a skin search that overflowed them is redone
+  // on the host; its lists are never served)
+  const int32_t* skin_cap;
+  int64_t skin_size;
 };
 // each centre's neighbour row = its skin list's records that pass the FP64
 // predicate ((dx*dx + dy*dy) + dz*dz) <= (krad*h)^2, in skin-list order
@@ -452,8 +500,8 @@ void launch_radexch(double* cols, int64_t ld, const int32_t* orig, int64_t nrows
 // up to 8 single reduction slots set in one launch: p[off[i]] = val[i]
 struct SlotInit {
   int n;
-  int off[8];
-  unsigned long long val[8];
+  int off[12];
+  unsigned long long val[12];
 };
 void launch_init_slots(unsigned long long* p, const SlotInit& in, cudaStream_t s);
 void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s);
@@ -509,6 +557,7 @@ struct C1Args {
   int active_slot;                  // red slot the sweep marks when a particle stays active
   const unsigned long long* gate;   // if set and zero, the sweep has nothing to do
   int first;                        // the iterate's first sweep
+  const int* iter_dev;              // if set: the first sweep is the one where *iter_dev == 0
 };
 void launch_c1_newton(int prec, int kernel, int dim, const C1Args& a, PackBufs pb, Params P,
                       cudaStream_t s);

@@ -175,27 +175,6 @@ def test_batch_device_loop_reorders_rows(engine_lib, cuda_ok, prec):
 
 
 @pytest.mark.gpu
-def test_batch_device_loop_builds_no_skin_lists(engine_lib, cuda_ok):
-    """Instances at the default skin (0.1) joining the device loop, which
-    searches afresh every iterate: their start-up iterate builds no lists
-    either, so the runs equal the host path without lists bit for bit."""
-    alone = _alone(engine_lib)
-    eng = [abi.Engine(st, store, "m6", lib=engine_lib) for st, store in _instances()]
-    try:
-        with abi.Batch(eng) as b:
-            b.run_to(T_END)
-            assert b.status() == [0] * len(eng)
-        for e, (s1, t1) in zip(eng, alone):
-            c = e.counters()
-            assert c["skin_builds"] == 0 and c["graph_steps"] > 0, c
-            assert np.array_equal(e.get_state(), t1)
-            assert np.array_equal(e.get_store(), s1)
-    finally:
-        for e in eng:
-            e.close()
-
-
-@pytest.mark.gpu
 def test_batch_device_loop_redoes_on_the_host(engine_lib, cuda_ok):
     """A Newton tolerance no sweep count meets makes every device-resident
     step report it; the loop stops, that instance's step is redone on the

@@ -202,3 +202,85 @@ def test_skin_lists_survive_a_table_upload(engine_lib, oracle_lib, cuda_ok):
         e.set_store(table)
         e.density()
         assert e.counters()["skin_builds"] == b0 + 1  # a changed type ends them
+
+
+# ---- skin lists of the device-resident step (the batch's device loop, SPH_P_GRAPH) ----
+
+def _device_runs(lib, sets, prec, skin, run):
+    eng = [abi.Engine(st, store, "m6", precision=prec, lib=lib) for st, store in sets]
+    try:
+        for e in eng:
+            e.set_param(abi.P_SKIN, skin)
+        run(eng)
+        return [(e.get_store(), e.get_state(), e.counters(), e.get_neighbour_digest())
+                for e in eng]
+    finally:
+        for e in eng:
+            e.close()
+
+
+def _ways(c):
+    return {k: c[k] for k in ("steps", "iterates", "searches", "skin_builds", "skin_reuses",
+                              "graph_steps", "graph_redos")}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [FP64, FP32])
+def test_device_loop_skin_lists(engine_lib, oracle_lib, cuda_ok, prec):
+    """The batch's device loop at the default skin: the lattices at rest are
+    served from the lists nearly every iterate (a search after each row
+    reorder), the sets after the run equal a fresh oracle search on the
+    final table (FP64), and the fields equal the loop's without lists to the
+    summation order (FP64) or within the FP32 tolerances."""
+    tf = 2e-3
+    sets = [ic.diffusion2d(n, ddw=ddw, tfinish=tf, sts_stages=4)
+            for n, ddw in ((12, "fab"), (16, "n2w"), (20, "2nw_ds"))]
+
+    def batch(eng):
+        with abi.Batch(eng) as b:
+            b.run_to(tf)
+            assert b.status() == [0] * len(eng)
+
+    fresh = _device_runs(engine_lib, sets, prec, 0.0, batch)
+    skin = _device_runs(engine_lib, sets, prec, 0.1, batch)
+    for (s0, t0, c0, _), (s1, t1, c1, dg) in zip(fresh, skin):
+        info = _ways(c1)
+        assert c1["graph_steps"] > 0 and c1["skin_builds"] >= 1, info
+        assert 2 * c1["skin_reuses"] >= c1["iterates"], info
+        assert c1["searches"] + c1["skin_reuses"] == c1["iterates"], info
+        assert c0["steps"] == c1["steps"]
+        tol = (1e-12, 1e-12) if prec == FP64 else (1e-6, 1e-5)
+        assert abs(t1[consts.ec["time"] - 1] - t0[consts.ec["time"] - 1]) <= 1e-12
+        for f in ("den", "h"):
+            assert rel_particle(s1[:, COL[f]], s0[:, COL[f]]) < tol[0], f
+        assert rel_field(s1[:, COL["t"]], s0[:, COL["t"]]) < tol[1]
+        if prec == FP64:
+            with abi.Engine(t1, s1, "m6", precision=FP64, lib=oracle_lib) as o:
+                o.density()
+                ref = o.get_neighbour_digest()
+            assert np.array_equal(dg[0], ref[0]) and np.array_equal(dg[1], ref[1])
+
+
+@pytest.mark.gpu
+def test_graph_steps_skin_lists_hydro(engine_lib, cuda_ok):
+    """Device-resident steps (SPH_P_GRAPH) of the Sedov blast with skin
+    lists: served while the records move little, searched afresh (plainly in
+    a pause after short-lived lists) once the blast moves them; the fields
+    equal the steps without lists to the summation order."""
+    st, store = ic.sedov3d(n=24, npics=1)
+
+    def steps(eng):
+        for e in eng:
+            e.set_param(abi.P_GRAPH, 1.0)
+            e.step(12)
+
+    (s0, t0, c0, _), = _device_runs(engine_lib, [(st, store)], FP64, 0.0, steps)
+    (s1, t1, c1, _), = _device_runs(engine_lib, [(st, store)], FP64, 0.1, steps)
+    info = _ways(c1)
+    assert c1["graph_steps"] >= 10 and c1["skin_builds"] >= 1, info
+    assert c1["searches"] + c1["skin_reuses"] == c1["iterates"], info
+    assert abs(t1[consts.ec["time"] - 1] - t0[consts.ec["time"] - 1]) <= 1e-12 * t0[consts.ec["time"] - 1]
+    for f in ("den", "h", "om"):
+        assert rel_particle(s1[:, COL[f]], s0[:, COL[f]]) < 1e-12, f
+    for f in ("rx", "ry", "rz", "vx", "vy", "vz", "u"):
+        assert rel_field(s1[:, COL[f]], s0[:, COL[f]]) < 1e-12, f
