@@ -16,6 +16,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -94,30 +96,105 @@ KBase kbase(int id) {
 // device allocations made by DevBuf::ensure on this thread's current handle
 thread_local int64_t* t_alloc_count = nullptr;
 
+// Device memory of all handles of the process, cached: a block given back
+// (a handle destroyed, a buffer outgrown) waits in its device's free list
+// for the next request of a similar size instead of going back to the
+// driver.  cudaMalloc and cudaFree cost tens of microseconds each and
+// cudaFree waits for the whole device; a batch's instances start with
+// about 80 buffers each.  A block is given back only when no work of its
+// handle can still use it (the handle's stream synchronised, or the device
+// for an outgrown buffer); a request the driver cannot serve first returns
+// the device's cached blocks to it.  At most kCacheMax bytes wait per device.
+class DevCache {
+ public:
+  static DevCache& get() {
+    static DevCache* c = new DevCache();  // (never destroyed: handles may outlive statics)
+    return *c;
+  }
+  cudaError_t take(size_t want, void** p, size_t* got, int* dev) {
+    cudaGetDevice(dev);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto& f = free_[*dev];
+      auto it = f.lower_bound(want);
+      // a cached block at most 1.5x the request (no large block for a small one)
+      if (it != f.end() && it->first <= want + want / 2) {
+        *p = it->second;
+        *got = it->first;
+        cached_[*dev] -= it->first;
+        f.erase(it);
+        return cudaSuccess;
+      }
+    }
+    cudaError_t e = cudaMalloc(p, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      release(*dev);
+      e = cudaMalloc(p, want);
+    }
+    if (e == cudaSuccess) *got = want;
+    return e;
+  }
+  void give(void* p, size_t bytes, int dev) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (cached_[dev] + bytes <= kCacheMax) {
+        free_[dev].insert({bytes, p});
+        cached_[dev] += bytes;
+        return;
+      }
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    cudaFree(p);
+    if (cur != dev) cudaSetDevice(cur);
+  }
+
+ private:
+  static constexpr size_t kCacheMax = size_t(16) << 30;
+  void release(int dev) {
+    std::multimap<size_t, void*> f;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      f.swap(free_[dev]);
+      cached_[dev] = 0;
+    }
+    for (auto& b : f) cudaFree(b.second);
+  }
+  std::mutex mu_;
+  std::map<int, std::multimap<size_t, void*>> free_;
+  std::map<int, size_t> cached_;
+};
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  int dev = 0;
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p) DevCache::get().give(p, bytes, dev);
   }
   int ensure(size_t b) {
     if (b <= bytes && p) return SPH_OK;
-    if (p) cudaFree(p);
+    if (p) {
+      // work queued before this call may still use the old block
+      cudaDeviceSynchronize();
+      DevCache::get().give(p, bytes, dev);
+    }
     p = nullptr;
     bytes = 0;
     // 25% headroom: sizes that follow the image count move by a few rows
-    // between steps and must not trigger a free/allocate (which would also
-    // synchronise the device) every time
+    // between steps and must not trigger a new block every time
     size_t nb = std::max<size_t>(b + b / 4, 256);
     if (t_alloc_count) ++*t_alloc_count;
     static const bool log_allocs = std::getenv("SPH_ALLOC_LOG") != nullptr;
     if (log_allocs) std::fprintf(stderr, "sph: device allocation of %zu bytes\n", nb);
-    cudaError_t e = cudaMalloc(&p, nb);
+    cudaError_t e = DevCache::get().take(nb, &p, &bytes, &dev);
     if (e != cudaSuccess) {
-      cudaGetLastError();
+      p = nullptr;
+      bytes = 0;
       return fail(SPH_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
-    bytes = nb;
     return SPH_OK;
   }
   template <class T> T* as() const { return static_cast<T*>(p); }
@@ -236,7 +313,12 @@ struct sph_handle {
   DevBuf dskin;
   bool dlists_ok = false;
   DevBuf c1_iter;  // the sweep count of the device-resident Newton loop
-  cudaStream_t cap_s = nullptr;  // captures the bodies of conditional nodes
+  // the device-resident STS loop: its stage index and the coefficients of
+  // stages 2 .. s (mu, nu, muhat, gmhat), for the s they were made for
+  DevBuf sts_j, sts_coef;
+  int sts_coef_s = 0;
+  std::vector<cudaStream_t> cap_s;  // capture the bodies of conditional nodes, one per level
+  int cap_depth = 0;
   int64_t nghost_cap = 0, nall_cap = 0;
   int end_bit_cap = 0;
   // captured steps, one per table pointer pair: a row reorder swaps the
@@ -549,6 +631,7 @@ struct sph_handle {
                         skin_sig.as<uint8_t>(), skin_sig_alt.as<uint8_t>(), s);
     std::swap(skin_sig.p, skin_sig_alt.p);
     std::swap(skin_sig.bytes, skin_sig_alt.bytes);
+    std::swap(skin_sig.dev, skin_sig_alt.dev);
     return SPH_OK;
   }
 
@@ -570,8 +653,10 @@ struct sph_handle {
                    orig_alt.as<int32_t>(), perm, nrows, nrows, nrows, s);
     std::swap(cols.p, cols_alt.p);
     std::swap(cols.bytes, cols_alt.bytes);
+    std::swap(cols.dev, cols_alt.dev);
     std::swap(orig.p, orig_alt.p);
     std::swap(orig.bytes, orig_alt.bytes);
+    std::swap(orig.dev, orig_alt.dev);
     if (skin_valid) {
       // the skin lists name records, which stay; what names rows follows
       RC(skin_inv.ensure(sizeof(int32_t) * nrows));
@@ -1445,14 +1530,23 @@ struct sph_handle {
     cudaGraphNode_t node;
     CK(cudaGraphAddNode(&node, g, deps, nd, &cp));
     CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-    if (!cap_s) CK(cudaStreamCreateWithFlags(&cap_s, cudaStreamNonBlocking));
-    CK(cudaStreamBeginCaptureToGraph(cap_s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+    // (one capture stream per nesting level: the levels above still capture)
+    if (int(cap_s.size()) <= cap_depth) {
+      cudaStream_t ns = nullptr;
+      CK(cudaStreamCreateWithFlags(&ns, cudaStreamNonBlocking));
+      cap_s.push_back(ns);
+    }
+    cudaStream_t bs = cap_s[cap_depth];
+    CK(cudaStreamBeginCaptureToGraph(bs, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                      cudaStreamCaptureModeThreadLocal));
-    std::swap(s, cap_s);
+    cudaStream_t outer = s;
+    s = bs;
+    ++cap_depth;
     const int rc = body(hnd);
-    std::swap(s, cap_s);
+    --cap_depth;
+    s = outer;
     cudaGraph_t out;
-    const cudaError_t e = cudaStreamEndCapture(cap_s, &out);
+    const cudaError_t e = cudaStreamEndCapture(bs, &out);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(SPH_ERR_CUDA, std::string("if node body: ") + cudaGetErrorString(e));
     return SPH_OK;
@@ -1697,7 +1791,10 @@ struct sph_handle {
     RC(c1_iter.ensure(sizeof(int)));
     RC(drs_save.ensure(sizeof(double) * NCOL * size_t(nrows)));
     RC(bclk_save.ensure(sizeof(DevClock)));
-    if (eq_sts) RC(stsY.ensure(sizeof(double) * 6 * nrows));
+    if (eq_sts) {
+      RC(stsY.ensure(sizeof(double) * 6 * nrows));
+      RC(sts_coef_upload(ival(ec_stsfixeds)));
+    }
     const double skin = skin_fraction();
     if (skin > 0) {
       // the device-resident lists: the host lists' buffers at the device
@@ -2063,15 +2160,32 @@ struct sph_handle {
     return SPH_OK;
   }
 
+  // sts_integrator.f90:10-51: the stage coefficients
+  static double sts_b(int j) { return j <= 2 ? 1. / 3. : (double(j * j + j) - 2.) / (2. * j * (j + 1.)); }
+  static double sts_mu(int j) { return (2. * j - 1.) / j * sts_b(j) / sts_b(j - 1); }
+  static double sts_nu(int j) { return -((j - 1.) / j * sts_b(j) / sts_b(j - 2)); }
+  static double sts_w(int s_) { return 4. / (double(s_ * s_ + s_) - 2.); }
+  static double sts_mu_hat(int j, int s_) { return j == 1 ? sts_b(1) * sts_w(s_) : sts_mu(j) * sts_w(s_); }
+  static double sts_gm_hat(int j, int s_) { return -(1 - sts_b(j - 1)) * sts_mu_hat(j, s_); }
+  int sts_coef_upload(int sts_s) {
+    RC(sts_j.ensure(sizeof(int)));
+    if (sts_s < 2 || (sts_coef.p && sts_coef_s == sts_s)) return SPH_OK;
+    std::vector<double> c(4 * size_t(sts_s - 1));
+    for (int j = 2; j <= sts_s; ++j) {
+      double* q = c.data() + 4 * (j - 2);
+      q[0] = sts_mu(j); q[1] = sts_nu(j); q[2] = sts_mu_hat(j, sts_s); q[3] = sts_gm_hat(j, sts_s);
+    }
+    RC(sts_coef.ensure(sizeof(double) * c.size()));
+    CK(cudaMemcpy(sts_coef.p, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+    sts_coef_s = sts_s;
+    return SPH_OK;
+  }
   int sts_integrate(int sts_s, double dt) {
     // sts_integrator.f90:87-124; coefficients :10-51
-    auto b = [](int j) { return j <= 2 ? 1. / 3. : (double(j * j + j) - 2.) / (2. * j * (j + 1.)); };
-    auto a_ = [&](int j) { return 1 - b(j); };
-    auto mu = [&](int j) { return (2. * j - 1.) / j * b(j) / b(j - 1); };
-    auto nu = [&](int j) { return -((j - 1.) / j * b(j) / b(j - 2)); };
-    auto w = [](int s_) { return 4. / (double(s_ * s_ + s_) - 2.); };
-    auto mu_hat = [&](int j, int s_) { return j == 1 ? b(1) * w(s_) : mu(j) * w(s_); };
-    auto gm_hat = [&](int j, int s_) { return -a_(j - 1) * mu_hat(j, s_); };
+    auto mu = [](int j) { return sts_mu(j); };
+    auto nu = [](int j) { return sts_nu(j); };
+    auto mu_hat = [](int j, int s_) { return sts_mu_hat(j, s_); };
+    auto gm_hat = [](int j, int s_) { return sts_gm_hat(j, s_); };
     RC(stsY.ensure(sizeof(double) * 6 * nrows));
     double* Y = stsY.as<double>();
     {
@@ -2084,6 +2198,21 @@ struct sph_handle {
       launch_sts_stage(1, cols.as<double>(), nrows, nrows, Y, mu_hat(1, sts_s), 0, 0, 0, 0,
                        ctrl.as<double>(), s);
     }
+    if (dplan && sts_s >= 2) {
+      // the device-resident step: stages 2 .. s as a while node over one
+      // captured iterate (coefficients uploaded with the step's buffers)
+      int* jd = sts_j.as<int>();
+      const double* coef = sts_coef.as<double>();
+      RC(capture_cond(
+          cudaGraphCondTypeWhile,
+          [&](cudaGraphConditionalHandle hw) { launch_sts_loop_init(jd, sts_s, hw, s); },
+          [&](cudaGraphConditionalHandle hw) {
+            RC(iterate(true));
+            launch_sts_stage_dev(cols.as<double>(), nrows, nrows, Y, coef, jd, ctrl.as<double>(), s);
+            launch_sts_loop_ctl(jd, sts_s, hw, s);
+            return SPH_OK;
+          }));
+    } else
     for (int j = 2; j <= sts_s; ++j) {
       RC(iterate(true));
       Phase ph(this, SPH_T_STS);
@@ -2394,7 +2523,7 @@ struct sph_handle {
     if (h_red) cudaFreeHost(h_red);
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (h_i32) cudaFreeHost(h_i32);
-    if (cap_s) cudaStreamDestroy(cap_s);
+    for (auto c : cap_s) cudaStreamDestroy(c);
     if (s) cudaStreamDestroy(s);
   }
 };
@@ -2433,6 +2562,7 @@ struct BatchGraph {
     g = nullptr;
   }
   ~BatchGraph() {
+    if (s) cudaStreamSynchronize(s);  // (its buffers go back to the cache)
     drop();
     if (s) cudaStreamDestroy(s);
   }

@@ -2057,9 +2057,14 @@ __global__ void k_fill_u64(unsigned long long* p, int n, unsigned long long v) {
 enum { Y0 = 0, YJM1, YJM2, YJ, DY0, DYJM1 };
 __global__ void k_sts(int kind, double* __restrict__ cols, int64_t ld, int64_t n,
                       double* __restrict__ Y, double a0, double a1, double a2, double a3,
-                      double a4, const double* __restrict__ ctrl) {
+                      double a4, const double* __restrict__ ctrl,
+                      const double* __restrict__ coef = nullptr, const int* __restrict__ jdev = nullptr) {
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= n) return;
+  if (coef) {  // stage j of the device-resident loop
+    const double* c = coef + 4 * (*jdev - 2);
+    a0 = c[0]; a1 = c[1]; a2 = c[2]; a3 = c[3];
+  }
   auto y = [&](int s) -> double& { return Y[s * ld + i]; };
   double* T = cols + es_t * ld;
   const double* ddt = cols + es_ddt * ld;
@@ -2626,6 +2631,26 @@ void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, 
                       double a1, double a2, double a3, double a4, const double* ctrl,
                       cudaStream_t s) {
   k_sts<<<nblocks(n), TPB, 0, s>>>(kind, cols, ld, n, Y, a0, a1, a2, a3, a4, ctrl);
+  note_launch();
+}
+void launch_sts_stage_dev(double* cols, int64_t ld, int64_t n, double* Y, const double* coef,
+                          const int* jdev, const double* ctrl, cudaStream_t s) {
+  k_sts<<<nblocks(n), TPB, 0, s>>>(2, cols, ld, n, Y, 0., 0., 0., 0., 0., ctrl, coef, jdev);
+  note_launch();
+}
+__global__ void k_sts_loop(int* __restrict__ jdev, int sts_s, cudaGraphConditionalHandle h,
+                           int init) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const int j = init ? 2 : *jdev + 1;
+  *jdev = j;
+  cudaGraphSetConditional(h, j <= sts_s ? 1u : 0u);
+}
+void launch_sts_loop_init(int* jdev, int sts_s, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_sts_loop<<<1, 32, 0, s>>>(jdev, sts_s, h, 1);
+  note_launch();
+}
+void launch_sts_loop_ctl(int* jdev, int sts_s, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_sts_loop<<<1, 32, 0, s>>>(jdev, sts_s, h, 0);
   note_launch();
 }
 void launch_eos(double* cols, int64_t ld, int64_t nreal, Params P, cudaStream_t s) {

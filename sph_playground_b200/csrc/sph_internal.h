@@ -508,6 +508,14 @@ void launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t s);
 void launch_sts_stage(int kind, double* cols, int64_t ld, int64_t n, double* Y, double a0,
                       double a1, double a2, double a3, double a4, const double* ctrl,
                       cudaStream_t s);
+// the device-resident step's stages j = 2 .. s as a while node: stage j
+// (kind 2) with its coefficients coef[4 (j - 2) + 0..3] (mu, nu, muhat,
+// gmhat) for j = *jdev; sts_loop_init sets *jdev = 2 and the handle (2 <= s),
+// sts_loop_ctl advances j and sets it again (j <= s)
+void launch_sts_stage_dev(double* cols, int64_t ld, int64_t n, double* Y, const double* coef,
+                          const int* jdev, const double* ctrl, cudaStream_t s);
+void launch_sts_loop_init(int* jdev, int sts_s, cudaGraphConditionalHandle h, cudaStream_t s);
+void launch_sts_loop_ctl(int* jdev, int sts_s, cudaGraphConditionalHandle h, cudaStream_t s);
 void launch_eos(double* cols, int64_t ld, int64_t nreal, Params P, cudaStream_t s);
 void launch_apply_mti(double* cols, int64_t ld, const int32_t* orig, int64_t nrows,
                       int64_t nreal, int lowres, cudaStream_t s);
