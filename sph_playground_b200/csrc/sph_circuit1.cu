@@ -27,6 +27,8 @@ inline int nblocks(int64_t n, int tpb = TPB) {
 
 template <class R> struct PosAccess;
 template <> struct PosAccess<double> {
+  using Pos = PairPos<double>;
+  static __device__ __forceinline__ double unit(const PackBufs&) { return 1.0; }
   static __device__ __forceinline__ PairPos<double> load(const PackBufs& pb, int64_t j, double& m) {
     double2 a = __ldg(&pb.p[0][j]);
     double2 b = __ldg(&pb.p[1][j]);
@@ -40,13 +42,13 @@ template <> struct PosAccess<double> {
   }
 };
 template <> struct PosAccess<float> {
-  static __device__ __forceinline__ PairPos<float> load(const PackBufs& pb, int64_t j, float& m) {
-    float4 a = __ldg(&pb.q[0][j]);
-    float4 b = __ldg(&pb.q[1][j]);
+  using Pos = FixPos;
+  static __device__ __forceinline__ float unit(const PackBufs& pb) { return *pb.unit; }
+  static __device__ __forceinline__ FixPos load(const PackBufs& pb, int64_t j, float& m) {
+    const float4 a = __ldg(&pb.q[6][j]);
     m = a.w;
-    PairPos<float> r;
-    r.xh = a.x; r.yh = a.y; r.zh = a.z;
-    r.xl = b.x; r.yl = b.y; r.zl = b.z;
+    FixPos r;
+    r.x = __float_as_int(a.x); r.y = __float_as_int(a.y); r.z = __float_as_int(a.z);
     return r;
   }
   static __device__ __forceinline__ float temp(const PackBufs& pb, int64_t j) {
@@ -113,7 +115,8 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
     double* cols = a.cols;
     const int64_t ld = a.ld;
     R mi;
-    const PairPos<R> pi = PosAccess<R>::load(pb, k, mi);
+    const typename PosAccess<R>::Pos pi = PosAccess<R>::load(pb, k, mi);
+    const R punit = PosAccess<R>::unit(pb);
     const double ma = cols[es_m * ld + p];
     const double ha0 = cols[es_h * ld + p];
     const int n = a.ncnt[c];
@@ -148,7 +151,7 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
         int64_t jj[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) jj[u] = jn[u];
-        PairPos<R> pj[U];
+        typename PosAccess<R>::Pos pj[U];
         R mj[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) pj[u] = PosAccess<R>::load(pb, jj[u] >= 0 ? jj[u] : 0, mj[u]);
@@ -161,7 +164,7 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
         for (int u = 0; u < U; ++u) {
           if (jj[u] < 0) continue;
           R dx, dy, dz;
-          pos_delta(pi, pj[u], dx, dy, dz);
+          pos_delta(pi, pj[u], dx, dy, dz, punit);
           R r2 = dx * dx;
           if (DIM >= 2) r2 += dy * dy;
           if (DIM == 3) r2 += dz * dz;
@@ -255,7 +258,8 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
     const int64_t ld = a.ld;
     if (a.simple || a.eps[p] > P.tol) {
       R mi;
-      const PairPos<R> pi = PosAccess<R>::load(pb, k, mi);
+      const typename PosAccess<R>::Pos pi = PosAccess<R>::load(pb, k, mi);
+      const R punit = PosAccess<R>::unit(pb);
       const double ma = cols[es_m * ld + p];
       const double ha0 = cols[es_h * ld + p];
       const double ha = a.hk_s[k], rhoa = a.dk_s[k], oma = a.ok_s[k];
@@ -278,10 +282,10 @@ k_c1_sweep(C1Args a, PackBufs pb, Params P) {
       for (int l = lane; l < n; l += G) {
         const int64_t j = jnext;
         R mj;
-        const PairPos<R> pj = PosAccess<R>::load(pb, j, mj);
+        const typename PosAccess<R>::Pos pj = PosAccess<R>::load(pb, j, mj);
         if (l + G < n) jnext = row[l + G];
         R dx, dy, dz;
-        pos_delta(pi, pj, dx, dy, dz);
+        pos_delta(pi, pj, dx, dy, dz, punit);
         R r2 = dx * dx;
         if (DIM >= 2) r2 += dy * dy;
         if (DIM == 3) r2 += dz * dz;

@@ -248,6 +248,22 @@ __device__ __forceinline__ void pos_delta(const PairPos<double>& a, const PairPo
                                           double& dx, double& dy, double& dz) {
   dx = a.x - b.x; dy = a.y - b.y; dz = a.z - b.z;
 }
+// the density pass's FP32 positions: 31-bit fixed point over the packing
+// frame; a separation is an exact integer difference rounded once to FP32
+// (the scaling by the power-of-two unit is exact)
+struct FixPos {
+  int32_t x, y, z;
+};
+__device__ __forceinline__ void pos_delta(const FixPos& a, const FixPos& b, float& dx, float& dy,
+                                          float& dz, float unit) {
+  dx = __int2float_rn(a.x - b.x) * unit;
+  dy = __int2float_rn(a.y - b.y) * unit;
+  dz = __int2float_rn(a.z - b.z) * unit;
+}
+__device__ __forceinline__ void pos_delta(const PairPos<double>& a, const PairPos<double>& b,
+                                          double& dx, double& dy, double& dz, double) {
+  pos_delta(a, b, dx, dy, dz);
+}
 __device__ __forceinline__ void pos_delta(const PairPos<float>& a, const PairPos<float>& b,
                                           float& dx, float& dy, float& dz) {
   dx = (a.xh - b.xh) + (a.xl - b.xl);

@@ -248,7 +248,7 @@ struct sph_handle {
   // sorted arrays
   DevBuf sx, sy, sz, s32, ssrc, cflag, cpos, centre_k, centre_p;
   DevBuf hk_s, dk_s, ok_s;
-  DevBuf pk[11], qk[6];
+  DevBuf pk[11], qk[7], qunit;
   // neighbours: one row per centre inside nl, rows sized from each
   // particle's previous count (CSR with slack)
   DevBuf nl, ncnt, rowoff, rowcap, rowcap64, count_prev, h_prev, scan64_tmp, overflow;
@@ -591,14 +591,16 @@ struct sph_handle {
     if (prec == SPH_PREC_FP64) {
       for (int i = 0; i < 11; ++i) RC(pk[i].ensure(sizeof(double2) * nall));
     } else {
-      for (int i = 0; i < 6; ++i) RC(qk[i].ensure(sizeof(float4) * nall));
+      for (int i = 0; i < 7; ++i) RC(qk[i].ensure(sizeof(float4) * nall));
+      RC(qunit.ensure(sizeof(float)));
     }
     return SPH_OK;
   }
   PackBufs packs() const {
     PackBufs pb;
     for (int i = 0; i < 11; ++i) pb.p[i] = pk[i].as<double2>();
-    for (int i = 0; i < 6; ++i) pb.q[i] = qk[i].as<float4>();
+    for (int i = 0; i < 7; ++i) pb.q[i] = qk[i].as<float4>();
+    pb.unit = qunit.as<float>();
     return pb;
   }
 

@@ -1619,6 +1619,13 @@ __global__ void k_rowcap(int64_t nc, const int32_t* __restrict__ centre_p,
 }
 
 // ---- pair-data packing (sorted order) --------------------------------------------------------
+// a position in fixed-point units of the packing frame, in [0, 2^31)
+__device__ __forceinline__ int32_t fixpos(double t) {
+  t = rint(t);
+  if (!(t >= 0.0)) return 0;
+  if (t > 2147483647.0) return 2147483647;
+  return int32_t(t);
+}
 __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restrict__ ssrc,
                        const double* __restrict__ sx, const double* __restrict__ sy,
                        const double* __restrict__ sz, const double* __restrict__ cols, int64_t ld,
@@ -1654,24 +1661,31 @@ __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restric
     }
   } else {
     if (groups & PACK_POS) {
-      double xs = (sx[k] - pg.ox) + pg.shift;
-      double ys = (sy[k] - pg.oy) + pg.shift;
-      double zs = (sz[k] - pg.oz) + pg.shift;
-      float xh = __double2float_rn(xs), yh = __double2float_rn(ys), zh = __double2float_rn(zs);
-      float xl = __double2float_rn(xs - double(xh));
-      float yl = __double2float_rn(ys - double(yh));
-      float zl = __double2float_rn(zs - double(zh));
-      pb.q[0][k] = make_float4(xh, yh, zh, float(m));
-      pb.q[1][k] = make_float4(xl, yl, zl, float(1.0 / C(es_h)));
+      // the density pass: 31-bit fixed point over the frame (every record
+      // has 0 <= x - origin < shift), one 16-byte record per neighbour
+      const double sc = 2147483648.0 / pg.shift;  // (a power of two)
+      const int32_t xi = fixpos((sx[k] - pg.ox) * sc);
+      const int32_t yi = fixpos((sy[k] - pg.oy) * sc);
+      const int32_t zi = fixpos((sz[k] - pg.oz) * sc);
+      pb.q[6][k] = make_float4(__int_as_float(xi), __int_as_float(yi), __int_as_float(zi), float(m));
+      if (k == 0) *pb.unit = float(pg.shift / 2147483648.0);
       if (groups & PACK_TEMP)
         pb.q[4][k] = make_float4(float(C(es_t)), float(C(es_kappa)), float(C(es_dtdx)),
                                float(C(es_dtdy)));
     }
     if (groups & PACK_HYDRO) {
+      // the force pass: high and low FP32 parts in one binade (the highs'
+      // differences are exact)
+      const double xs = (sx[k] - pg.ox) + pg.shift;
+      const double ys = (sy[k] - pg.oy) + pg.shift;
+      const double zs = (sz[k] - pg.oz) + pg.shift;
+      const float xh = __double2float_rn(xs), yh = __double2float_rn(ys), zh = __double2float_rn(zs);
+      const float xl = __double2float_rn(xs - double(xh));
+      const float yl = __double2float_rn(ys - double(yh));
+      const float zl = __double2float_rn(zs - double(zh));
       double h = C(es_h), rho = C(es_den), om = C(es_om), P = C(es_p);
-      float4 q1 = pb.q[1][k];
-      q1.w = float(1.0 / h);
-      pb.q[1][k] = q1;
+      pb.q[0][k] = make_float4(xh, yh, zh, float(m));
+      pb.q[1][k] = make_float4(xl, yl, zl, float(1.0 / h));
       pb.q[2][k] = make_float4(float(rho), float(1.0 / (rho * rho * om)), float(P), float(C(es_c)));
       pb.q[3][k] = make_float4(float(C(es_u)), float(C(es_vx)), float(C(es_vy)), float(C(es_vz)));
     }
