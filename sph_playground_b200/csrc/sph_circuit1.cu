@@ -130,9 +130,12 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
     bool bad = false;
     for (;;) {
       ++it;
+      // (the separations stay in fixed-point units: 1/h carries the unit, a
+      // power of two, so q is the same as from physical separations)
       const double ihd_full = 1.0 / ha;
-      const R ih = R(ihd_full);
-      const R ih_lo = R(ihd_full - double(ih));
+      const R ih0 = R(ihd_full);
+      const R ih = ih0 * punit;
+      const R ih_lo = R(ihd_full - double(ih0)) * punit;
       // the density sum keeps its two-sum partials (its smoothness in h is
       // what the Newton iteration needs); the d rho / dh sum only scales the
       // Newton step and Omega, so a plain per-lane sum suffices
@@ -164,7 +167,7 @@ k_c1_newton(C1Args a, PackBufs pb, Params P) {
         for (int u = 0; u < U; ++u) {
           if (jj[u] < 0) continue;
           R dx, dy, dz;
-          pos_delta(pi, pj[u], dx, dy, dz, punit);
+          pos_delta(pi, pj[u], dx, dy, dz, R(1));
           R r2 = dx * dx;
           if (DIM >= 2) r2 += dy * dy;
           if (DIM == 3) r2 += dz * dz;
