@@ -294,6 +294,30 @@ struct Params {
   double c_iso;  // c of row 1 for eos_isothermal
 };
 
+// Counters of a block: each v[k] summed (or, with is_max[k], maximised) over
+// the block's threads into thread 0's v[k], through shared memory, so that
+// a kernel issues its counter atomics once per block, not once per warp
+// (hundreds of thousands of same-address atomics per launch otherwise).
+// Every thread of the block must call it; blocks of at most 1024 threads.
+template <int N>
+__device__ __forceinline__ void block_counters(unsigned long long (&v)[N], const bool (&is_max)[N]) {
+  __shared__ unsigned long long part[32][N];
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long t = __shfl_xor_sync(0xffffffffu, v[k], o);
+      v[k] = is_max[k] ? (t > v[k] ? t : v[k]) : v[k] + t;
+    }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < N; ++k) part[w][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 1; i < int((blockDim.x + 31) >> 5); ++i)
+      for (int k = 0; k < N; ++k)
+        v[k] = is_max[k] ? (part[i][k] > v[k] ? part[i][k] : v[k]) : v[k] + part[i][k];
+}
+
 // status word helper: first error wins
 __device__ __forceinline__ void raise_status(int* status, int code) {
   atomicCAS(status, 0, code);

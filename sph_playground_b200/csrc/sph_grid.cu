@@ -318,8 +318,10 @@ __global__ void k_cell_count(const uint32_t* __restrict__ keys, int64_t n,
   const int64_t u = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   int m = 0;
   if (u < n) m = atomicAdd(&count[keys[u]], 1) + 1;
-  const int wm = __reduce_max_sync(0xffffffffu, m);
-  if ((threadIdx.x & 31) == 0 && wm) atomicMax(maxc, wm);
+  unsigned long long v[1] = {(unsigned long long)m};
+  const bool is_max[1] = {true};
+  block_counters<1>(v, is_max);
+  if (threadIdx.x == 0 && v[0]) atomicMax(maxc, int(v[0]));
 }
 __global__ void k_cell_scatter(const uint32_t* __restrict__ keys, int64_t n,
                                const int32_t* __restrict__ cstart, int32_t* __restrict__ fill,
@@ -931,23 +933,19 @@ k_neighbours(NeibArgs a) {
     a.h_prev[a.orig[p]] = float(a.hcol[p]);
     nfound = unsigned(cnt);
   }
-  // the longest row and any overflow leave the warp as one atomic each (one
-  // per centre on a single address would serialise in its L2 slice)
-  {
-    const int wmax = __reduce_max_sync(FULL, active ? cnt : 0);
-    const bool wovf = __any_sync(FULL, active && cnt > rcap);
-    if (wl == 0) {
-      if (wmax) atomicMax(a.maxcnt, wmax);
-      if (wovf) atomicOr(a.overflow, 1);
-    }
-  }
-  unsigned int wc = __reduce_add_sync(FULL, ncand);
-  unsigned int wf = __reduce_add_sync(FULL, nfound);
-  unsigned int we = __reduce_add_sync(FULL, nexact);
-  if (wl == 0) {
-    atomicAdd(&a.dcnt[DC_CANDIDATES], (unsigned long long)wc);
-    if (!a.skin_search) atomicAdd(&a.dcnt[DC_NEIB_PAIRS], (unsigned long long)wf);
-    atomicAdd(&a.dcnt[DC_EXACT_TESTS], (unsigned long long)we);
+  // the longest row, any overflow and the counters leave the block as one
+  // atomic each (one per centre or warp on a single address would
+  // serialise in its L2 slice)
+  unsigned long long v[5] = {active ? (unsigned long long)cnt : 0ull,
+                             (active && cnt > rcap) ? 1ull : 0ull, ncand, nfound, nexact};
+  const bool is_max[5] = {true, true, false, false, false};
+  block_counters<5>(v, is_max);
+  if (threadIdx.x == 0) {
+    if (v[0]) atomicMax(a.maxcnt, int(v[0]));
+    if (v[1]) atomicOr(a.overflow, 1);
+    if (v[2]) atomicAdd(&a.dcnt[DC_CANDIDATES], v[2]);
+    if (v[3] && !a.skin_search) atomicAdd(&a.dcnt[DC_NEIB_PAIRS], v[3]);
+    if (v[4]) atomicAdd(&a.dcnt[DC_EXACT_TESTS], v[4]);
   }
 }
 
@@ -1104,21 +1102,21 @@ __global__ void k_skin_cells(int64_t n, const float* __restrict__ dsp, float tau
     fast_cell[cx + int64_t(g.nx) * (cy + int64_t(g.ny) * cz)] = 1;
   }
 }
-// out[c] = OR of in over the cells within w of c along `axis`
+// out[c] = OR of in over the cells within w of c along `axis` (out zeroed
+// before): every marked cell writes its window, so the work follows the
+// marks (a few per cent of the cells while the lists serve), not the grid
 __global__ void k_dilate(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, Grid g,
                          int axis, int w) {
   const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int64_t ncell = int64_t(g.nx) * g.ny * g.nz;
-  if (c >= ncell) return;
+  if (c >= ncell || !in[c]) return;
   int n, i;
   int64_t stride;
   if (axis == 0) { n = g.nx; i = int(c % g.nx); stride = 1; }
   else if (axis == 1) { n = g.ny; i = int((c / g.nx) % g.ny); stride = g.nx; }
   else { n = g.nz; i = int(c / (int64_t(g.nx) * g.ny)); stride = int64_t(g.nx) * g.ny; }
   const int a = max(0, i - w), b = min(n - 1, i + w);
-  uint8_t v = 0;
-  for (int j = a; j <= b && !v; ++j) v = in[c + int64_t(j - i) * stride];
-  out[c] = v;
+  for (int j = a; j <= b; ++j) out[c + int64_t(j - i) * stride] = 1;
 }
 
 // The way of each centre (mode: 0 filter, 1 fresh search, 2 keep; dflag =
@@ -1163,11 +1161,12 @@ __global__ void k_skin_classify(int64_t nc, const int32_t* __restrict__ centre_k
   }
   // rows kept and their neighbours: nkept[0], nkept[1]
   const bool kp = c < nc && w == 2;
-  const unsigned kept = __ballot_sync(0xffffffffu, kp);
-  const unsigned pairs = __reduce_add_sync(0xffffffffu, kp ? unsigned(ncnt[c]) : 0u);
-  if ((threadIdx.x & 31) == 0 && kept) {
-    atomicAdd(nkept, (unsigned long long)__popc(kept));
-    atomicAdd(nkept + 1, (unsigned long long)pairs);
+  unsigned long long v[2] = {kp ? 1ull : 0ull, kp ? (unsigned long long)ncnt[c] : 0ull};
+  const bool is_max[2] = {false, false};
+  block_counters<2>(v, is_max);
+  if (threadIdx.x == 0 && v[0]) {
+    atomicAdd(nkept, v[0]);
+    atomicAdd(nkept + 1, v[1]);
   }
 }
 
@@ -2401,6 +2400,7 @@ void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const 
     uint8_t* a = f;
     uint8_t* b = tmp;
     for (int axis = 0; axis < dim; ++axis) {
+      cudaMemsetAsync(b, 0, size_t(ncell), s);
       k_dilate<<<nblocks(ncell), TPB, 0, s>>>(a, b, g, axis, w);
       note_launch();
       std::swap(a, b);
