@@ -2243,6 +2243,10 @@ struct sph_handle {
     }
     RC(iterate(true));
     if (stop_before_correct) return SPH_OK;
+    return fixed_step_correct(dt);
+  }
+  // the rest of fixed_step after its force pass
+  int fixed_step_correct(double dt) {
     {
       Phase ph(this, SPH_T_CORRECT);
       launch_correct(cols.as<double>(), nrows, orig.as<int32_t>(), nrows, n_int, save.as<double>(),
@@ -2260,6 +2264,67 @@ struct sph_handle {
   }
   double* ckpt(int i) { return adj_ckpt.as<double>() + size_t(i) * NCOL * nrows; }
   double* seg(int i) { return adj_seg.as<double>() + size_t(i) * NCOL * nrows; }
+  // What the VJP of a step reads from its force pass, kept per step of a
+  // segment while the segment is replayed, so that the backward sweep does
+  // not run each step's forward a second time: the table after the force
+  // pass, the sorted records, the centres and the neighbour lists.  Slots
+  // are sized at the sweep's start; a step whose pass outgrew them (more
+  // images, longer lists) is recomputed instead.
+  DevBuf adj_mid;
+  size_t adj_mid_slot = 0;
+  int64_t adj_mid_nall = 0, adj_mid_nl = 0;
+  std::vector<char> adj_mid_ok;
+  std::vector<int64_t> adj_mid_used;  // per slot: the pass's record count and list size
+  struct MidPart { DevBuf* b; size_t bytes; };
+  void mid_parts(MidPart (&p)[9], int64_t nall, int64_t nl) {
+    p[0] = {&cols, table_bytes()};
+    p[1] = {&sx, sizeof(double) * size_t(nall)};
+    p[2] = {&sy, sizeof(double) * size_t(nall)};
+    p[3] = {&sz, sizeof(double) * size_t(nall)};
+    p[4] = {&ssrc, sizeof(int32_t) * size_t(nall)};
+    p[5] = {&centre_k, sizeof(int32_t) * size_t(nreal)};
+    p[6] = {&centre_p, sizeof(int32_t) * size_t(nreal)};
+    p[7] = {&rowoff, sizeof(int64_t) * size_t(nreal)};
+    p[8] = {&ncnt, sizeof(int32_t) * size_t(nreal)};
+    (void)nl;
+  }
+  static size_t mid_round(size_t b) { return (b + 255) & ~size_t(255); }
+  size_t mid_slot_bytes(int64_t nall, int64_t nl) {
+    MidPart p[9];
+    mid_parts(p, nall, nl);
+    size_t t = mid_round(sizeof(int32_t) * size_t(nl));
+    for (auto& q : p) t += mid_round(q.bytes);
+    return t;
+  }
+  // copy the pass's buffers into slot i (to) or back (from); false: the
+  // pass does not fit the slot
+  int mid_copy(int i, bool save, bool* fits) {
+    int64_t nall = nrows + nghost, nlu = nl_size;
+    if (save) {
+      adj_mid_used[2 * size_t(i)] = nall;
+      adj_mid_used[2 * size_t(i) + 1] = nlu;
+    } else {
+      nall = adj_mid_used[2 * size_t(i)];
+      nlu = adj_mid_used[2 * size_t(i) + 1];
+    }
+    *fits = nall <= adj_mid_nall && nlu <= adj_mid_nl;
+    if (!*fits) return SPH_OK;
+    char* base = adj_mid.as<char>() + size_t(i) * adj_mid_slot;
+    MidPart p[9];
+    mid_parts(p, nall, nlu);
+    size_t off = 0;
+    auto cp = [&](void* dev, size_t bytes, size_t cap) -> int {
+      void* slot = base + off;
+      CK(cudaMemcpyAsync(save ? slot : dev, save ? dev : slot, bytes, cudaMemcpyDeviceToDevice, s));
+      off += mid_round(cap);
+      return SPH_OK;
+    };
+    MidPart cap[9];
+    mid_parts(cap, adj_mid_nall, adj_mid_nl);
+    for (int k = 0; k < 9; ++k) RC(cp(p[k].b->p, p[k].bytes, cap[k].bytes));
+    RC(cp(nl.p, sizeof(int32_t) * size_t(nlu), sizeof(int32_t) * size_t(adj_mid_nl)));
+    return SPH_OK;
+  }
 
   // the hydro subset the adjoint kernels differentiate
   // which adjoint applies: the hydro one, or (adj_diff) the diffusion one
@@ -2402,19 +2467,52 @@ struct sph_handle {
     RC(load(dl_dr, AJ_LR, 3));
     RC(load(dl_dT, AJ_LT, 1));
     const int G = lanes_pair();
+    // per-step slots of the force passes when they fit a quarter of the free
+    // device memory (at most 16 GB): 25 % room for more images and longer lists
+    bool mid_on = false;
+    {
+      adj_mid_nall = (nrows + nghost) + (nghost + 3) / 4 + 1024;
+      adj_mid_nl = nl_size + nl_size / 4 + 1024;
+      adj_mid_slot = mid_slot_bytes(adj_mid_nall, adj_mid_nl);
+      const size_t want = adj_mid_slot * size_t(adj_every);
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = 0;
+      }
+      if (want <= std::min(free_b / 4, size_t(16) << 30)) {
+        RC(adj_mid.ensure(want));
+        mid_on = true;
+      }
+      adj_mid_ok.assign(size_t(adj_every), 0);
+      adj_mid_used.assign(2 * size_t(adj_every), 0);
+    }
     for (int sgi = adj_ncp - 1; sgi >= 0; --sgi) {
       const int n0 = sgi * adj_every, n1 = std::min(adj_nsteps, n0 + adj_every);
-      // replay the segment, keeping the state before every step
+      // replay the segment, keeping the state before every step and (where
+      // it fits) what the step's VJP reads from its force pass
       RC(copy_table(cols.p, ckpt(1 + sgi)));
       for (int n = n0; n < n1; ++n) {
         RC(copy_table(seg(n - n0), cols.p));
         st[ec_time] = adj_t0 + n * adj_dt;
-        RC(fixed_step(adj_dt));
+        if (!mid_on) {
+          RC(fixed_step(adj_dt));
+          continue;
+        }
+        RC(fixed_step(adj_dt, true));
+        bool fits = false;
+        RC(mid_copy(n - n0, true, &fits));
+        adj_mid_ok[size_t(n - n0)] = fits ? 1 : 0;
+        RC(fixed_step_correct(adj_dt));
       }
       for (int n = n1 - 1; n >= n0; --n) {
-        RC(copy_table(cols.p, seg(n - n0)));
-        st[ec_time] = adj_t0 + n * adj_dt;
-        RC(fixed_step(adj_dt, true));
+        bool fits = mid_on && adj_mid_ok[size_t(n - n0)];
+        if (fits) RC(mid_copy(n - n0, false, &fits));
+        if (!fits) {
+          RC(copy_table(cols.p, seg(n - n0)));
+          st[ec_time] = adj_t0 + n * adj_dt;
+          RC(fixed_step(adj_dt, true));
+        }
         launch_adj_step(kernel_id, d, G, adj_args(), adj_dt, 0, s);
       }
     }
