@@ -210,32 +210,11 @@ template <> struct Acc<double> {
   __device__ __forceinline__ double dval() const { return s; }
 };
 
-// ---- packed pair data (sorted order) ----------------------------------------------
-// FP64: eleven double2 streams.  FP32: six float4 streams; positions are a
+// ---- packed pair data (sorted order; the streams are listed at PackBufs) ----------
+// FP64 positions are the sorted records' own; the FP32 force pass takes a
 // hi/lo float pair of (x - origin + 2^E), all in one binade, so hi_i - hi_j
-// is exact and dx = (hi_i - hi_j) + (lo_i - lo_j) carries one FP32 rounding.
-struct PackF64 {
-  const double2* p0;  // x, y
-  const double2* p1;  // z, m
-  const double2* p2;  // h, rho
-  const double2* p3;  // om, P
-  const double2* p4;  // c, u
-  const double2* p5;  // vx, vy
-  const double2* p6;  // vz, T
-  const double2* p7;  // kappa, dtdx
-  const double2* p8;  // dtdy, dtdz
-  const double2* p9;  // bx, by
-  const double2* p10; // bz, 0
-};
-struct PackF32 {
-  const float4* q0;  // xhi, yhi, zhi, m
-  const float4* q1;  // xlo, ylo, zlo, h
-  const float4* q2;  // rho, om, P, c
-  const float4* q3;  // u, vx, vy, vz
-  const float4* q4;  // T, kappa, dtdx, dtdy
-  const float4* q5;  // dtdz, bx, by, bz
-};
-
+// is exact and dx = (hi_i - hi_j) + (lo_i - lo_j) carries one FP32 rounding;
+// the FP32 density pass takes 31-bit fixed point (FixPos).
 template <class R> struct PairPos;  // position handle for dx computation
 template <> struct PairPos<double> {
   double x, y, z;
