@@ -2275,6 +2275,7 @@ struct sph_handle {
   int64_t adj_mid_nall = 0, adj_mid_nl = 0;
   std::vector<char> adj_mid_ok;
   std::vector<int64_t> adj_mid_used;  // per slot: the pass's record count and list size
+  int64_t adj_mid_restored = 0;
   struct MidPart { DevBuf* b; size_t bytes; };
   void mid_parts(MidPart (&p)[9], int64_t nall, int64_t nl) {
     p[0] = {&cols, table_bytes()};
@@ -2470,6 +2471,7 @@ struct sph_handle {
     // per-step slots of the force passes when they fit a quarter of the free
     // device memory (at most 16 GB): 25 % room for more images and longer lists
     bool mid_on = false;
+    adj_mid_restored = 0;
     {
       adj_mid_nall = (nrows + nghost) + (nghost + 3) / 4 + 1024;
       adj_mid_nl = nl_size + nl_size / 4 + 1024;
@@ -2486,6 +2488,12 @@ struct sph_handle {
       }
       adj_mid_ok.assign(size_t(adj_every), 0);
       adj_mid_used.assign(2 * size_t(adj_every), 0);
+      // (SPH_ADJ_TRACE in the environment: the slots' use, on stderr)
+      static const bool trace = std::getenv("SPH_ADJ_TRACE") != nullptr;
+      if (trace)
+        std::fprintf(stderr, "adjoint backward: %s, %d slots of %.1f MB, free %.1f GB\n",
+                     mid_on ? "force passes kept" : "force passes recomputed", adj_every,
+                     adj_mid_slot / 1e6, free_b / 1e9);
     }
     for (int sgi = adj_ncp - 1; sgi >= 0; --sgi) {
       const int n0 = sgi * adj_every, n1 = std::min(adj_nsteps, n0 + adj_every);
@@ -2508,6 +2516,7 @@ struct sph_handle {
       for (int n = n1 - 1; n >= n0; --n) {
         bool fits = mid_on && adj_mid_ok[size_t(n - n0)];
         if (fits) RC(mid_copy(n - n0, false, &fits));
+        adj_mid_restored += fits ? 1 : 0;
         if (!fits) {
           RC(copy_table(cols.p, seg(n - n0)));
           st[ec_time] = adj_t0 + n * adj_dt;
@@ -2538,6 +2547,9 @@ struct sph_handle {
       CK(cudaStreamSynchronize(s));
       for (int k = 0; k < npar && k < 3; ++k) g_par[k] = h_ctrl[1 + k];
     }
+    if (std::getenv("SPH_ADJ_TRACE"))
+      std::fprintf(stderr, "adjoint backward: %lld of %d steps from kept force passes\n",
+                   (long long)adj_mid_restored, adj_nsteps);
     // back to the state at the end of the forward run
     RC(copy_table(cols.p, ckpt(adj_ncp + 1)));
     st[ec_time] = adj_t0 + adj_nsteps * adj_dt;
