@@ -287,6 +287,7 @@ struct sph_handle {
   // iterate after the end of the table's fixed part (skin_end[0]): their
   // capacities and the scan of those
   DevBuf skin_end, skin_dcap, skin_doff;
+  DevBuf skin_gate;  // the iterate's checks and mark windows (k_skin_gate)
   // rows renamed: spare signatures, the two permutations, the old types, a flag
   DevBuf skin_sig_alt, skin_inv, skin_perm, skin_type, skin_flag;
   int64_t skin_nl_size = 0;
@@ -802,6 +803,7 @@ struct sph_handle {
   }
   int skin_alloc(int64_t nall) {
     RC(skin_alloc_common(nall));
+    RC(skin_gate.ensure(sizeof(int) * 4));
     RC(skin_dflag.ensure(sizeof(int32_t) * (nreal + 1)));
     RC(skin_dpos.ensure(sizeof(int32_t) * (nreal + 1)));
     RC(skin_dlist.ensure(sizeof(int32_t) * nreal));
@@ -1063,49 +1065,24 @@ struct sph_handle {
                           skin_bx.as<double>(), skin_by.as<double>(), skin_bz.as<double>(),
                           sx.as<double>(), sy.as<double>(), sz.as<double>(), s32.as<float4>(),
                           pgeom, skin_dsp.as<float>(), tau, eps, skin_hrec.as<double>(), rb, s);
-      CK(cudaMemcpyAsync(h_red, rb, sizeof(unsigned long long) * RED_TOTAL,
-                         cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      CK(cudaGetLastError());
-    }
-    const double D = dkey_inv(h_red[RED_SKIN_D]);
-    const double hmax = dkey_inv(h_red[RED_SKIN_HMAX]);
-    const double hmaxb = dkey_inv(h_red[RED_SKIN_HMAXB]);
-    const unsigned long long nfast = h_red[RED_SKIN_NFAST], nmove = h_red[RED_SKIN_NMOVE];
-    // (SPH_SKIN_TRACE in the environment: why lists end, on stderr)
-    auto end_lists = [&](const char* why) {
-      if (skin_trace)
-        std::fprintf(stderr, "skin lists end after %d iterates: %s (D %.3g, fast %llu, moving %llu)\n",
-                     skin_age, why, D, nfast, nmove);
-      return SPH_OK;
-    };
-    if (h_red[RED_SKIN_SIG]) return end_lists("an image set changed");
-    const double dcap = P.krad * skin_hmin;
-    if (!(D <= dcap)) return end_lists("records moved a search radius");
-    if (!(hmax > 0) || !std::isfinite(hmax) || !(hmaxb > 0)) return end_lists("h");
-    // every record inside the FP32 packing's binade: 0 <= x - origin < shift
-    const double o[3] = {pgeom.ox, pgeom.oy, pgeom.oz};
-    for (int k = 0; k < 3; ++k) {
-      const double lo = dkey_inv(h_red[RED_LO_X + k]), hi = dkey_inv(h_red[RED_HI_X + k]);
-      if (!(lo >= o[k]) || !(hi - o[k] < pgeom.shift * (1.0 - 1e-9)))
-        return end_lists("a record left the FP32 binade");
-    }
-    // the marks, in cells: around fast records every centre that may see
-    // them now (reach_f), around moving ones every skin list holding them
-    // (reach_m)
-    const double reach_f = (P.krad * hmax + skin_tau) * (1.0 + 1e-9);
-    const double reach_m = (1.0 + skin_s) * P.krad * hmaxb * (1.0 + 1e-9);
-    const int wf = int(std::ceil(reach_f * grid.invL)) + 1;
-    const int wm = int(std::ceil(reach_m * grid.invL)) + 1;
-    if (wf > 256 || wm > 256) return end_lists("a search radius spans too many cells");
-    const int64_t ncell = int64_t(grid.nx) * grid.ny * grid.nz;
-    RC(skin_fcell.ensure(size_t(ncell)));
-    RC(skin_mcell.ensure(size_t(ncell)));
-    RC(skin_ctmp.ensure(size_t(ncell)));
-    {
-      Phase ph(this, SPH_T_NEIGHBOURS);
+      // the checks and the marks' windows on the device, then the marks and
+      // every centre's way: the iterate asks the host once, after the ways
+      // (when a check failed, the host ends the lists and drops the ways)
+      SkinGateIn gi{};
+      gi.dcap = P.krad * skin_hmin;
+      gi.krad = P.krad;
+      gi.tau = skin_tau;
+      gi.kfac = 1.0 + skin_s;
+      gi.invL = grid.invL;
+      gi.pg = pgeom;
+      int* gate = skin_gate.as<int>();
+      launch_skin_gate(rb, gi, gate, s);
+      const int64_t ncell = int64_t(grid.nx) * grid.ny * grid.nz;
+      RC(skin_fcell.ensure(size_t(ncell)));
+      RC(skin_mcell.ensure(size_t(ncell)));
+      RC(skin_ctmp.ensure(size_t(ncell)));
       launch_skin_marks(nall, skin_dsp.as<float>(), tau, eps, keys_alt.as<uint32_t>(),
-                        sx.as<double>(), sy.as<double>(), sz.as<double>(), grid, d, wf, wm,
+                        sx.as<double>(), sy.as<double>(), sz.as<double>(), grid, d, gate + 1,
                         skin_fcell.as<uint8_t>(), skin_mcell.as<uint8_t>(),
                         skin_ctmp.as<uint8_t>(), s);
       launch_skin_classify(nreal, centre_k.as<int32_t>(), skin_hrec.as<double>(),
@@ -1116,11 +1093,30 @@ struct sph_handle {
                            skin_ways.as<int64_t>(), skin_wpos.as<int64_t>(),
                            skin_dlist.as<int32_t>(), skin_flist.as<int32_t>(), scan64_tmp.p,
                            scan64_tmp.bytes, ncnt.as<int32_t>(), rb + RED_SKIN_NKEPT, s);
+      CK(cudaMemcpyAsync(h_red, rb, sizeof(unsigned long long) * RED_TOTAL,
+                         cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(h_red + RED_TOTAL, skin_wpos.as<int64_t>() + nreal, sizeof(int64_t),
                          cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(h_red + RED_SKIN_NKEPT, rb + RED_SKIN_NKEPT,
-                         2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(h_i32 + 8, gate, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
+      CK(cudaGetLastError());
+    }
+    const double D = dkey_inv(h_red[RED_SKIN_D]);
+    const unsigned long long nfast = h_red[RED_SKIN_NFAST], nmove = h_red[RED_SKIN_NMOVE];
+    // (SPH_SKIN_TRACE in the environment: why lists end, on stderr)
+    auto end_lists = [&](const char* why) {
+      if (skin_trace)
+        std::fprintf(stderr, "skin lists end after %d iterates: %s (D %.3g, fast %llu, moving %llu)\n",
+                     skin_age, why, D, nfast, nmove);
+      return SPH_OK;
+    };
+    switch (h_i32[8]) {
+      case 0: break;
+      case 1: return end_lists("an image set changed");
+      case 2: return end_lists("records moved a search radius");
+      case 3: return end_lists("h");
+      case 4: return end_lists("a record left the FP32 binade");
+      default: return end_lists("a search radius spans too many cells");
     }
     const int64_t counts = reinterpret_cast<const int64_t*>(h_red + RED_TOTAL)[0];
     const int64_t ndirty = counts & 0xffffffffll, nfilter = counts >> 32;
@@ -3000,7 +2996,7 @@ int sph_create(const double* state49, const double* store, int64_t n_rows, int k
   if (cudaMallocHost(&h->h_red, sizeof(unsigned long long) * (RED_TOTAL + 2)) != cudaSuccess ||
       cudaMallocHost(&h->h_ctrl, sizeof(double) * 16) != cudaSuccess ||
       cudaMallocHost(&h->h_plan, sizeof(DevPlan)) != cudaSuccess ||
-      cudaMallocHost(&h->h_i32, sizeof(int32_t) * 8) != cudaSuccess) {
+      cudaMallocHost(&h->h_i32, sizeof(int32_t) * 16) != cudaSuccess) {
     cudaGetLastError();
     h->destroy();
     delete h;

@@ -1106,10 +1106,11 @@ __global__ void k_skin_cells(int64_t n, const float* __restrict__ dsp, float tau
 // before): every marked cell writes its window, so the work follows the
 // marks (a few per cent of the cells while the lists serve), not the grid
 __global__ void k_dilate(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, Grid g,
-                         int axis, int w) {
+                         int axis, const int* __restrict__ wp) {
   const int64_t c = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int64_t ncell = int64_t(g.nx) * g.ny * g.nz;
   if (c >= ncell || !in[c]) return;
+  const int w = *wp;
   int n, i;
   int64_t stride;
   if (axis == 0) { n = g.nx; i = int(c % g.nx); stride = 1; }
@@ -2386,7 +2387,7 @@ void launch_dskin_built(DevSkin* ds, const unsigned long long* red, cudaStream_t
 }
 void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const uint32_t* keys,
                        const double* sx, const double* sy, const double* sz, Grid g, int dim,
-                       int wf, int wm, uint8_t* fast_cell, uint8_t* move_cell, uint8_t* tmp,
+                       const int* w, uint8_t* fast_cell, uint8_t* move_cell, uint8_t* tmp,
                        cudaStream_t s) {
   const int64_t ncell = int64_t(g.nx) * g.ny * g.nz;
   if (n <= 0 || ncell <= 0) return;
@@ -2396,19 +2397,55 @@ void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const 
                                           move_cell);
   note_launch();
   // dilate in place through tmp: axis 0 into tmp, 1 back, 2 into tmp, copy back
-  auto dilate = [&](uint8_t* f, int w) {
+  auto dilate = [&](uint8_t* f, const int* wp) {
     uint8_t* a = f;
     uint8_t* b = tmp;
     for (int axis = 0; axis < dim; ++axis) {
       cudaMemsetAsync(b, 0, size_t(ncell), s);
-      k_dilate<<<nblocks(ncell), TPB, 0, s>>>(a, b, g, axis, w);
+      k_dilate<<<nblocks(ncell), TPB, 0, s>>>(a, b, g, axis, wp);
       note_launch();
       std::swap(a, b);
     }
     if (a != f) cudaMemcpyAsync(f, a, size_t(ncell), cudaMemcpyDeviceToDevice, s);
   };
-  dilate(fast_cell, wf);
-  if (move_cell) dilate(move_cell, wm);
+  dilate(fast_cell, w);
+  if (move_cell) dilate(move_cell, w + 1);
+}
+__global__ void k_skin_gate(const unsigned long long* __restrict__ red, SkinGateIn in,
+                            int* __restrict__ gate) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const double D = dkey_inv(red[RED_SKIN_D]);
+  const double hmax = dkey_inv(red[RED_SKIN_HMAX]);
+  const double hmaxb = dkey_inv(red[RED_SKIN_HMAXB]);
+  int why = 0;
+  if (red[RED_SKIN_SIG]) why = 1;
+  else if (!(D <= in.dcap)) why = 2;
+  else if (!(hmax > 0) || !isfinite(hmax) || !(hmaxb > 0)) why = 3;
+  if (!why) {
+    // every record inside the FP32 packing's binade: 0 <= x - origin < shift
+    const double o[3] = {in.pg.ox, in.pg.oy, in.pg.oz};
+    for (int k = 0; k < 3; ++k) {
+      const double lo = dkey_inv(red[RED_LO_X + k]), hi = dkey_inv(red[RED_HI_X + k]);
+      if (!(lo >= o[k]) || !(hi - o[k] < in.pg.shift * (1.0 - 1e-9))) why = 4;
+    }
+  }
+  int wf = 0, wm = 0;
+  if (!why) {
+    // around fast records every centre that may see them now (reach_f),
+    // around moving ones every skin list holding them (reach_m)
+    const double reach_f = (in.krad * hmax + in.tau) * (1.0 + 1e-9);
+    const double reach_m = in.kfac * in.krad * hmaxb * (1.0 + 1e-9);
+    const double ef = ceil(reach_f * in.invL) + 1.0, em = ceil(reach_m * in.invL) + 1.0;
+    if (!(ef <= 256.0) || !(em <= 256.0)) why = 5;
+    else { wf = int(ef); wm = int(em); }
+  }
+  gate[0] = why;
+  gate[1] = wf;
+  gate[2] = wm;
+}
+void launch_skin_gate(const unsigned long long* red, SkinGateIn in, int* gate, cudaStream_t s) {
+  k_skin_gate<<<1, 32, 0, s>>>(red, in, gate);
+  note_launch();
 }
 void launch_skin_classify(int64_t nc, const int32_t* centre_k, const double* hrec,
                           const double* hb, double* hdev, const float* gap, double krad,

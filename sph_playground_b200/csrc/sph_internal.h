@@ -325,13 +325,24 @@ void launch_dskin_decide(DevSkin* ds, const unsigned long long* red, const DevPl
                          cudaStream_t s);
 // after the search: its lists are live when it was a skin search
 void launch_dskin_built(DevSkin* ds, const unsigned long long* red, cudaStream_t s);
+// The checks of a skin-list iterate on the refreshed records, on the
+// device so that the iterate asks the host once: gate[0] = 0 when the
+// lists may serve, else why not (1 an image set changed, 2 a record moved
+// a search radius dcap, 3 h, 4 a record left the FP32 binade, 5 a window
+// spans more than 256 cells); gate[1], gate[2] = the windows wf, wm of the
+// marks in cells (0 when gate[0] != 0)
+struct SkinGateIn {
+  double dcap, krad, tau, kfac, invL;
+  PackGeom pg;
+};
+void launch_skin_gate(const unsigned long long* red, SkinGateIn in, int* gate, cudaStream_t s);
 // cell flags of the records that moved more than tau (fast_cell, by their
 // position now) and eps (move_cell, may be NULL; by the cell they were
-// sorted into), dilated by wf / wm cells per side along each of dim axes
-// (tmp: a spare field of the cell count)
+// sorted into), dilated by w[0] / w[1] cells per side along each of dim
+// axes (w in device memory; tmp: a spare field of the cell count)
 void launch_skin_marks(int64_t n, const float* dsp, float tau, float eps, const uint32_t* keys,
                        const double* sx, const double* sy, const double* sz, Grid g, int dim,
-                       int wf, int wm, uint8_t* fast_cell, uint8_t* move_cell, uint8_t* tmp,
+                       const int* w, uint8_t* fast_cell, uint8_t* move_cell, uint8_t* tmp,
                        cudaStream_t s);
 // mode[c] = 0 (filter the skin list), 1 (search afresh) or 2 (keep the row)
 // for every centre (see sph_grid.cu), near_f / near_m the dilated cell
