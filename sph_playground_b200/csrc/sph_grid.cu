@@ -1511,16 +1511,29 @@ __global__ void __launch_bounds__(128) k_search_few(FewArgs a) {
     const int rcap = room <= 0 ? 0 : (room < int64_t(rcap0) ? int(room) : rcap0);
     int32_t* const dst = a.nl + off;
     int cnt = 0;
-    for (int cz = cz0; cz <= cz1; ++cz) {
-      const double dzc = DIM == 3 ? fmax(0.0, fmax(double(cz) - uz, uz - double(cz + 1))) : 0.0;
-      for (int cy = cy0; cy <= cy1; ++cy) {
+    // the rows of cells in (z, y) order, G at a time: each lane finds one
+    // row's run of records (its two cell-start loads issued side by side
+    // with the other lanes'), then the group walks the G runs in order
+    const int ny_r = cy1 - cy0 + 1;
+    const int nrows_r = ny_r * (cz1 - cz0 + 1);
+    for (int r0 = 0; r0 < nrows_r; r0 += G) {
+      int32_t mq0 = 0, mq1 = 0;
+      const int r = r0 + lane;
+      if (r < nrows_r) {
+        const int cy = cy0 + r % ny_r, cz = cz0 + r / ny_r;
+        const double dzc = DIM == 3 ? fmax(0.0, fmax(double(cz) - uz, uz - double(cz + 1))) : 0.0;
         const double dyc = DIM >= 2 ? fmax(0.0, fmax(double(cy) - uy, uy - double(cy + 1))) : 0.0;
         const double rem = rr * rr - dyc * dyc - dzc * dzc;
-        if (rem < 0.0) continue;
-        const double w = sqrt(rem);
-        const int cx0 = clamp_cell(ux - w, g.nx), cx1 = clamp_cell(ux + w, g.nx);
-        const int64_t rowc = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
-        const int32_t q0 = __ldg(a.cstart + rowc + cx0), q1 = __ldg(a.cstart + rowc + cx1 + 1);
+        if (rem >= 0.0) {
+          const double w = sqrt(rem);
+          const int cx0 = clamp_cell(ux - w, g.nx), cx1 = clamp_cell(ux + w, g.nx);
+          const int64_t rowc = int64_t(g.nx) * (cy + int64_t(g.ny) * cz);
+          mq0 = __ldg(a.cstart + rowc + cx0);
+          mq1 = __ldg(a.cstart + rowc + cx1 + 1);
+        }
+      }
+      for (int jr = 0; jr < G; ++jr) {
+        const int32_t q0 = __shfl_sync(gmask, mq0, jr, G), q1 = __shfl_sync(gmask, mq1, jr, G);
         ncand += (lane == 0) ? unsigned(q1 - q0) : 0u;
         for (int32_t b = q0; b < q1; b += G) {
           const int32_t q = b + lane;
