@@ -284,3 +284,28 @@ def test_graph_steps_skin_lists_hydro(engine_lib, cuda_ok):
         assert rel_particle(s1[:, COL[f]], s0[:, COL[f]]) < 1e-12, f
     for f in ("rx", "ry", "rz", "vx", "vy", "vz", "u"):
         assert rel_field(s1[:, COL[f]], s0[:, COL[f]]) < 1e-12, f
+
+
+@pytest.mark.gpu
+def test_skin_lists_end_on_a_long_move(engine_lib, oracle_lib, cuda_ok):
+    """A record moved by the caller farther than a search radius ends the
+    lists (the device-side checks of the iterate); the next pass searches
+    afresh and its sets equal the oracle's."""
+    st, store = ic.density3d(n=16, seed=2)
+    with abi.Engine(st, store, "m6", precision=FP64, lib=engine_lib) as e:
+        e.set_param(abi.P_SKIN, 0.1)
+        for _ in range(5):
+            e.density()
+        b0 = e.counters()["skin_builds"]
+        x = e.get_columns(["rx"])
+        x[0, 7] = (x[0, 7] + 0.31) % 1.0  # (the unit box: about five spacings)
+        e.set_columns(["rx"], x)
+        mst = e.get_state()
+        table = e.get_store()
+        e.density()
+        assert e.counters()["skin_builds"] == b0 + 1
+        got = e.get_neighbour_digest()
+    with abi.Engine(mst, table, "m6", precision=FP64, lib=oracle_lib) as o:
+        o.density()
+        ref = o.get_neighbour_digest()
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
