@@ -273,6 +273,23 @@ struct sph_handle {
   // searches afresh every iterate: lists built then would serve none
   bool skin_suspended = false;
   DevBuf colbuf;  // staging of sph_get_columns / sph_set_columns
+  // A table upload or download crosses PCIe in kXferChunks pieces on the
+  // copy stream xs while the compute stream transposes the piece before
+  // (upload: after) it; xfer_ev orders the two
+  static constexpr int kXferChunks = 8;
+  cudaStream_t xs = nullptr;
+  std::vector<cudaEvent_t> xfer_ev;
+  DevBuf dl_inv;  // the inverse of orig for a download
+  int xfer_setup() {
+    if (!xs) CK(cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking));
+    while (xfer_ev.size() < size_t(kXferChunks + 1)) {
+      cudaEvent_t e = nullptr;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      xfer_ev.push_back(e);
+    }
+    return SPH_OK;
+  }
+  int64_t xfer_rows() const { return ((nrows + kXferChunks - 1) / kXferChunks + 31) / 32 * 32; }
   // skin lists (SPH_P_SKIN): the lists of the last skin search (CSR like nl),
   // the records' positions and the centres' h at that search, the rows'
   // image signatures then; per record the largest displacement since; per
@@ -2632,6 +2649,11 @@ struct sph_handle {
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (h_i32) cudaFreeHost(h_i32);
     for (auto c : cap_s) cudaStreamDestroy(c);
+    for (auto e : xfer_ev) cudaEventDestroy(e);
+    if (xs) {
+      cudaStreamSynchronize(xs);
+      cudaStreamDestroy(xs);
+    }
     if (s) cudaStreamDestroy(s);
   }
 };
@@ -3071,9 +3093,24 @@ int sph_set_store(sph_handle* h, const double* store, int64_t n_rows) {
                        cudaMemcpyDeviceToDevice, h->s));
     CK(cudaMemsetAsync(h->skin_flag.p, 0, sizeof(int32_t), h->s));
   }
-  CK(cudaMemcpyAsync(h->staging.p, store, sizeof(double) * NCOL * n_rows, cudaMemcpyHostToDevice, h->s));
   h->dlists_ok = false;
-  launch_upload_store(h->staging.as<double>(), h->cols.as<double>(), h->orig.as<int32_t>(), n_rows, h->s);
+  {
+    // in pieces: piece c crosses PCIe on the copy stream while piece c - 1
+    // is transposed (the staging buffer waits for the work queued before)
+    RC(h->xfer_setup());
+    const int64_t cr = h->xfer_rows();
+    CK(cudaEventRecord(h->xfer_ev[sph_handle::kXferChunks], h->s));
+    CK(cudaStreamWaitEvent(h->xs, h->xfer_ev[sph_handle::kXferChunks], 0));
+    double* stg = h->staging.as<double>();
+    for (int c = 0; int64_t(c) * cr < n_rows; ++c) {
+      const int64_t a = int64_t(c) * cr, b = std::min(n_rows, a + cr);
+      CK(cudaMemcpyAsync(stg + a * NCOL, store + a * NCOL, sizeof(double) * NCOL * (b - a),
+                         cudaMemcpyHostToDevice, h->xs));
+      CK(cudaEventRecord(h->xfer_ev[c], h->xs));
+      CK(cudaStreamWaitEvent(h->s, h->xfer_ev[c], 0));
+      launch_upload_rows(stg, h->cols.as<double>(), h->orig.as<int32_t>(), n_rows, a, b, h->s);
+    }
+  }
   if (keep) {
     launch_inverse(h->skin_inv.as<int32_t>(), n_rows, h->skin_perm.as<int32_t>(), h->s);
     launch_type_changed(h->cols.as<double>(), n_rows, h->skin_type.as<double>(),
@@ -3151,10 +3188,23 @@ int sph_run_to(sph_handle* h, double tfinish) {
 
 int sph_get_store(sph_handle* h, double* out, int64_t cap_rows) {
   if (!h || !out || cap_rows < h->nrows) return fail(SPH_ERR_ARG, "buffer too small");
-  launch_download_store(h->cols.as<double>(), h->orig.as<int32_t>(), h->staging.as<double>(),
-                        h->nrows, h->s);
-  CK(cudaMemcpyAsync(out, h->staging.p, sizeof(double) * NCOL * h->nrows, cudaMemcpyDeviceToHost, h->s));
-  CK(cudaStreamSynchronize(h->s));
+  // in pieces of caller rows: piece c is transposed while piece c - 1
+  // crosses PCIe on the copy stream
+  RC(h->xfer_setup());
+  RC(h->dl_inv.ensure(sizeof(int32_t) * size_t(h->nrows)));
+  launch_inverse(h->orig.as<int32_t>(), h->nrows, h->dl_inv.as<int32_t>(), h->s);
+  const int64_t cr = h->xfer_rows();
+  double* stg = h->staging.as<double>();
+  for (int c = 0; int64_t(c) * cr < h->nrows; ++c) {
+    const int64_t a = int64_t(c) * cr, b = std::min(h->nrows, a + cr);
+    launch_download_rows(h->cols.as<double>(), h->dl_inv.as<int32_t>(), stg, h->nrows, a, b,
+                         h->s);
+    CK(cudaEventRecord(h->xfer_ev[c], h->s));
+    CK(cudaStreamWaitEvent(h->xs, h->xfer_ev[c], 0));
+    CK(cudaMemcpyAsync(out + a * NCOL, stg + a * NCOL, sizeof(double) * NCOL * (b - a),
+                       cudaMemcpyDeviceToHost, h->xs));
+  }
+  CK(cudaStreamSynchronize(h->xs));
   CK(cudaGetLastError());
   return SPH_OK;
 }

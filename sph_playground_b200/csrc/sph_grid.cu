@@ -46,19 +46,37 @@ __device__ __forceinline__ double warp_max(double v) {
 static_assert(NCOL == 32, "the tile transposes assume 32 fields");
 __global__ void __launch_bounds__(256)
 k_upload(const double* __restrict__ rm, double* __restrict__ cols, int32_t* __restrict__ orig,
-         int64_t n) {
+         int64_t n, int64_t a, int64_t b) {
+  // rows a .. b - 1 of the n (a a multiple of 32)
   __shared__ double tile[32][33];
-  const int64_t r0 = int64_t(blockIdx.x) * 32;
+  const int64_t r0 = a + int64_t(blockIdx.x) * 32;
   for (int k = threadIdx.y; k < 32; k += 8) {  // row r0 + k, field threadIdx.x
     const int64_t i = r0 + k;
-    if (i < n) tile[k][threadIdx.x] = rm[i * NCOL + threadIdx.x];
+    if (i < b) tile[k][threadIdx.x] = rm[i * NCOL + threadIdx.x];
   }
   __syncthreads();
   for (int f = threadIdx.y; f < NCOL; f += 8) {  // field f, row r0 + threadIdx.x
     const int64_t i = r0 + threadIdx.x;
-    if (i < n) cols[f * n + i] = tile[threadIdx.x][f];
+    if (i < b) cols[f * n + i] = tile[threadIdx.x][f];
   }
-  if (threadIdx.y == 0 && r0 + threadIdx.x < n) orig[r0 + threadIdx.x] = int32_t(r0 + threadIdx.x);
+  if (threadIdx.y == 0 && r0 + threadIdx.x < b) orig[r0 + threadIdx.x] = int32_t(r0 + threadIdx.x);
+}
+// caller rows a .. b - 1 of the row-major table from the column store:
+// caller row j is physical row inv[j] (inv the inverse of orig)
+__global__ void __launch_bounds__(256)
+k_download_gather(const double* __restrict__ cols, const int32_t* __restrict__ inv,
+                  double* __restrict__ rm, int64_t n, int64_t a, int64_t b) {
+  __shared__ double tile[32][33];
+  const int64_t r0 = a + int64_t(blockIdx.x) * 32;
+  const int64_t j = r0 + threadIdx.x;
+  const int64_t p = j < b ? int64_t(inv[j]) : 0;
+  for (int f = threadIdx.y; f < NCOL; f += 8)  // field f of caller row j
+    if (j < b) tile[threadIdx.x][f] = cols[f * n + p];
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8) {
+    const int64_t i = r0 + k;
+    if (i < b) rm[i * NCOL + threadIdx.x] = tile[k][threadIdx.x];
+  }
 }
 
 __global__ void __launch_bounds__(256)
@@ -2162,7 +2180,19 @@ __global__ void k_set(double* col, int64_t n, double v) {
 // ---- launchers ------------------------------------------------------------------------------
 void launch_upload_store(const double* rm, double* cols, int32_t* orig, int64_t n, cudaStream_t s) {
   if (n <= 0) return;
-  k_upload<<<unsigned((n + 31) / 32), dim3(32, 8), 0, s>>>(rm, cols, orig, n);
+  k_upload<<<unsigned((n + 31) / 32), dim3(32, 8), 0, s>>>(rm, cols, orig, n, 0, n);
+  note_launch();
+}
+void launch_upload_rows(const double* rm, double* cols, int32_t* orig, int64_t n, int64_t a,
+                        int64_t b, cudaStream_t s) {
+  if (b <= a) return;
+  k_upload<<<unsigned((b - a + 31) / 32), dim3(32, 8), 0, s>>>(rm, cols, orig, n, a, b);
+  note_launch();
+}
+void launch_download_rows(const double* cols, const int32_t* inv, double* rm, int64_t n, int64_t a,
+                          int64_t b, cudaStream_t s) {
+  if (b <= a) return;
+  k_download_gather<<<unsigned((b - a + 31) / 32), dim3(32, 8), 0, s>>>(cols, inv, rm, n, a, b);
   note_launch();
 }
 void launch_download_store(const double* cols, const int32_t* orig, double* rm, int64_t n,

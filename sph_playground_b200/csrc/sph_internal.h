@@ -121,6 +121,14 @@ void launch_upload_store(const double* rowmajor, double* cols, int32_t* orig, in
                          cudaStream_t s);
 void launch_download_store(const double* cols, const int32_t* orig, double* rowmajor,
                            int64_t n, cudaStream_t s);
+// the same for rows a .. b - 1 only (a a multiple of 32), so that a table
+// crosses PCIe in pieces while the next piece is transposed: upload rows
+// in caller order (orig[i] = i); download caller rows through inv, the
+// inverse of orig
+void launch_upload_rows(const double* rowmajor, double* cols, int32_t* orig, int64_t n, int64_t a,
+                        int64_t b, cudaStream_t s);
+void launch_download_rows(const double* cols, const int32_t* inv, double* rowmajor, int64_t n,
+                          int64_t a, int64_t b, cudaStream_t s);
 void launch_reorder(const double* cols_in, double* cols_out, const int32_t* orig_in,
                     int32_t* orig_out, const int32_t* perm, int64_t n, int64_t ld_in,
                     int64_t ld_out, cudaStream_t s);
