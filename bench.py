@@ -728,6 +728,10 @@ def main():
         host_in = torch.empty((N, 32), dtype=torch.float64).pin_memory().numpy()
         host_out = torch.empty((N, 32), dtype=torch.float64).pin_memory().numpy()
         e.get_store(host_in)
+        # one untimed round trip (the first touch of the pinned buffers)
+        e.set_store(host_in)
+        e.step(1)
+        e.get_store(host_in)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):

@@ -557,6 +557,8 @@ struct sph_handle {
     RC(orig.ensure(sizeof(int32_t) * nrows));
     RC(orig_alt.ensure(sizeof(int32_t) * nrows));
     RC(staging.ensure(sizeof(double) * NCOL * nrows));
+    RC(dl_inv.ensure(sizeof(int32_t) * nrows));
+    RC(xfer_setup());  // (the table transfers' copy stream and events)
     RC(save.ensure(sizeof(double) * 9 * nrows));
     RC(hkp1.ensure(sizeof(double) * nrows));
     RC(dkp1.ensure(sizeof(double) * nrows));
