@@ -87,7 +87,8 @@ extern "C" {
                                       when particles moved too far.  0 = a
                                       fresh search every iterate.  Default 0.1.
                                       (The device-resident steps of SPH_P_GRAPH
-                                      and the batch loop search afresh.)       */
+                                      and the batch loop keep or rebuild all
+                                      lists at once, decided on the device.)   */
 #define SPH_P_LAST            65
 
 /* ---- status codes --------------------------------------------------------- */
