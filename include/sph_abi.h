@@ -321,8 +321,7 @@ void sph_batch_destroy(sph_batch* b);
  * No periodic images.  All intermediate data lives in a fixed static device
  * array of SPH_NOALLOC_SCRATCH_BYTES on every GPU that loads the library;
  * n above SPH_NOALLOC_MAX_PARTICLES is rejected with SPH_ERR_ARG.  The first
- * call on a device looks the array up (make it before any stream capture).
- * Calls share the array: calls that overlap on the GPU race.  `stream` is a
+ * call on a device looks the array up.  Calls share the array: calls that overlap on the GPU race.  `stream` is a
  * cudaStream_t of the current device (NULL = default stream; a stream of
  * another device is rejected with SPH_ERR_ARG); the call synchronises it. */
 #define SPH_NOALLOC_MAX_PARTICLES 262144

@@ -14,11 +14,11 @@
 // The array is SPH_NOALLOC_SCRATCH_BYTES per GPU and exists on every GPU that
 // loads the library until the process exits.  Its device address is looked
 // up once per device, with that device current, on the first call made on
-// it (cudaGetSymbolAddress); that first call should come before any stream
-// capture.  Every call uses the same array, so calls that overlap on the GPU
-// (concurrent streams, several host threads) race and give wrong results;
-// the function synchronises its stream before returning.  What must start at
-// zero or at a sentinel is cleared by the call itself.
+// it (cudaGetSymbolAddress).  Every call uses the same array, so calls that
+// overlap on the GPU (concurrent streams, several host threads) race and
+// give wrong results; the function synchronises its stream before
+// returning.  What must start at zero or at a sentinel is cleared by the
+// call itself.
 //
 // The density is circuit1's direct summation (circuit1.f90:253-296):
 //   rho_i = sum_{j != i, r_ij <= krad h_i} m_j W(r_ij, h_i) + m_i W(0, h_i)
