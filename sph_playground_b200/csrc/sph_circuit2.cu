@@ -114,6 +114,12 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     const int64_t ld = a.ld;
     Part<R> A;
     Loader<R>::hydro(pb, k, A);
+    if constexpr (sizeof(R) == 4) {
+      // the FP32 record's second rho field is wCv Pi / h^(d+1), the
+      // neighbour-side product; the centre takes Pi itself
+      const double rr = cols[es_den * ld + p], oo = cols[es_om * ld + p];
+      A.Pi = float(1.0 / (rr * rr * oo));
+    }
     const R wcv = R(P.wCv);
     R Ka = A.invh;
     for (int d = 0; d < DIM; ++d) Ka *= A.invh;
@@ -204,11 +210,28 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         dfa = kshape_df<K, R>(qa);
       }
       const R dfb = kshape_df<K, R>(qb);
-      R Kb = B.invh;
-      for (int d = 0; d < DIM; ++d) Kb *= B.invh;
-      Kb *= wcv;
       const R ga = (Ka * invr) * dfa;  // nabla W_a = ga * r_ab
-      const R gb = (Kb * invr) * dfb;  // nabla W_b = gb * r_ab
+      // nabla W_b = gb r_ab, which always meets Pi_b: gbPi = gb Pi_b, and
+      // cbr = wCv f'_b rho_b Pi_b / h_b^(d+1) for the conductivity.  The FP32
+      // record carries wCv Pi_b / h_b^(d+1) (a product formed in FP64 when
+      // packed, five products per pair fewer); FP64 forms them per pair.
+      R gb = R(0), gbPi, cbr;
+      if constexpr (sizeof(R) == 4) {
+        gbPi = (B.Pi * invr) * dfb;
+        cbr = (B.Pi * dfb) * B.rho;
+      } else {
+        R Kb = B.invh;
+        for (int d = 0; d < DIM; ++d) Kb *= B.invh;
+        Kb *= wcv;
+        gb = (Kb * invr) * dfb;
+        gbPi = gb * B.Pi;
+        cbr = Kb * dfb * B.rho * B.Pi;
+      }
+      // the neighbour's term gb x Pi_b of the general path
+      auto gbx = [&](R x) {
+        if constexpr (sizeof(R) == 4) return gbPi * x;
+        else return gb * x * B.Pi;
+      };
       const R mb = B.m;
       const R mgv = mb * ga * vr;      // m_b nabla W_a . v_ab
       if (adden) drho.add(mgv);        // circuit2.f90:265-267
@@ -228,9 +251,9 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         Fb = qbv;
         Da = qav * A.rho;
         if (use_au) {
-          const R faba = Ka * dfa, fabb = Kb * dfb;
+          const R faba = Ka * dfa;
           const R vsigu = fsqrt<R>(fdiv<R>(fabs(A.P - B.P), R(0.5) * (A.rho + B.rho)));
-          du.add(mb * (au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + fabb * B.rho * B.Pi))));
+          du.add(mb * (au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + cbr))));
         }
       }
       if (hydro) {
@@ -239,7 +262,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         Fb += B.P;
         Da += A.P;
       }
-      const R F = ga * A.Pi * Fa + gb * B.Pi * Fb;
+      const R F = ga * A.Pi * Fa + gbPi * Fb;
       du.add(mgv * A.Pi * Da);
       if constexpr (GENERAL) {
         PartX<R> BX;
@@ -283,7 +306,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
             for (int x = 0; x < 3; ++x) kgb[x] = ktb[x][0] * gb3[0] + ktb[x][1] * gb3[1] + ktb[x][2] * gb3[2];
             R ka_r = R(0), kb_r = R(0);
             for (int x = 0; x < DIM; ++x) { ka_r += kga[x] * rab[x]; kb_r += kgb[x] * rab[x]; }
-            if (ddw == esd_2nw_ds) ddt.add(mb * (ga * ka_r * A.Pi + gb * kb_r * B.Pi));
+            if (ddw == esd_2nw_ds) ddt.add(mb * (ga * ka_r * A.Pi + gbx(kb_r)));
             else ddt.add(mb * A.Pi * ga * (kb_r - ka_r));  // esd_2nw_sd
           }
         }
@@ -297,7 +320,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
             const R rx = x < DIM ? rab[x] : R(0);
             const R ma_x = (halfB2a * rx - Ba[x] * Bar) * mu0inv;  // MPa . r_ab
             const R mb_x = (halfB2b * rx - Bb[x] * Bbr) * mu0inv;
-            dv[x].add(-mb * (ga * ma_x * A.Pi + gb * mb_x * B.Pi));
+            dv[x].add(-mb * (ga * ma_x * A.Pi + gbx(mb_x)));
             db[x].add(-mb * rPiA * ga * (vab[x] * Bar - Bb[x] * vr));
           }
         }

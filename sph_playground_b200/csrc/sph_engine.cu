@@ -1455,6 +1455,8 @@ struct sph_handle {
     // the positions (PACK_POS) were packed for circuit1 in this iterate and
     // have not moved; h, rho, Omega, P, c and grad T are new
     int groups = PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
+    pb.kp_wcv = P.wCv;
+    pb.kp_dim = P.dim;
     {
       Phase pk(this, SPH_T_PACK);
       if (dplan)

@@ -1717,7 +1717,12 @@ __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restric
       double h = C(es_h), rho = C(es_den), om = C(es_om), P = C(es_p);
       pb.q[0][k] = make_float4(xh, yh, zh, float(m));
       pb.q[1][k] = make_float4(xl, yl, zl, float(1.0 / h));
-      pb.q[2][k] = make_float4(float(rho), float(1.0 / (rho * rho * om)), float(P), float(C(es_c)));
+      // wCv / (h^(d+1) rho^2 Omega): the neighbour's kernel factor and
+      // 1/(rho^2 Omega) always meet as this product in the force pass
+      const double ih = 1.0 / h;
+      double kp = pb.kp_wcv;
+      for (int d = 0; d <= pb.kp_dim; ++d) kp *= ih;
+      pb.q[2][k] = make_float4(float(rho), float(kp / (rho * rho * om)), float(P), float(C(es_c)));
       pb.q[3][k] = make_float4(float(C(es_u)), float(C(es_vx)), float(C(es_vy)), float(C(es_vz)));
     }
     if (groups & PACK_EXTRA) {
