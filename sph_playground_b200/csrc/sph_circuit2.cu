@@ -28,6 +28,7 @@ inline int nblocks(int64_t n, int tpb = TPB) {
 template <class R> struct Part {
   PairPos<R> pos;
   R m, invh, rho, Pi, P, c, u, vx, vy, vz;
+  R hrho, ac;  // rho / 2 and alpha c (the FP32 record's own fields)
 };
 template <class R> struct PartX {
   R T, kappa, gx, gy, gz, bx, by, bz;
@@ -56,7 +57,7 @@ template <> struct Loader<float> {
            d = __ldg(&pb.q[3][j]);
     o.pos.xh = a.x; o.pos.yh = a.y; o.pos.zh = a.z; o.m = a.w;
     o.pos.xl = b.x; o.pos.yl = b.y; o.pos.zl = b.z; o.invh = b.w;
-    o.rho = c.x; o.Pi = c.y; o.P = c.z; o.c = c.w;
+    o.hrho = c.x; o.rho = 2.f * c.x; o.Pi = c.y; o.P = c.z; o.ac = c.w;
     o.u = d.x; o.vx = d.y; o.vy = d.z; o.vz = d.w;
   }
   static __device__ __forceinline__ void extra(const PackBufs& pb, int64_t j, PartX<float>& o) {
@@ -131,7 +132,10 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     // vanish, so it is skipped for both
     const bool use_au = P.au != -1.0 && P.au != 0.0;
     const R rPiA = A.rho * A.Pi;  // 1 / (rho_a Omega_a)
-    const R hrhoa = R(-0.5) * A.rho, alpha_ca = alpha * A.c;
+    R alpha_ca;
+    if constexpr (sizeof(R) == 4) alpha_ca = A.ac;
+    else alpha_ca = alpha * A.c;
+    const R hrhoa = R(-0.5) * A.rho, hrho_a = R(0.5) * A.rho, rPiA_h = R(0.5) * rPiA;
     // force-type sums: plain per lane (a few tens of terms), FP64 over lanes
     SumAcc<R> dv[3], du, drho, ddt, db[3];
     for (int d = 0; d < 3; ++d) { dv[d].init(); db[d].init(); }
@@ -218,7 +222,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
       R gb = R(0), gbPi, cbr;
       if constexpr (sizeof(R) == 4) {
         gbPi = (B.Pi * invr) * dfb;
-        cbr = (B.Pi * dfb) * B.rho;
+        cbr = (B.Pi * dfb) * B.hrho;  // half of it: the conductivity's 1/2 is folded in
       } else {
         R Kb = B.invh;
         for (int d = 0; d < DIM; ++d) Kb *= B.invh;
@@ -246,14 +250,27 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         const R dvr = vr * invr;
         const R dneg = dvr < R(0) ? dvr : R(0);
         const R qav = hrhoa * (alpha_ca - beta * dneg) * dneg;
-        const R qbv = (R(-0.5) * B.rho) * (alpha * B.c - beta * dneg) * dneg;
+        // (FP32: the record carries rho_b / 2 and alpha c_b; the halvings
+        // are exact, so only alpha c_b is rounded differently)
+        R hrhob, acb;
+        if constexpr (sizeof(R) == 4) {
+          hrhob = B.hrho;
+          acb = B.ac;
+        } else {
+          hrhob = R(0.5) * B.rho;
+          acb = alpha * B.c;
+        }
+        const R qbv = (-hrhob) * (acb - beta * dneg) * dneg;
         Fa = qav;
         Fb = qbv;
         Da = qav * A.rho;
         if (use_au) {
           const R faba = Ka * dfa;
-          const R vsigu = fsqrt<R>(fdiv<R>(fabs(A.P - B.P), R(0.5) * (A.rho + B.rho)));
-          du.add(mb * (au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + cbr))));
+          const R vsigu = fsqrt<R>(fdiv<R>(fabs(A.P - B.P), hrho_a + hrhob));
+          if constexpr (sizeof(R) == 4)
+            du.add(mb * (au * (vsigu * (A.u - B.u) * (faba * rPiA_h + cbr))));
+          else
+            du.add(mb * (au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + cbr))));
         }
       }
       if (hydro) {

@@ -1456,6 +1456,7 @@ struct sph_handle {
     // have not moved; h, rho, Omega, P, c and grad T are new
     int groups = PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
     pb.kp_wcv = P.wCv;
+    pb.kp_alpha = P.alpha;
     pb.kp_dim = P.dim;
     {
       Phase pk(this, SPH_T_PACK);

@@ -1722,7 +1722,8 @@ __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restric
       const double ih = 1.0 / h;
       double kp = pb.kp_wcv;
       for (int d = 0; d <= pb.kp_dim; ++d) kp *= ih;
-      pb.q[2][k] = make_float4(float(rho), float(kp / (rho * rho * om)), float(P), float(C(es_c)));
+      pb.q[2][k] = make_float4(float(0.5 * rho), float(kp / (rho * rho * om)), float(P),
+                               float(pb.kp_alpha * C(es_c)));
       pb.q[3][k] = make_float4(float(C(es_u)), float(C(es_vx)), float(C(es_vy)), float(C(es_vz)));
     }
     if (groups & PACK_EXTRA) {
