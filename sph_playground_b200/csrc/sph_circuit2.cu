@@ -136,6 +136,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
     if constexpr (sizeof(R) == 4) alpha_ca = A.ac;
     else alpha_ca = alpha * A.c;
     const R hrhoa = R(-0.5) * A.rho, hrho_a = R(0.5) * A.rho, rPiA_h = R(0.5) * rPiA;
+    const R PiPa = hydro ? A.Pi * A.P : R(0);  // Pi_a P_a (the FP32 path's F and du)
     // force-type sums: plain per lane (a few tens of terms), FP64 over lanes
     SumAcc<R> dv[3], du, drho, ddt, db[3];
     for (int d = 0; d < 3; ++d) { dv[d].init(); db[d].init(); }
@@ -245,6 +246,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
       // mgv Pi_a (qav rho_a), and the pressure work of :343-344 is
       // mgv Pi_a P_a.
       R Fa = R(0), Fb = R(0), Da = R(0);
+      R FaPi = PiPa, DaPi = PiPa;  // FP32: Pi_a Fa and Pi_a Da, Pi_a folded in
       if (artts) {
         // circuit2.f90:294-336; the Monaghan switch dvr < 0 as a clamp
         const R dvr = vr * invr;
@@ -264,6 +266,8 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         Fa = qav;
         Fb = qbv;
         Da = qav * A.rho;
+        FaPi = A.Pi * qav + PiPa;
+        DaPi = qav * rPiA + PiPa;
         if (use_au) {
           const R faba = Ka * dfa;
           const R vsigu = fsqrt<R>(fdiv<R>(fabs(A.P - B.P), hrho_a + hrhob));
@@ -279,8 +283,14 @@ k_c2(C2Args a, PackBufs pb, Params P) {
         Fb += B.P;
         Da += A.P;
       }
-      const R F = ga * A.Pi * Fa + gbPi * Fb;
-      du.add(mgv * A.Pi * Da);
+      R F;
+      if constexpr (sizeof(R) == 4) {
+        F = ga * FaPi + gbPi * Fb;
+        du.add(mgv * DaPi);
+      } else {
+        F = ga * A.Pi * Fa + gbPi * Fb;
+        du.add(mgv * A.Pi * Da);
+      }
       if constexpr (GENERAL) {
         PartX<R> BX;
         Loader<R>::extra(pb, j, BX);
