@@ -39,12 +39,12 @@ UNIT = "particle-steps/s"
 F1_C1 = 50.0
 F2_C2 = 150.0
 # DRAM bytes per in-support pair of the FP32-comp circuit2 launch:
-# dram__bytes_read.sum + dram__bytes_write.sum = 864.75 MB + 76.86 MB over
+# dram__bytes_read.sum + dram__bytes_write.sum = 862.28 MB + 73.97 MB over
 # 157.49M pairs of an ncu capture of k_c2 on the Sedov 96^3 step (FP32-comp, 4
 # lanes per centre, cell edge 0.4 krad h_min, an iterate served from skin
 # lists) (the neighbour index, 4 B, plus the gathered pair data that misses
 # L2); the traffic scales with the pairs a launch processes
-C2_DRAM_BYTES_PER_PAIR = (864.75e6 + 76.86e6) / 157.49e6
+C2_DRAM_BYTES_PER_PAIR = (862.28e6 + 73.97e6) / 157.49e6
 # DRAM bytes per in-support pair of the neighbour search (k_neighbours),
 # same capture workload: 198.36 MB read + 684.48 MB written over 157.49M
 # pairs; the search's algorithmic bytes are the 4 B list entry per pair it
@@ -706,8 +706,8 @@ def main():
                 "traffic": kernels[dom]["traffic"],
                 "step_frac": step_ach / p32, "step_achieved_tflops": step_ach,
                 "kernels": kernels,
-                "binding_unit": {"circuit2": {"unit": "L1/TEX data path", "ncu_pct_of_peak": 96.2,
-                                              "fma_pipe_pct": 54.9, "issue_active_pct": 75.9,
+                "binding_unit": {"circuit2": {"unit": "L1/TEX data path", "ncu_pct_of_peak": 96.9,
+                                              "fma_pipe_pct": 52.5, "issue_active_pct": 74.8,
                                               "source": "profiles/k_c2_fp32_sedov3d_96.md"}},
                 "traffic_source": "ncu DRAM bytes per pair of the kernel's capture on the "
                                   "Sedov 96^3 step, times this launch's pairs",
