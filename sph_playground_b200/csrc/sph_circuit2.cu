@@ -272,7 +272,7 @@ k_c2(C2Args a, PackBufs pb, Params P) {
           const R faba = Ka * dfa;
           const R vsigu = fsqrt<R>(fdiv<R>(fabs(A.P - B.P), hrho_a + hrhob));
           if constexpr (sizeof(R) == 4)
-            du.add(mb * (au * (vsigu * (A.u - B.u) * (faba * rPiA_h + cbr))));
+            du.add(mb * (vsigu * (A.u - B.u) * (faba * rPiA_h + cbr)));  // (FP32 u is au u)
           else
             du.add(mb * (au * (vsigu * (A.u - B.u) * R(0.5) * (faba * rPiA + cbr))));
         }

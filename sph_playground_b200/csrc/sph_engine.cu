@@ -1457,6 +1457,7 @@ struct sph_handle {
     int groups = PACK_HYDRO | ((eq_diff || eq_magneto) ? PACK_EXTRA : 0);
     pb.kp_wcv = P.wCv;
     pb.kp_alpha = P.alpha;
+    pb.kp_au = P.au;
     pb.kp_dim = P.dim;
     {
       Phase pk(this, SPH_T_PACK);

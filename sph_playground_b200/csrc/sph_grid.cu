@@ -1724,7 +1724,8 @@ __global__ void k_pack(int prec, int groups, int64_t n, const int32_t* __restric
       for (int d = 0; d <= pb.kp_dim; ++d) kp *= ih;
       pb.q[2][k] = make_float4(float(0.5 * rho), float(kp / (rho * rho * om)), float(P),
                                float(pb.kp_alpha * C(es_c)));
-      pb.q[3][k] = make_float4(float(C(es_u)), float(C(es_vx)), float(C(es_vy)), float(C(es_vz)));
+      pb.q[3][k] = make_float4(float(pb.kp_au * C(es_u)), float(C(es_vx)), float(C(es_vy)),
+                               float(C(es_vz)));
     }
     if (groups & PACK_EXTRA) {
       pb.q[4][k] = make_float4(float(C(es_t)), float(C(es_kappa)), float(C(es_dtdx)),

@@ -493,7 +493,7 @@ enum PackGroup : int { PACK_POS = 1, PACK_HYDRO = 2, PACK_EXTRA = 4, PACK_TEMP =
 struct PackBufs {
   double2* p[11];
   // FP32: q[0] = (x, y, z high parts, m), q[1] = (x, y, z low parts, 1/h),
-  // q[2] = (rho / 2, wCv / (h^(d+1) rho^2 Omega), P, alpha c), q[3] = (u, v), q[4] / q[5] the
+  // q[2] = (rho / 2, wCv / (h^(d+1) rho^2 Omega), P, alpha c), q[3] = (au u, v), q[4] / q[5] the
   // temperature, diffusion and field quantities (the force pass); q[6] =
   // (x, y, z as 31-bit fixed point over the packing frame, m) (the density
   // pass: one 16-byte record per neighbour)
@@ -501,9 +501,9 @@ struct PackBufs {
   // the length of one fixed-point unit (shift 2^-31), written by the pack
   // kernel (the frame may be planned on the device)
   float* unit;
-  // the force pass's FP32 factor wCv / h^(d+1) and the viscosity's alpha
-  // (set before its packing)
-  double kp_wcv = 0.0, kp_alpha = 0.0;
+  // the force pass's FP32 factor wCv / h^(d+1), the viscosity's alpha and
+  // the conductivity's au (set before its packing)
+  double kp_wcv = 0.0, kp_alpha = 0.0, kp_au = 0.0;
   int kp_dim = 0;
 };
 void launch_pack_dev(int prec, int groups, int64_t ncap, const int32_t* ssrc, const double* sx,
